@@ -1,0 +1,170 @@
+"""ctypes binding of the CPU oracle (oracle/pm_oracle.c) -- test infrastructure only.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline import this module, and only
+as the checker.  ``build()`` compiles the C restatement with gcc into oracle/liboracle.so.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+SWITCH = {"cutoff": 0, "C1": 1, "C2": 2}
+E_COULOMB, E_LJ, E_BOND, E_ANGLE = 0, 1, 2, 3
+
+
+def build(force=False):
+    src = [os.path.join(HERE, "pm_oracle.c")]
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(s) for s in src + [os.path.join(HERE, "pm_oracle.h")]):
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c99", "-o", LIB] + src + ["-lm"])
+    return LIB
+
+
+class OrcSystem(C.Structure):
+    _fields_ = [("n", C.c_int), ("ntypes", C.c_int),
+                ("charge", C.c_void_p), ("mass", C.c_void_p), ("type", C.c_void_p),
+                ("molecule", C.c_void_p), ("lj", C.c_void_p),
+                ("nexcl", C.c_int), ("excl_pairs", C.c_void_p), ("excl_kind", C.c_void_p),
+                ("nbonds", C.c_int), ("bonds", C.c_void_p), ("bond_k", C.c_void_p),
+                ("bond_r0", C.c_void_p), ("nangles", C.c_int), ("angles", C.c_void_p),
+                ("angle_k", C.c_void_p), ("angle_theta0", C.c_void_p), ("ub_k", C.c_void_p),
+                ("ub_r0", C.c_void_p), ("box", C.c_double * 3), ("coulomb_scaling", C.c_double)]
+
+
+class OrcCutoff(C.Structure):
+    _fields_ = [("do_lj", C.c_int), ("lj_switch", C.c_int), ("lj_switchon", C.c_double),
+                ("lj_cutoff", C.c_double), ("do_coul", C.c_int), ("coul_switch", C.c_int),
+                ("coul_switchon", C.c_double), ("coul_cutoff", C.c_double)]
+
+
+class OrcPME(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("order", C.c_int),
+                ("cutoff", C.c_double), ("accuracy", C.c_double), ("alpha", C.c_double),
+                ("real_switch", C.c_int), ("do_real", C.c_int), ("do_recip", C.c_int),
+                ("do_corr", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB)
+        for fn in ("orc_cutoff", "orc_pme", "orc_bonded", "orc_leapfrog"):
+            getattr(_lib, fn).restype = C.c_int
+        _lib.orc_pme_alpha.restype = C.c_double
+        _lib.orc_pme_alpha.argtypes = [C.c_double, C.c_double]
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class System:
+    """Owns contiguous numpy copies of a topology dict (keys as written by the fixtures and by
+    protomol3_b200.waterbox) and the matching orc_system struct."""
+
+    def __init__(self, topo):
+        n = len(topo["charge"])
+        self.n = n
+        self.keep = {}
+
+        def arr(key, dtype, default=None, shape=None):
+            v = topo.get(key, default)
+            a = np.ascontiguousarray(np.asarray(v, dtype=dtype).reshape(-1) if v is not None
+                                     else np.zeros(0, dtype))
+            self.keep[key] = a
+            return a
+        lj = arr("lj", np.float64)
+        nt = int(round((lj.size // 4) ** 0.5))
+        s = OrcSystem()
+        s.n = n
+        s.ntypes = nt
+        s.charge = _p(arr("charge", np.float64))
+        s.mass = _p(arr("mass", np.float64, np.ones(n)))
+        s.type = _p(arr("type", np.int32))
+        s.molecule = _p(arr("molecule", np.int32))
+        s.lj = _p(lj)
+        ep = arr("excl_pairs", np.int32, np.zeros((0, 2)))
+        s.nexcl = ep.size // 2
+        s.excl_pairs = _p(ep)
+        s.excl_kind = _p(arr("excl_kind", np.int32, np.zeros(0)))
+        b = arr("bonds", np.int32, np.zeros((0, 2)))
+        s.nbonds = b.size // 2
+        s.bonds = _p(b)
+        s.bond_k = _p(arr("bond_k", np.float64, np.zeros(0)))
+        s.bond_r0 = _p(arr("bond_r0", np.float64, np.zeros(0)))
+        a = arr("angles", np.int32, np.zeros((0, 3)))
+        s.nangles = a.size // 3
+        s.angles = _p(a)
+        s.angle_k = _p(arr("angle_k", np.float64, np.zeros(0)))
+        s.angle_theta0 = _p(arr("angle_theta0", np.float64, np.zeros(0)))
+        s.ub_k = _p(arr("ub_k", np.float64, np.zeros(0)))
+        s.ub_r0 = _p(arr("ub_r0", np.float64, np.zeros(0)))
+        box = np.asarray(topo["box"], np.float64)
+        for k in range(3):
+            s.box[k] = box[k]
+        s.coulomb_scaling = float(topo.get("coulomb_scaling", 1.0))
+        self.s = s
+
+
+def cutoff_params(lj=None, coul=None):
+    """lj / coul: (switch_name, switchon, cutoff) or None."""
+    p = OrcCutoff()
+    if lj is not None:
+        p.do_lj, p.lj_switch, p.lj_switchon, p.lj_cutoff = 1, SWITCH[lj[0]], lj[1], lj[2]
+    if coul is not None:
+        p.do_coul, p.coul_switch, p.coul_switchon, p.coul_cutoff = 1, SWITCH[coul[0]], coul[1], coul[2]
+    return p
+
+
+def pme_params(grid, cutoff, order=4, accuracy=1e-6, alpha=-1.0, real_switch="cutoff",
+               real=True, recip=True, corr=True):
+    p = OrcPME()
+    p.nx, p.ny, p.nz = grid
+    p.order, p.cutoff, p.accuracy, p.alpha = order, cutoff, accuracy, alpha
+    p.real_switch = SWITCH[real_switch]
+    p.do_real, p.do_recip, p.do_corr = int(real), int(recip), int(corr)
+    return p
+
+
+def evaluate(system, pos, cutoff=None, pme=None, bonded=False, virial=False):
+    """Forces (n,3), energies[4] (Coulomb, LJ, bond, angle), virial (9,) for one configuration."""
+    L = lib()
+    pos = np.ascontiguousarray(pos, np.float64)
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    v = np.zeros(9)
+    vp = _p(v) if virial else None
+    terms = np.zeros(5)
+    alpha = C.c_double(0.0)
+    if bonded:
+        L.orc_bonded(C.byref(system.s), _p(pos), _p(f), _p(e), vp)
+    if cutoff is not None:
+        L.orc_cutoff(C.byref(system.s), _p(pos), C.byref(cutoff), _p(f), _p(e), vp)
+    if pme is not None:
+        L.orc_pme(C.byref(system.s), _p(pos), C.byref(pme), _p(f), _p(e), vp,
+                  C.byref(alpha), _p(terms))
+    return f, e, v, {"alpha": alpha.value, "terms": terms}
+
+
+def leapfrog(system, pos, vel, dt, nsteps, cutoff=None, pme=None, bonded=True):
+    L = lib()
+    pos = np.ascontiguousarray(pos, np.float64).copy()
+    vel = np.ascontiguousarray(vel, np.float64).copy()
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    L.orc_leapfrog(C.byref(system.s), C.byref(cutoff) if cutoff is not None else None,
+                   C.byref(pme) if pme is not None else None, int(bonded), C.c_double(dt),
+                   int(nsteps), _p(pos), _p(vel), _p(f), _p(e))
+    return pos, vel, f, e
+
+
+def pme_alpha(cutoff, accuracy):
+    return lib().orc_pme_alpha(cutoff, accuracy)
