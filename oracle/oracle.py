@@ -168,3 +168,93 @@ def leapfrog(system, pos, vel, dt, nsteps, cutoff=None, pme=None, bonded=True):
 
 def pme_alpha(cutoff, accuracy):
     return lib().orc_pme_alpha(cutoff, accuracy)
+
+
+# ---------------------------------------------------------------------------------------------
+# ProtoMol's own force path compiled from the reference sources (oracle/_ref/libpmref.so,
+# built by ``make -C oracle ref`` where the reference tree is present).
+# ---------------------------------------------------------------------------------------------
+REF_LIB = os.path.join(HERE, "_ref", "libpmref.so")
+
+
+class RefInput(C.Structure):
+    _fields_ = [("n", C.c_int), ("ntypes", C.c_int), ("pos", C.c_void_p), ("charge", C.c_void_p),
+                ("mass", C.c_void_p), ("type", C.c_void_p), ("molecule", C.c_void_p),
+                ("lj", C.c_void_p), ("nexcl", C.c_int), ("excl_pairs", C.c_void_p),
+                ("excl_kind", C.c_void_p), ("nbonds", C.c_int), ("bonds", C.c_void_p),
+                ("bond_k", C.c_void_p), ("bond_r0", C.c_void_p), ("nangles", C.c_int),
+                ("angles", C.c_void_p), ("angle_k", C.c_void_p), ("angle_theta0", C.c_void_p),
+                ("ub_k", C.c_void_p), ("ub_r0", C.c_void_p), ("box", C.c_double * 3),
+                ("origin", C.c_double * 3), ("cellsize", C.c_double),
+                ("coulomb_scaling", C.c_double)]
+
+
+class RefCutoff(C.Structure):
+    _fields_ = OrcCutoff._fields_
+
+
+class RefPME(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("order", C.c_int),
+                ("cutoff", C.c_double), ("accuracy", C.c_double), ("alpha", C.c_double),
+                ("real_switch", C.c_int)]
+
+
+_ref = None
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def build_ref(ref_root="/root/reference"):
+    if os.path.isdir(ref_root):
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", "REF=" + ref_root])
+    return ref_available()
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(REF_LIB)
+    return _ref
+
+
+def _ref_input(system, pos, cellsize):
+    k = system.keep
+    r = RefInput()
+    s = system.s
+    r.n, r.ntypes = s.n, s.ntypes
+    r.pos = _p(pos)
+    for name in ("charge", "mass", "type", "molecule", "lj", "excl_pairs", "excl_kind", "bonds",
+                 "bond_k", "bond_r0", "angles", "angle_k", "angle_theta0", "ub_k", "ub_r0"):
+        setattr(r, name, getattr(s, name))
+    r.nexcl, r.nbonds, r.nangles = s.nexcl, s.nbonds, s.nangles
+    for q in range(3):
+        r.box[q] = s.box[q]
+        r.origin[q] = 0.0
+    r.cellsize = cellsize
+    r.coulomb_scaling = s.coulomb_scaling
+    return r
+
+
+def ref_evaluate(system, pos, cutoff=None, pme=None, bonded=False, virial=False, cellsize=5.0):
+    """Same contract as ``evaluate`` but through the reference's own C++ force classes."""
+    L = ref_lib()
+    pos = np.ascontiguousarray(pos, np.float64)
+    r = _ref_input(system, pos, cellsize)
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    v = np.zeros(9)
+    vp = _p(v) if virial else None
+    if bonded:
+        L.ref_bonded_eval(C.byref(r), _p(f), _p(e), vp)
+    if cutoff is not None:
+        c = RefCutoff()
+        C.memmove(C.byref(c), C.byref(cutoff), C.sizeof(c))
+        L.ref_cutoff_eval(C.byref(r), C.byref(c), _p(f), _p(e), vp)
+    if pme is not None:
+        p = RefPME()
+        p.nx, p.ny, p.nz, p.order = pme.nx, pme.ny, pme.nz, pme.order
+        p.cutoff, p.accuracy, p.alpha, p.real_switch = pme.cutoff, pme.accuracy, pme.alpha, pme.real_switch
+        L.ref_pme_eval(C.byref(r), C.byref(p), _p(f), _p(e), vp)
+    return f, e, v
