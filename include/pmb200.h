@@ -1,0 +1,158 @@
+/*
+ * libpmb200 -- B200 (sm_100a) implementation of ProtoMol 3's nonbonded force path behind a
+ * plain C ABI: cell-list cutoff Lennard-Jones + Coulomb with C1/C2 switching, and particle-mesh
+ * Ewald (B-spline spreading, 3-D FFT, influence function, gather, Ewald real-space, self and
+ * exclusion corrections), with the bonded water terms and leapfrog / Langevin integrators that
+ * the ns/day metric needs.
+ *
+ * Every entry point returns 0 (PMB_OK) or a PMB_ERR_* status; pmb_last_error() gives the message
+ * (thread local).  Handles are not re-entrant: one host thread drives a system at a time, as
+ * ProtoMol drives SystemForce::evaluate.
+ *
+ * A system is a batch of one or more independent periodic boxes.  Per-atom host arrays are the
+ * concatenation of the boxes' atoms in box order; per-box outputs are PMB_E_STRIDE doubles each:
+ *   [PMB_E_COULOMB, PMB_E_LJ, PMB_E_BOND, PMB_E_ANGLE, PMB_E_VIRIAL + 0..8 (row-major 3x3), pad]
+ * matching ProtoMol's ScalarStructure slots COULOMB, LENNARDJONES, BOND, ANGLE, VIRIALXX..ZZ
+ * (type/ScalarStructure.h:26-54).
+ */
+#ifndef PMB200_H
+#define PMB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define PMB_OK 0
+#define PMB_ERR_ARG 1         /* invalid argument (ProtoMol: report << error, doMake -> NULL) */
+#define PMB_ERR_CUDA 2        /* CUDA runtime error or no device */
+#define PMB_ERR_CAPACITY 3    /* a neighbour or tile list overflowed its buffer */
+#define PMB_ERR_UNSUPPORTED 4 /* configuration outside what this build implements */
+#define PMB_ERR_STATE 5       /* call out of order (e.g. run before set_state) */
+#define PMB_ERR_NUMERIC 6     /* non-finite input or result */
+
+enum { PMB_FP64 = 0, PMB_MIXED = 1 };
+enum { PMB_SWITCH_CUTOFF = 0, PMB_SWITCH_C1 = 1, PMB_SWITCH_C2 = 2 };
+enum { PMB_FORCE_CUTOFF = 1, PMB_FORCE_PME = 2, PMB_FORCE_BONDED = 3 };
+enum { PMB_LEAPFROG = 0, PMB_LANGEVIN = 1 };
+enum {
+  PMB_E_COULOMB = 0,
+  PMB_E_LJ = 1,
+  PMB_E_BOND = 2,
+  PMB_E_ANGLE = 3,
+  PMB_E_VIRIAL = 4,
+  PMB_E_STRIDE = 16
+};
+
+typedef struct pmb_system pmb_system;
+typedef struct pmb_force pmb_force;
+typedef struct pmb_md pmb_md;
+
+/* One periodic box: the parts of ProtoMol's GenericTopology the force path reads
+ * (topology/GenericTopology.h:142-164) plus its PeriodicBoundaryConditions. */
+typedef struct {
+  int n_atoms, n_types;
+  const double *charge;   /* [n_atoms] scaled charge = e * 18.2226123264 (Atom::scaledCharge) */
+  const double *mass;     /* [n_atoms] (Atom::scaledMass); integrators only, may be NULL */
+  const int *type;        /* [n_atoms] LJ type index (Atom::type) */
+  const int *molecule;    /* [n_atoms] (Atom::molecule) */
+  const double *lj;       /* [n_types * n_types * 4] {A, B, A14, B14} (LennardJonesParameterTable) */
+  int n_excl;             /* ExclusionTable::getTable() */
+  const int *excl_pairs;  /* [2 * n_excl] atom indices within the box */
+  const int *excl_kind;   /* [n_excl] 1 = EXCLUSION_MODIFIED, 2 = EXCLUSION_FULL */
+  int n_bonds;
+  const int *bonds;       /* [2 * n_bonds] */
+  const double *bond_k, *bond_r0;
+  int n_angles;
+  const int *angles;      /* [3 * n_angles] */
+  const double *angle_k, *angle_theta0, *ub_k, *ub_r0;
+  double box[3];          /* orthogonal box edges (cellBasisVector1..3) */
+  double coulomb_scaling; /* GenericTopology::coulombScalingFactor */
+} pmb_box_desc;
+
+/* One force term.  PMB_FORCE_CUTOFF replaces NonbondedCutoffSystemForce with
+ * OneAtomPair(Two)<PBC, Switch, LennardJonesForce [, Switch, CoulombForce]>
+ * (force/nonbonded/NonbondedCutoffSystemForce.h:45-55); PMB_FORCE_PME replaces
+ * NonbondedPMEwaldSystemForce<PBC, CubicCellManager, real, reciprocal, correction, BSpline,
+ * Cutoff|C1> (mdl/interface/force/nonbonded/NonbondedPMEwaldSystemForce.h:245-319) with the
+ * parameters of its getParameters() (:1003-1014); PMB_FORCE_BONDED replaces BondSystemForce +
+ * AngleSystemForce. */
+typedef struct {
+  int kind;
+  /* cutoff: -switchingFunction, -switchon, -cutoff per potential */
+  int lj, lj_switch;
+  double lj_switchon, lj_cutoff;
+  int coulomb, coulomb_switch;
+  double coulomb_switchon, coulomb_cutoff;
+  /* PME: -gridsize nx ny nz, -cutoff, -order, -accuracy, -alpha (<= 0: bisection) */
+  int grid[3];
+  const int *box_grids;   /* optional [3 * n_boxes] per-box grid sizes (batched systems) */
+  int order;
+  double cutoff, accuracy, alpha;
+  int real_switch;        /* PMB_SWITCH_CUTOFF or PMB_SWITCH_C1 */
+  int real, reciprocal, correction;
+} pmb_force_desc;
+
+typedef struct {
+  int kind;                 /* PMB_LEAPFROG or PMB_LANGEVIN */
+  double timestep_fs;
+  double temperature;       /* Langevin temperature (K) */
+  double gamma_ps;          /* Langevin friction (1/ps) */
+  unsigned long long seed;  /* Langevin noise seed */
+} pmb_integrator_desc;
+
+const char *pmb_last_error(void);
+int pmb_device_count(void);
+
+/* Systems ------------------------------------------------------------------------------------ */
+pmb_system *pmb_system_create(const pmb_box_desc *boxes, int n_boxes, int precision);
+int pmb_system_destroy(pmb_system *sys);
+int pmb_system_set_stream(pmb_system *sys, void *cuda_stream);
+int pmb_system_n_atoms(const pmb_system *sys);
+int pmb_system_n_boxes(const pmb_system *sys);
+
+/* Forces ------------------------------------------------------------------------------------- */
+pmb_force *pmb_force_create(pmb_system *sys, const pmb_force_desc *desc);
+int pmb_force_destroy(pmb_force *f);
+/* Ewald splitting parameter in use (NonbondedPMEwaldSystemForce::initialize, :520-537). */
+int pmb_force_alpha(const pmb_force *f, double *alpha);
+
+/* SystemForce::evaluate(topology, positions, forces, energies) for one force: host positions
+ * [3 N], forces += [3 N], energies += [n_boxes * PMB_E_STRIDE]; virial != 0 also fills the
+ * virial slots (ScalarStructure::virial()). */
+int pmb_force_evaluate(pmb_force *f, const double *positions, double *forces, double *energies,
+                       int virial);
+/* Several forces of one system in one device pass (ForceGroup::evaluateSystemForces). */
+int pmb_evaluate(pmb_system *sys, pmb_force *const *forces, int n_forces, const double *positions,
+                 double *forces_out, double *energies, int virial);
+/* Same, with device pointers and no host synchronisation: d_forces and d_energies are
+ * overwritten (not accumulated), on the system's stream. */
+int pmb_evaluate_device(pmb_system *sys, pmb_force *const *forces, int n_forces,
+                        const double *d_positions, double *d_forces, double *d_energies,
+                        int virial);
+
+/* Device-resident MD (the integrator owns the step; one CUDA graph per step) ----------------- */
+pmb_md *pmb_md_create(pmb_system *sys, pmb_force *const *forces, int n_forces,
+                      const pmb_integrator_desc *desc);
+int pmb_md_destroy(pmb_md *md);
+/* Host state in; computes the initial forces (StandardIntegrator::initializeForces). */
+int pmb_md_set_state(pmb_md *md, const double *positions, const double *velocities);
+int pmb_md_get_state(pmb_md *md, double *positions, double *velocities);
+int pmb_md_get_forces(pmb_md *md, double *forces);
+/* LeapfrogIntegrator::run(n) / StandardIntegrator::run(n) semantics. */
+int pmb_md_run(pmb_md *md, int n_steps);
+/* Energies of the last force evaluation [n_boxes * PMB_E_STRIDE] and kinetic energy per box. */
+int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
+int pmb_md_use_graph(pmb_md *md, int enable);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMB200_H */

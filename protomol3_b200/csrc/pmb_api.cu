@@ -1,0 +1,1126 @@
+// C ABI of libpmb200: systems (batches of periodic boxes), force terms and the device MD loop.
+//
+// Host-side set-up mirrors what the reference does once per force:
+//   * alpha by bisection on erfc(alpha rc)/rc = accuracy
+//     (mdl/interface/force/nonbonded/NonbondedPMEwaldSystemForce.h:520-537);
+//   * self energy -alpha/sqrt(pi) sum q^2 and charged-system energy (:555-575);
+//   * lattice vectors for boxes smaller than twice the cutoff
+//     (topology/PeriodicBoundaryConditions.cpp:79-106);
+//   * grid tables exp(-pi^2 m^2/alpha^2) and the B-spline moduli (Grid.h:498-600).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pmb200.h"
+#include "pmb_internal.h"
+
+namespace pmb {
+static thread_local std::string g_err;
+void set_error(const std::string &m) { g_err = m; }
+}  // namespace pmb
+
+using namespace pmb;
+
+namespace {
+
+#define CK(expr)                                                                          \
+  do {                                                                                    \
+    cudaError_t _e = (expr);                                                              \
+    if (_e != cudaSuccess) {                                                              \
+      set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));                      \
+      return PMB_ERR_CUDA;                                                                \
+    }                                                                                     \
+  } while (0)
+
+int fail(int code, const std::string &m) {
+  set_error(m);
+  return code;
+}
+
+struct Allocs {
+  std::vector<void *> ptrs;
+  ~Allocs() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  T *get(size_t n, bool zero = true) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    if (zero) cudaMemset(p, 0, n * sizeof(T));
+    ptrs.push_back(p);
+    return static_cast<T *>(p);
+  }
+};
+
+template <typename T>
+int upload(Allocs &a, T *&dst, const std::vector<T> &src) {
+  dst = a.get<T>(src.size(), false);
+  if (!dst) return fail(PMB_ERR_CUDA, "cudaMalloc failed");
+  if (!src.empty()) CK(cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return PMB_OK;
+}
+
+double poly5h(double ar) {
+  double t = 1.0 / (1.0 + 0.3275911 * ar);
+  return t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 + t * 1.061405429))));
+}
+
+void bspline_h(int P, double w, double *th) {
+  if (P == 2) {
+    th[1] = w;
+    th[0] = 1.0 - w;
+    return;
+  }
+  th[P - 1] = 0.0;
+  th[1] = w;
+  th[0] = 1.0 - w;
+  for (int k = 2; k < P - 1; k++) {
+    double div = 1.0 / k;
+    th[k] = div * w * th[k - 1];
+    for (int j = 1; j < k; j++) th[k - j] = div * ((w + j) * th[k - j - 1] + ((double)(k + 1 - j) - w) * th[k - j]);
+    th[0] = div * (1 - w) * th[0];
+  }
+  double div = 1.0 / (P - 1.0);
+  th[P - 1] = div * w * th[P - 2];
+  for (int j = 1; j < P - 1; j++) th[P - 1 - j] = div * ((w + j) * th[P - j - 2] + ((double)(P - j) - w) * th[P - 1 - j]);
+  th[0] = div * (1 - w) * th[0];
+}
+
+double alpha_bisect(double rc, double acc) {
+  double a = 1.0;
+  while (std::erfc(a * rc) / rc >= acc) a *= 2.0;
+  double lo = 0.0, hi = a;
+  for (int i = 0; i < 100; ++i) {
+    a = 0.5 * (lo + hi);
+    if (std::erfc(a * rc) / rc >= acc) lo = a;
+    else hi = a;
+  }
+  return a;
+}
+
+// Lattice vectors with |v| <= 2 rc, (0,0,0) first, by increasing norm.
+std::vector<double> lattice_vectors(const double L[3], double rc) {
+  int bk = (int)std::floor(rc / L[0] + 1.0), bl = (int)std::floor(rc / L[1] + 1.0),
+      bm = (int)std::floor(rc / L[2] + 1.0);
+  std::vector<std::pair<double, std::vector<double>>> v;
+  for (int k = -bk; k <= bk; k++)
+    for (int l = -bl; l <= bl; l++)
+      for (int m = -bm; m <= bm; m++)
+        if (k || l || m) {
+          std::vector<double> c = {L[0] * k, L[1] * l, L[2] * m};
+          double n2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+          if (std::sqrt(n2) <= 2 * rc) v.push_back({n2, c});
+        }
+  std::stable_sort(v.begin(), v.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+  std::vector<double> out = {0, 0, 0};
+  for (auto &e : v) out.insert(out.end(), e.second.begin(), e.second.end());
+  return out;
+}
+
+bool factor235(int n, std::vector<int> &rad) {
+  rad.clear();
+  while (n % 4 == 0) { rad.push_back(4); n /= 4; }
+  while (n % 2 == 0) { rad.push_back(2); n /= 2; }
+  while (n % 3 == 0) { rad.push_back(3); n /= 3; }
+  while (n % 5 == 0) { rad.push_back(5); n /= 5; }
+  return n == 1;
+}
+
+SwitchDev make_switch(int kind, double switchon, double cutoff) {
+  SwitchDev w;
+  std::memset(&w, 0, sizeof(w));
+  w.kind = kind;
+  w.rc2 = cutoff * cutoff;
+  w.ron2 = switchon * switchon;
+  double d = cutoff * cutoff - switchon * switchon;
+  if (kind == SW_C2) {
+    w.s1 = 1.0 / (d * d * d);
+    w.s2 = cutoff * cutoff - 3.0 * switchon * switchon;
+    w.s3 = 4.0 / (d * d * d);
+  }
+  w.c15_1 = 1.5 / cutoff;
+  w.c05_3 = 0.5 / (cutoff * cutoff * cutoff);
+  w.c15_3 = 1.5 / (cutoff * cutoff * cutoff);
+  return w;
+}
+
+void switch_host(const SwitchDev &w, double r2, double &val, double &der) {
+  if (w.kind == SW_C2) {
+    der = 0.0;
+    if (r2 > w.rc2) val = 0.0;
+    else if (r2 >= w.ron2) {
+      double c2 = w.rc2 - r2, c4 = c2 * (w.s2 + 2.0 * r2);
+      val = w.s1 * (c2 * c4);
+      der = w.s3 * (c2 * c2 - c4);
+    } else val = 1.0;
+  } else if (w.kind == SW_C1) {
+    if (r2 > w.rc2) { val = 0; der = 0; return; }
+    double d = std::sqrt(r2);
+    val = 1.0 - d * (w.c15_1 - r2 * w.c05_3);
+    der = -w.c15_1 / d + d * w.c15_3;
+  } else {
+    der = 0.0;
+    val = r2 > w.rc2 ? 0.0 : 1.0;
+  }
+}
+
+int valid_switch(int k) { return k == SW_CUTOFF || k == SW_C1 || k == SW_C2; }
+
+}  // namespace
+
+// ================================================================================== system
+struct pmb_system {
+  int precision = 0, nbox = 0, natoms = 0, ntypes = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Allocs a;
+  std::vector<BoxDev> hbox;
+  std::vector<int> h_atom_box;
+  std::vector<double> h_charge, h_lj, h_mass;
+  std::vector<int> h_excl_pairs, h_excl_kind;  // global indices
+  double coulomb_scaling = 1.0;
+  BoxDev *d_box = nullptr;
+  int *d_atom_box = nullptr, *d_type = nullptr, *d_mol = nullptr;
+  double *d_pos = nullptr, *d_charge = nullptr, *d_mass = nullptr, *d_lj = nullptr;
+  int *d_excl_start = nullptr, *d_excl_partner = nullptr, *d_excl_kindc = nullptr;
+  int *d_excl_pairs = nullptr, *d_excl_kind = nullptr;
+  BondedDev bonded{};
+  long long *d_facc = nullptr, *d_eacc = nullptr;
+  double *d_fout = nullptr, *d_eout = nullptr;
+  double *h_fout = nullptr, *h_eout = nullptr;  // pinned
+  int *h_status = nullptr;                      // pinned
+  // neighbour list
+  bool nb_ready = false;
+  double nb_cutoff = 0.0;
+  NbListDev nb{};
+  Allocs nba;
+  int n_bonded = 0;
+
+  SystemDev dev() const {
+    SystemDev s;
+    s.nbox = nbox;
+    s.natoms = natoms;
+    s.box = d_box;
+    s.atom_box = d_atom_box;
+    s.pos = d_pos;
+    s.charge = d_charge;
+    s.type = d_type;
+    s.molecule = d_mol;
+    s.excl_start = d_excl_start;
+    s.excl_partner = d_excl_partner;
+    s.excl_kind = d_excl_kindc;
+    s.facc = d_facc;
+    s.eacc = d_eacc;
+    return s;
+  }
+  ~pmb_system() {
+    if (h_fout) cudaFreeHost(h_fout);
+    if (h_eout) cudaFreeHost(h_eout);
+    if (h_status) cudaFreeHost(h_status);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+struct pmb_force {
+  pmb_system *sys = nullptr;
+  pmb_force_desc d{};
+  int kind = 0;
+  // PME
+  double alpha = 0.0;
+  Allocs a;
+  PmeDev pm{};
+  std::vector<PmeBoxPlan> plans;
+  std::vector<double> const_e;  // [nbox * ACC_PER_BOX] self / charged / self-image energies
+  std::vector<double> const_vir;
+  double *d_lattice = nullptr;
+};
+
+namespace {
+
+// Neighbour-list storage sized for list cutoff rl.
+int nblist_alloc(pmb_system *s, double rl) {
+  s->nba.~Allocs();
+  new (&s->nba) Allocs();
+  NbListDev &nb = s->nb;
+  std::memset(&nb, 0, sizeof(nb));
+  int nblk = 0;
+  for (auto &b : s->hbox) nblk += b.nblk;
+  nb.nblk_total = nblk;
+  nb.nslot = nblk * BLOCK;
+  std::vector<int> blk_box(nblk), jcap_off(nblk + 1, 0);
+  long long tiles = 0;
+  for (int bi = 0; bi < s->nbox; bi++) {
+    const BoxDev &b = s->hbox[bi];
+    double V = b.L[0] * b.L[1] * b.L[2], rho = b.natoms / V;
+    double est = 1.5 * rho * (4.0 / 3.0) * M_PI * std::pow(rl + 8.0, 3) / 2.0 + 256.0;
+    int cap = (int)std::min<double>(((b.natoms + 31) / 32) * 32.0, ((long long)est + 31) / 32 * 32.0);
+    if (cap < 32) cap = 32;
+    for (int k = 0; k < b.nblk; k++) {
+      blk_box[b.blk0 + k] = bi;
+      jcap_off[b.blk0 + k + 1] = cap;
+      tiles += 1 + cap / 32;
+    }
+  }
+  for (int k = 0; k < nblk; k++) jcap_off[k + 1] += jcap_off[k];
+  if (tiles > 0x7fffffffLL || jcap_off[nblk] < 0) return fail(PMB_ERR_CAPACITY, "neighbour list too large");
+  nb.tile_cap = (int)tiles;
+  int *d_blk_box, *d_jcap;
+  if (upload(s->nba, d_blk_box, blk_box) || upload(s->nba, d_jcap, jcap_off)) return PMB_ERR_CUDA;
+  nb.blk_box = d_blk_box;
+  nb.jcap_off = d_jcap;
+  nb.blk_lo = s->nba.get<uint4>(nblk);
+  nb.blk_hi = s->nba.get<uint4>(nblk);
+  nb.jcount = s->nba.get<int>(nblk + 1);
+  nb.jlist = s->nba.get<int>((size_t)jcap_off[nblk], false);
+  nb.tile_off = s->nba.get<int>(nblk + 1);
+  nb.tile_blk = s->nba.get<int>(nb.tile_cap);
+  nb.tile_k = s->nba.get<int>(nb.tile_cap);
+  nb.status = s->nba.get<int>(4);
+  nb.slot_orig = s->nba.get<int>(nb.nslot, false);
+  if (nb.slot_orig) cudaMemset(nb.slot_orig, 0xff, sizeof(int) * nb.nslot);  // -1 padding
+  nb.slot_fx = s->nba.get<uint4>(nb.nslot);
+  nb.want_fp64 = s->precision == PMB_FP64;
+  nb.slot_pq = nb.want_fp64 ? s->nba.get<double4>(nb.nslot) : nullptr;
+  nb.slot_meta = s->nba.get<int4>(nb.nslot);
+  // sort bins
+  std::vector<int> bin_box;
+  for (int bi = 0; bi < s->nbox; bi++) {
+    int ncm = std::max(s->hbox[bi].nc[0], std::max(s->hbox[bi].nc[1], s->hbox[bi].nc[2]));
+    long long nk = (long long)ncm * ncm * ncm;
+    bin_box.insert(bin_box.end(), (size_t)nk, bi);
+  }
+  nb.nkeys = (int)bin_box.size();
+  int *d_bin_box;
+  if (upload(s->nba, d_bin_box, bin_box)) return PMB_ERR_CUDA;
+  nb.bin_box = d_bin_box;
+  nb.key = s->nba.get<int>(s->natoms);
+  nb.rank = s->nba.get<int>(s->natoms);
+  nb.bin_count = s->nba.get<int>(nb.nkeys + 1);
+  nb.bin_start = s->nba.get<int>(nb.nkeys + 1);
+  int maxn = std::max(nb.nkeys, nblk) + 1;
+  nb.scan_tmp = s->nba.get<int>(maxn / 4096 + 2);
+  if (!nb.blk_lo || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.scan_tmp || !nb.bin_start)
+    return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
+  s->nb_cutoff = rl;
+  s->nb_ready = true;
+  CK(cudaDeviceSynchronize());
+  return PMB_OK;
+}
+
+int ensure_nblist(pmb_system *s, double rl) {
+  if (s->nb_ready && rl <= s->nb_cutoff) return PMB_OK;
+  return nblist_alloc(s, rl);
+}
+
+double force_pair_cutoff(const pmb_force *f) {
+  if (f->kind == PMB_FORCE_CUTOFF)
+    return std::max(f->d.lj ? f->d.lj_cutoff : 0.0, f->d.coulomb ? f->d.coulomb_cutoff : 0.0);
+  if (f->kind == PMB_FORCE_PME && f->d.real) return f->d.cutoff;
+  return 0.0;
+}
+
+struct PairJob {
+  PairParams p;
+  const double *lattice;
+};
+
+PairParams base_params(const pmb_system *s, int virial) {
+  PairParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.ntypes = s->ntypes;
+  p.coulomb_scaling = s->coulomb_scaling;
+  p.virial = virial;
+  return p;
+}
+
+// Pair jobs of a force set; a cutoff LJ-only force and a PME real-space term are fused into one
+// launch (LJ + Ewald real space).
+std::vector<PairJob> pair_jobs(pmb_system *s, pmb_force *const *fs, int n, int virial) {
+  std::vector<PairJob> jobs;
+  const pmb_force *ljonly = nullptr, *pme = nullptr;
+  for (int i = 0; i < n; i++) {
+    if (fs[i]->kind == PMB_FORCE_CUTOFF && fs[i]->d.lj && !fs[i]->d.coulomb && !ljonly) ljonly = fs[i];
+    if (fs[i]->kind == PMB_FORCE_PME && fs[i]->d.real && !pme) pme = fs[i];
+  }
+  const bool fuse = ljonly && pme;
+  for (int i = 0; i < n; i++) {
+    const pmb_force *f = fs[i];
+    if (f->kind == PMB_FORCE_CUTOFF) {
+      if (fuse && f == ljonly) continue;
+      PairJob j;
+      j.p = base_params(s, virial);
+      j.lattice = nullptr;
+      j.p.do_lj = f->d.lj;
+      j.p.coul_mode = f->d.coulomb ? 1 : 0;
+      j.p.lj_sw = make_switch(f->d.lj_switch, f->d.lj_switchon, f->d.lj_cutoff);
+      j.p.coul_sw = make_switch(f->d.coulomb_switch, f->d.coulomb_switchon, f->d.coulomb_cutoff);
+      j.p.lj_cut2 = f->d.lj_cutoff * f->d.lj_cutoff;
+      j.p.coul_cut2 = f->d.coulomb_cutoff * f->d.coulomb_cutoff;
+      double rc = force_pair_cutoff(f);
+      j.p.cut2 = rc * rc;
+      jobs.push_back(j);
+    } else if (f->kind == PMB_FORCE_PME && f->d.real) {
+      PairJob j;
+      j.p = base_params(s, virial);
+      j.lattice = f->d_lattice;
+      j.p.coul_mode = 2;
+      j.p.coul_sw = make_switch(f->d.real_switch, 0.0, f->d.cutoff);
+      j.p.coul_cut2 = f->d.cutoff * f->d.cutoff;
+      j.p.alpha = f->alpha;
+      j.p.a2pi = 2.0 * f->alpha / std::sqrt(M_PI);
+      double rc = f->d.cutoff;
+      if (fuse && f == pme) {
+        j.p.do_lj = 1;
+        j.p.lj_sw = make_switch(ljonly->d.lj_switch, ljonly->d.lj_switchon, ljonly->d.lj_cutoff);
+        j.p.lj_cut2 = ljonly->d.lj_cutoff * ljonly->d.lj_cutoff;
+        rc = std::max(rc, ljonly->d.lj_cutoff);
+      }
+      j.p.cut2 = rc * rc;
+      jobs.push_back(j);
+    }
+  }
+  return jobs;
+}
+
+// Enqueues every force of the set on the system stream; accumulators must be zero.
+int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
+  SystemDev sd = s->dev();
+  cudaStream_t st = s->stream;
+  double rl = 0.0;
+  for (int i = 0; i < n; i++) rl = std::max(rl, force_pair_cutoff(fs[i]));
+  std::vector<PairJob> jobs = pair_jobs(s, fs, n, virial);
+  if (!jobs.empty()) {
+    int rc = ensure_nblist(s, rl + 1e-3);
+    if (rc) return rc;
+    nblist_build(sd, s->nb, rl + 1e-3, st);
+    for (auto &j : jobs) {
+      PairLaunch pl;
+      pl.precision = s->precision;
+      pl.p = j.p;
+      pl.lj = s->d_lj;
+      pl.lattice = j.lattice;
+      if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    pmb_force *f = fs[i];
+    if (f->kind == PMB_FORCE_PME) {
+      f->pm.virial = virial;
+      if (f->d.reciprocal) {
+        if (!s->nb_ready) {
+          int rc = ensure_nblist(s, std::max(rl, 1.0) + 1e-3);
+          if (rc) return rc;
+        }
+        if (jobs.empty()) nblist_build(sd, s->nb, std::max(s->nb_cutoff, 1.0), st);
+        pme_recip_launch(sd, s->nb, f->pm, st);
+      }
+      if (f->d.correction)
+        pme_correction_launch(sd, f->pm, s->d_excl_pairs, s->d_excl_kind, (int)s->h_excl_kind.size(),
+                              s->coulomb_scaling, st);
+    } else if (f->kind == PMB_FORCE_BONDED) {
+      BondedDev b = s->bonded;
+      b.virial = virial;
+      bonded_launch(sd, b, st);
+    }
+  }
+  CK(cudaGetLastError());
+  return PMB_OK;
+}
+
+void add_const(pmb_force *const *fs, int n, int nbox, int virial, double *e) {
+  for (int i = 0; i < n; i++) {
+    if (fs[i]->kind != PMB_FORCE_PME || !fs[i]->d.correction) continue;
+    for (int b = 0; b < nbox; b++) {
+      e[b * ACC_PER_BOX + E_COUL] += fs[i]->const_e[b];
+      if (virial)
+        for (int k = 0; k < 9; k++) e[b * ACC_PER_BOX + E_VIR + k] += fs[i]->const_vir[b * 9 + k];
+    }
+  }
+}
+
+int check_status(pmb_system *s) {
+  if (!s->nb_ready) return PMB_OK;
+  CK(cudaMemcpyAsync(s->h_status, s->nb.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (s->h_status[0] || s->h_status[1]) {
+    cudaMemsetAsync(s->nb.status, 0, 4 * sizeof(int), s->stream);
+    return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded (atoms denser than expected)");
+  }
+  return PMB_OK;
+}
+
+int grow_and_retry_needed(pmb_system *s) {
+  // doubles the per-block list capacity by pretending a larger list cutoff
+  return nblist_alloc(s, s->nb_cutoff * 1.26 + 1.0);
+}
+
+}  // namespace
+
+// ======================================================================================= ABI
+extern "C" {
+
+const char *pmb_last_error(void) { return g_err.c_str(); }
+
+int pmb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+pmb_system *pmb_system_create(const pmb_box_desc *boxes, int n_boxes, int precision) {
+  if (!boxes || n_boxes <= 0) return fail(PMB_ERR_ARG, "no boxes"), nullptr;
+  if (precision != PMB_FP64 && precision != PMB_MIXED) return fail(PMB_ERR_ARG, "precision"), nullptr;
+  if (pmb_device_count() <= 0) return fail(PMB_ERR_CUDA, "no CUDA device"), nullptr;
+  pmb_system *s = new pmb_system();
+  s->precision = precision;
+  s->nbox = n_boxes;
+  s->ntypes = boxes[0].n_types;
+  if (s->ntypes <= 0 || s->ntypes > MAX_LJ_TYPES || !boxes[0].lj) {
+    delete s;
+    return fail(PMB_ERR_UNSUPPORTED, "1 <= n_types <= 32 required"), nullptr;
+  }
+  s->h_lj.assign(boxes[0].lj, boxes[0].lj + 4 * s->ntypes * s->ntypes);
+  s->coulomb_scaling = boxes[0].coulomb_scaling;
+  std::vector<int> type, mol, estart, epart, ekind, bonds, angles;
+  std::vector<double> bk, br, ak, at, uk, ur;
+  int blk = 0, key0 = 0, mol0 = 0;
+  for (int bi = 0; bi < n_boxes; bi++) {
+    const pmb_box_desc &d = boxes[bi];
+    if (d.n_atoms <= 0 || !d.charge || !d.type || !d.molecule) {
+      delete s;
+      return fail(PMB_ERR_ARG, "box " + std::to_string(bi) + ": atoms, charge, type, molecule required"), nullptr;
+    }
+    if (d.n_types != s->ntypes ||
+        std::memcmp(d.lj, s->h_lj.data(), sizeof(double) * s->h_lj.size()) != 0 ||
+        d.coulomb_scaling != s->coulomb_scaling) {
+      delete s;
+      return fail(PMB_ERR_UNSUPPORTED, "all boxes of a system must share the LJ table and coulombScalingFactor"), nullptr;
+    }
+    BoxDev b;
+    std::memset(&b, 0, sizeof(b));
+    for (int k = 0; k < 3; k++) {
+      if (!(d.box[k] > 0.0)) {
+        delete s;
+        return fail(PMB_ERR_ARG, "box edges must be positive"), nullptr;
+      }
+      b.L[k] = d.box[k];
+      b.Lr[k] = 1.0 / d.box[k];
+      double lo = -d.box[k] * 0.5, hi = d.box[k] * 0.5;
+      b.H[k] = hi - lo;
+      b.H2[k] = b.H[k] * 0.5;
+      int nc = 1;
+      while (nc < 512 && d.box[k] / (2 * nc) >= 2.4) nc *= 2;
+      b.nc[k] = nc;
+    }
+    b.D = std::min((d.box[0] * 0.5) * (d.box[0] * 0.5),
+                   std::min((d.box[1] * 0.5) * (d.box[1] * 0.5), (d.box[2] * 0.5) * (d.box[2] * 0.5)));
+    int ncm = std::max(b.nc[0], std::max(b.nc[1], b.nc[2]));
+    b.nc[0] = b.nc[1] = b.nc[2] = ncm;  // one Morton space per box
+    b.atom0 = s->natoms;
+    b.natoms = d.n_atoms;
+    b.blk0 = blk;
+    b.nblk = (d.n_atoms + BLOCK - 1) / BLOCK;
+    b.key0 = key0;
+    b.nlat = 1;
+    blk += b.nblk;
+    key0 += ncm * ncm * ncm;
+    s->hbox.push_back(b);
+    int mmax = 0;
+    for (int i = 0; i < d.n_atoms; i++) {
+      if (d.type[i] < 0 || d.type[i] >= s->ntypes) {
+        delete s;
+        return fail(PMB_ERR_ARG, "atom type out of range"), nullptr;
+      }
+      s->h_atom_box.push_back(bi);
+      s->h_charge.push_back(d.charge[i]);
+      s->h_mass.push_back(d.mass ? d.mass[i] : 1.0);
+      type.push_back(d.type[i]);
+      mol.push_back(mol0 + d.molecule[i]);
+      mmax = std::max(mmax, d.molecule[i] + 1);
+    }
+    mol0 += mmax;
+    for (int k = 0; k < d.n_excl; k++) {
+      int a1 = d.excl_pairs[2 * k], a2 = d.excl_pairs[2 * k + 1];
+      if (a1 < 0 || a2 < 0 || a1 >= d.n_atoms || a2 >= d.n_atoms || a1 == a2) {
+        delete s;
+        return fail(PMB_ERR_ARG, "exclusion pair out of range"), nullptr;
+      }
+      s->h_excl_pairs.push_back(s->natoms + std::min(a1, a2));
+      s->h_excl_pairs.push_back(s->natoms + std::max(a1, a2));
+      s->h_excl_kind.push_back(d.excl_kind ? d.excl_kind[k] : 2);
+    }
+    for (int k = 0; k < d.n_bonds; k++)
+      if (d.bonds[2 * k] < 0 || d.bonds[2 * k] >= d.n_atoms || d.bonds[2 * k + 1] < 0 ||
+          d.bonds[2 * k + 1] >= d.n_atoms || d.bonds[2 * k] == d.bonds[2 * k + 1]) {
+        delete s;
+        return fail(PMB_ERR_ARG, "bond atom index out of range"), nullptr;
+      }
+    for (int k = 0; k < d.n_angles; k++)
+      for (int c = 0; c < 3; c++)
+        if (d.angles[3 * k + c] < 0 || d.angles[3 * k + c] >= d.n_atoms) {
+          delete s;
+          return fail(PMB_ERR_ARG, "angle atom index out of range"), nullptr;
+        }
+    for (int k = 0; k < d.n_bonds; k++) {
+      bonds.push_back(s->natoms + d.bonds[2 * k]);
+      bonds.push_back(s->natoms + d.bonds[2 * k + 1]);
+      bk.push_back(d.bond_k[k]);
+      br.push_back(d.bond_r0[k]);
+    }
+    for (int k = 0; k < d.n_angles; k++) {
+      for (int c = 0; c < 3; c++) angles.push_back(s->natoms + d.angles[3 * k + c]);
+      ak.push_back(d.angle_k[k]);
+      at.push_back(d.angle_theta0[k]);
+      uk.push_back(d.ub_k ? d.ub_k[k] : 0.0);
+      ur.push_back(d.ub_r0 ? d.ub_r0[k] : 0.0);
+    }
+    s->natoms += d.n_atoms;
+  }
+  // exclusion CSR per atom (both directions)
+  int N = s->natoms;
+  estart.assign(N + 1, 0);
+  size_t ne = s->h_excl_kind.size();
+  for (size_t k = 0; k < ne; k++) {
+    estart[s->h_excl_pairs[2 * k] + 1]++;
+    estart[s->h_excl_pairs[2 * k + 1] + 1]++;
+  }
+  for (int i = 0; i < N; i++) estart[i + 1] += estart[i];
+  epart.assign(2 * ne + 1, -1);
+  ekind.assign(2 * ne + 1, 0);
+  std::vector<int> fill(N, 0);
+  for (size_t k = 0; k < ne; k++) {
+    int a = s->h_excl_pairs[2 * k], b = s->h_excl_pairs[2 * k + 1];
+    epart[estart[a] + fill[a]] = b;
+    ekind[estart[a] + fill[a]++] = s->h_excl_kind[k];
+    epart[estart[b] + fill[b]] = a;
+    ekind[estart[b] + fill[b]++] = s->h_excl_kind[k];
+  }
+  int rc = 0;
+  rc |= upload(s->a, s->d_box, s->hbox);
+  rc |= upload(s->a, s->d_atom_box, s->h_atom_box);
+  rc |= upload(s->a, s->d_charge, s->h_charge);
+  rc |= upload(s->a, s->d_mass, s->h_mass);
+  rc |= upload(s->a, s->d_type, type);
+  rc |= upload(s->a, s->d_mol, mol);
+  rc |= upload(s->a, s->d_lj, s->h_lj);
+  rc |= upload(s->a, s->d_excl_start, estart);
+  rc |= upload(s->a, s->d_excl_partner, epart);
+  rc |= upload(s->a, s->d_excl_kindc, ekind);
+  rc |= upload(s->a, s->d_excl_pairs, s->h_excl_pairs);
+  rc |= upload(s->a, s->d_excl_kind, s->h_excl_kind);
+  int *d_bonds, *d_angles;
+  double *d_bk, *d_br, *d_ak, *d_at, *d_uk, *d_ur;
+  rc |= upload(s->a, d_bonds, bonds);
+  rc |= upload(s->a, d_bk, bk);
+  rc |= upload(s->a, d_br, br);
+  rc |= upload(s->a, d_angles, angles);
+  rc |= upload(s->a, d_ak, ak);
+  rc |= upload(s->a, d_at, at);
+  rc |= upload(s->a, d_uk, uk);
+  rc |= upload(s->a, d_ur, ur);
+  s->bonded.nbonds = (int)bk.size();
+  s->bonded.nangles = (int)ak.size();
+  s->bonded.bonds = d_bonds;
+  s->bonded.bond_k = d_bk;
+  s->bonded.bond_r0 = d_br;
+  s->bonded.angles = d_angles;
+  s->bonded.angle_k = d_ak;
+  s->bonded.angle_theta0 = d_at;
+  s->bonded.ub_k = d_uk;
+  s->bonded.ub_r0 = d_ur;
+  s->d_pos = s->a.get<double>(3 * (size_t)N);
+  s->d_facc = s->a.get<long long>(3 * (size_t)N);
+  s->d_eacc = s->a.get<long long>((size_t)n_boxes * ACC_PER_BOX);
+  s->d_fout = s->a.get<double>(3 * (size_t)N);
+  s->d_eout = s->a.get<double>((size_t)n_boxes * ACC_PER_BOX);
+  if (rc || !s->d_pos || !s->d_facc || !s->d_eacc || !s->d_fout || !s->d_eout ||
+      cudaMallocHost(&s->h_fout, sizeof(double) * 3 * (size_t)N) != cudaSuccess ||
+      cudaMallocHost(&s->h_eout, sizeof(double) * n_boxes * ACC_PER_BOX) != cudaSuccess ||
+      cudaMallocHost(&s->h_status, sizeof(int) * 4) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete s;
+    return fail(PMB_ERR_CUDA, "device allocation failed"), nullptr;
+  }
+  s->own_stream = true;
+  return s;
+}
+
+int pmb_system_destroy(pmb_system *s) {
+  if (!s) return PMB_OK;
+  cudaDeviceSynchronize();
+  delete s;
+  return PMB_OK;
+}
+
+int pmb_system_set_stream(pmb_system *s, void *stream) {
+  if (!s) return fail(PMB_ERR_ARG, "null system");
+  if (s->own_stream && s->stream) {
+    cudaStreamSynchronize(s->stream);
+    cudaStreamDestroy(s->stream);
+  }
+  s->own_stream = false;
+  s->stream = (cudaStream_t)stream;
+  return PMB_OK;
+}
+
+int pmb_system_n_atoms(const pmb_system *s) { return s ? s->natoms : 0; }
+int pmb_system_n_boxes(const pmb_system *s) { return s ? s->nbox : 0; }
+
+pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
+  if (!s || !d) return fail(PMB_ERR_ARG, "null argument"), nullptr;
+  pmb_force *f = new pmb_force();
+  f->sys = s;
+  f->d = *d;
+  f->kind = d->kind;
+  auto bad = [&](int code, const std::string &m) {
+    delete f;
+    fail(code, m);
+    return (pmb_force *)nullptr;
+  };
+  if (d->kind == PMB_FORCE_CUTOFF) {
+    if (!d->lj && !d->coulomb) return bad(PMB_ERR_ARG, "cutoff force needs LennardJones and/or Coulomb");
+    if ((d->lj && (!valid_switch(d->lj_switch) || !(d->lj_cutoff > 0))) ||
+        (d->coulomb && (!valid_switch(d->coulomb_switch) || !(d->coulomb_cutoff > 0))))
+      return bad(PMB_ERR_ARG, "invalid switching function or cutoff");
+    if ((d->lj && d->lj_switch == SW_C2 && !(d->lj_switchon >= 0 && d->lj_switchon < d->lj_cutoff)) ||
+        (d->coulomb && d->coulomb_switch == SW_C2 &&
+         !(d->coulomb_switchon >= 0 && d->coulomb_switchon < d->coulomb_cutoff)))
+      return bad(PMB_ERR_ARG, "C2 switching function: 0 <= switchon < cutoff");
+    return f;
+  }
+  if (d->kind == PMB_FORCE_BONDED) return f;
+  if (d->kind != PMB_FORCE_PME) return bad(PMB_ERR_ARG, "unknown force kind");
+  // ---- PME: NonbondedPMEwaldSystemForce::doMake checks (:1033-1058)
+  if (d->order < 2 || (d->order % 2) != 0 || d->order > 8) return bad(PMB_ERR_ARG, "order > 1, even and <= 8");
+  if (!(d->cutoff > 0)) return bad(PMB_ERR_ARG, "PMEwald cutoff > 0");
+  if (!(d->accuracy > 0)) return bad(PMB_ERR_ARG, "PMEwald accuracy > 0");
+  if (d->real && d->real_switch != SW_CUTOFF && d->real_switch != SW_C1)
+    return bad(PMB_ERR_ARG, "PME real-space switching function must be Cutoff or C1");
+  f->alpha = d->alpha > 0.0 ? d->alpha : alpha_bisect(d->cutoff, d->accuracy);
+  const int nbox = s->nbox, P = d->order;
+  f->const_e.assign(nbox, 0.0);
+  f->const_vir.assign(9 * (size_t)nbox, 0.0);
+  // constants per box
+  SwitchDev rsw = make_switch(d->real_switch, 0.0, d->cutoff);
+  std::vector<double> lat_all;
+  for (int bi = 0; bi < nbox; bi++) {
+    BoxDev &b = s->hbox[bi];
+    double q2 = 0.0, q1 = 0.0;
+    for (int i = b.atom0; i < b.atom0 + b.natoms; i++) {
+      q2 += s->h_charge[i] * s->h_charge[i];
+      q1 += s->h_charge[i];
+    }
+    double V = b.L[0] * b.L[1] * b.L[2];
+    double self = -q2 * f->alpha / std::sqrt(M_PI);
+    double charged = std::fabs(q1 * 0.00268283) > 1.0e-5 ? -M_PI / (2.0 * V * f->alpha * f->alpha) * q1 * q1 : 0.0;
+    f->const_e[bi] = self + charged;
+    f->const_vir[9 * bi + 0] += charged;
+    f->const_vir[9 * bi + 4] += charged;
+    f->const_vir[9 * bi + 8] += charged;
+    if (d->real) {
+      std::vector<double> lat = lattice_vectors(b.L, d->cutoff);
+      int nl = (int)lat.size() / 3;
+      b.lat0 = (int)lat_all.size() / 3;
+      b.nlat = nl;
+      b.multi_image = nl > 1;
+      lat_all.insert(lat_all.end(), lat.begin(), lat.end());
+      // i == j lattice images (realTerm with i == j): energy only, forces cancel
+      double a2pi = 2.0 * f->alpha / std::sqrt(M_PI);
+      for (int k = 1; k < nl; k++) {
+        double r2 = lat[3 * k] * lat[3 * k] + lat[3 * k + 1] * lat[3 * k + 1] + lat[3 * k + 2] * lat[3 * k + 2];
+        if (r2 > d->cutoff * d->cutoff) continue;
+        double r = std::sqrt(r2), rr = 1.0 / r, ar = f->alpha * r;
+        double g = std::exp(-ar * ar), e0 = poly5h(ar) * g * rr, f0 = (e0 + a2pi * g) * rr * rr, val, der;
+        switch_host(rsw, r2, val, der);
+        f0 = f0 * val - e0 * der;
+        e0 = e0 * val;
+        f->const_e[bi] += q2 * e0;
+        for (int p = 0; p < 3; p++)
+          for (int q = 0; q < 3; q++) f->const_vir[9 * bi + 3 * p + q] += q2 * f0 * lat[3 * k + p] * lat[3 * k + q];
+      }
+    }
+  }
+  if (d->real) {
+    if (upload(f->a, f->d_lattice, lat_all)) return bad(PMB_ERR_CUDA, "upload failed");
+    if (cudaMemcpy(s->d_box, s->hbox.data(), sizeof(BoxDev) * nbox, cudaMemcpyHostToDevice) != cudaSuccess)
+      return bad(PMB_ERR_CUDA, "upload failed");
+    s->nb_ready = false;  // list culling depends on multi_image
+  }
+  if (d->reciprocal) {
+    std::vector<double2> tw;
+    std::vector<float2> twf;
+    std::vector<double> infl;
+    std::vector<int> radix;
+    std::vector<int4> zwork;
+    std::vector<int2> pwork;
+    long long g0 = 0, c0 = 0;
+    int maxpe = 0;
+    const int plane_cap = pme_max_plane_elems(s->precision);
+    double th0[8];
+    bspline_h(P, 0.0, th0);
+    for (int bi = 0; bi < nbox; bi++) {
+      const BoxDev &b = s->hbox[bi];
+      PmeBoxPlan pl;
+      std::memset(&pl, 0, sizeof(pl));
+      for (int k = 0; k < 3; k++) {
+        int n = d->box_grids ? d->box_grids[3 * bi + k] : d->grid[k];
+        std::vector<int> rad;
+        if (n < P || n > 256 || !factor235(n, rad))
+          return bad(PMB_ERR_UNSUPPORTED, "PME grid sizes must be >= order, <= 256 and of the form 2^a 3^b 5^c");
+        pl.n[k] = n;
+        pl.hr[k] = n / b.L[k];
+        pl.mr[k] = 1.0 / b.L[k];
+        pl.tw0[k] = (int)tw.size();
+        for (int j = 0; j < n; j++) {
+          double ang = -2.0 * M_PI * j / n;
+          tw.push_back(make_double2(std::cos(ang), std::sin(ang)));
+          twf.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
+        }
+        pl.rad0[k] = (int)radix.size();
+        pl.nrad[k] = (int)rad.size();
+        radix.insert(radix.end(), rad.begin(), rad.end());
+        // influence factor B(m) exp(-pi^2 m^2/alpha^2) (Grid.h:523-571, dftmod :588-600)
+        pl.inf0[k] = (int)infl.size();
+        double fac = M_PI * M_PI / (f->alpha * f->alpha);
+        for (int i = 0; i < n; i++) {
+          int i0 = i <= n / 2 ? i : i - n;
+          double m = i0 * (1.0 / b.L[k]);
+          double ex = std::exp(-fac * (m * m));
+          double sc = 0.0, ss = 0.0;
+          for (int j = 0; j < P; j++) {
+            double x = M_PI * 2.0 * i * j / (double)n;
+            sc += th0[j] * std::cos(x);
+            ss += th0[j] * std::sin(x);
+          }
+          infl.push_back(ex / (sc * sc + ss * ss));
+        }
+      }
+      if (pl.n[0] * pl.n[1] > plane_cap)
+        return bad(PMB_ERR_UNSUPPORTED, "PME grid plane nx*ny too large for one CTA");
+      pl.grid0 = g0;
+      pl.cgrid0 = c0;
+      pl.piVr = 1.0 / (M_PI * b.L[0] * b.L[1] * b.L[2]);
+      pl.fac = M_PI * M_PI / (f->alpha * f->alpha);
+      pl.plane0 = (int)pwork.size();
+      g0 += (long long)pl.n[0] * pl.n[1] * pl.n[2];
+      c0 += (long long)(pl.n[2] / 2 + 1) * pl.n[0] * pl.n[1];
+      maxpe = std::max(maxpe, pl.n[0] * pl.n[1]);
+      for (int x = 0; x < pl.n[0]; x++)
+        for (int y0 = 0; y0 < pl.n[1]; y0 += 32) zwork.push_back(make_int4(bi, x, y0, std::min(32, pl.n[1] - y0)));
+      for (int kz = 0; kz <= pl.n[2] / 2; kz++) pwork.push_back(make_int2(bi, kz));
+      f->plans.push_back(pl);
+    }
+    PmeDev &pm = f->pm;
+    pm.nbox = nbox;
+    pm.order = P;
+    pm.precision = s->precision;
+    pm.alpha = f->alpha;
+    pm.a2pi = 2.0 * f->alpha / std::sqrt(M_PI);
+    PmeBoxPlan *dplan;
+    double2 *dtw;
+    float2 *dtwf;
+    double *dinf;
+    int *drad;
+    int4 *dz;
+    int2 *dp;
+    int rc = 0;
+    rc |= upload(f->a, dplan, f->plans);
+    rc |= upload(f->a, dtw, tw);
+    rc |= upload(f->a, dtwf, twf);
+    rc |= upload(f->a, dinf, infl);
+    rc |= upload(f->a, drad, radix);
+    rc |= upload(f->a, dz, zwork);
+    rc |= upload(f->a, dp, pwork);
+    pm.plan = dplan;
+    pm.twiddle = dtw;
+    pm.twiddlef = dtwf;
+    pm.infl = dinf;
+    pm.radix = drad;
+    pm.zwork = dz;
+    pm.nzwork = (int)zwork.size();
+    pm.pwork = dp;
+    pm.npwork = (int)pwork.size();
+    pm.max_plane_elems = maxpe;
+    pm.qgrid = f->a.get<long long>(g0);
+    pm.rgrid = s->precision ? (void *)f->a.get<float>(g0) : (void *)f->a.get<double>(g0);
+    pm.cgrid = s->precision ? (void *)f->a.get<float2>(c0) : (void *)f->a.get<double2>(c0);
+    pm.plane_part = f->a.get<double>(8 * (size_t)pwork.size());
+    if (rc || !pm.qgrid || !pm.rgrid || !pm.cgrid || !pm.plane_part) return bad(PMB_ERR_CUDA, "PME allocation failed");
+  } else {
+    f->pm.alpha = f->alpha;
+    f->pm.a2pi = 2.0 * f->alpha / std::sqrt(M_PI);
+    f->pm.precision = s->precision;
+  }
+  return f;
+}
+
+int pmb_force_destroy(pmb_force *f) {
+  if (f) {
+    cudaDeviceSynchronize();
+    delete f;
+  }
+  return PMB_OK;
+}
+
+int pmb_force_alpha(const pmb_force *f, double *alpha) {
+  if (!f || !alpha) return fail(PMB_ERR_ARG, "null argument");
+  *alpha = f->alpha;
+  return PMB_OK;
+}
+
+int pmb_evaluate_device(pmb_system *s, pmb_force *const *fs, int n, const double *d_pos,
+                        double *d_forces, double *d_energies, int virial) {
+  if (!s || (n > 0 && !fs)) return fail(PMB_ERR_ARG, "null argument");
+  for (int i = 0; i < n; i++)
+    if (!fs[i] || fs[i]->sys != s) return fail(PMB_ERR_ARG, "force belongs to another system");
+  cudaStream_t st = s->stream;
+  if (d_pos && d_pos != s->d_pos)
+    CK(cudaMemcpyAsync(s->d_pos, d_pos, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToDevice, st));
+  SystemDev sd = s->dev();
+  zero_accumulators(sd, st);
+  int rc = enqueue_forces(s, fs, n, virial);
+  if (rc) return rc;
+  if (d_forces) forces_to_double(sd, d_forces, st);
+  if (d_energies) energies_to_double(sd, nullptr, d_energies, st);
+  CK(cudaGetLastError());
+  return PMB_OK;
+}
+
+int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, double *forces,
+                 double *energies, int virial) {
+  if (!s || !pos) return fail(PMB_ERR_ARG, "null argument");
+  for (int i = 0; i < 3 * s->natoms; i++)
+    if (!std::isfinite(pos[i])) return fail(PMB_ERR_NUMERIC, "non-finite position");
+  cudaStream_t st = s->stream;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, st));
+    int rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(s->h_fout, s->d_fout, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(s->h_eout, s->d_eout, sizeof(double) * s->nbox * ACC_PER_BOX, cudaMemcpyDeviceToHost, st));
+    rc = check_status(s);
+    if (rc == PMB_ERR_CAPACITY) {
+      if (grow_and_retry_needed(s)) return PMB_ERR_CUDA;
+      continue;
+    }
+    if (rc) return rc;
+    if (forces)
+      for (int i = 0; i < 3 * s->natoms; i++) forces[i] += s->h_fout[i];
+    if (energies) {
+      add_const(fs, n, s->nbox, virial, s->h_eout);
+      for (int b = 0; b < s->nbox; b++) {
+        for (int k = 0; k < E_VIR; k++) energies[b * PMB_E_STRIDE + k] += s->h_eout[b * ACC_PER_BOX + k];
+        if (virial)
+          for (int k = 0; k < 9; k++)
+            energies[b * PMB_E_STRIDE + PMB_E_VIRIAL + k] += s->h_eout[b * ACC_PER_BOX + E_VIR + k];
+      }
+    }
+    return PMB_OK;
+  }
+  return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded after retries");
+}
+
+int pmb_force_evaluate(pmb_force *f, const double *pos, double *forces, double *energies, int virial) {
+  if (!f) return fail(PMB_ERR_ARG, "null force");
+  return pmb_evaluate(f->sys, &f, 1, pos, forces, energies, virial);
+}
+
+}  // extern "C"
+
+// ======================================================================================== MD
+struct pmb_md {
+  pmb_system *sys = nullptr;
+  std::vector<pmb_force *> forces;
+  pmb_integrator_desc d{};
+  IntegratorDev in{};
+  Allocs a;
+  double *d_vel = nullptr, *d_kin = nullptr;
+  long long *d_step = nullptr;
+  bool have_state = false, use_graph = true;
+  cudaGraphExec_t g_first = nullptr, g_next = nullptr;
+  std::vector<double> h_e, h_k;
+  ~pmb_md() {
+    if (g_first) cudaGraphExecDestroy(g_first);
+    if (g_next) cudaGraphExecDestroy(g_next);
+  }
+};
+
+namespace {
+
+int md_step_enqueue(pmb_md *m, double kick) {
+  pmb_system *s = m->sys;
+  SystemDev sd = s->dev();
+  integrate_kick_drift(sd, m->in, kick, s->stream);
+  return enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+}
+
+int md_capture(pmb_md *m, double kick, cudaGraphExec_t *out) {
+  pmb_system *s = m->sys;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = md_step_enqueue(m, kick);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(PMB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(PMB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return PMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pmb_md *pmb_md_create(pmb_system *s, pmb_force *const *fs, int n, const pmb_integrator_desc *d) {
+  if (!s || !d || n < 0 || (n > 0 && !fs)) return fail(PMB_ERR_ARG, "null argument"), nullptr;
+  if (d->kind != PMB_LEAPFROG && d->kind != PMB_LANGEVIN) return fail(PMB_ERR_ARG, "integrator kind"), nullptr;
+  if (!(d->timestep_fs > 0)) return fail(PMB_ERR_ARG, "timestep > 0"), nullptr;
+  if (d->kind == PMB_LANGEVIN && !(d->gamma_ps > 0 && d->temperature >= 0))
+    return fail(PMB_ERR_ARG, "Langevin needs gamma > 0 and temperature >= 0"), nullptr;
+  pmb_md *m = new pmb_md();
+  m->sys = s;
+  m->d = *d;
+  for (int i = 0; i < n; i++) {
+    if (!fs[i] || fs[i]->sys != s) {
+      delete m;
+      return fail(PMB_ERR_ARG, "force belongs to another system"), nullptr;
+    }
+    m->forces.push_back(fs[i]);
+  }
+  const double INV_TIMEFACTOR = 0.02045482828087295, BOLTZMANN = 0.001987191;
+  m->d_vel = m->a.get<double>(3 * (size_t)s->natoms);
+  m->d_kin = m->a.get<double>(s->nbox);
+  m->d_step = m->a.get<long long>(1);
+  if (!m->d_vel || !m->d_kin || !m->d_step) {
+    delete m;
+    return fail(PMB_ERR_CUDA, "allocation failed"), nullptr;
+  }
+  m->in.kind = d->kind;
+  m->in.h = d->timestep_fs * INV_TIMEFACTOR;
+  m->in.gamma = d->gamma_ps / (1000 * INV_TIMEFACTOR);  // LangevinLeapfrogIntegrator.cpp:28
+  m->in.kT = BOLTZMANN * d->temperature;
+  m->in.seed = d->seed;
+  m->in.mass = s->d_mass;
+  m->in.pos = s->d_pos;
+  m->in.vel = m->d_vel;
+  m->in.step = m->d_step;
+  m->h_e.assign((size_t)s->nbox * ACC_PER_BOX, 0.0);
+  m->h_k.assign(s->nbox, 0.0);
+  return m;
+}
+
+int pmb_md_destroy(pmb_md *m) {
+  if (m) {
+    cudaDeviceSynchronize();
+    delete m;
+  }
+  return PMB_OK;
+}
+
+int pmb_md_use_graph(pmb_md *m, int enable) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  m->use_graph = enable != 0;
+  return PMB_OK;
+}
+
+int pmb_md_set_state(pmb_md *m, const double *pos, const double *vel) {
+  if (!m || !pos) return fail(PMB_ERR_ARG, "null argument");
+  pmb_system *s = m->sys;
+  for (int i = 0; i < 3 * s->natoms; i++)
+    if (!std::isfinite(pos[i]) || (vel && !std::isfinite(vel[i]))) return fail(PMB_ERR_NUMERIC, "non-finite state");
+  CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
+  if (vel) CK(cudaMemcpyAsync(m->d_vel, vel, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
+  else CK(cudaMemsetAsync(m->d_vel, 0, sizeof(double) * 3 * s->natoms, s->stream));
+  CK(cudaMemsetAsync(m->d_step, 0, sizeof(long long), s->stream));
+  SystemDev sd = s->dev();
+  for (int attempt = 0; attempt < 3; attempt++) {
+    zero_accumulators(sd, s->stream);
+    int rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+    if (rc) return rc;
+    rc = check_status(s);
+    if (rc == PMB_ERR_CAPACITY) {
+      if (grow_and_retry_needed(s)) return PMB_ERR_CUDA;
+      if (m->g_first) { cudaGraphExecDestroy(m->g_first); m->g_first = nullptr; }
+      if (m->g_next) { cudaGraphExecDestroy(m->g_next); m->g_next = nullptr; }
+      continue;
+    }
+    if (rc) return rc;
+    m->have_state = true;
+    return PMB_OK;
+  }
+  return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded");
+}
+
+int pmb_md_run(pmb_md *m, int n) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  if (!m->have_state) return fail(PMB_ERR_STATE, "pmb_md_set_state must come first");
+  if (n < 1) return PMB_OK;
+  pmb_system *s = m->sys;
+  if (m->use_graph) {
+    if (!m->g_first) {
+      int rc = md_capture(m, 0.5, &m->g_first);
+      if (rc) return rc;
+    }
+    if (n > 1 && !m->g_next) {
+      int rc = md_capture(m, 1.0, &m->g_next);
+      if (rc) return rc;
+    }
+    CK(cudaGraphLaunch(m->g_first, s->stream));
+    for (int i = 1; i < n; i++) CK(cudaGraphLaunch(m->g_next, s->stream));
+  } else {
+    int rc = md_step_enqueue(m, 0.5);
+    if (rc) return rc;
+    for (int i = 1; i < n; i++) {
+      rc = md_step_enqueue(m, 1.0);
+      if (rc) return rc;
+    }
+  }
+  integrate_half_kick(s->dev(), m->in, s->stream);
+  CK(cudaGetLastError());
+  return PMB_OK;
+}
+
+int pmb_md_get_state(pmb_md *m, double *pos, double *vel) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  pmb_system *s = m->sys;
+  if (pos) CK(cudaMemcpyAsync(pos, s->d_pos, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToHost, s->stream));
+  if (vel) CK(cudaMemcpyAsync(vel, m->d_vel, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return check_status(s);
+}
+
+int pmb_md_get_forces(pmb_md *m, double *forces) {
+  if (!m || !forces) return fail(PMB_ERR_ARG, "null argument");
+  pmb_system *s = m->sys;
+  forces_to_double(s->dev(), s->d_fout, s->stream);
+  CK(cudaMemcpyAsync(forces, s->d_fout, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return PMB_OK;
+}
+
+int pmb_md_energies(pmb_md *m, double *energies, double *kinetic) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  pmb_system *s = m->sys;
+  SystemDev sd = s->dev();
+  energies_to_double(sd, nullptr, s->d_eout, s->stream);
+  kinetic_energy(sd, m->in, m->d_kin, s->stream);
+  CK(cudaMemcpyAsync(m->h_e.data(), s->d_eout, sizeof(double) * m->h_e.size(), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(m->h_k.data(), m->d_kin, sizeof(double) * m->h_k.size(), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  add_const(m->forces.data(), (int)m->forces.size(), s->nbox, 0, m->h_e.data());
+  for (int b = 0; b < s->nbox; b++) {
+    if (energies)
+      for (int k = 0; k < PMB_E_STRIDE; k++) energies[b * PMB_E_STRIDE + k] = k < E_VIR ? m->h_e[b * ACC_PER_BOX + k] : 0.0;
+    if (kinetic) kinetic[b] = m->h_k[b];
+  }
+  return check_status(s);
+}
+
+}  // extern "C"

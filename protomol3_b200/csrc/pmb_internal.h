@@ -1,0 +1,151 @@
+// Host-side declarations shared by the .cu translation units of libpmb200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "pmb_common.cuh"
+
+namespace pmb {
+
+void set_error(const std::string &msg);
+
+#define PMB_CUDA(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess) {                                                             \
+      ::pmb::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));              \
+      return PMB_ERR_CUDA;                                                               \
+    }                                                                                    \
+  } while (0)
+
+enum {
+  PMB_OK_ = 0,
+};
+
+// ------------------------------------------------------------------ neighbour list (nblist.cu)
+struct NbListDev {
+  // per block
+  int nblk_total;
+  const int *blk_box;          // [nblk]
+  float4 *blk_center;          // [nblk] fractional-fixed centre (as uint bits) and count
+  uint4 *blk_lo, *blk_hi;      // [nblk] fixed-point extents (x, y, z)
+  int *jcap_off;               // [nblk+1] offset of each block's j-slot list region
+  int *jcount;                 // [nblk] tiles per block (1 diagonal + list tiles)
+  int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding)
+  int *tile_off;               // [nblk+1] exclusive scan of jcount
+  int *tile_blk;               // [tile_cap] block of each tile
+  int *tile_k;                 // [tile_cap] tile index within the block
+  int tile_cap;
+  int *status;                 // [4] overflow flags
+  // per slot
+  int nslot;
+  int *slot_orig;              // [nslot] original atom index or -1
+  uint4 *slot_fx;              // [nslot] fractional fixed-point x, y, z (2^32 per edge) + q bits
+  double4 *slot_pq;            // [nslot] raw double position + q (FP64 path)
+  int4 *slot_meta;             // [nslot] orig, molecule, type, box
+  // sort
+  int nkeys;
+  int *key;                    // [natoms]
+  int *rank;                   // [natoms]
+  int *bin_count;              // [nkeys + 1]
+  int *bin_start;              // [nkeys + 1]
+  int *scan_tmp;               // scratch for scans
+  const int *bin_box;          // [nkeys] box of each sort bin
+  int want_fp64;               // also pack raw double positions
+};
+
+struct SystemDev {
+  int nbox, natoms;
+  const BoxDev *box;           // [nbox]
+  const int *atom_box;         // [natoms]
+  const double *pos;           // [3 natoms] caller order
+  const double *charge;        // [natoms]
+  const int *type, *molecule;  // [natoms]
+  const int *excl_start, *excl_partner, *excl_kind;  // CSR by atom
+  long long *facc;             // [3 natoms]
+  long long *eacc;             // [nbox * ACC_PER_BOX]
+};
+
+int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st);
+
+// ------------------------------------------------------------------ pair kernel (pair.cu)
+struct PairLaunch {
+  int precision;                  // 0 fp64, 1 mixed
+  int do_lj, coul_mode, virial;
+  const double *lj;               // [ntypes*ntypes*4] device
+  const float *ljf;               // float copy
+  const double *lattice;          // [nlat_total*3]
+  PairParams p;
+};
+int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st);
+
+// ------------------------------------------------------------------ PME (pme.cu)
+struct PmeBoxPlan {
+  int n[3];
+  long long grid0;    // offset of this box's real/fixed grid (elements)
+  long long cgrid0;   // offset of this box's half-complex grid (elements)
+  int tw0[3];         // offsets of twiddle tables (complex elements)
+  int inf0[3];        // offsets of influence tables
+  int rad0[3], nrad[3];
+  int plane0;         // first energy-partial slot of this box
+  int pad_;
+  double hr[3];       // n / L
+  double mr[3];       // 1 / L
+  double piVr, fac;   // 1/(pi V), pi^2 / alpha^2
+};
+
+struct PmeDev {
+  int nbox, order, precision;
+  const PmeBoxPlan *plan;     // [nbox] device
+  long long *qgrid;           // fixed-point charge grid
+  void *cgrid;                // half-complex grid (float2 or double2), layout [kz][x][y]
+  void *rgrid;                // real potential grid (float or double), layout [x][y][z]
+  const double2 *twiddle;     // per dim tables exp(-2 pi i k / n)
+  const float2 *twiddlef;
+  const double *infl;         // per dim influence factor B(m) exp(-pi^2 m^2/alpha^2)
+  const int *radix;           // radices per dim
+  const int4 *zwork;          // z-pass work items: box, x, y0, count
+  int nzwork;
+  const int2 *pwork;          // plane work items: box, kz
+  int npwork;
+  double *plane_part;         // [npwork * 7] energy + virial partials
+  int max_plane_elems;
+  double alpha, a2pi;
+  int virial;
+};
+int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st);
+int pme_max_plane_elems(int precision);
+int pme_correction_launch(const SystemDev &s, const PmeDev &pm, const int *excl_pairs,
+                          const int *excl_kind, int nexcl, double coulomb_scaling, cudaStream_t st);
+
+// ------------------------------------------------------------------ bonded / integrator (md.cu)
+struct BondedDev {
+  int nbonds, nangles;
+  const int *bonds;
+  const double *bond_k, *bond_r0;
+  const int *angles;
+  const double *angle_k, *angle_theta0, *ub_k, *ub_r0;
+  int virial;
+};
+int bonded_launch(const SystemDev &s, const BondedDev &b, cudaStream_t st);
+int forces_to_double(const SystemDev &s, double *out, cudaStream_t st);
+int energies_to_double(const SystemDev &s, const double *const_e, double *out, cudaStream_t st);
+int zero_accumulators(const SystemDev &s, cudaStream_t st);
+
+struct IntegratorDev {
+  int kind;            // 0 leapfrog, 1 Langevin
+  double h;            // dt * INV_TIMEFACTOR
+  double gamma, kT;    // Langevin (internal units)
+  unsigned long long seed;
+  const double *mass;  // [natoms]
+  double *pos, *vel;
+  long long *step;     // device step counter
+};
+int integrate_kick_drift(const SystemDev &s, const IntegratorDev &in, double kick, cudaStream_t st);
+int integrate_half_kick(const SystemDev &s, const IntegratorDev &in, cudaStream_t st);
+int kinetic_energy(const SystemDev &s, const IntegratorDev &in, double *out_per_box, cudaStream_t st);
+
+}  // namespace pmb

@@ -1,0 +1,338 @@
+// Device cell-list / neighbour build: the B200 replacement of Topology::updateCellLists
+// (topology/Topology.h:44-81) and CellListEnumerator<PBC, CubicCellManager>
+// (topology/CellListEnumeratorPeriodicBoundaries.h:25-134).
+//
+// Instead of linked cell lists walked pair-of-cells by pair-of-cells, atoms are binned on a fine
+// Morton-ordered grid with a deterministic counting sort, packed into 32-atom blocks ("slots"),
+// and each block I gets a compacted list of atoms of blocks J > I that lie within the list
+// cutoff of I's bounding box.  The pair kernel then sees (I, 32 j-atoms) tiles; the pair set it
+// evaluates is exactly the reference's: every unordered pair once, minimal image, r^2 <= rc^2.
+#include "pmb_internal.h"
+
+namespace pmb {
+
+namespace {
+
+constexpr int SCAN_CHUNK = 4096;  // elements per CTA (1024 threads x 4)
+
+__device__ __forceinline__ unsigned part1by2(unsigned x) {
+  x &= 0x3ff;
+  x = (x | (x << 16)) & 0x030000ff;
+  x = (x | (x << 8)) & 0x0300f00f;
+  x = (x | (x << 4)) & 0x030c30c3;
+  x = (x | (x << 2)) & 0x09249249;
+  return x;
+}
+
+__device__ __forceinline__ unsigned frac_fixed(double x, double Lr) {
+  double u = x * Lr;
+  u -= floor(u);
+  double s = u * 4294967296.0;
+  if (!(s >= 0.0)) s = 0.0;                 // also catches NaN
+  if (s >= 4294967295.0) s = 4294967295.0;
+  return (unsigned)s;
+}
+
+// ---------------------------------------------------------------- scans
+__device__ int block_exclusive_scan(int v, int *total) {
+  __shared__ int warp_tot[32];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int nw = blockDim.x >> 5;
+    int t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < nw) warp_tot[lane] = t;
+  }
+  __syncthreads();
+  int off = w > 0 ? warp_tot[w - 1] : 0;
+  if (total) *total = warp_tot[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return off + x - v;
+}
+
+__global__ void k_scan_reduce(const int *in, int n, int *chunk) {
+  long long base = (long long)blockIdx.x * SCAN_CHUNK + threadIdx.x * 4;
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+    if (base + k < n) s += in[base + k];
+  int tot;
+  block_exclusive_scan(s, &tot);
+  if (threadIdx.x == 0) chunk[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_chunks(int *chunk, int nchunk) {
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b = 0; b < nchunk; b += blockDim.x) {
+    int i = b + threadIdx.x;
+    int v = i < nchunk ? chunk[i] : 0;
+    int tot;
+    int ex = block_exclusive_scan(v, &tot);
+    if (i < nchunk) chunk[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) chunk[nchunk] = carry;
+}
+
+__global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out) {
+  long long base = (long long)blockIdx.x * SCAN_CHUNK + threadIdx.x * 4;
+  int v[4], s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  int ex = block_exclusive_scan(s, nullptr) + chunk[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (base + k < n) out[base + k] = ex;
+    ex += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = chunk[gridDim.x];
+}
+
+// ---------------------------------------------------------------- binning and sort
+__global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.natoms) return;
+  const BoxDev &b = s.box[s.atom_box[i]];
+  unsigned c[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    unsigned f = frac_fixed(s.pos[3 * i + k], b.Lr[k]);
+    c[k] = (unsigned)(((unsigned long long)f * (unsigned)b.nc[k]) >> 32);
+  }
+  int kk = b.key0 + (int)(part1by2(c[0]) | (part1by2(c[1]) << 1) | (part1by2(c[2]) << 2));
+  key[i] = kk;
+  rank[i] = atomicAdd(&bin_count[kk], 1);
+}
+
+__global__ void k_scatter(SystemDev s, const int *key, const int *rank, const int *bin_start,
+                          int *slot_orig) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.natoms) return;
+  const BoxDev &b = s.box[s.atom_box[i]];
+  int base = b.blk0 * BLOCK - bin_start[b.key0];
+  slot_orig[base + bin_start[key[i]] + rank[i]] = i;
+}
+
+// Makes the within-bin order deterministic (ascending original index).
+__global__ void k_sort_bins(SystemDev s, const int *bin_box, const int *bin_start,
+                            const int *bin_count, int nkeys, int *slot_orig) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nkeys) return;
+  int cnt = bin_count[k];
+  if (cnt < 2) return;
+  const BoxDev &b = s.box[bin_box[k]];
+  int *p = slot_orig + b.blk0 * BLOCK - bin_start[b.key0] + bin_start[k];
+  for (int a = 1; a < cnt; a++) {
+    int v = p[a], j = a - 1;
+    while (j >= 0 && p[j] > v) {
+      p[j + 1] = p[j];
+      j--;
+    }
+    p[j + 1] = v;
+  }
+}
+
+__global__ void k_pack(SystemDev s, NbListDev nb, int want_fp64) {
+  int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nb.nslot) return;
+  int o = nb.slot_orig[sl];
+  if (o < 0) {
+    nb.slot_meta[sl] = make_int4(-1, -1, 0, nb.blk_box[sl / BLOCK]);
+    nb.slot_fx[sl] = make_uint4(0, 0, 0, 0);
+    if (want_fp64) nb.slot_pq[sl] = make_double4(0, 0, 0, 0);
+    return;
+  }
+  int bi = s.atom_box[o];
+  const BoxDev &b = s.box[bi];
+  double x = s.pos[3 * o], y = s.pos[3 * o + 1], z = s.pos[3 * o + 2], q = s.charge[o];
+  nb.slot_meta[sl] = make_int4(o, s.molecule[o], s.type[o], bi);
+  nb.slot_fx[sl] = make_uint4(frac_fixed(x, b.Lr[0]), frac_fixed(y, b.Lr[1]),
+                              frac_fixed(z, b.Lr[2]), __float_as_uint((float)q));
+  if (want_fp64) nb.slot_pq[sl] = make_double4(x, y, z, q);
+}
+
+__global__ void k_block_bbox(NbListDev nb) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nb.nblk_total) return;
+  int sl = warp * BLOCK + lane;
+  bool valid = nb.slot_orig[sl] >= 0;
+  uint4 f = nb.slot_fx[sl];
+  unsigned lo[3] = {valid ? f.x : 0xffffffffu, valid ? f.y : 0xffffffffu, valid ? f.z : 0xffffffffu};
+  unsigned hi[3] = {valid ? f.x : 0u, valid ? f.y : 0u, valid ? f.z : 0u};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  int cnt = __popc(__ballot_sync(0xffffffffu, valid));
+  if (lane == 0) {
+    if (cnt == 0) {
+      lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
+    }
+    nb.blk_lo[warp] = make_uint4(lo[0], lo[1], lo[2], (unsigned)cnt);
+    nb.blk_hi[warp] = make_uint4(hi[0], hi[1], hi[2], 0u);
+  }
+}
+
+// Gap (in A) between a point / box and a box, in fractional fixed-point coordinates with the
+// minimal image taken by 32-bit wrap-around.
+__device__ __forceinline__ double box_gap2(const BoxDev &b, const unsigned c1[3], const unsigned h1[3],
+                                           const unsigned c2[3], const unsigned h2[3]) {
+  double g2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    long long d = (long long)(int)(c2[k] - c1[k]);
+    long long a = d < 0 ? -d : d;
+    long long gap = a - (long long)h1[k] - (long long)h2[k];
+    if (gap > 0) {
+      double ga = (double)gap * b.L[k] * (1.0 / 4294967296.0);
+      g2 += ga * ga;
+    }
+  }
+  return g2;
+}
+
+__device__ __forceinline__ void center_half(uint4 lo, uint4 hi, unsigned c[3], unsigned h[3]) {
+  unsigned l[3] = {lo.x, lo.y, lo.z}, u[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    h[k] = (u[k] - l[k]) / 2u + 1u;
+    c[k] = l[k] + (u[k] - l[k]) / 2u;
+  }
+}
+
+// One warp per block I: candidate blocks J > I of the same box by bounding-box gap, then the
+// atoms of each candidate within the list cutoff of I's box, compacted into I's j-list.
+__global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
+  int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (I >= nb.nblk_total) return;
+  int bi = nb.blk_box[I];
+  const BoxDev &b = s.box[bi];
+  uint4 loI = nb.blk_lo[I], hiI = nb.blk_hi[I];
+  if (loI.w == 0) {
+    if (lane == 0) nb.jcount[I] = 0;
+    return;
+  }
+  unsigned cI[3], hI[3];
+  center_half(loI, hiI, cI, hI);
+  int jend = b.blk0 + b.nblk;
+  int cap = nb.jcap_off[I + 1] - nb.jcap_off[I];
+  int *out = nb.jlist + nb.jcap_off[I];
+  int count = 0;
+  bool overflow = false;
+  unsigned zero[3] = {0, 0, 0};
+  for (int J0 = I + 1; J0 < jend; J0 += 32) {
+    int J = J0 + lane;
+    bool cand = false;
+    if (J < jend) {
+      uint4 loJ = nb.blk_lo[J], hiJ = nb.blk_hi[J];
+      if (loJ.w > 0) {
+        if (b.multi_image) cand = true;
+        else {
+          unsigned cJ[3], hJ[3];
+          center_half(loJ, hiJ, cJ, hJ);
+          cand = box_gap2(b, cI, hI, cJ, hJ) <= rlist2;
+        }
+      }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, cand);
+    while (m) {
+      int src = __ffs(m) - 1;
+      m &= m - 1;
+      int Jc = J0 + src;
+      int sl = Jc * BLOCK + lane;
+      bool take = false;
+      if (nb.slot_orig[sl] >= 0) {
+        if (b.multi_image) take = true;
+        else {
+          uint4 f = nb.slot_fx[sl];
+          unsigned p[3] = {f.x, f.y, f.z};
+          take = box_gap2(b, cI, hI, p, zero) <= rlist2;
+        }
+      }
+      unsigned tm = __ballot_sync(0xffffffffu, take);
+      int n = __popc(tm);
+      if (count + n > cap) {
+        overflow = true;
+        break;
+      }
+      if (take) out[count + __popc(tm & ((1u << lane) - 1u))] = sl;
+      count += n;
+    }
+    if (overflow) break;
+  }
+  int padded = (count + 31) & ~31;
+  if (!overflow)
+    for (int k = count + lane; k < padded; k += 32) out[k] = -1;
+  if (lane == 0) {
+    if (overflow) atomicExch(&nb.status[0], 1);
+    nb.jcount[I] = overflow ? 1 : 1 + padded / 32;
+  }
+}
+
+__global__ void k_tile_map(NbListDev nb) {
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nb.nblk_total) return;
+  int off = nb.tile_off[I], cnt = nb.jcount[I];
+  if (off + cnt > nb.tile_cap) {
+    atomicExch(&nb.status[1], 1);
+    return;
+  }
+  for (int k = 0; k < cnt; k++) {
+    nb.tile_blk[off + k] = I;
+    nb.tile_k[off + k] = k;
+  }
+}
+
+int scan_exclusive(const int *in, int *out, int n, int *tmp, cudaStream_t st) {
+  int nchunk = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+  if (nchunk < 1) nchunk = 1;
+  k_scan_reduce<<<nchunk, 1024, 0, st>>>(in, n, tmp);
+  k_scan_chunks<<<1, 1024, 0, st>>>(tmp, nchunk);
+  k_scan_apply<<<nchunk, 1024, 0, st>>>(in, n, tmp, out);
+  return 0;
+}
+
+}  // namespace
+
+int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st) {
+  const int T = 256;
+  int na = s.natoms;
+  if (na <= 0) return 0;
+  cudaMemsetAsync(nb.bin_count, 0, sizeof(int) * (size_t)(nb.nkeys + 1), st);
+  k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count);
+  scan_exclusive(nb.bin_count, nb.bin_start, nb.nkeys, nb.scan_tmp, st);
+  k_scatter<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_start, nb.slot_orig);
+  k_sort_bins<<<(nb.nkeys + T - 1) / T, T, 0, st>>>(s, nb.bin_box, nb.bin_start, nb.bin_count,
+                                                   nb.nkeys, nb.slot_orig);
+  k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
+  int wthreads = nb.nblk_total * 32;
+  k_block_bbox<<<(wthreads + T - 1) / T, T, 0, st>>>(nb);
+  k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
+  scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st);
+  k_tile_map<<<(nb.nblk_total + T - 1) / T, T, 0, st>>>(nb);
+  return 0;
+}
+
+}  // namespace pmb

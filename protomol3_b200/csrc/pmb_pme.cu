@@ -1,0 +1,601 @@
+// Particle-mesh Ewald reciprocal term and exclusion corrections.
+//
+// Reference: mdl/interface/force/nonbonded/Grid.h (anterpolateCharge :107-154, interpolateForce
+// :158-189, scalarSum :236-341, initialize :498-586, dftmod :588-600), BSpline.cpp:55-105,
+// NonbondedPMEwaldSystemForce.h (reciprocalTerm :812-864, correctionTerm :874-911).
+//
+// Pipeline per step (every kernel batched over the boxes of a system):
+//   k_spread      one thread per atom slot, B-spline weights, 64 int64 fixed-point atomics
+//   k_fft_z_fwd   z-lines of the fixed-point grid (cleared as it is read), two real lines packed
+//                 per complex FFT, half spectrum written as [kz][x][y]
+//   k_fft_plane   one CTA per (box, kz) plane in shared memory: forward FFT along y and x,
+//                 influence function multiply with energy and virial, inverse along x and y
+//   k_fft_z_inv   inverse z transform back to the real potential grid [x][y][z]
+//   k_gather      one thread per atom slot, 64-point stencil, fixed-point force atomics
+//   k_pme_energy  fixed-order sum of the per-plane partials into the box accumulators
+// The transforms are unnormalised, as the reference's ZFFT/FFTW calls; r2c/c2r replace the
+// reference's full complex transform of a real grid (identical result: the spectrum is Hermitian
+// and the influence function even in m).
+#include <type_traits>
+
+#include "pmb_internal.h"
+
+namespace pmb {
+
+namespace {
+
+constexpr int MAXP = 8;  // largest supported interpolation order
+
+template <typename T>
+struct C2;
+template <>
+struct C2<float> {
+  using t = float2;
+};
+template <>
+struct C2<double> {
+  using t = double2;
+};
+
+__device__ __forceinline__ float2 cmk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 cmk(double a, double b) { return make_double2(a, b); }
+
+template <typename T2>
+__device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+  return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T2>
+__device__ __forceinline__ T2 cadd(T2 a, T2 b) { return cmk(a.x + b.x, a.y + b.y); }
+template <typename T2>
+__device__ __forceinline__ T2 csub(T2 a, T2 b) { return cmk(a.x - b.x, a.y - b.y); }
+// multiply by (i * sign)
+template <typename T2>
+__device__ __forceinline__ T2 cis(T2 a, int sign) { return sign > 0 ? cmk(-a.y, a.x) : cmk(a.y, -a.x); }
+template <typename T2, typename S>
+__device__ __forceinline__ T2 cscale(T2 a, S s) { return cmk(a.x * s, a.y * s); }
+
+// Small DFTs X_k = sum_n x_n exp(sign 2 pi i n k / R).
+template <int R, typename T2>
+__device__ __forceinline__ void dft_small(T2 *v, int sign) {
+  using S = decltype(v[0].x);
+  if constexpr (R == 2) {
+    T2 a = cadd(v[0], v[1]), b = csub(v[0], v[1]);
+    v[0] = a; v[1] = b;
+  } else if constexpr (R == 3) {
+    const S h = S(0.86602540378443864676);
+    T2 t1 = cadd(v[1], v[2]);
+    T2 t2 = csub(v[0], cscale(t1, S(0.5)));
+    T2 t3 = cis(cscale(csub(v[1], v[2]), h), sign);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  } else if constexpr (R == 4) {
+    T2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]), c = cadd(v[1], v[3]);
+    T2 d = cis(csub(v[1], v[3]), sign);
+    v[0] = cadd(a, c); v[1] = cadd(b, d); v[2] = csub(a, c); v[3] = csub(b, d);
+  } else if constexpr (R == 5) {
+    const S c1 = S(0.30901699437494742410), c2 = S(-0.80901699437494742410),
+            s1 = S(0.95105651629515357212), s2 = S(0.58778525229247312917);
+    T2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    T2 a1 = cadd(v[0], cadd(cscale(t1, c1), cscale(t2, c2)));
+    T2 a2 = cadd(v[0], cadd(cscale(t1, c2), cscale(t2, c1)));
+    T2 b1 = cis(cadd(cscale(t3, s1), cscale(t4, s2)), sign);
+    T2 b2 = cis(csub(cscale(t3, s2), cscale(t4, s1)), sign);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, b1); v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2); v[3] = csub(a2, b2);
+  }
+}
+
+// One Stockham stage, in place: every thread first reads all of its butterfly inputs into
+// registers, the CTA synchronises, then the outputs are written (so no ping-pong buffer).
+template <int R, int THREADS, int MAXE, typename T2>
+__device__ __forceinline__ void fft_stage(T2 *buf, int n, int nlines, int lstride, int estride,
+                                          int Ns, const T2 *tw, int sign) {
+  constexpr int MB = (MAXE + R * THREADS - 1) / (R * THREADS);
+  const int nb = n / R, total = nb * nlines, step = n / (Ns * R);
+  T2 v[MB][R];
+#pragma unroll
+  for (int mb = 0; mb < MB; mb++) {
+    int b = threadIdx.x + mb * THREADS;
+    if (b < total) {
+      // contiguous lines: consecutive threads take consecutive butterflies of one line;
+      // strided lines: consecutive threads take the same butterfly of consecutive lines
+      int line = estride == 1 ? b / nb : b % nlines, j = estride == 1 ? b % nb : b / nlines;
+      T2 *L = buf + line * lstride;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[mb][r] = L[(j + r * nb) * estride];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int mb = 0; mb < MB; mb++) {
+    int b = threadIdx.x + mb * THREADS;
+    if (b < total) {
+      int line = estride == 1 ? b / nb : b % nlines, j = estride == 1 ? b % nb : b / nlines;
+      int k = j % Ns;
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        T2 w = tw[r * k * step];
+        if (sign > 0) w.y = -w.y;
+        v[mb][r] = cmul(v[mb][r], w);
+      }
+      dft_small<R>(v[mb], sign);
+      int out = (j / Ns) * Ns * R + k;
+      T2 *L = buf + line * lstride;
+#pragma unroll
+      for (int r = 0; r < R; r++) L[(out + r * Ns) * estride] = v[mb][r];
+    }
+  }
+  __syncthreads();
+}
+
+// Batched 1-D FFTs of length n over shared memory (element e of line l at
+// buf[l*lstride + e*estride]); radices[0..nrad) multiply to n.
+template <int THREADS, int MAXE, typename T2>
+__device__ void fft_lines(T2 *buf, int n, int nlines, int lstride, int estride, const int *radices,
+                          int nrad, const T2 *tw, int sign) {
+  int Ns = 1;
+  for (int s = 0; s < nrad; s++) {
+    int R = radices[s];
+    if (R == 4) fft_stage<4, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
+    else if (R == 2) fft_stage<2, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
+    else if (R == 3) fft_stage<3, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
+    else fft_stage<5, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
+    Ns *= R;
+  }
+}
+
+// B-spline weights of order P at w (BSpline::set, BSpline.cpp:55-105).
+template <typename T>
+__device__ __forceinline__ void bspline(int P, T w, T *th, T *dth) {
+  if (P == 2) {
+    th[1] = w; th[0] = T(1) - w;
+    if (dth) { dth[1] = T(1); dth[0] = T(-1); }
+    return;
+  }
+  th[P - 1] = T(0);
+  th[1] = w;
+  th[0] = T(1) - w;
+  for (int k = 2; k < P - 1; k++) {
+    T div = T(1) / T(k);
+    th[k] = div * w * th[k - 1];
+    for (int j = 1; j < k; j++)
+      th[k - j] = div * ((w + T(j)) * th[k - j - 1] + (T(k + 1 - j) - w) * th[k - j]);
+    th[0] = div * (T(1) - w) * th[0];
+  }
+  if (dth) {
+    dth[0] = -th[0];
+    for (int j = 1; j <= P - 1; j++) dth[j] = th[j - 1] - th[j];
+  }
+  T div = T(1) / (T(P) - T(1));
+  th[P - 1] = div * w * th[P - 2];
+  for (int j = 1; j < P - 1; j++)
+    th[P - 1 - j] = div * ((w + T(j)) * th[P - j - 2] + (T(P - j) - w) * th[P - 1 - j]);
+  th[0] = div * (T(1) - w) * th[0];
+}
+
+// Grid coordinate of one dimension: base index (already offset by -(P-1)/2 and wrapped to
+// [0, n)) and the fractional weight w.
+template <bool MIXED>
+__device__ __forceinline__ void grid_coord(unsigned fx, double x, double hr, int n, int P, int &base,
+                                           typename std::conditional<MIXED, float, double>::type &w) {
+  int iu;
+  if constexpr (MIXED) {
+    unsigned long long prod = (unsigned long long)fx * (unsigned)n;
+    iu = (int)(prod >> 32);
+    w = (float)(unsigned)(prod & 0xffffffffull) * 2.3283064365386963e-10f;
+  } else {
+    // Grid.h:110-121: u = x n / L wrapped into [0, n) by repeated +-n, then truncated.
+    double u = x * hr;
+    for (int it = 0; it < 4 && u < 0.0; it++) u += n;
+    for (int it = 0; it < 4 && u >= n; it++) u -= n;
+    if (!(u >= 0.0 && u < n)) {
+      u -= n * floor(u / n);
+      if (!(u >= 0.0 && u < n)) u = 0.0;
+    }
+    iu = (int)u;
+    w = u - iu;
+  }
+  base = iu - (P - 1) / 2 + n;  // myNXOffset = -(order-1)/2 + n
+}
+
+template <bool MIXED>
+__global__ void k_spread(NbListDev nb, PmeDev pm) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nb.nslot) return;
+  int4 m = nb.slot_meta[sl];
+  if (m.x < 0) return;
+  const PmeBoxPlan &pl = pm.plan[m.w];
+  const int P = pm.order;
+  T th[3][MAXP];
+  int base[3];
+  T q;
+  if constexpr (MIXED) {
+    uint4 f = nb.slot_fx[sl];
+    unsigned fx[3] = {f.x, f.y, f.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T w;
+      grid_coord<true>(fx[d], 0.0, 0.0, pl.n[d], P, base[d], w);
+      bspline<T>(P, w, th[d], nullptr);
+    }
+    q = __uint_as_float(f.w);
+  } else {
+    double4 pq = nb.slot_pq[sl];
+    double x[3] = {pq.x, pq.y, pq.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T w;
+      grid_coord<false>(0u, x[d], pl.hr[d], pl.n[d], P, base[d], w);
+      bspline<T>(P, w, th[d], nullptr);
+    }
+    q = pq.w;
+  }
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
+  long long *g = pm.qgrid + pl.grid0;
+  for (int i = 0; i < P; i++) {
+    T a = q * th[0][i];
+    int i1 = (i + base[0]) % nx;
+    for (int j = 0; j < P; j++) {
+      T ab = a * th[1][j];
+      int j1 = (j + base[1]) % ny;
+      long long *row = g + ((long long)i1 * ny + j1) * nz;
+      for (int k = 0; k < P; k++) {
+        int k1 = (k + base[2]) % nz;
+        long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
+        if (v) red_add(row + k1, v);
+      }
+    }
+  }
+}
+
+template <bool MIXED>
+__global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nb.nslot) return;
+  int4 m = nb.slot_meta[sl];
+  if (m.x < 0) return;
+  const PmeBoxPlan &pl = pm.plan[m.w];
+  const int P = pm.order;
+  T th[3][MAXP], dth[3][MAXP];
+  int base[3];
+  T q;
+  if constexpr (MIXED) {
+    uint4 f = nb.slot_fx[sl];
+    unsigned fx[3] = {f.x, f.y, f.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T w;
+      grid_coord<true>(fx[d], 0.0, 0.0, pl.n[d], P, base[d], w);
+      bspline<T>(P, w, th[d], dth[d]);
+    }
+    q = __uint_as_float(f.w);
+  } else {
+    double4 pq = nb.slot_pq[sl];
+    double x[3] = {pq.x, pq.y, pq.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T w;
+      grid_coord<false>(0u, x[d], pl.hr[d], pl.n[d], P, base[d], w);
+      bspline<T>(P, w, th[d], dth[d]);
+    }
+    q = pq.w;
+  }
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
+  const T *g = reinterpret_cast<const T *>(pm.rgrid) + pl.grid0;
+  T fx = 0, fy = 0, fz = 0;
+  for (int i = 0; i < P; i++) {
+    int i1 = (i + base[0]) % nx;
+    for (int j = 0; j < P; j++) {
+      int j1 = (j + base[1]) % ny;
+      T xij = dth[0][i] * th[1][j], yij = th[0][i] * dth[1][j], zij = th[0][i] * th[1][j];
+      const T *row = g + ((long long)i1 * ny + j1) * nz;
+      for (int k = 0; k < P; k++) {
+        int k1 = (k + base[2]) % nz;
+        T term = row[k1];
+        fx -= term * xij * th[2][k];
+        fy -= term * yij * th[2][k];
+        fz -= term * zij * dth[2][k];
+      }
+    }
+  }
+  long long *f = s.facc + 3 * (long long)m.x;
+  red_add(f, f2fix((double)(fx * T(pl.hr[0]) * q), FORCE_SCALE));
+  red_add(f + 1, f2fix((double)(fy * T(pl.hr[1]) * q), FORCE_SCALE));
+  red_add(f + 2, f2fix((double)(fz * T(pl.hr[2]) * q), FORCE_SCALE));
+}
+
+constexpr int ZT = 256;          // threads of the z-line kernels
+constexpr int ZMAXE = 16 * 256;  // 16 packed line pairs x nz <= 256
+
+template <typename T>
+__global__ void __launch_bounds__(ZT) k_fft_z_fwd(PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ unsigned char smem_raw[];
+  const int4 wk = pm.zwork[blockIdx.x];
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], x = wk.y, y0 = wk.z, cnt = wk.w;
+  const int npair = (cnt + 1) / 2;
+  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
+  T2 *buf = tw + nz;
+  for (int k = threadIdx.x; k < nz; k += ZT) {
+    if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[2] + k];
+    else tw[k] = pm.twiddle[pl.tw0[2] + k];
+  }
+  long long *g = pm.qgrid + pl.grid0 + ((long long)x * ny + y0) * nz;
+  for (int e = threadIdx.x; e < npair * 2 * nz; e += ZT) {
+    int line = e / nz, z = e % nz;
+    T v = T(0);
+    if (line < cnt) {
+      long long q = g[(long long)line * nz + z];
+      g[(long long)line * nz + z] = 0;  // the charge grid is cleared as it is consumed
+      v = T((double)q * (1.0 / GRID_SCALE));
+    }
+    T *dst = reinterpret_cast<T *>(buf + (line >> 1) * nz + z);
+    dst[line & 1] = v;
+  }
+  __syncthreads();
+  fft_lines<ZT, ZMAXE>(buf, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, -1);
+  const int nh = nz / 2 + 1;
+  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0;
+  for (int e = threadIdx.x; e < npair * nh; e += ZT) {
+    int pi = e % npair, k = e / npair;
+    T2 zk = buf[pi * nz + k], zn = buf[pi * nz + (nz - k) % nz];
+    // X = (Z_k + conj(Z_{n-k})) / 2, Y = -i/2 (Z_k - conj(Z_{n-k}))
+    T2 X = cmk(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
+    T2 Y = cmk(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
+    T2 *row = C + ((long long)k * nx + x) * ny + y0 + 2 * pi;
+    row[0] = X;
+    if (2 * pi + 1 < cnt) row[1] = Y;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(ZT) k_fft_z_inv(PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ unsigned char smem_raw[];
+  const int4 wk = pm.zwork[blockIdx.x];
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], x = wk.y, y0 = wk.z, cnt = wk.w;
+  const int npair = (cnt + 1) / 2, nh = nz / 2 + 1;
+  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
+  T2 *buf = tw + nz;
+  for (int k = threadIdx.x; k < nz; k += ZT) {
+    if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[2] + k];
+    else tw[k] = pm.twiddle[pl.tw0[2] + k];
+  }
+  const T2 *C = reinterpret_cast<const T2 *>(pm.cgrid) + pl.cgrid0;
+  for (int e = threadIdx.x; e < npair * nh; e += ZT) {
+    int pi = e % npair, k = e / npair;
+    const T2 *row = C + ((long long)k * nx + x) * ny + y0 + 2 * pi;
+    T2 X = row[0];
+    T2 Y = (2 * pi + 1 < cnt) ? row[1] : cmk(T(0), T(0));
+    if (k == 0 || (2 * k == nz)) {
+      X.y = T(0);
+      Y.y = T(0);
+    }
+    buf[pi * nz + k] = cmk(X.x - Y.y, X.y + Y.x);
+    if (k > 0 && 2 * k != nz) buf[pi * nz + nz - k] = cmk(X.x + Y.y, Y.x - X.y);
+  }
+  __syncthreads();
+  fft_lines<ZT, ZMAXE>(buf, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, +1);
+  T *R = reinterpret_cast<T *>(pm.rgrid) + pl.grid0 + ((long long)x * ny + y0) * nz;
+  for (int e = threadIdx.x; e < cnt * nz; e += ZT) {
+    int line = e / nz, z = e % nz;
+    T2 v = buf[(line >> 1) * nz + z];
+    R[(long long)line * nz + z] = (line & 1) ? v.y : v.x;
+  }
+}
+
+template <int THREADS, typename T>
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < THREADS / 32 ? red[threadIdx.x] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;
+}
+
+constexpr int PT = 1024;  // plane-kernel threads
+
+template <typename T, int MAXE>
+__global__ void __launch_bounds__(PT) k_fft_plane(PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ unsigned char smem_raw[];
+  const int2 wk = pm.pwork[blockIdx.x];
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], kz = wk.y;
+  double *red = reinterpret_cast<double *>(smem_raw);  // 32 doubles
+  T2 *twx = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
+  T2 *twy = twx + nx;
+  T2 *buf = twy + ny;
+  for (int k = threadIdx.x; k < nx; k += PT) {
+    if constexpr (sizeof(T) == 4) twx[k] = pm.twiddlef[pl.tw0[0] + k];
+    else twx[k] = pm.twiddle[pl.tw0[0] + k];
+  }
+  for (int k = threadIdx.x; k < ny; k += PT) {
+    if constexpr (sizeof(T) == 4) twy[k] = pm.twiddlef[pl.tw0[1] + k];
+    else twy[k] = pm.twiddle[pl.tw0[1] + k];
+  }
+  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + (long long)kz * nx * ny;
+  const int ne = nx * ny;
+  for (int e = threadIdx.x; e < ne; e += PT) buf[e] = C[e];
+  __syncthreads();
+  // forward along y (lines = x rows, contiguous) then along x (lines = y columns, stride ny)
+  fft_lines<PT, MAXE>(buf, ny, nx, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], twy, -1);
+  fft_lines<PT, MAXE>(buf, nx, ny, 1, ny, pm.radix + pl.rad0[0], pl.nrad[0], twx, -1);
+  // influence function, energy and virial (Grid.h:236-341) on the half spectrum kz <= nz/2
+  const double *bxt = pm.infl + pl.inf0[0], *byt = pm.infl + pl.inf0[1], *bzt = pm.infl + pl.inf0[2];
+  const double mk = kz * pl.mr[2];
+  const double wz = (kz > 0 && ((2 * kz != nz) || (nz & 1))) ? 2.0 : 1.0;
+  double en = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+  for (int e = threadIdx.x; e < ne; e += PT) {
+    int i = e / ny, j = e % ny;
+    if (i == 0 && j == 0 && kz == 0) {
+      buf[e] = cmk(T(0), T(0));
+      continue;
+    }
+    int i0 = i <= nx / 2 ? i : i - nx, j0 = j <= ny / 2 ? j : j - ny;
+    double mi = i0 * pl.mr[0], mj = j0 * pl.mr[1];
+    double m2 = mi * mi + mj * mj + mk * mk;
+    double theta = bxt[i] * byt[j] * bzt[kz] * pl.piVr / m2;
+    T2 c = buf[e];
+    double qq = (double)c.x * (double)c.x + (double)c.y * (double)c.y;
+    double ee = wz * qq * theta;
+    en += ee;
+    if (pm.virial) {
+      double v = 2.0 * (1.0 / m2 + pl.fac);
+      vxx += ee * (1.0 - v * mi * mi); vxy -= ee * (v * mi * mj); vxz -= ee * (v * mi * mk);
+      vyy += ee * (1.0 - v * mj * mj); vyz -= ee * (v * mj * mk); vzz += ee * (1.0 - v * mk * mk);
+    }
+    buf[e] = cmk(c.x * T(theta), c.y * T(theta));
+  }
+  double part[7] = {en, vxx, vxy, vxz, vyy, vyz, vzz};
+  const int np = pm.virial ? 7 : 1;
+  for (int c = 0; c < np; c++) {
+    double r = block_sum<PT, T>(part[c], red);
+    if (threadIdx.x == 0) pm.plane_part[(long long)blockIdx.x * 8 + c] = r;
+  }
+  __syncthreads();
+  fft_lines<PT, MAXE>(buf, nx, ny, 1, ny, pm.radix + pl.rad0[0], pl.nrad[0], twx, +1);
+  fft_lines<PT, MAXE>(buf, ny, nx, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], twy, +1);
+  for (int e = threadIdx.x; e < ne; e += PT) C[e] = buf[e];
+}
+
+// Per box: fixed-order sum of its planes' partials, x 0.5 (Grid.h:319-337), into the box
+// accumulators.
+__global__ void k_pme_energy(const SystemDev s, PmeDev pm) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= pm.nbox) return;
+  const PmeBoxPlan &pl = pm.plan[b];
+  int p0 = pl.plane0, np = pl.n[2] / 2 + 1;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int p = p0; p < p0 + np; p++)
+    for (int c = 0; c < 7; c++) acc[c] += pm.plane_part[(long long)p * 8 + c];
+  long long *e = s.eacc + (long long)b * ACC_PER_BOX;
+  red_add(e + E_COUL, f2fix(acc[0] * 0.5, ENERGY_SCALE));
+  if (pm.virial) {
+    // xx xy xz yy yz zz -> row-major 3x3
+    const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+    for (int c = 0; c < 6; c++) {
+      long long v = f2fix(acc[1 + c] * 0.5, ENERGY_SCALE);
+      red_add(e + E_VIR + slot[c][0], v);
+      if (slot[c][1] != slot[c][0]) red_add(e + E_VIR + slot[c][1], v);
+    }
+  }
+}
+
+// Exclusion correction in FP64 with the exact erf (NonbondedPMEwaldSystemForce.h:874-911).
+__global__ void k_correction(const SystemDev s, const int *pairs, const int *kind, int n,
+                             double alpha, double a2pi, double csf, int virial) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int lane = threadIdx.x & 31;
+  bool valid = k < n;
+  long long efix = 0, vfix[6] = {0, 0, 0, 0, 0, 0};
+  int box = -1;
+  if (valid) {
+    int a1 = pairs[2 * k], a2 = pairs[2 * k + 1];
+    box = s.atom_box[a1];
+    const BoxDev &b = s.box[box];
+    double rij[3];
+    double r2 = min_diff(b, s.pos + 3 * a1, s.pos + 3 * a2, rij);
+    double qq = s.charge[a1] * s.charge[a2];
+    if (kind[k] == 1) qq *= 1 - csf;
+    double r = sqrt(r2), rr = 1 / r, e = erf(alpha * r) * rr;
+    efix = f2fix(-qq * e, ENERGY_SCALE);
+    double fs = qq * (a2pi * exp(-alpha * alpha * r2) - e) * rr * rr;
+    double fij[3] = {rij[0] * fs, rij[1] * fs, rij[2] * fs};
+    long long *f1 = s.facc + 3 * (long long)a1, *f2 = s.facc + 3 * (long long)a2;
+    for (int c = 0; c < 3; c++) {
+      long long v = f2fix(fij[c], FORCE_SCALE);
+      red_add(f1 + c, -v);
+      red_add(f2 + c, v);
+    }
+    if (virial) {
+      vfix[0] = f2fix(fij[0] * rij[0], ENERGY_SCALE); vfix[1] = f2fix(fij[0] * rij[1], ENERGY_SCALE);
+      vfix[2] = f2fix(fij[0] * rij[2], ENERGY_SCALE); vfix[3] = f2fix(fij[1] * rij[1], ENERGY_SCALE);
+      vfix[4] = f2fix(fij[1] * rij[2], ENERGY_SCALE); vfix[5] = f2fix(fij[2] * rij[2], ENERGY_SCALE);
+    }
+  }
+  // integer warp sums are exact, so grouping does not change the result
+  int b0 = __shfl_sync(0xffffffffu, box, 0);
+  bool same = __all_sync(0xffffffffu, !valid || box == b0);
+  const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+  if (same) {
+    long long es = warp_sum_ll(efix);
+    long long vs[6];
+    for (int c = 0; c < 6; c++) vs[c] = virial ? warp_sum_ll(vfix[c]) : 0;
+    if (lane == 0 && b0 >= 0) {
+      long long *e = s.eacc + (long long)b0 * ACC_PER_BOX;
+      red_add(e + E_COUL, es);
+      if (virial)
+        for (int c = 0; c < 6; c++) {
+          red_add(e + E_VIR + slot[c][0], vs[c]);
+          if (slot[c][1] != slot[c][0]) red_add(e + E_VIR + slot[c][1], vs[c]);
+        }
+    }
+  } else if (valid) {
+    long long *e = s.eacc + (long long)box * ACC_PER_BOX;
+    red_add(e + E_COUL, efix);
+    if (virial)
+      for (int c = 0; c < 6; c++) {
+        red_add(e + E_VIR + slot[c][0], vfix[c]);
+        if (slot[c][1] != slot[c][0]) red_add(e + E_VIR + slot[c][1], vfix[c]);
+      }
+  }
+}
+
+template <typename T>
+int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st) {
+  using T2 = typename C2<T>::t;
+  const int TB = 256;
+  constexpr bool MIXED = sizeof(T) == 4;
+  k_spread<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
+  size_t zsmem = sizeof(T2) * (256 + ZMAXE);
+  static bool zconf = false;
+  if (!zconf) {
+    cudaFuncSetAttribute(k_fft_z_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
+    cudaFuncSetAttribute(k_fft_z_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
+    zconf = true;
+  }
+  k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  constexpr int PMAXE = MIXED ? 16384 : 13312;
+  size_t psmem = 32 * sizeof(double) + sizeof(T2) * (512 + (size_t)pm.max_plane_elems);
+  static size_t pconf = 0;
+  if (pconf != psmem) {
+    cudaFuncSetAttribute(k_fft_plane<T, PMAXE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+    pconf = psmem;
+  }
+  k_fft_plane<T, PMAXE><<<pm.npwork, PT, psmem, st>>>(pm);
+  k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  k_gather<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
+  k_pme_energy<<<(pm.nbox + 127) / 128, 128, 0, st>>>(s, pm);
+  return 0;
+}
+
+}  // namespace
+
+int pme_max_plane_elems(int precision) { return precision ? 16384 : 13312; }
+
+int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st) {
+  return pm.precision ? recip_t<float>(s, nb, pm, st) : recip_t<double>(s, nb, pm, st);
+}
+
+int pme_correction_launch(const SystemDev &s, const PmeDev &pm, const int *excl_pairs,
+                          const int *excl_kind, int nexcl, double coulomb_scaling, cudaStream_t st) {
+  if (nexcl <= 0) return 0;
+  const int TB = 256;
+  k_correction<<<(nexcl + TB - 1) / TB, TB, 0, st>>>(s, excl_pairs, excl_kind, nexcl, pm.alpha,
+                                                     pm.a2pi, coulomb_scaling, pm.virial);
+  return 0;
+}
+
+}  // namespace pmb

@@ -1,0 +1,364 @@
+"""Host-side mirror of ProtoMol's force plugin surface over the B200 C ABI.
+
+ProtoMol selects a force by name from a ``.conf`` file (``force LennardJones -algorithm
+NonbondedCutoff -switchingFunction C2 -switchon 7 -cutoff 8``), builds it through
+``ForceFactory::make`` (factory/ForceFactory.cpp:21) and calls
+``SystemForce::evaluate(topology, positions, forces, energies)`` once per step
+(force/system/SystemForce.h:32-35), with ``forces`` accumulated into (+=) and energies added to
+the ScalarStructure slots.  This module keeps those names, argument meanings and error
+behaviour:
+
+* ``Topology`` -- the GenericTopology content the path reads (atoms, types, LJ table, exclusions,
+  bonds, angles, periodic box); one or several boxes;
+* ``ScalarStructure`` -- energies and virial per box, in ProtoMol's slot order;
+* ``NonbondedCutoffSystemForce``, ``NonbondedPMEwaldSystemForce``, ``BondedSystemForce`` --
+  ``evaluate(topology, positions, forces, energies)``;
+* ``ForceFactory.make(definition)`` -- parses the reference's force definition strings; unknown or
+  invalid definitions raise ``ValueError`` (ProtoMol reports an error and returns NULL);
+* ``Integrator`` -- the device-resident leapfrog / Langevin loop with ``run(n)`` semantics of
+  LeapfrogIntegrator::run (integrator/leapfrog/LeapfrogIntegrator.cpp:89-104).
+
+Every computation runs in libpmb200 on the GPU; there is no CPU fallback.
+"""
+import ctypes as C
+import shlex
+
+import numpy as np
+
+from . import _lib as L
+
+PRECISIONS = {"fp64": L.FP64, "mixed": L.MIXED}
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class ScalarStructure:
+    """Energies and virial per box (type/ScalarStructure.h:26-54 slot order)."""
+    COULOMB, LENNARDJONES, BOND, ANGLE, VIRIAL = L.E_COULOMB, L.E_LJ, L.E_BOND, L.E_ANGLE, L.E_VIRIAL
+
+    def __init__(self, n_boxes=1, virial=False):
+        self.table = np.zeros((n_boxes, L.E_STRIDE))
+        self.do_virial = virial
+
+    def clear(self):
+        self.table[:] = 0.0
+
+    def __getitem__(self, slot):
+        return self.table[0, slot] if self.table.shape[0] == 1 else self.table[:, slot]
+
+    def virial(self, box=0):
+        return self.table[box, L.E_VIRIAL:L.E_VIRIAL + 9].reshape(3, 3)
+
+    def potential_energy(self):
+        return self.table[:, :4].sum(axis=1)
+
+
+class Topology:
+    """One or more periodic boxes.  ``boxes`` are dicts with the keys produced by
+    protomol3_b200.waterbox.water_box (charge already scaled by 18.2226123264)."""
+
+    def __init__(self, boxes, precision="mixed"):
+        if isinstance(boxes, dict):
+            boxes = [boxes]
+        self.boxes = boxes
+        self.precision = precision
+        self._keep = []
+        self._sys = None
+        self.n_atoms = int(sum(len(b["charge"]) for b in boxes))
+        self.n_boxes = len(boxes)
+
+    def _arr(self, v, dt):
+        a = np.ascontiguousarray(np.asarray(v, dt).reshape(-1))
+        self._keep.append(a)
+        return a
+
+    def system(self):
+        if self._sys is None:
+            descs = (L.BoxDesc * len(self.boxes))()
+            for d, b in zip(descs, self.boxes):
+                n = len(b["charge"])
+                lj = self._arr(b["lj"], np.float64)
+                d.n_atoms = n
+                d.n_types = int(round((lj.size // 4) ** 0.5))
+                d.charge = _p(self._arr(b["charge"], np.float64))
+                d.mass = _p(self._arr(b.get("mass", np.ones(n)), np.float64))
+                d.type = _p(self._arr(b["type"], np.int32))
+                d.molecule = _p(self._arr(b["molecule"], np.int32))
+                d.lj = _p(lj)
+                ep = self._arr(b.get("excl_pairs", np.zeros((0, 2))), np.int32)
+                d.n_excl = ep.size // 2
+                d.excl_pairs = _p(ep)
+                d.excl_kind = _p(self._arr(b.get("excl_kind", np.full(ep.size // 2, 2)), np.int32))
+                bo = self._arr(b.get("bonds", np.zeros((0, 2))), np.int32)
+                d.n_bonds = bo.size // 2
+                d.bonds = _p(bo)
+                d.bond_k = _p(self._arr(b.get("bond_k", np.zeros(0)), np.float64))
+                d.bond_r0 = _p(self._arr(b.get("bond_r0", np.zeros(0)), np.float64))
+                an = self._arr(b.get("angles", np.zeros((0, 3))), np.int32)
+                d.n_angles = an.size // 3
+                d.angles = _p(an)
+                d.angle_k = _p(self._arr(b.get("angle_k", np.zeros(0)), np.float64))
+                d.angle_theta0 = _p(self._arr(b.get("angle_theta0", np.zeros(0)), np.float64))
+                d.ub_k = _p(self._arr(b.get("ub_k", np.zeros(d.n_angles)), np.float64))
+                d.ub_r0 = _p(self._arr(b.get("ub_r0", np.zeros(d.n_angles)), np.float64))
+                for k in range(3):
+                    d.box[k] = float(b["box"][k])
+                d.coulomb_scaling = float(b.get("coulomb_scaling", 1.0))
+            self._sys = L.checked_ptr(L.lib().pmb_system_create(
+                C.cast(descs, C.c_void_p), len(self.boxes), PRECISIONS[self.precision]))
+        return self._sys
+
+    def set_stream(self, stream_handle):
+        L.check(L.lib().pmb_system_set_stream(self.system(), C.c_void_p(stream_handle)))
+
+    def positions(self):
+        return np.concatenate([np.asarray(b["pos"], np.float64).reshape(-1, 3) for b in self.boxes])
+
+    def velocities(self):
+        return np.concatenate([np.asarray(b["vel"], np.float64).reshape(-1, 3) for b in self.boxes])
+
+    def close(self):
+        if self._sys is not None:
+            L.lib().pmb_system_destroy(self._sys)
+            self._sys = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SystemForce:
+    """Base of the B200 forces: ``evaluate(topology, positions, forces, energies)``."""
+    keyword = None
+
+    def __init__(self, desc):
+        self.desc = desc
+        self._handle = None
+        self._topo = None
+
+    def handle(self, topo):
+        if self._handle is None or self._topo is not topo:
+            self._release()
+            self._topo = topo
+            self._handle = L.checked_ptr(L.lib().pmb_force_create(topo.system(), C.byref(self.desc)))
+        return self._handle
+
+    def evaluate(self, topo, positions, forces, energies):
+        """forces (N,3) and energies (ScalarStructure) are accumulated into, never overwritten."""
+        pos = np.ascontiguousarray(positions, np.float64)
+        if pos.shape != (topo.n_atoms, 3) or forces.shape != (topo.n_atoms, 3):
+            raise ValueError("positions/forces must be (%d, 3)" % topo.n_atoms)
+        f = np.ascontiguousarray(forces)
+        L.check(L.lib().pmb_force_evaluate(self.handle(topo), _p(pos), _p(f),
+                                           _p(energies.table), int(energies.do_virial)))
+        if f is not forces:
+            forces[:] = f
+
+    def alpha(self, topo):
+        a = C.c_double(0.0)
+        L.check(L.lib().pmb_force_alpha(self.handle(topo), C.byref(a)))
+        return a.value
+
+    def _release(self):
+        if self._handle is not None:
+            L.lib().pmb_force_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
+
+
+class NonbondedCutoffSystemForce(SystemForce):
+    """``LennardJones [Coulomb] -algorithm NonbondedCutoff`` with per-potential switching
+    (module/NonbondedCutoffForceModule.cpp:40-88)."""
+    keyword = "NonbondedCutoff"
+
+    def __init__(self, lj=None, coulomb=None):
+        d = L.ForceDesc()
+        d.kind = L.FORCE_CUTOFF
+        if lj is not None:
+            d.lj, d.lj_switch, d.lj_switchon, d.lj_cutoff = 1, L.SWITCH[lj[0]], lj[1], lj[2]
+        if coulomb is not None:
+            d.coulomb, d.coulomb_switch = 1, L.SWITCH[coulomb[0]]
+            d.coulomb_switchon, d.coulomb_cutoff = coulomb[1], coulomb[2]
+        super().__init__(d)
+
+
+class NonbondedPMEwaldSystemForce(SystemForce):
+    """``Coulomb -algorithm PMEwald -real -reciprocal -correction -interpolation BSpline
+    -gridsize nx ny nz -cutoff rc -order p -accuracy a -alpha a``
+    (mdl/interface/force/nonbonded/NonbondedPMEwaldSystemForce.h:1003-1061)."""
+    keyword = "PMEwald"
+
+    def __init__(self, gridsize, cutoff, order=4, accuracy=1e-6, alpha=-1.0, real=True,
+                 reciprocal=True, correction=True, switching="Cutoff", box_grids=None):
+        d = L.ForceDesc()
+        d.kind = L.FORCE_PME
+        for k in range(3):
+            d.grid[k] = int(gridsize[k])
+        self._bg = None
+        if box_grids is not None:
+            self._bg = np.ascontiguousarray(np.asarray(box_grids, np.int32).reshape(-1))
+            d.box_grids = _p(self._bg)
+        d.order, d.cutoff, d.accuracy, d.alpha = int(order), cutoff, accuracy, alpha
+        d.real_switch = L.SWITCH[switching]
+        d.real, d.reciprocal, d.correction = int(real), int(reciprocal), int(correction)
+        super().__init__(d)
+
+
+class BondedSystemForce(SystemForce):
+    """``force Bond, Angle`` (module/BondedForcesModule.cpp:30-31)."""
+    keyword = "Bond, Angle"
+
+    def __init__(self):
+        d = L.ForceDesc()
+        d.kind = L.FORCE_BONDED
+        super().__init__(d)
+
+
+def evaluate_all(topo, force_list, positions, forces, energies):
+    """ForceGroup::evaluateSystemForces (force/ForceGroup.cpp:54-70) in one device pass."""
+    hs = (C.c_void_p * len(force_list))(*[f.handle(topo) for f in force_list])
+    pos = np.ascontiguousarray(positions, np.float64)
+    f = np.ascontiguousarray(forces)
+    L.check(L.lib().pmb_evaluate(topo.system(), C.cast(hs, C.c_void_p), len(force_list), _p(pos),
+                                 _p(f), _p(energies.table), int(energies.do_virial)))
+    if f is not forces:
+        forces[:] = f
+
+
+class ForceFactory:
+    """Parses ProtoMol force definitions (the text after ``force`` in a .conf file).
+
+    Recognised: ``Bond``/``Angle`` (bonded), ``LennardJones``/``Coulomb`` with
+    ``-algorithm NonbondedCutoff`` (and the ``NonbondedCutoffB200`` alias), and ``Coulomb
+    -algorithm PMEwald`` (alias ``PMEwaldB200``)."""
+
+    @staticmethod
+    def make(definition):
+        toks = shlex.split(definition.replace(",", " "))
+        if not toks:
+            raise ValueError("empty force definition")
+        names, i = [], 0
+        while i < len(toks) and not toks[i].startswith("-"):
+            names.append(toks[i])
+            i += 1
+        opts, cur = {}, None
+        for t in toks[i:]:
+            if t.startswith("-") and not _is_number(t):
+                cur = t[1:]
+                opts.setdefault(cur, [])
+            elif cur is None:
+                raise ValueError("value without option in %r" % definition)
+            else:
+                opts[cur].append(t)
+        if set(names) <= {"Bond", "Angle"}:
+            return BondedSystemForce()
+        algo = (opts.get("algorithm") or [None])[0]
+        if algo in ("NonbondedCutoff", "NonbondedCutoffB200"):
+            sw = opts.get("switchingFunction", [])
+            son = [float(v) for v in opts.get("switchon", [])]
+            cut = [float(v) for v in opts.get("cutoff", [])]
+            pots = [n for n in names if n in ("LennardJones", "Coulomb")]
+            if not pots or len(pots) != len(names):
+                raise ValueError("unknown potential in %r" % definition)
+            spec = {}
+            si = oi = 0
+            for k, pname in enumerate(pots):
+                s = sw[k] if k < len(sw) else (sw[-1] if sw else "Cutoff")
+                if s not in ("C1", "C2", "Cutoff"):
+                    raise ValueError("unknown switching function %r" % s)
+                on = 0.0
+                if s == "C2":
+                    if oi >= len(son):
+                        raise ValueError("C2 needs -switchon")
+                    on = son[oi]
+                    oi += 1
+                if si >= len(cut):
+                    raise ValueError("missing -cutoff")
+                spec[pname] = (s, on, cut[si])
+                si += 1 if si + 1 < len(cut) else 0
+            return NonbondedCutoffSystemForce(lj=spec.get("LennardJones"), coulomb=spec.get("Coulomb"))
+        if algo in ("PMEwald", "PMEwaldB200"):
+            if names != ["Coulomb"]:
+                raise ValueError("PMEwald is a Coulomb algorithm")
+            g = [int(v) for v in opts.get("gridsize", [])]
+            if len(g) != 3:
+                raise ValueError("-gridsize nx ny nz required")
+            return NonbondedPMEwaldSystemForce(
+                g, float(opts["cutoff"][0]), order=int((opts.get("order") or [4])[0]),
+                accuracy=float((opts.get("accuracy") or [1e-6])[0]),
+                alpha=float((opts.get("alpha") or [-1.0])[0]),
+                real="real" in opts or not ({"real", "reciprocal", "correction"} & set(opts)),
+                reciprocal="reciprocal" in opts or not ({"real", "reciprocal", "correction"} & set(opts)),
+                correction="correction" in opts or not ({"real", "reciprocal", "correction"} & set(opts)),
+                switching=(opts.get("switchingFunction") or ["Cutoff"])[0])
+        raise ValueError("no B200 force registered for %r" % definition)
+
+
+def _is_number(t):
+    try:
+        float(t)
+        return True
+    except ValueError:
+        return False
+
+
+class Integrator:
+    """Device-resident MD: ``run(n)`` has LeapfrogIntegrator::run semantics (or
+    StandardIntegrator::run for Langevin); the step is replayed from a CUDA graph."""
+
+    def __init__(self, topo, force_list, timestep=1.0, kind="leapfrog", temperature=300.0,
+                 gamma=1.0, seed=1234, use_graph=True):
+        self.topo = topo
+        self.forces = list(force_list)
+        d = L.IntegratorDesc()
+        d.kind = L.LEAPFROG if kind == "leapfrog" else L.LANGEVIN
+        d.timestep_fs, d.temperature, d.gamma_ps, d.seed = timestep, temperature, gamma, seed
+        hs = (C.c_void_p * len(self.forces))(*[f.handle(topo) for f in self.forces])
+        self._h = L.checked_ptr(L.lib().pmb_md_create(topo.system(), C.cast(hs, C.c_void_p),
+                                                      len(self.forces), C.byref(d)))
+        L.check(L.lib().pmb_md_use_graph(self._h, int(use_graph)))
+
+    def set_state(self, positions, velocities=None):
+        pos = np.ascontiguousarray(positions, np.float64)
+        vel = None if velocities is None else np.ascontiguousarray(velocities, np.float64)
+        L.check(L.lib().pmb_md_set_state(self._h, _p(pos), _p(vel)))
+
+    def run(self, n):
+        L.check(L.lib().pmb_md_run(self._h, int(n)))
+
+    def state(self):
+        n = self.topo.n_atoms
+        pos, vel = np.zeros((n, 3)), np.zeros((n, 3))
+        L.check(L.lib().pmb_md_get_state(self._h, _p(pos), _p(vel)))
+        return pos, vel
+
+    def forces_now(self):
+        f = np.zeros((self.topo.n_atoms, 3))
+        L.check(L.lib().pmb_md_get_forces(self._h, _p(f)))
+        return f
+
+    def energies(self):
+        e = np.zeros((self.topo.n_boxes, L.E_STRIDE))
+        k = np.zeros(self.topo.n_boxes)
+        L.check(L.lib().pmb_md_energies(self._h, _p(e), _p(k)))
+        return e, k
+
+    def close(self):
+        if self._h is not None:
+            L.lib().pmb_md_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,179 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and the golden vectors.
+
+Tolerances:
+  * FP64 path: relative RMS force error <= 1e-9 and relative energy error <= 1e-9 against the
+    FP64 oracle (only summation order and fixed-point accumulation at 2^-40 differ);
+  * mixed path: relative RMS force error <= 1e-5 (the target stated for the mixed precision path)
+    and relative energy error <= 1e-5;
+  * golden water_CHARMM_PERIODIC_L trajectory: absolute 1e-5, ProtoMol's own test tolerance
+    (test/test.py:14).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from protomol3_b200 import forces as F
+from protomol3_b200 import waterbox as W
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL = {"fp64": 1e-9, "mixed": 1e-5}
+
+
+def rel_rms(f, ref):
+    return float(np.sqrt(((f - ref) ** 2).sum() / (ref ** 2).sum()))
+
+
+def gpu_eval(box, force_list, precision, virial=False, positions=None):
+    topo = F.Topology(box, precision)
+    pos = topo.positions() if positions is None else positions
+    frc = np.zeros((topo.n_atoms, 3))
+    e = F.ScalarStructure(topo.n_boxes, virial=virial)
+    F.evaluate_all(topo, force_list, pos, frc, e)
+    return frc, e, topo
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cutoff_golden_water423(precision):
+    d = dict(np.load(os.path.join(GOLD, "water423_periodic.npz")))
+    d["box"] = np.array([28.0, 28.0, 28.0])
+    cut = F.ForceFactory.make("LennardJones Coulomb -algorithm NonbondedCutoff "
+                              "-switchingFunction C2 -switchingFunction C1 -switchon 0.1 -cutoff 6.5")
+    f, e, _ = gpu_eval(d, [cut, F.BondedSystemForce()], precision, virial=True)
+    s = O.System(d)
+    fo, eo, vo, _ = O.evaluate(s, d["pos"], cutoff=O.cutoff_params(lj=("C2", 0.1, 6.5),
+                                                                   coul=("C1", 0.0, 6.5)),
+                               bonded=True, virial=True)
+    assert rel_rms(f, fo) < TOL[precision]
+    for slot, k in ((F.ScalarStructure.LENNARDJONES, O.E_LJ), (F.ScalarStructure.COULOMB, O.E_COULOMB),
+                    (F.ScalarStructure.BOND, O.E_BOND), (F.ScalarStructure.ANGLE, O.E_ANGLE)):
+        assert abs(e[slot] - eo[k]) <= TOL[precision] * abs(eo[k]) + 1e-9
+    np.testing.assert_allclose(e.virial().ravel(), vo, rtol=10 * TOL[precision], atol=1e-6)
+    # and against the reference's own golden step-0 forces (absolute 1e-5)
+    if precision == "fp64":
+        assert np.abs(f - d["exp_forces0"]).max() < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pentane_lj_energy(precision):
+    d = dict(np.load(os.path.join(GOLD, "pentane320_periodic.npz")))
+    lj = F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 9.0))
+    f, e, _ = gpu_eval(d, [lj], precision)
+    assert abs(e[F.ScalarStructure.LENNARDJONES] - d["exp_lj_energy0"]) < (1e-5 if precision == "fp64" else 1e-3)
+    fo, eo, _, _ = O.evaluate(O.System(d), d["pos"], cutoff=O.cutoff_params(lj=("C2", 8.0, 9.0)))
+    assert rel_rms(f, fo) < TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nw,grid,rc", [(216, 20, 8.0), (60, 12, 9.0), (500, 24, 9.0)])
+def test_pme_vs_oracle(precision, nw, grid, rc):
+    b = W.water_box(nw, seed=5)
+    pme = F.NonbondedPMEwaldSystemForce((grid,) * 3, rc)
+    f, e, topo = gpu_eval(b, [pme], precision, virial=True)
+    fo, eo, vo, info = O.evaluate(O.System(b), b["pos"], pme=O.pme_params((grid,) * 3, rc), virial=True)
+    assert abs(pme.alpha(topo) - info["alpha"]) < 1e-15
+    assert rel_rms(f, fo) < TOL[precision]
+    assert abs(e[F.ScalarStructure.COULOMB] - eo[O.E_COULOMB]) < TOL[precision] * abs(eo[O.E_COULOMB])
+    np.testing.assert_allclose(e.virial().ravel(), vo, rtol=0, atol=TOL[precision] * np.abs(vo).max() * 10)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_lj_plus_pme_fused(precision):
+    """LJ C2 8->10 with PME real space 10 A, the config-2 force set, on a 1,000-water box."""
+    b = W.water_box(1000, seed=9)
+    grid = W.pme_grid_for(b["box"][0])
+    lj = F.ForceFactory.make("LennardJones -algorithm NonbondedCutoff -switchingFunction C2 "
+                             "-switchon 8 -cutoff 10")
+    pme = F.ForceFactory.make("Coulomb -algorithm PMEwald -real -reciprocal -correction "
+                              "-interpolation BSpline -gridsize %d %d %d -cutoff 10 -order 4 "
+                              "-accuracy 1e-6" % (grid, grid, grid))
+    f, e, _ = gpu_eval(b, [lj, pme, F.BondedSystemForce()], precision)
+    s = O.System(b)
+    fo, eo, _, _ = O.evaluate(s, b["pos"], cutoff=O.cutoff_params(lj=("C2", 8.0, 10.0)),
+                              pme=O.pme_params((grid,) * 3, 10.0), bonded=True)
+    assert rel_rms(f, fo) < TOL[precision]
+    for slot, k in ((F.ScalarStructure.LENNARDJONES, O.E_LJ), (F.ScalarStructure.COULOMB, O.E_COULOMB)):
+        assert abs(e[slot] - eo[k]) < TOL[precision] * abs(eo[k])
+
+
+def test_mixed_bit_reproducible():
+    b = W.water_box(2000, seed=21)
+    grid = W.pme_grid_for(b["box"][0])
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0)),
+          F.NonbondedPMEwaldSystemForce((grid,) * 3, 10.0), F.BondedSystemForce()]
+    topo = F.Topology(b, "mixed")
+    outs = []
+    for _ in range(3):
+        frc = np.zeros((topo.n_atoms, 3))
+        e = F.ScalarStructure(1)
+        F.evaluate_all(topo, fl, topo.positions(), frc, e)
+        outs.append((frc.copy(), e.table.copy()))
+    for frc, et in outs[1:]:
+        assert np.array_equal(frc, outs[0][0])
+        assert np.array_equal(et, outs[0][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_boxes_match_single(precision):
+    boxes = [W.water_box(n, seed=30 + n) for n in (100, 257, 640)]
+    grids = [W.pme_grid_for(b["box"][0]) for b in boxes]
+
+    def forces(bg):
+        return [F.NonbondedCutoffSystemForce(lj=("C2", 7.5, 9.0)),
+                F.NonbondedPMEwaldSystemForce((0, 0, 0), 9.0, box_grids=bg), F.BondedSystemForce()]
+    fb, eb, _ = gpu_eval(boxes, forces([[g] * 3 for g in grids]), precision)
+    off = 0
+    for b, g in zip(boxes, grids):
+        fs, es, _ = gpu_eval(b, forces([[g] * 3]), precision)
+        n = len(b["charge"])
+        assert np.array_equal(fb[off:off + n], fs)
+        off += n
+
+
+def test_leapfrog_golden_trajectory_fp64():
+    """200 leapfrog steps of water_CHARMM_PERIODIC_L on the device vs the reference's output."""
+    d = dict(np.load(os.path.join(GOLD, "water423_periodic.npz")))
+    topo = F.Topology(d, "fp64")
+    cut = F.NonbondedCutoffSystemForce(lj=("C2", 0.1, 6.5), coulomb=("C1", 0.0, 6.5))
+    md = F.Integrator(topo, [F.BondedSystemForce(), cut], timestep=0.5)
+    md.set_state(d["pos"], d["vel"])
+    assert np.abs(md.forces_now() - d["exp_forces0"]).max() < 1e-5
+    md.run(200)
+    pos, vel = md.state()
+    assert np.abs(pos - d["exp_pos"]).max() < 1e-5
+    assert np.abs(vel - d["exp_vel"]).max() < 1e-5
+    assert np.abs(md.forces_now() - d["exp_forces_end"]).max() < 1e-5
+    e, _ = md.energies()
+    row = d["exp_energy"][1]
+    np.testing.assert_allclose(e[0, [2, 3, 1, 0]], row[[5, 6, 9, 10]], rtol=1e-7, atol=1e-4)
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_leapfrog_matches_oracle_pme(graph):
+    b = W.water_box(216, seed=2)
+    topo = F.Topology(b, "fp64")
+    fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
+          F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0)]
+    md = F.Integrator(topo, fl, timestep=1.0, use_graph=graph)
+    md.set_state(b["pos"], b["vel"])
+    md.run(20)
+    pos, vel = md.state()
+    po, vo, _, _ = O.leapfrog(O.System(b), b["pos"], b["vel"], 1.0, 20,
+                              cutoff=O.cutoff_params(lj=("C2", 7.0, 8.0)),
+                              pme=O.pme_params((20, 20, 20), 8.0))
+    assert np.abs(pos - po).max() < 1e-8
+    assert np.abs(vel - vo).max() < 1e-8
+
+
+def test_config2_size_mixed_vs_oracle():
+    """The full 98,304-atom box (32,768 waters, 96^3 grid, rc 10, LJ C2 8->10)."""
+    b = W.water_box(32768, seed=1234)
+    lj = F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0))
+    pme = F.NonbondedPMEwaldSystemForce((96, 96, 96), 10.0)
+    f, e, _ = gpu_eval(b, [lj, pme], "mixed")
+    fo, eo, _, _ = O.evaluate(O.System(b), b["pos"], cutoff=O.cutoff_params(lj=("C2", 8.0, 10.0)),
+                              pme=O.pme_params((96, 96, 96), 10.0))
+    assert rel_rms(f, fo) < 1e-5
+    assert abs(e[F.ScalarStructure.COULOMB] - eo[O.E_COULOMB]) < 1e-5 * abs(eo[O.E_COULOMB])
