@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 nonbonded / PME force path: ns/day of one MD step on the 98,304-atom
+flexible TIP3P box (32,768 waters, 99.3 A, 1.0 g/cm^3), Lennard-Jones C2 8 -> 10 A, PME
+96^3 / order 4 / real-space cutoff 10 A / accuracy 1e-6, bonds + angles, leapfrog 1 fs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  ``value`` is the device-resident step (inputs resident in HBM,
+one CUDA graph per step, CUDA events on the launching stream, L2 flushed by a 256 MB write
+before every timed step, max over ranks); ``e2e`` drives the same step through the C ABI with
+pinned host buffers (positions host->device, forces and energies device->host, leapfrog update
+on the host); ``roofline`` covers the dominant kernel (the fused LJ + Ewald real-space pair
+kernel), ``cpu_baseline`` the reference's own force classes compiled from its sources, timed on
+one host core.  For --gpus N > 1 every rank runs an independent replica (no collective).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT_FS = 1.0
+N_WATERS = 32768
+GRID = 96
+RC = 10.0
+SWITCHON = 8.0
+FLOPS_PER_PAIR = 70  # fixed convention for the pair kernel's algorithmic work
+
+
+def ns_per_day(ms_per_step, dt_fs=DT_FS):
+    return 86400.0 * dt_fs * 1e-6 / (ms_per_step * 1e-3)
+
+
+def workload(rank=0):
+    from protomol3_b200 import waterbox as W
+    return W.water_box(N_WATERS, seed=1234 + rank)
+
+
+def config_dict():
+    return {"workload": "TIP3P water box, 32768 waters (98304 atoms), 99.34 A periodic, LJ C2 8->10 A, "
+                        "PME 96^3 order 4 rc 10 A accuracy 1e-6, bonds+angles, leapfrog 1 fs",
+            "atoms": 3 * N_WATERS, "pme_grid": GRID, "cutoff": RC, "timestep_fs": DT_FS,
+            "l2": "flushed (256 MB write) before every timed step"}
+
+
+# ------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in open(self.path):
+            t = [x.strip() for x in ln.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                smax.append(float(t[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if t[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------------------- helpers
+def pair_count(box, rc):
+    """Exact number of unordered atom pairs within rc (minimal image) minus excluded pairs."""
+    from scipy.spatial import cKDTree
+    L = box["box"][0]
+    pos = np.mod(box["pos"], L)
+    pos[pos >= L] -= L
+    tree = cKDTree(pos, boxsize=L)
+    n_ordered = tree.count_neighbors(tree, rc)
+    n = len(pos)
+    return (n_ordered - n) // 2 - len(box["excl_pairs"])
+
+
+def read_profile_traffic():
+    """DRAM bytes per launch of the pair kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "pair_kernel_config2.md")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(ln.split(":")[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(box, steps=1):
+    """The reference's own force classes (compiled from its sources into oracle/_ref) on one
+    core; falls back to the C restatement (oracle/) when the compiled reference is absent."""
+    import ctypes as C
+    from oracle import oracle as O
+    s = O.System(box)
+    pos = np.ascontiguousarray(box["pos"])
+    f = np.zeros((s.n, 3))
+    e = np.zeros(4)
+    if O.ref_available():
+        L = O.ref_lib()
+        r = O._ref_input(s, pos, 5.0)
+        c = O.RefCutoff()
+        cp = O.cutoff_params(lj=("C2", SWITCHON, RC))
+        C.memmove(C.byref(c), C.byref(cp), C.sizeof(c))
+        p = O.RefPME()
+        p.nx = p.ny = p.nz = GRID
+        p.order, p.cutoff, p.accuracy, p.alpha, p.real_switch = 4, RC, 1e-6, -1.0, 0
+        t0 = time.perf_counter()
+        L.ref_time_step(C.byref(r), C.byref(c), C.byref(p), int(steps), O._p(f), O._p(e))
+        dt = (time.perf_counter() - t0) / steps
+        kind = "reference"
+    else:
+        cp = O.cutoff_params(lj=("C2", SWITCHON, RC))
+        pm = O.pme_params((GRID,) * 3, RC)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            O.evaluate(s, pos, cutoff=cp, pme=pm, bonded=True)
+        dt = (time.perf_counter() - t0) / steps
+        kind = "port"
+    return {"value": ns_per_day(dt * 1e3), "unit": "ns/day", "cores": 1, "kind": kind,
+            "sample": "%d full force evaluation(s) (LJ C2 + PME 96^3 + corrections) of the 98,304-atom "
+                      "box, single-threaded; %.2f s per step" % (steps, dt)}
+
+
+# ------------------------------------------------------------------------------- B200 arm
+def run_b200(args, rank, world, local_rank):
+    import torch
+    from protomol3_b200 import forces as F
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    box = workload(rank)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def make(precision):
+        topo = F.Topology(box, precision)
+        topo.set_stream(stream.cuda_stream)
+        fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", SWITCHON, RC)),
+              F.NonbondedPMEwaldSystemForce((GRID,) * 3, RC)]
+        return topo, fl
+
+    def time_md(topo, fl, steps, warmup):
+        md = F.Integrator(topo, fl, timestep=DT_FS)
+        md.set_state(box["pos"], box["vel"])
+        for _ in range(warmup):
+            flush.zero_()
+            md.run(1)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            md.run(1)
+            b.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        kps = md.kernels_per_step()
+        pos, vel = md.state()
+        if not np.isfinite(pos).all():
+            raise RuntimeError("non-finite positions after the timed run")
+        md.close()
+        return ms, kps
+
+    clocks = ClockSampler(local_rank)
+    topo, fl = make(args.precision)
+    clocks.start()
+    ms, kps = time_md(topo, fl, args.steps, args.warmup)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * ns_per_day(ms)
+
+    # stage profile of one force evaluation (cold L2) -> pair-kernel roofline
+    stages = F.profile(topo, [fl[1], fl[2], fl[0]], nrep=5, flush_l2=True)
+    t_pair = stages.get("pair")
+    peak = F.fp32_peak()
+    npairs = pair_count(box, RC) if rank == 0 else None
+
+    # end-to-end through the C ABI with pinned host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        n = topo.n_atoms
+        hpos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        hfrc = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        hpos[:] = box["pos"]
+        vel = box["vel"].copy()
+        inv_m = (1.0 / box["mass"])[:, None]
+        h = DT_FS * 0.02045482828087295
+        en = F.ScalarStructure(1)
+        nsteps = max(3, args.steps // 2)
+        for it in range(nsteps + 2):
+            if it == 2:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+            hfrc[:] = 0.0
+            en.clear()
+            F.evaluate_all(topo, fl, hpos, hfrc, en)
+            vel += hfrc * (h * inv_m)
+            hpos += vel * h
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / nsteps
+        e2e = {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "ms_per_step": e2e_ms,
+               "h2d_bytes_per_step": int(hpos.nbytes), "d2h_bytes_per_step": int(hfrc.nbytes + 16 * 8),
+               "path": "pmb_evaluate (C ABI) with pinned host positions/forces + host leapfrog"}
+
+    # plain FP64 path on the same workload (the drop-in); the headline is the mixed path
+    fp64 = None
+    if args.precision == "mixed" and not args.no_fp64:
+        topo64, fl64 = make("fp64")
+        ms64, _ = time_md(topo64, fl64, max(3, args.steps // 2), 3)
+        if dist:
+            t = torch.tensor([ms64], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms64 = float(t.item())
+        fp64 = {"value": world * ns_per_day(ms64), "ms_per_step": ms64,
+                "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64)}
+        topo64.close()
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        base = cpu_baseline(box, steps=args.cpu_steps)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    achieved = FLOPS_PER_PAIR * npairs / (t_pair * 1e-3) / 1e12 if t_pair else None
+    traffic = read_profile_traffic()
+    line = {
+        "metric": "ns/day at 98k atoms (TIP3P, LJ C2 + PME 96^3, 1 fs leapfrog)",
+        "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": dict(config_dict(), precision=args.precision,
+                       parallelism="replicas" if world > 1 else "single"),
+        "clocks": clk, "gpu_launches": (kps + 1) * args.steps, "e2e": e2e,
+        "roofline": {"bound": "fp32", "kernel": "k_pair (LJ C2 + Ewald real space)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if achieved and peak else None, "traffic": traffic,
+                     "work": "%d FLOP x %d in-cutoff pairs per launch" % (FLOPS_PER_PAIR, npairs),
+                     "kernel_ms": t_pair, "peak_source": "measured FP32 FMA issue rate (pmb_fp32_peak)"},
+        "stages_ms": stages, "plain_fp64": fp64, "cpu_baseline": base,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_profile(args):
+    """A bounded case for ncu: builds the box and evaluates the force set ``--steps`` times
+    through the C ABI (no MD loop, no CPU legs)."""
+    import torch
+    from protomol3_b200 import forces as F
+    torch.cuda.set_device(0)
+    box = workload(0)
+    topo = F.Topology(box, args.precision)
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", SWITCHON, RC)),
+          F.NonbondedPMEwaldSystemForce((GRID,) * 3, RC), F.BondedSystemForce()]
+    frc = np.zeros((topo.n_atoms, 3))
+    for _ in range(args.steps):
+        frc[:] = 0.0
+        F.evaluate_all(topo, fl, box["pos"], frc, F.ScalarStructure(1))
+    print(json.dumps({"mode": "profile", "precision": args.precision, "evaluations": args.steps,
+                      "force_rms": float(np.sqrt((frc ** 2).mean()))}))
+
+
+# ------------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    box = workload(0)
+    steps = max(1, min(args.steps, args.ref_steps))
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(box, steps=1)
+    base = cpu_baseline(box, steps=steps)
+    line = {"metric": "ns/day at 98k atoms (TIP3P, LJ C2 + PME 96^3, 1 fs leapfrog)", "impl": "reference",
+            "value": base["value"], "unit": "ns/day", "n_gpus": world, "steps": steps,
+            "warmup": min(args.warmup, 1), "ms_per_step": 86400.0 * DT_FS * 1e-6 / base["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": dict(config_dict(), precision="fp64", parallelism="cpu"),
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-steps", type=int, default=5)
+    ap.add_argument("--mode", choices=["bench", "profile"], default="bench",
+                    help="profile: only --steps force evaluations (bounded case for ncu)")
+    args = ap.parse_args()
+    if args.mode == "profile":
+        run_profile(args)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "WORLD_SIZE" not in os.environ:
+        world = 1
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_b200(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

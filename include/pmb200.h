@@ -147,6 +147,18 @@ int pmb_md_run(pmb_md *md, int n_steps);
 /* Energies of the last force evaluation [n_boxes * PMB_E_STRIDE] and kinetic energy per box. */
 int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
 int pmb_md_use_graph(pmb_md *md, int enable);
+/* Kernel launches in one captured MD step (0 before the first graph run). */
+int pmb_md_kernels_per_step(pmb_md *md, int *n);
+
+/* Diagnostics -------------------------------------------------------------------------------- */
+/* Runs the force set nrep times with CUDA events between pipeline stages (TimerStatistic /
+ * DEBUG_PME_TIMING of the reference, as device times); flush_l2 writes a 256 MB buffer before
+ * each repetition.  stage_ms[i] is the mean time of stage i, names receives the comma-separated
+ * stage names. */
+int pmb_profile(pmb_system *sys, pmb_force *const *forces, int n_forces, int nrep, int flush_l2,
+                double *stage_ms, int max_stages, int *n_stages, char *names, int names_len);
+/* Measured FP32 FMA issue rate of the device (TFLOP/s), the roofline of the pair kernel. */
+int pmb_fp32_peak(double *tflops);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -198,6 +198,9 @@ struct pmb_system {
   NbListDev nb{};
   Allocs nba;
   int n_bonded = 0;
+  // stage profiler: events recorded between launches when non-null
+  std::vector<std::pair<std::string, cudaEvent_t>> *prof = nullptr;
+  void *flush_buf = nullptr;  // > L2 scratch for cold-cache profiling
 
   SystemDev dev() const {
     SystemDev s;
@@ -217,6 +220,7 @@ struct pmb_system {
     return s;
   }
   ~pmb_system() {
+    if (flush_buf) cudaFree(flush_buf);
     if (h_fout) cudaFreeHost(h_fout);
     if (h_eout) cudaFreeHost(h_eout);
     if (h_status) cudaFreeHost(h_status);
@@ -385,6 +389,15 @@ std::vector<PairJob> pair_jobs(pmb_system *s, pmb_force *const *fs, int n, int v
   return jobs;
 }
 
+void mark(void *ctx, const char *name) {
+  pmb_system *s = static_cast<pmb_system *>(ctx);
+  if (!s->prof) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, s->stream);
+  s->prof->push_back({name, e});
+}
+
 // Enqueues every force of the set on the system stream; accumulators must be zero.
 int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   SystemDev sd = s->dev();
@@ -396,6 +409,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     int rc = ensure_nblist(s, rl + 1e-3);
     if (rc) return rc;
     nblist_build(sd, s->nb, rl + 1e-3, st);
+    mark(s, "nblist");
     for (auto &j : jobs) {
       PairLaunch pl;
       pl.precision = s->precision;
@@ -403,6 +417,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
       pl.lj = s->d_lj;
       pl.lattice = j.lattice;
       if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+      mark(s, "pair");
     }
   }
   for (int i = 0; i < n; i++) {
@@ -414,16 +429,22 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
           int rc = ensure_nblist(s, std::max(rl, 1.0) + 1e-3);
           if (rc) return rc;
         }
-        if (jobs.empty()) nblist_build(sd, s->nb, std::max(s->nb_cutoff, 1.0), st);
-        pme_recip_launch(sd, s->nb, f->pm, st);
+        if (jobs.empty()) {
+          nblist_build(sd, s->nb, std::max(s->nb_cutoff, 1.0), st);
+          mark(s, "nblist");
+        }
+        pme_recip_launch(sd, s->nb, f->pm, st, mark, s);
       }
-      if (f->d.correction)
+      if (f->d.correction) {
         pme_correction_launch(sd, f->pm, s->d_excl_pairs, s->d_excl_kind, (int)s->h_excl_kind.size(),
                               s->coulomb_scaling, st);
+        mark(s, "pme_correction");
+      }
     } else if (f->kind == PMB_FORCE_BONDED) {
       BondedDev b = s->bonded;
       b.virial = virial;
       bonded_launch(sd, b, st);
+      mark(s, "bonded");
     }
   }
   CK(cudaGetLastError());
@@ -928,6 +949,64 @@ int pmb_force_evaluate(pmb_force *f, const double *pos, double *forces, double *
   return pmb_evaluate(f->sys, &f, 1, pos, forces, energies, virial);
 }
 
+int pmb_profile(pmb_system *s, pmb_force *const *fs, int n, int nrep, int flush_l2, double *stage_ms,
+                int max_stages, int *n_stages, char *names, int names_len) {
+  if (!s || (n > 0 && !fs) || nrep < 1 || !stage_ms || !n_stages)
+    return fail(PMB_ERR_ARG, "null argument");
+  cudaStream_t st = s->stream;
+  const size_t flush_bytes = 256ull << 20;  // twice the 126 MB L2
+  if (flush_l2 && !s->flush_buf) CK(cudaMalloc(&s->flush_buf, flush_bytes));
+  SystemDev sd = s->dev();
+  zero_accumulators(sd, st);
+  int rc = enqueue_forces(s, fs, n, 0);  // warm-up (also sizes the neighbour list)
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(st));
+  std::vector<std::string> order;
+  std::vector<double> acc;
+  for (int r = 0; r < nrep; r++) {
+    if (flush_l2) CK(cudaMemsetAsync(s->flush_buf, r & 0xff, flush_bytes, st));
+    zero_accumulators(sd, st);
+    std::vector<std::pair<std::string, cudaEvent_t>> ev;
+    s->prof = &ev;
+    mark(s, "start");
+    rc = enqueue_forces(s, fs, n, 0);
+    s->prof = nullptr;
+    cudaStreamSynchronize(st);
+    for (size_t i = 1; i < ev.size() && rc == 0; i++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[i - 1].second, ev[i].second);
+      auto it = std::find(order.begin(), order.end(), ev[i].first);
+      if (it == order.end()) {
+        order.push_back(ev[i].first);
+        acc.push_back(ms);
+      } else {
+        acc[it - order.begin()] += ms;
+      }
+    }
+    for (auto &e : ev) cudaEventDestroy(e.second);
+    if (rc) return rc;
+  }
+  *n_stages = (int)std::min<size_t>(order.size(), (size_t)max_stages);
+  std::string joined;
+  for (int i = 0; i < *n_stages; i++) {
+    stage_ms[i] = acc[i] / nrep;
+    joined += (i ? "," : "") + order[i];
+  }
+  if (names && names_len > 0) {
+    std::strncpy(names, joined.c_str(), (size_t)names_len - 1);
+    names[names_len - 1] = 0;
+  }
+  CK(cudaGetLastError());
+  return check_status(s);
+}
+
+int pmb_fp32_peak(double *tflops) {
+  if (!tflops) return fail(PMB_ERR_ARG, "null argument");
+  if (pmb_device_count() <= 0) return fail(PMB_ERR_CUDA, "no CUDA device");
+  if (fp32_peak_probe(tflops)) return fail(PMB_ERR_CUDA, "FMA probe failed");
+  return PMB_OK;
+}
+
 }  // extern "C"
 
 // ======================================================================================== MD
@@ -941,6 +1020,7 @@ struct pmb_md {
   long long *d_step = nullptr;
   bool have_state = false, use_graph = true;
   cudaGraphExec_t g_first = nullptr, g_next = nullptr;
+  int kernels_per_step = 0;
   std::vector<double> h_e, h_k;
   ~pmb_md() {
     if (g_first) cudaGraphExecDestroy(g_first);
@@ -968,6 +1048,17 @@ int md_capture(pmb_md *m, double kick, cudaGraphExec_t *out) {
     return rc;
   }
   if (e != cudaSuccess) return fail(PMB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  size_t nn = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+    std::vector<cudaGraphNode_t> nodes(nn);
+    int kern = 0;
+    if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+      for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kern++;
+      }
+    m->kernels_per_step = kern;
+  }
   e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(PMB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
@@ -1027,6 +1118,12 @@ int pmb_md_destroy(pmb_md *m) {
 int pmb_md_use_graph(pmb_md *m, int enable) {
   if (!m) return fail(PMB_ERR_ARG, "null md");
   m->use_graph = enable != 0;
+  return PMB_OK;
+}
+
+int pmb_md_kernels_per_step(pmb_md *m, int *n) {
+  if (!m || !n) return fail(PMB_ERR_ARG, "null argument");
+  *n = m->kernels_per_step;
   return PMB_OK;
 }
 

@@ -89,6 +89,45 @@ __device__ inline long long warp_sum_ll(long long v) {
   return v;
 }
 
+// Adds one energy (slot) and optionally a symmetric virial (xx xy xz yy yz zz) per lane to the
+// per-box accumulators.  When every valid lane of the warp belongs to the same box the warp sums
+// first (one atomic per warp instead of 32 on the same address); the lane-to-term mapping of the
+// callers is fixed, so the grouping and therefore the rounding are reproducible.
+__device__ inline void box_accumulate(long long *eacc, int box, bool valid, int slot, double e,
+                                      const double *vir6) {
+  const int lane = threadIdx.x & 31;
+  const unsigned act = __ballot_sync(0xffffffffu, valid);
+  if (!act) return;
+  const int b0 = __shfl_sync(0xffffffffu, box, __ffs(act) - 1);
+  const bool same = __all_sync(0xffffffffu, !valid || box == b0);
+  const int map[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+  if (same) {
+    double es = warp_sum(valid ? e : 0.0);
+    double vs[6];
+    if (vir6)
+      for (int c = 0; c < 6; c++) vs[c] = warp_sum(valid ? vir6[c] : 0.0);
+    if (lane == 0) {
+      long long *acc = eacc + (long long)b0 * ACC_PER_BOX;
+      red_add(acc + slot, f2fix(es, ENERGY_SCALE));
+      if (vir6)
+        for (int c = 0; c < 6; c++) {
+          long long v = f2fix(vs[c], ENERGY_SCALE);
+          red_add(acc + E_VIR + map[c][0], v);
+          if (map[c][1] != map[c][0]) red_add(acc + E_VIR + map[c][1], v);
+        }
+    }
+  } else if (valid) {
+    long long *acc = eacc + (long long)box * ACC_PER_BOX;
+    red_add(acc + slot, f2fix(e, ENERGY_SCALE));
+    if (vir6)
+      for (int c = 0; c < 6; c++) {
+        long long v = f2fix(vir6[c], ENERGY_SCALE);
+        red_add(acc + E_VIR + map[c][0], v);
+        if (map[c][1] != map[c][0]) red_add(acc + E_VIR + map[c][1], v);
+      }
+  }
+}
+
 // Switching function value and derivative/r (same branch structure as the reference).
 template <typename T>
 __device__ __forceinline__ void switch_eval(const SwitchDev &w, T r2, T &val, T &der) {

@@ -70,6 +70,7 @@ struct SystemDev {
 };
 
 int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st);
+int fp32_peak_probe(double *tflops);
 
 // ------------------------------------------------------------------ pair kernel (pair.cu)
 struct PairLaunch {
@@ -116,7 +117,10 @@ struct PmeDev {
   double alpha, a2pi;
   int virial;
 };
-int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st);
+// Optional stage marker (profiling): called on the host between kernel launches.
+typedef void (*StageMark)(void *ctx, const char *stage);
+int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,
+                     StageMark mark = nullptr, void *mark_ctx = nullptr);
 int pme_max_plane_elems(int precision);
 int pme_correction_launch(const SystemDev &s, const PmeDev &pm, const int *excl_pairs,
                           const int *excl_kind, int nexcl, double coulomb_scaling, cudaStream_t st);

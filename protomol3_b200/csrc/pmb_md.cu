@@ -14,77 +14,73 @@ namespace pmb {
 
 namespace {
 
-__device__ __forceinline__ void add_vir(long long *acc, const double f[3], const double d[3]) {
-  red_add(acc + E_VIR + 0, f2fix(f[0] * d[0], ENERGY_SCALE));
-  long long xy = f2fix(f[0] * d[1], ENERGY_SCALE), xz = f2fix(f[0] * d[2], ENERGY_SCALE),
-            yz = f2fix(f[1] * d[2], ENERGY_SCALE);
-  red_add(acc + E_VIR + 1, xy); red_add(acc + E_VIR + 3, xy);
-  red_add(acc + E_VIR + 2, xz); red_add(acc + E_VIR + 6, xz);
-  red_add(acc + E_VIR + 4, f2fix(f[1] * d[1], ENERGY_SCALE));
-  red_add(acc + E_VIR + 5, yz); red_add(acc + E_VIR + 7, yz);
-  red_add(acc + E_VIR + 8, f2fix(f[2] * d[2], ENERGY_SCALE));
-}
-
 __global__ void k_bonds(const SystemDev s, BondedDev b) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= b.nbonds) return;
-  int a1 = b.bonds[2 * k], a2 = b.bonds[2 * k + 1];
-  int box = s.atom_box[a1];
-  double r12[3];
-  min_diff(s.box[box], s.pos + 3 * a2, s.pos + 3 * a1, r12);  // atom1 - atom2
-  double r = sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2]);
-  double dpotdr = 2.0 * b.bond_k[k] * (r - b.bond_r0[k]);
-  double f1[3] = {r12[0] * (-dpotdr / r), r12[1] * (-dpotdr / r), r12[2] * (-dpotdr / r)};
-  for (int c = 0; c < 3; c++) {
-    long long v = f2fix(f1[c], FORCE_SCALE);
-    red_add(s.facc + 3 * (long long)a1 + c, v);
-    red_add(s.facc + 3 * (long long)a2 + c, -v);
+  bool valid = k < b.nbonds;
+  int box = -1;
+  double en = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
+  if (valid) {
+    int a1 = b.bonds[2 * k], a2 = b.bonds[2 * k + 1];
+    box = s.atom_box[a1];
+    double r12[3];
+    min_diff(s.box[box], s.pos + 3 * a2, s.pos + 3 * a1, r12);  // atom1 - atom2
+    double r = sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2]);
+    double dpotdr = 2.0 * b.bond_k[k] * (r - b.bond_r0[k]);
+    double f1[3] = {r12[0] * (-dpotdr / r), r12[1] * (-dpotdr / r), r12[2] * (-dpotdr / r)};
+    for (int c = 0; c < 3; c++) {
+      long long v = f2fix(f1[c], FORCE_SCALE);
+      red_add(s.facc + 3 * (long long)a1 + c, v);
+      red_add(s.facc + 3 * (long long)a2 + c, -v);
+    }
+    en = b.bond_k[k] * (r - b.bond_r0[k]) * (r - b.bond_r0[k]);
+    vir[0] = f1[0] * r12[0]; vir[1] = f1[0] * r12[1]; vir[2] = f1[0] * r12[2];
+    vir[3] = f1[1] * r12[1]; vir[4] = f1[1] * r12[2]; vir[5] = f1[2] * r12[2];
   }
-  long long *acc = s.eacc + (long long)box * ACC_PER_BOX;
-  red_add(acc + E_BOND, f2fix(b.bond_k[k] * (r - b.bond_r0[k]) * (r - b.bond_r0[k]), ENERGY_SCALE));
-  if (b.virial) add_vir(acc, f1, r12);
+  box_accumulate(s.eacc, box, valid, E_BOND, en, b.virial ? vir : nullptr);
 }
 
 __global__ void k_angles(const SystemDev s, BondedDev b) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= b.nangles) return;
-  int a1 = b.angles[3 * k], a2 = b.angles[3 * k + 1], a3 = b.angles[3 * k + 2];
-  int box = s.atom_box[a1];
-  const BoxDev &bx = s.box[box];
-  double r12[3], r32[3], r13[3];
-  min_diff(bx, s.pos + 3 * a2, s.pos + 3 * a1, r12);
-  min_diff(bx, s.pos + 3 * a2, s.pos + 3 * a3, r32);
-  min_diff(bx, s.pos + 3 * a3, s.pos + 3 * a1, r13);
-  double d12 = sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2]);
-  double d32 = sqrt(r32[0] * r32[0] + r32[1] * r32[1] + r32[2] * r32[2]);
-  double d13 = sqrt(r13[0] * r13[0] + r13[1] * r13[1] + r13[2] * r13[2]);
-  double cr[3] = {r12[1] * r32[2] - r12[2] * r32[1], r12[2] * r32[0] - r12[0] * r32[2],
-                  r12[0] * r32[1] - r12[1] * r32[0]};
-  double theta = atan2(sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]),
-                       r12[0] * r32[0] + r12[1] * r32[1] + r12[2] * r32[2]);
-  double sn = sin(theta), cs = cos(theta);
-  double kth = b.angle_k[k], th0 = b.angle_theta0[k], ubk = b.ub_k[k], ubr = b.ub_r0[k];
-  double dpot = 2.0 * kth * (theta - th0);
-  double f1[3], f3[3];
-  for (int c = 0; c < 3; c++) {
-    double dr12 = r12[c] / d12, dr32 = r32[c] / d32, dr13 = r13[c] / d13;
-    double dt1 = (dr12 * cs - dr32) / (sn * d12);
-    double dt3 = (dr32 * cs - dr12) / (sn * d32);
-    double ub1 = dr13 * (2.0 * ubk * (d13 - ubr));
-    f1[c] = -dt1 * dpot - ub1;
-    f3[c] = -dt3 * dpot + ub1;
-    long long v1 = f2fix(f1[c], FORCE_SCALE), v3 = f2fix(f3[c], FORCE_SCALE);
-    red_add(s.facc + 3 * (long long)a1 + c, v1);
-    red_add(s.facc + 3 * (long long)a3 + c, v3);
-    red_add(s.facc + 3 * (long long)a2 + c, f2fix(-f1[c] - f3[c], FORCE_SCALE));
+  bool valid = k < b.nangles;
+  int box = -1;
+  double en = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
+  if (valid) {
+    int a1 = b.angles[3 * k], a2 = b.angles[3 * k + 1], a3 = b.angles[3 * k + 2];
+    box = s.atom_box[a1];
+    const BoxDev &bx = s.box[box];
+    double r12[3], r32[3], r13[3];
+    min_diff(bx, s.pos + 3 * a2, s.pos + 3 * a1, r12);
+    min_diff(bx, s.pos + 3 * a2, s.pos + 3 * a3, r32);
+    min_diff(bx, s.pos + 3 * a3, s.pos + 3 * a1, r13);
+    double d12 = sqrt(r12[0] * r12[0] + r12[1] * r12[1] + r12[2] * r12[2]);
+    double d32 = sqrt(r32[0] * r32[0] + r32[1] * r32[1] + r32[2] * r32[2]);
+    double d13 = sqrt(r13[0] * r13[0] + r13[1] * r13[1] + r13[2] * r13[2]);
+    double cr[3] = {r12[1] * r32[2] - r12[2] * r32[1], r12[2] * r32[0] - r12[0] * r32[2],
+                    r12[0] * r32[1] - r12[1] * r32[0]};
+    double theta = atan2(sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]),
+                         r12[0] * r32[0] + r12[1] * r32[1] + r12[2] * r32[2]);
+    double sn = sin(theta), cs = cos(theta);
+    double kth = b.angle_k[k], th0 = b.angle_theta0[k], ubk = b.ub_k[k], ubr = b.ub_r0[k];
+    double dpot = 2.0 * kth * (theta - th0);
+    double f1[3], f3[3];
+    for (int c = 0; c < 3; c++) {
+      double dr12 = r12[c] / d12, dr32 = r32[c] / d32, dr13 = r13[c] / d13;
+      double dt1 = (dr12 * cs - dr32) / (sn * d12);
+      double dt3 = (dr32 * cs - dr12) / (sn * d32);
+      double ub1 = dr13 * (2.0 * ubk * (d13 - ubr));
+      f1[c] = -dt1 * dpot - ub1;
+      f3[c] = -dt3 * dpot + ub1;
+      red_add(s.facc + 3 * (long long)a1 + c, f2fix(f1[c], FORCE_SCALE));
+      red_add(s.facc + 3 * (long long)a3 + c, f2fix(f3[c], FORCE_SCALE));
+      red_add(s.facc + 3 * (long long)a2 + c, f2fix(-f1[c] - f3[c], FORCE_SCALE));
+    }
+    en = kth * (theta - th0) * (theta - th0) + ubk * (d13 - ubr) * (d13 - ubr);
+    // AngleSystemForce.h:151-170: virial = f1 (x) r12 + f3 (x) r32
+    vir[0] = f1[0] * r12[0] + f3[0] * r32[0]; vir[1] = f1[0] * r12[1] + f3[0] * r32[1];
+    vir[2] = f1[0] * r12[2] + f3[0] * r32[2]; vir[3] = f1[1] * r12[1] + f3[1] * r32[1];
+    vir[4] = f1[1] * r12[2] + f3[1] * r32[2]; vir[5] = f1[2] * r12[2] + f3[2] * r32[2];
   }
-  long long *acc = s.eacc + (long long)box * ACC_PER_BOX;
-  red_add(acc + E_ANGLE, f2fix(kth * (theta - th0) * (theta - th0) + ubk * (d13 - ubr) * (d13 - ubr),
-                               ENERGY_SCALE));
-  if (b.virial) {
-    add_vir(acc, f1, r12);
-    add_vir(acc, f3, r32);
-  }
+  box_accumulate(s.eacc, box, valid, E_ANGLE, en, b.virial ? vir : nullptr);
 }
 
 __global__ void k_forces_to_double(const SystemDev s, double *out) {
@@ -224,7 +220,50 @@ __global__ void k_kinetic(const SystemDev s, IntegratorDev in, double *out) {
   }
 }
 
+// FP32 FMA issue-rate probe: 8 independent dependency chains per thread keep the FMA pipes
+// full; the result is written out so nothing is eliminated.
+__global__ void k_fma_probe(float *out, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) x[c] = threadIdx.x * 1e-3f + c;
+  for (int i = 0; i < iters; i++)
+#pragma unroll
+    for (int c = 0; c < 8; c++) x[c] = fmaf(x[c], a, b);
+  float r = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; c++) r += x[c];
+  if (r == 1234.5f) out[0] = r;
+}
+
 }  // namespace
+
+int fp32_peak_probe(double *tflops) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  float *out = nullptr;
+  if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int threads = 256, blocks = nsm * 8, iters = 1 << 14;
+  double best = 0.0;
+  for (int r = 0; r < 4; r++) {
+    cudaEventRecord(e0);
+    k_fma_probe<<<blocks, threads>>>(out, iters, 0.999f, 1e-4f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    double fl = 2.0 * 8.0 * iters * (double)threads * blocks;
+    if (r > 0 && ms > 0) best = fl / (ms * 1e-3) / 1e12 > best ? fl / (ms * 1e-3) / 1e12 : best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  *tflops = best;
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 int bonded_launch(const SystemDev &s, const BondedDev &b, cudaStream_t st) {
   const int T = 256;

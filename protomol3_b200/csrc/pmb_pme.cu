@@ -497,9 +497,8 @@ __global__ void k_pme_energy(const SystemDev s, PmeDev pm) {
 __global__ void k_correction(const SystemDev s, const int *pairs, const int *kind, int n,
                              double alpha, double a2pi, double csf, int virial) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  int lane = threadIdx.x & 31;
   bool valid = k < n;
-  long long efix = 0, vfix[6] = {0, 0, 0, 0, 0, 0};
+  double en = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
   int box = -1;
   if (valid) {
     int a1 = pairs[2 * k], a2 = pairs[2 * k + 1];
@@ -510,7 +509,7 @@ __global__ void k_correction(const SystemDev s, const int *pairs, const int *kin
     double qq = s.charge[a1] * s.charge[a2];
     if (kind[k] == 1) qq *= 1 - csf;
     double r = sqrt(r2), rr = 1 / r, e = erf(alpha * r) * rr;
-    efix = f2fix(-qq * e, ENERGY_SCALE);
+    en = -qq * e;
     double fs = qq * (a2pi * exp(-alpha * alpha * r2) - e) * rr * rr;
     double fij[3] = {rij[0] * fs, rij[1] * fs, rij[2] * fs};
     long long *f1 = s.facc + 3 * (long long)a1, *f2 = s.facc + 3 * (long long)a2;
@@ -519,46 +518,20 @@ __global__ void k_correction(const SystemDev s, const int *pairs, const int *kin
       red_add(f1 + c, -v);
       red_add(f2 + c, v);
     }
-    if (virial) {
-      vfix[0] = f2fix(fij[0] * rij[0], ENERGY_SCALE); vfix[1] = f2fix(fij[0] * rij[1], ENERGY_SCALE);
-      vfix[2] = f2fix(fij[0] * rij[2], ENERGY_SCALE); vfix[3] = f2fix(fij[1] * rij[1], ENERGY_SCALE);
-      vfix[4] = f2fix(fij[1] * rij[2], ENERGY_SCALE); vfix[5] = f2fix(fij[2] * rij[2], ENERGY_SCALE);
-    }
+    vir[0] = fij[0] * rij[0]; vir[1] = fij[0] * rij[1]; vir[2] = fij[0] * rij[2];
+    vir[3] = fij[1] * rij[1]; vir[4] = fij[1] * rij[2]; vir[5] = fij[2] * rij[2];
   }
-  // integer warp sums are exact, so grouping does not change the result
-  int b0 = __shfl_sync(0xffffffffu, box, 0);
-  bool same = __all_sync(0xffffffffu, !valid || box == b0);
-  const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
-  if (same) {
-    long long es = warp_sum_ll(efix);
-    long long vs[6];
-    for (int c = 0; c < 6; c++) vs[c] = virial ? warp_sum_ll(vfix[c]) : 0;
-    if (lane == 0 && b0 >= 0) {
-      long long *e = s.eacc + (long long)b0 * ACC_PER_BOX;
-      red_add(e + E_COUL, es);
-      if (virial)
-        for (int c = 0; c < 6; c++) {
-          red_add(e + E_VIR + slot[c][0], vs[c]);
-          if (slot[c][1] != slot[c][0]) red_add(e + E_VIR + slot[c][1], vs[c]);
-        }
-    }
-  } else if (valid) {
-    long long *e = s.eacc + (long long)box * ACC_PER_BOX;
-    red_add(e + E_COUL, efix);
-    if (virial)
-      for (int c = 0; c < 6; c++) {
-        red_add(e + E_VIR + slot[c][0], vfix[c]);
-        if (slot[c][1] != slot[c][0]) red_add(e + E_VIR + slot[c][1], vfix[c]);
-      }
-  }
+  box_accumulate(s.eacc, box, valid, E_COUL, en, virial ? vir : nullptr);
 }
 
 template <typename T>
-int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st) {
+int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,
+            StageMark mark, void *mctx) {
   using T2 = typename C2<T>::t;
   const int TB = 256;
   constexpr bool MIXED = sizeof(T) == 4;
   k_spread<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
+  if (mark) mark(mctx, "pme_spread");
   size_t zsmem = sizeof(T2) * (256 + ZMAXE);
   static bool zconf = false;
   if (!zconf) {
@@ -576,8 +549,11 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   }
   k_fft_plane<T, PMAXE><<<pm.npwork, PT, psmem, st>>>(pm);
   k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  if (mark) mark(mctx, "pme_fft");
   k_gather<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
+  if (mark) mark(mctx, "pme_gather");
   k_pme_energy<<<(pm.nbox + 127) / 128, 128, 0, st>>>(s, pm);
+  if (mark) mark(mctx, "pme_energy");
   return 0;
 }
 
@@ -585,8 +561,10 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
 
 int pme_max_plane_elems(int precision) { return precision ? 16384 : 13312; }
 
-int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st) {
-  return pm.precision ? recip_t<float>(s, nb, pm, st) : recip_t<double>(s, nb, pm, st);
+int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,
+                     StageMark mark, void *mctx) {
+  return pm.precision ? recip_t<float>(s, nb, pm, st, mark, mctx)
+                      : recip_t<double>(s, nb, pm, st, mark, mctx);
 }
 
 int pme_correction_launch(const SystemDev &s, const PmeDev &pm, const int *excl_pairs,

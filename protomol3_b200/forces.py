@@ -234,6 +234,24 @@ def evaluate_all(topo, force_list, positions, forces, energies):
         forces[:] = f
 
 
+def profile(topo, force_list, nrep=10, flush_l2=True):
+    """Mean device time (ms) per pipeline stage of ``force_list``, measured with CUDA events."""
+    hs = (C.c_void_p * len(force_list))(*[f.handle(topo) for f in force_list])
+    ms = np.zeros(32)
+    n = C.c_int(0)
+    names = C.create_string_buffer(1024)
+    L.check(L.lib().pmb_profile(topo.system(), C.cast(hs, C.c_void_p), len(force_list), int(nrep),
+                                int(flush_l2), _p(ms), 32, C.byref(n), names, 1024))
+    return dict(zip(names.value.decode().split(","), ms[:n.value].tolist()))
+
+
+def fp32_peak():
+    """Measured FP32 FMA throughput of the current device in TFLOP/s."""
+    t = C.c_double(0.0)
+    L.check(L.lib().pmb_fp32_peak(C.byref(t)))
+    return t.value
+
+
 class ForceFactory:
     """Parses ProtoMol force definitions (the text after ``force`` in a .conf file).
 
@@ -340,6 +358,11 @@ class Integrator:
         pos, vel = np.zeros((n, 3)), np.zeros((n, 3))
         L.check(L.lib().pmb_md_get_state(self._h, _p(pos), _p(vel)))
         return pos, vel
+
+    def kernels_per_step(self):
+        n = C.c_int(0)
+        L.check(L.lib().pmb_md_kernels_per_step(self._h, C.byref(n)))
+        return n.value
 
     def forces_now(self):
         f = np.zeros((self.topo.n_atoms, 3))
