@@ -174,7 +174,9 @@ def run_b200(args, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     box = workload(rank)
-    stream = torch.cuda.current_stream()
+    # a non-default stream: the legacy default stream cannot be captured into a CUDA graph
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def make(precision):

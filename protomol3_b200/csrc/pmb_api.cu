@@ -1160,7 +1160,9 @@ int pmb_md_run(pmb_md *m, int n) {
   if (!m->have_state) return fail(PMB_ERR_STATE, "pmb_md_set_state must come first");
   if (n < 1) return PMB_OK;
   pmb_system *s = m->sys;
-  if (m->use_graph) {
+  // the legacy default stream cannot be captured: replay eagerly there
+  const bool graph_ok = s->stream != nullptr && s->stream != cudaStreamLegacy;
+  if (m->use_graph && graph_ok) {
     if (!m->g_first) {
       int rc = md_capture(m, 0.5, &m->g_first);
       if (rc) return rc;

@@ -170,28 +170,29 @@ __global__ void k_pack(SystemDev s, NbListDev nb, int want_fp64) {
   if (want_fp64) nb.slot_pq[sl] = make_double4(x, y, z, q);
 }
 
+// Bounding box of every 16-slot block in fractional fixed point; a warp covers two blocks.
 __global__ void k_block_bbox(NbListDev nb) {
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= nb.nblk_total) return;
-  int sl = warp * BLOCK + lane;
-  bool valid = nb.slot_orig[sl] >= 0;
-  uint4 f = nb.slot_fx[sl];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int blk = t / BLOCK, lane = threadIdx.x & 31;
+  bool inr = blk < nb.nblk_total;
+  int sl = inr ? t : 0;
+  bool valid = inr && nb.slot_orig[sl] >= 0;
+  uint4 f = inr ? nb.slot_fx[sl] : make_uint4(0, 0, 0, 0);
   unsigned lo[3] = {valid ? f.x : 0xffffffffu, valid ? f.y : 0xffffffffu, valid ? f.z : 0xffffffffu};
   unsigned hi[3] = {valid ? f.x : 0u, valid ? f.y : 0u, valid ? f.z : 0u};
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
+  for (int o = BLOCK / 2; o > 0; o >>= 1)
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
       hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
     }
-  int cnt = __popc(__ballot_sync(0xffffffffu, valid));
-  if (lane == 0) {
-    if (cnt == 0) {
-      lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
-    }
-    nb.blk_lo[warp] = make_uint4(lo[0], lo[1], lo[2], (unsigned)cnt);
-    nb.blk_hi[warp] = make_uint4(hi[0], hi[1], hi[2], 0u);
+  unsigned bal = __ballot_sync(0xffffffffu, valid);
+  int cnt = __popc(bal & (0xffffu << (lane & 16)));
+  if (inr && (lane & (BLOCK - 1)) == 0) {
+    if (cnt == 0) lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
+    nb.blk_lo[blk] = make_uint4(lo[0], lo[1], lo[2], (unsigned)cnt);
+    nb.blk_hi[blk] = make_uint4(hi[0], hi[1], hi[2], 0u);
   }
 }
 
@@ -258,17 +259,23 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
     }
     unsigned m = __ballot_sync(0xffffffffu, cand);
     while (m) {
-      int src = __ffs(m) - 1;
+      // two candidate blocks per pass: lanes 0-15 test the atoms of the first, 16-31 the second
+      int srcA = __ffs(m) - 1;
       m &= m - 1;
-      int Jc = J0 + src;
-      int sl = Jc * BLOCK + lane;
+      int srcB = m ? __ffs(m) - 1 : -1;
+      if (m) m &= m - 1;
+      int src = lane < BLOCK ? srcA : srcB;
       bool take = false;
-      if (nb.slot_orig[sl] >= 0) {
-        if (b.multi_image) take = true;
-        else {
-          uint4 f = nb.slot_fx[sl];
-          unsigned p[3] = {f.x, f.y, f.z};
-          take = box_gap2(b, cI, hI, p, zero) <= rlist2;
+      int sl = -1;
+      if (src >= 0) {
+        sl = (J0 + src) * BLOCK + (lane & (BLOCK - 1));
+        if (nb.slot_orig[sl] >= 0) {
+          if (b.multi_image) take = true;
+          else {
+            uint4 f = nb.slot_fx[sl];
+            unsigned p[3] = {f.x, f.y, f.z};
+            take = box_gap2(b, cI, hI, p, zero) <= rlist2;
+          }
         }
       }
       unsigned tm = __ballot_sync(0xffffffffu, take);
@@ -327,8 +334,8 @@ int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   k_sort_bins<<<(nb.nkeys + T - 1) / T, T, 0, st>>>(s, nb.bin_box, nb.bin_start, nb.bin_count,
                                                    nb.nkeys, nb.slot_orig);
   k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
+  k_block_bbox<<<(nb.nslot + T - 1) / T, T, 0, st>>>(nb);
   int wthreads = nb.nblk_total * 32;
-  k_block_bbox<<<(wthreads + T - 1) / T, T, 0, st>>>(nb);
   k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
   scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st);
   k_tile_map<<<(nb.nblk_total + T - 1) / T, T, 0, st>>>(nb);

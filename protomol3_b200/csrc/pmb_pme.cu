@@ -473,13 +473,17 @@ __global__ void __launch_bounds__(PT) k_fft_plane(PmeDev pm) {
 // Per box: fixed-order sum of its planes' partials, x 0.5 (Grid.h:319-337), into the box
 // accumulators.
 __global__ void k_pme_energy(const SystemDev s, PmeDev pm) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per box; lane-strided partial sums then a fixed shuffle tree (reproducible)
+  int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (b >= pm.nbox) return;
   const PmeBoxPlan &pl = pm.plan[b];
   int p0 = pl.plane0, np = pl.n[2] / 2 + 1;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int p = p0; p < p0 + np; p++)
-    for (int c = 0; c < 7; c++) acc[c] += pm.plane_part[(long long)p * 8 + c];
+  const int nc = pm.virial ? 7 : 1;
+  for (int p = p0 + lane; p < p0 + np; p += 32)
+    for (int c = 0; c < nc; c++) acc[c] += pm.plane_part[(long long)p * 8 + c];
+  for (int c = 0; c < nc; c++) acc[c] = warp_sum(acc[c]);
+  if (lane != 0) return;
   long long *e = s.eacc + (long long)b * ACC_PER_BOX;
   red_add(e + E_COUL, f2fix(acc[0] * 0.5, ENERGY_SCALE));
   if (pm.virial) {
@@ -552,7 +556,7 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   if (mark) mark(mctx, "pme_fft");
   k_gather<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   if (mark) mark(mctx, "pme_gather");
-  k_pme_energy<<<(pm.nbox + 127) / 128, 128, 0, st>>>(s, pm);
+  k_pme_energy<<<(pm.nbox * 32 + 127) / 128, 128, 0, st>>>(s, pm);
   if (mark) mark(mctx, "pme_energy");
   return 0;
 }
