@@ -194,7 +194,9 @@ struct pmb_system {
   int *h_status = nullptr;                      // pinned
   // neighbour list
   bool nb_ready = false;
-  double nb_cutoff = 0.0;
+  double nb_cutoff = 0.0;    // radius the list storage is sized for
+  double nb_build_rl = -1.0; // radius the current list was built with
+  double skin = 0.4;         // list radius = pair cutoff + skin
   NbListDev nb{};
   Allocs nba;
   int n_bonded = 0;
@@ -306,6 +308,13 @@ int nblist_alloc(pmb_system *s, double rl) {
   nb.bin_start = s->nba.get<int>(nb.nkeys + 1);
   int maxn = std::max(nb.nkeys, nblk) + 1;
   nb.scan_tmp = s->nba.get<int>(maxn / 4096 + 2);
+  nb.xref = s->nba.get<double>(3 * (size_t)s->natoms);
+  nb.ctl = s->nba.get<unsigned>(4);
+  nb.half_skin2 = (float)(0.25 * s->skin * s->skin);
+  if (!nb.xref || !nb.ctl) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
+  const unsigned ctl0[4] = {0u, 0u, 0u, 1u};  // first use builds the list
+  CK(cudaMemcpy(nb.ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice));
+  s->nb_build_rl = -1.0;
   if (!nb.blk_lo || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.scan_tmp || !nb.bin_start)
     return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
   s->nb_cutoff = rl;
@@ -405,17 +414,30 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   double rl = 0.0;
   for (int i = 0; i < n; i++) rl = std::max(rl, force_pair_cutoff(fs[i]));
   std::vector<PairJob> jobs = pair_jobs(s, fs, n, virial);
-  if (!jobs.empty()) {
-    int rc = ensure_nblist(s, rl + 1e-3);
+  bool need_pme_slots = false;
+  for (int i = 0; i < n; i++) need_pme_slots |= fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal;
+  if (!jobs.empty() || need_pme_slots) {
+    // list radius: pair cutoff + skin (+ a margin for the fixed-point culling)
+    const double rlist = std::max(rl, 1.0) + s->skin + 1e-3;
+    int rc = ensure_nblist(s, rlist);
     if (rc) return rc;
-    nblist_build(sd, s->nb, rl + 1e-3, st);
+    if (rlist != s->nb_build_rl) {  // a list built for another radius cannot be reused
+      CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, st));
+      s->nb_build_rl = rlist;
+    }
+    nblist_build(sd, s->nb, rlist, st);
     mark(s, "nblist");
+  }
+  if (!jobs.empty()) {
     for (auto &j : jobs) {
       PairLaunch pl;
       pl.precision = s->precision;
       pl.p = j.p;
       pl.lj = s->d_lj;
       pl.lattice = j.lattice;
+      pl.multi = 0;
+      if (j.p.coul_mode == 2 && j.lattice)
+        for (const BoxDev &b : s->hbox) pl.multi |= b.multi_image;
       if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
       mark(s, "pair");
     }
@@ -425,14 +447,6 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     if (f->kind == PMB_FORCE_PME) {
       f->pm.virial = virial;
       if (f->d.reciprocal) {
-        if (!s->nb_ready) {
-          int rc = ensure_nblist(s, std::max(rl, 1.0) + 1e-3);
-          if (rc) return rc;
-        }
-        if (jobs.empty()) {
-          nblist_build(sd, s->nb, std::max(s->nb_cutoff, 1.0), st);
-          mark(s, "nblist");
-        }
         pme_recip_launch(sd, s->nb, f->pm, st, mark, s);
       }
       if (f->d.correction) {
@@ -690,6 +704,14 @@ int pmb_system_set_stream(pmb_system *s, void *stream) {
 int pmb_system_n_atoms(const pmb_system *s) { return s ? s->natoms : 0; }
 int pmb_system_n_boxes(const pmb_system *s) { return s ? s->nbox : 0; }
 
+int pmb_system_set_skin(pmb_system *s, double skin) {
+  if (!s || !(skin >= 0.0) || skin > 5.0) return fail(PMB_ERR_ARG, "skin must be in [0, 5] A");
+  cudaStreamSynchronize(s->stream);
+  s->skin = skin;
+  s->nb_ready = false;  // storage is sized for cutoff + skin
+  return PMB_OK;
+}
+
 pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
   if (!s || !d) return fail(PMB_ERR_ARG, "null argument"), nullptr;
   pmb_force *f = new pmb_force();
@@ -776,10 +798,9 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     std::vector<double> infl;
     std::vector<int> radix;
     std::vector<int4> zwork;
-    std::vector<int2> pwork;
+    std::vector<int4> ywork, xwork;
     long long g0 = 0, c0 = 0;
-    int maxpe = 0;
-    const int plane_cap = pme_max_plane_elems(s->precision);
+    const int lcap = pme_line_capacity();
     double th0[8];
     bspline_h(P, 0.0, th0);
     for (int bi = 0; bi < nbox; bi++) {
@@ -819,19 +840,22 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
           infl.push_back(ex / (sc * sc + ss * ss));
         }
       }
-      if (pl.n[0] * pl.n[1] > plane_cap)
-        return bad(PMB_ERR_UNSUPPORTED, "PME grid plane nx*ny too large for one CTA");
       pl.grid0 = g0;
       pl.cgrid0 = c0;
       pl.piVr = 1.0 / (M_PI * b.L[0] * b.L[1] * b.L[2]);
       pl.fac = M_PI * M_PI / (f->alpha * f->alpha);
-      pl.plane0 = (int)pwork.size();
+      pl.plane0 = (int)xwork.size();
       g0 += (long long)pl.n[0] * pl.n[1] * pl.n[2];
       c0 += (long long)(pl.n[2] / 2 + 1) * pl.n[0] * pl.n[1];
-      maxpe = std::max(maxpe, pl.n[0] * pl.n[1]);
+      // z-lines in groups of 16 consecutive y (8 packed complex lines per CTA)
       for (int x = 0; x < pl.n[0]; x++)
-        for (int y0 = 0; y0 < pl.n[1]; y0 += 32) zwork.push_back(make_int4(bi, x, y0, std::min(32, pl.n[1] - y0)));
-      for (int kz = 0; kz <= pl.n[2] / 2; kz++) pwork.push_back(make_int2(bi, kz));
+        for (int y0 = 0; y0 < pl.n[1]; y0 += 16) zwork.push_back(make_int4(bi, x, y0, std::min(16, pl.n[1] - y0)));
+      const int rows = std::max(1, std::min(32, lcap / pl.n[1])), cols = std::max(1, std::min(32, lcap / pl.n[0]));
+      for (int kz = 0; kz <= pl.n[2] / 2; kz++) {
+        for (int x0 = 0; x0 < pl.n[0]; x0 += rows) ywork.push_back(make_int4(bi, kz, x0, std::min(rows, pl.n[0] - x0)));
+        for (int y0 = 0; y0 < pl.n[1]; y0 += cols) xwork.push_back(make_int4(bi, kz, y0, std::min(cols, pl.n[1] - y0)));
+      }
+      pl.nparts = (int)xwork.size() - pl.plane0;
       f->plans.push_back(pl);
     }
     PmeDev &pm = f->pm;
@@ -845,8 +869,7 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     float2 *dtwf;
     double *dinf;
     int *drad;
-    int4 *dz;
-    int2 *dp;
+    int4 *dz, *dy, *dx;
     int rc = 0;
     rc |= upload(f->a, dplan, f->plans);
     rc |= upload(f->a, dtw, tw);
@@ -854,7 +877,8 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     rc |= upload(f->a, dinf, infl);
     rc |= upload(f->a, drad, radix);
     rc |= upload(f->a, dz, zwork);
-    rc |= upload(f->a, dp, pwork);
+    rc |= upload(f->a, dy, ywork);
+    rc |= upload(f->a, dx, xwork);
     pm.plan = dplan;
     pm.twiddle = dtw;
     pm.twiddlef = dtwf;
@@ -862,13 +886,14 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     pm.radix = drad;
     pm.zwork = dz;
     pm.nzwork = (int)zwork.size();
-    pm.pwork = dp;
-    pm.npwork = (int)pwork.size();
-    pm.max_plane_elems = maxpe;
+    pm.ywork = dy;
+    pm.nywork = (int)ywork.size();
+    pm.xwork = dx;
+    pm.nxwork = (int)xwork.size();
     pm.qgrid = f->a.get<long long>(g0);
     pm.rgrid = s->precision ? (void *)f->a.get<float>(g0) : (void *)f->a.get<double>(g0);
     pm.cgrid = s->precision ? (void *)f->a.get<float2>(c0) : (void *)f->a.get<double2>(c0);
-    pm.plane_part = f->a.get<double>(8 * (size_t)pwork.size());
+    pm.plane_part = f->a.get<double>(8 * (size_t)xwork.size());
     if (rc || !pm.qgrid || !pm.rgrid || !pm.cgrid || !pm.plane_part) return bad(PMB_ERR_CUDA, "PME allocation failed");
   } else {
     f->pm.alpha = f->alpha;

@@ -55,6 +55,11 @@ struct NbListDev {
   int *scan_tmp;               // scratch for scans
   const int *bin_box;          // [nkeys] box of each sort bin
   int want_fp64;               // also pack raw double positions
+  // list reuse: the list is built with cutoff + skin and rebuilt only once some atom moved more
+  // than skin/2 since the last build (decided on the device, every step)
+  double *xref;                // [3 natoms] positions at the last build
+  unsigned *ctl;               // [4] max displacement^2 (float bits), rebuild flag, block counter, force
+  float half_skin2;
 };
 
 struct SystemDev {
@@ -79,6 +84,7 @@ struct PairLaunch {
   const double *lj;               // [ntypes*ntypes*4] device
   const float *ljf;               // float copy
   const double *lattice;          // [nlat_total*3]
+  int multi;                      // some box needs Ewald lattice images
   PairParams p;
 };
 int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st);
@@ -91,8 +97,8 @@ struct PmeBoxPlan {
   int tw0[3];         // offsets of twiddle tables (complex elements)
   int inf0[3];        // offsets of influence tables
   int rad0[3], nrad[3];
-  int plane0;         // first energy-partial slot of this box
-  int pad_;
+  int plane0;         // first energy-partial slot (x-line work item) of this box
+  int nparts;         // number of x-line work items of this box
   double hr[3];       // n / L
   double mr[3];       // 1 / L
   double piVr, fac;   // 1/(pi V), pi^2 / alpha^2
@@ -110,10 +116,11 @@ struct PmeDev {
   const int *radix;           // radices per dim
   const int4 *zwork;          // z-pass work items: box, x, y0, count
   int nzwork;
-  const int2 *pwork;          // plane work items: box, kz
-  int npwork;
-  double *plane_part;         // [npwork * 7] energy + virial partials
-  int max_plane_elems;
+  const int4 *ywork;          // y-line work items: box, kz, x0, rows
+  int nywork;
+  const int4 *xwork;          // x-line work items: box, kz, y0, columns
+  int nxwork;
+  double *plane_part;         // [nxwork * 8] energy + virial partials
   double alpha, a2pi;
   int virial;
 };
@@ -121,7 +128,7 @@ struct PmeDev {
 typedef void (*StageMark)(void *ctx, const char *stage);
 int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,
                      StageMark mark = nullptr, void *mark_ctx = nullptr);
-int pme_max_plane_elems(int precision);
+int pme_line_capacity();
 int pme_correction_launch(const SystemDev &s, const PmeDev &pm, const int *excl_pairs,
                           const int *excl_kind, int nexcl, double coulomb_scaling, cudaStream_t st);
 

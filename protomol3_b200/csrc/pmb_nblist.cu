@@ -62,7 +62,8 @@ __device__ int block_exclusive_scan(int v, int *total) {
   return off + x - v;
 }
 
-__global__ void k_scan_reduce(const int *in, int n, int *chunk) {
+__global__ void k_scan_reduce(const int *in, int n, int *chunk, const unsigned *go) {
+  if (go && !go[1]) return;
   long long base = (long long)blockIdx.x * SCAN_CHUNK + threadIdx.x * 4;
   int s = 0;
 #pragma unroll
@@ -73,7 +74,8 @@ __global__ void k_scan_reduce(const int *in, int n, int *chunk) {
   if (threadIdx.x == 0) chunk[blockIdx.x] = tot;
 }
 
-__global__ void k_scan_chunks(int *chunk, int nchunk) {
+__global__ void k_scan_chunks(int *chunk, int nchunk, const unsigned *go) {
+  if (go && !go[1]) return;
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -90,7 +92,8 @@ __global__ void k_scan_chunks(int *chunk, int nchunk) {
   if (threadIdx.x == 0) chunk[nchunk] = carry;
 }
 
-__global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out) {
+__global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out, const unsigned *go) {
+  if (go && !go[1]) return;
   long long base = (long long)blockIdx.x * SCAN_CHUNK + threadIdx.x * 4;
   int v[4], s = 0;
 #pragma unroll
@@ -108,7 +111,48 @@ __global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out) {
 }
 
 // ---------------------------------------------------------------- binning and sort
-__global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count) {
+// Rebuild decision: max |x - x_ref|^2 over all atoms (last block decides, no host round trip);
+// ctl = {max displacement^2 as float bits, rebuild flag, finished blocks, forced rebuild}.
+__global__ void k_disp_check(SystemDev s, NbListDev nb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float d2 = 0.f;
+  if (i < s.natoms) {
+    double dx = s.pos[3 * i] - nb.xref[3 * i], dy = s.pos[3 * i + 1] - nb.xref[3 * i + 1],
+           dz = s.pos[3 * i + 2] - nb.xref[3 * i + 2];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    d2 = r2 < 3.0e38 ? (float)r2 : 3.0e38f;
+    if (!(d2 >= 0.f)) d2 = 3.0e38f;  // NaN positions force a rebuild
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+  __shared__ float wmax[32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wmax[w]);
+    atomicMax(&nb.ctl[0], __float_as_uint(m));
+    __threadfence();
+    unsigned done = atomicAdd(&nb.ctl[2], 1u);
+    if (done == gridDim.x - 1) {
+      __threadfence();
+      float mx = __uint_as_float(atomicAdd(&nb.ctl[0], 0u));
+      nb.ctl[1] = (nb.ctl[3] != 0u || mx > nb.half_skin2) ? 1u : 0u;
+      nb.ctl[0] = 0u;
+      nb.ctl[2] = 0u;
+      nb.ctl[3] = 0u;
+    }
+  }
+}
+
+__global__ void k_zero_bins(int *bin_count, int n, const unsigned *go) {
+  if (!go[1]) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= n) bin_count[i] = 0;
+}
+
+__global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count, const unsigned *go) {
+  if (!go[1]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.natoms) return;
   const BoxDev &b = s.box[s.atom_box[i]];
@@ -124,7 +168,8 @@ __global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count) {
 }
 
 __global__ void k_scatter(SystemDev s, const int *key, const int *rank, const int *bin_start,
-                          int *slot_orig) {
+                          int *slot_orig, const unsigned *go) {
+  if (!go[1]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.natoms) return;
   const BoxDev &b = s.box[s.atom_box[i]];
@@ -134,7 +179,8 @@ __global__ void k_scatter(SystemDev s, const int *key, const int *rank, const in
 
 // Makes the within-bin order deterministic (ascending original index).
 __global__ void k_sort_bins(SystemDev s, const int *bin_box, const int *bin_start,
-                            const int *bin_count, int nkeys, int *slot_orig) {
+                            const int *bin_count, int nkeys, int *slot_orig, const unsigned *go) {
+  if (!go[1]) return;
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nkeys) return;
   int cnt = bin_count[k];
@@ -164,6 +210,11 @@ __global__ void k_pack(SystemDev s, NbListDev nb, int want_fp64) {
   int bi = s.atom_box[o];
   const BoxDev &b = s.box[bi];
   double x = s.pos[3 * o], y = s.pos[3 * o + 1], z = s.pos[3 * o + 2], q = s.charge[o];
+  if (nb.ctl[1]) {  // list rebuilt this step: new reference positions
+    nb.xref[3 * o] = x;
+    nb.xref[3 * o + 1] = y;
+    nb.xref[3 * o + 2] = z;
+  }
   nb.slot_meta[sl] = make_int4(o, s.molecule[o], s.type[o], bi);
   nb.slot_fx[sl] = make_uint4(frac_fixed(x, b.Lr[0]), frac_fixed(y, b.Lr[1]),
                               frac_fixed(z, b.Lr[2]), __float_as_uint((float)q));
@@ -172,6 +223,7 @@ __global__ void k_pack(SystemDev s, NbListDev nb, int want_fp64) {
 
 // Bounding box of every 16-slot block in fractional fixed point; a warp covers two blocks.
 __global__ void k_block_bbox(NbListDev nb) {
+  if (!nb.ctl[1]) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int blk = t / BLOCK, lane = threadIdx.x & 31;
   bool inr = blk < nb.nblk_total;
@@ -226,6 +278,7 @@ __device__ __forceinline__ void center_half(uint4 lo, uint4 hi, unsigned c[3], u
 // One warp per block I: candidate blocks J > I of the same box by bounding-box gap, then the
 // atoms of each candidate within the list cutoff of I's box, compacted into I's j-list.
 __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
+  if (!nb.ctl[1]) return;
   int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (I >= nb.nblk_total) return;
   int bi = nb.blk_box[I];
@@ -299,6 +352,7 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
 }
 
 __global__ void k_tile_map(NbListDev nb) {
+  if (!nb.ctl[1]) return;
   int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= nb.nblk_total) return;
   int off = nb.tile_off[I], cnt = nb.jcount[I];
@@ -312,12 +366,12 @@ __global__ void k_tile_map(NbListDev nb) {
   }
 }
 
-int scan_exclusive(const int *in, int *out, int n, int *tmp, cudaStream_t st) {
+int scan_exclusive(const int *in, int *out, int n, int *tmp, cudaStream_t st, const unsigned *go) {
   int nchunk = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
   if (nchunk < 1) nchunk = 1;
-  k_scan_reduce<<<nchunk, 1024, 0, st>>>(in, n, tmp);
-  k_scan_chunks<<<1, 1024, 0, st>>>(tmp, nchunk);
-  k_scan_apply<<<nchunk, 1024, 0, st>>>(in, n, tmp, out);
+  k_scan_reduce<<<nchunk, 1024, 0, st>>>(in, n, tmp, go);
+  k_scan_chunks<<<1, 1024, 0, st>>>(tmp, nchunk, go);
+  k_scan_apply<<<nchunk, 1024, 0, st>>>(in, n, tmp, out, go);
   return 0;
 }
 
@@ -327,17 +381,18 @@ int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   const int T = 256;
   int na = s.natoms;
   if (na <= 0) return 0;
-  cudaMemsetAsync(nb.bin_count, 0, sizeof(int) * (size_t)(nb.nkeys + 1), st);
-  k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count);
-  scan_exclusive(nb.bin_count, nb.bin_start, nb.nkeys, nb.scan_tmp, st);
-  k_scatter<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_start, nb.slot_orig);
+  k_disp_check<<<(na + T - 1) / T, T, 0, st>>>(s, nb);
+  k_zero_bins<<<(nb.nkeys + T) / T, T, 0, st>>>(nb.bin_count, nb.nkeys, nb.ctl);
+  k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count, nb.ctl);
+  scan_exclusive(nb.bin_count, nb.bin_start, nb.nkeys, nb.scan_tmp, st, nb.ctl);
+  k_scatter<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_start, nb.slot_orig, nb.ctl);
   k_sort_bins<<<(nb.nkeys + T - 1) / T, T, 0, st>>>(s, nb.bin_box, nb.bin_start, nb.bin_count,
-                                                   nb.nkeys, nb.slot_orig);
+                                                   nb.nkeys, nb.slot_orig, nb.ctl);
   k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
   k_block_bbox<<<(nb.nslot + T - 1) / T, T, 0, st>>>(nb);
   int wthreads = nb.nblk_total * 32;
   k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
-  scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st);
+  scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st, nb.ctl);
   k_tile_map<<<(nb.nblk_total + T - 1) / T, T, 0, st>>>(nb);
   return 0;
 }

@@ -51,19 +51,6 @@ __device__ __forceinline__ int excl_check(const SystemDev &s, int oi, int oj) {
   return 0;
 }
 
-template <bool MIXED>
-struct SlotData;
-template <>
-struct SlotData<true> {
-  uint4 p;   // fixed x, y, z, q bits
-  int4 m;    // orig, mol, type, box
-};
-template <>
-struct SlotData<false> {
-  double4 p; // x, y, z, q
-  int4 m;
-};
-
 // Switching function with compile-time kind K (SWR: run time).  value/derivative on r2 < rc2.
 template <int K, typename T>
 __device__ __forceinline__ void sw_apply(const SwitchDev &w, T r2, T &e, T &f) {
@@ -91,18 +78,38 @@ struct Acc {
   T fi[3], elj, ec, vir[6];
 };
 
+// MUFU approximations for the FP32 path (hand-written PTX; flush-to-zero is harmless here:
+// every operand is far from the denormal range).
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float ex2_ftz(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // One pair: LJ (kind LSW) + Coulomb (mode CM: 0 none, 1 plain, 2 Ewald; switch CSW).
-// Returns the scalar force/r; energies accumulate into a.  'in' masks the contribution.
+// Returns the scalar force/r; energies accumulate into a.  Masked lanes ('in' false) see zero
+// parameters (A = B = q = 0), so every term vanishes without output selects.
 template <bool MIXED, int LSW, int CM, int CSW>
 __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type pair_force(
     const PairParams &p, bool in, int ex, typename std::conditional<MIXED, float, double>::type r2,
     typename std::conditional<MIXED, float, double>::type qq,
-    const typename std::conditional<MIXED, float2, double2>::type ab, Acc<typename std::conditional<MIXED, float, double>::type> &a) {
+    typename std::conditional<MIXED, float2, double2>::type ab,
+    Acc<typename std::conditional<MIXED, float, double>::type> &a) {
   using T = typename std::conditional<MIXED, float, double>::type;
   const T r2s = in ? r2 : T(1);
   T rd2, rinv;
   if constexpr (MIXED) {
-    rinv = rsqrtf(r2s);
+    rinv = rsqrt_ftz(r2s);
     rd2 = rinv * rinv;
   } else {
     rd2 = 1.0 / r2s;
@@ -112,33 +119,29 @@ __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type
   if constexpr (LSW != NONE) {
     bool use = LSW != SWR || p.do_lj;
     if (use) {
-      T r6 = rd2 * rd2 * rd2, r12 = r6 * r6, r6B = ab.y * r6, r12A = ab.x * r12;
+      const bool inl = in && (p.lj_cut2 >= p.cut2 || r2s <= T(p.lj_cut2));
+      const T A = inl ? ab.x : T(0), B = inl ? ab.y : T(0);
+      T r6 = rd2 * rd2 * rd2, r12 = r6 * r6, r6B = B * r6, r12A = A * r12;
       T e = r12A - r6B;
       T f = T(12) * r12A * rd2 - T(6) * r6B * rd2;
       sw_apply<LSW>(p.lj_sw, r2s, e, f);
-      bool inl = in && r2s <= T(p.lj_cut2);
-      a.elj += inl ? e : T(0);
-      fs += inl ? f : T(0);
+      a.elj += e;
+      fs += f;
     }
   }
-  if constexpr (CM == 1) {
-    T e;
-    if constexpr (MIXED) e = qq * rinv;
-    else e = qq * sqrt(rd2);
-    if (ex == 1) e *= T(p.coulomb_scaling);
-    T f = e * rd2;
-    sw_apply<CSW>(p.coul_sw, r2s, e, f);
-    bool inc = in && r2s <= T(p.coul_cut2);
-    a.ec += inc ? e : T(0);
-    fs += inc ? f : T(0);
-  }
-  if constexpr (CM == 2) {
-    T q = ex == 1 ? qq * T(p.coulomb_scaling) : qq;
+  if constexpr (CM != 0) {
+    const bool inc = in && (p.coul_cut2 >= p.cut2 || r2s <= T(p.coul_cut2));
+    T q = inc ? qq : T(0);
+    if (ex == 1) q *= T(p.coulomb_scaling);
     T e, f;
-    if constexpr (MIXED) {
+    if constexpr (CM == 1) {
+      if constexpr (MIXED) e = q * rinv;
+      else e = q * sqrt(rd2);
+      f = e * rd2;
+    } else if constexpr (MIXED) {
       T r = r2s * rinv, ar = T(p.alpha) * r;
-      T g = q * exp2f(-ar * ar * 1.4426950408889634f);
-      T t = __fdividef(1.0f, fmaf(0.3275911f, ar, 1.0f));
+      T g = q * ex2_ftz(ar * ar * -1.4426950408889634f);
+      T t = rcp_ftz(fmaf(0.3275911f, ar, 1.0f));
       T poly = t * (0.254829592f + t * (-0.284496736f + t * (1.421413741f + t * (-1.453152027f + t * 1.061405429f))));
       e = poly * g * rinv;
       f = (e + T(p.a2pi) * g) * rd2;
@@ -149,15 +152,30 @@ __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type
       f = (e + p.a2pi * g) * rr * rr;
     }
     sw_apply<CSW>(p.coul_sw, r2s, e, f);
-    bool inc = in && r2s <= T(p.coul_cut2);
-    a.ec += inc ? e : T(0);
-    fs += inc ? f : T(0);
+    a.ec += e;
+    fs += f;
   }
   return fs;
 }
 
-template <bool MIXED, int LSW, int CM, int CSW, bool VIR>
-__global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
+// Shared-memory image of one j-atom of a tile.  Mixed: coordinates relative to the first atom
+// of the i-cluster (exact fixed-point difference, one rounding to FP32 per tile instead of per
+// pair); padding atoms sit at -1e6 A (i padding at +1e6 A) so the cutoff test masks them.
+template <bool MIXED>
+struct JStage;
+template <>
+struct JStage<true> {
+  float4 p;  // x, y, z relative, q
+  int2 m;    // molecule, type
+};
+template <>
+struct JStage<false> {
+  double4 p;  // raw x, y, z, q
+  int2 m;
+};
+
+template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI>
+__global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 2)
     k_pair(SystemDev s, NbListDev nb, PairParams p, const double *ljd, const double *lat) {
   using T = typename std::conditional<MIXED, float, double>::type;
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
@@ -165,7 +183,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
   const int nt = p.ntypes, ntt = nt * nt;
   T2 *ljab = reinterpret_cast<T2 *>(smem_raw);  // [ntt] {A, B} then [ntt] {A14, B14}
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  SlotData<MIXED> *stage = reinterpret_cast<SlotData<MIXED> *>(smem_raw + ljbytes);
+  JStage<MIXED> *stage = reinterpret_cast<JStage<MIXED> *>(smem_raw + ljbytes);
+  int *sorig_all = reinterpret_cast<int *>(stage + PAIR_WARPS * 32);
   for (int k = threadIdx.x; k < ntt; k += blockDim.x) {
     ljab[k] = T2{T(ljd[4 * k]), T(ljd[4 * k + 1])};
     ljab[ntt + k] = T2{T(ljd[4 * k + 2]), T(ljd[4 * k + 3])};
@@ -174,7 +193,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int half = lane & 16, li = lane & 15;
-  SlotData<MIXED> *sj = stage + wib * 32;
+  JStage<MIXED> *sj = stage + wib * 32;
+  int *sorig = sorig_all + wib * 32;
   const int gwarp = blockIdx.x * PAIR_WARPS + wib, nwarps = gridDim.x * PAIR_WARPS;
   int total = nb.tile_off[nb.nblk_total];
   if (total > nb.tile_cap) total = nb.tile_cap;
@@ -182,14 +202,17 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
   int curI = -1, curBox = -1;
   long long ifix[3] = {0, 0, 0};
   long long efix_lj = 0, efix_c = 0, vfix[6] = {0, 0, 0, 0, 0, 0};
-  SlotData<MIXED> si;
+  int4 im = make_int4(-1, -1, 0, 0);   // orig, mol, type, box of this lane's i-atom
+  T xi = 0, yi = 0, zi = 0, qi = 0;     // i-atom position (relative for the mixed path)
+  unsigned rx0 = 0, ry0 = 0, rz0 = 0;   // mixed: fixed-point reference (cluster atom 0)
   const BoxDev *bx = nullptr;
-  T sx = 0, sy = 0, sz = 0;
-  bool multi = false;
+  double sx = 0, sy = 0, sz = 0;
+  bool multi = false, wrap = !MIXED;
+  float Lf[3] = {0, 0, 0}, Lrf[3] = {0, 0, 0};
 
   auto flush_i = [&]() {
-    if (curI >= 0 && si.m.x >= 0 && half == 0) {
-      long long *f = s.facc + 3 * (long long)si.m.x;
+    if (curI >= 0 && im.x >= 0 && half == 0) {
+      long long *f = s.facc + 3 * (long long)im.x;
       if (ifix[0]) red_add(f, ifix[0]);
       if (ifix[1]) red_add(f + 1, ifix[1]);
       if (ifix[2]) red_add(f + 2, ifix[2]);
@@ -213,6 +236,26 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
     efix_lj = efix_c = 0;
     for (int c = 0; c < 6; c++) vfix[c] = 0;
   };
+  // stage one slot (or padding) as this lane's j-atom
+  auto stage_slot = [&](int sl, JStage<MIXED> &js, int &orig) {
+    if (sl >= 0) {
+      const int4 m = nb.slot_meta[sl];
+      orig = m.x;
+      js.m = make_int2(m.y, m.z);
+      if constexpr (MIXED) {
+        const uint4 f = nb.slot_fx[sl];
+        js.p = make_float4((float)((double)(int)(f.x - rx0) * sx), (float)((double)(int)(f.y - ry0) * sy),
+                           (float)((double)(int)(f.z - rz0) * sz), __uint_as_float(f.w));
+      } else {
+        js.p = nb.slot_pq[sl];
+      }
+    } else {
+      orig = -1;
+      js.m = make_int2(-1, 0);
+      if constexpr (MIXED) js.p = make_float4(-1e6f, -1e6f, -1e6f, 0.f);
+      else js.p = make_double4(-1e6, -1e6, -1e6, 0.0);
+    }
+  };
 
   for (int c0 = gwarp * CHUNK; c0 < total; c0 += nwarps * CHUNK) {
     const int cend = min(c0 + CHUNK, total);
@@ -225,37 +268,60 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
         flush_i();
         curI = I;
         const int sl = I * BLOCK + li;
-        si.m = nb.slot_meta[sl];
-        if constexpr (MIXED) si.p = nb.slot_fx[sl];
-        else si.p = nb.slot_pq[sl];
-        const int bidx = __shfl_sync(0xffffffffu, si.m.w, 0);
+        im = nb.slot_meta[sl];
+        const int bidx = __shfl_sync(0xffffffffu, im.w, 0);
         if (bidx != curBox) {
           flush_e();
           curBox = bidx;
           bx = s.box + bidx;
           multi = bx->multi_image != 0;
-          if constexpr (MIXED) {
-            sx = T(bx->L[0] * (1.0 / 4294967296.0));
-            sy = T(bx->L[1] * (1.0 / 4294967296.0));
-            sz = T(bx->L[2] * (1.0 / 4294967296.0));
+          sx = bx->L[0] * (1.0 / 4294967296.0);
+          sy = bx->L[1] * (1.0 / 4294967296.0);
+          sz = bx->L[2] * (1.0 / 4294967296.0);
+          for (int c = 0; c < 3; c++) {
+            Lf[c] = (float)bx->L[c];
+            Lrf[c] = (float)bx->Lr[c];
           }
+        }
+        if constexpr (MIXED) {
+          // coordinates relative to cluster atom 0 are minimal-image differences whenever
+          // L/2 > cutoff + cluster extent; otherwise (small boxes) every pair is wrapped again
+          const uint4 lo = nb.blk_lo[I], hi = nb.blk_hi[I];
+          const double rmax = sqrt(p.cut2) + 1e-3;
+          wrap = multi || (double)(hi.x - lo.x) * sx + rmax >= 0.5 * bx->L[0] ||
+                 (double)(hi.y - lo.y) * sy + rmax >= 0.5 * bx->L[1] ||
+                 (double)(hi.z - lo.z) * sz + rmax >= 0.5 * bx->L[2];
+          const uint4 f = nb.slot_fx[sl];
+          rx0 = __shfl_sync(0xffffffffu, f.x, 0);
+          ry0 = __shfl_sync(0xffffffffu, f.y, 0);
+          rz0 = __shfl_sync(0xffffffffu, f.z, 0);
+          if (im.x >= 0) {
+            xi = (float)((double)(int)(f.x - rx0) * sx);
+            yi = (float)((double)(int)(f.y - ry0) * sy);
+            zi = (float)((double)(int)(f.z - rz0) * sz);
+          } else {
+            xi = yi = zi = 1e6f;
+          }
+          qi = __uint_as_float(f.w);
+        } else {
+          const double4 q4 = nb.slot_pq[sl];
+          if (im.x >= 0) {
+            xi = q4.x; yi = q4.y; zi = q4.z;
+          } else {
+            xi = yi = zi = 1e6;
+          }
+          qi = q4.w;
         }
       }
       const bool diag = (k == 0);
       // diagonal tile: the cluster against itself (lanes 0-15); other tiles: 32 listed j-atoms
       const int jsl = diag ? (half ? -1 : I * BLOCK + li) : nb.jlist[nb.jcap_off[I] + (k - 1) * JCHUNK + lane];
-      SlotData<MIXED> mine;
-      if (jsl >= 0) {
-        mine.m = nb.slot_meta[jsl];
-        if constexpr (MIXED) mine.p = nb.slot_fx[jsl];
-        else mine.p = nb.slot_pq[jsl];
-      } else {
-        mine.m = make_int4(-1, -1, 0, curBox);
-        if constexpr (MIXED) mine.p = make_uint4(0, 0, 0, 0);
-        else mine.p = make_double4(0, 0, 0, 0);
-      }
+      JStage<MIXED> mine;
+      int jorig;
+      stage_slot(jsl, mine, jorig);
       __syncwarp();
       sj[lane] = mine;
+      sorig[lane] = jorig;
       __syncwarp();
 
       Acc<T> a;
@@ -263,87 +329,99 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
       a.elj = a.ec = T(0);
       for (int c = 0; c < 6; c++) a.vir[c] = T(0);
       T fj[3] = {T(0), T(0), T(0)};
-      const bool ivalid = si.m.x >= 0;
-      const int tio = si.m.z * nt;
-      T qi;
-      if constexpr (MIXED) qi = __uint_as_float(si.p.w);
-      else qi = si.p.w;
+      const int tio = im.z * nt;
       const int nxt = half | ((li + 1) & 15);
+      const T cut2 = T(p.cut2);
 
+      const bool ivalid = im.x >= 0;
+      auto body = [&](auto diag_tag, auto wrap_tag) {
+        constexpr bool DIAG = decltype(diag_tag)::value;
+        constexpr bool WRAP = decltype(wrap_tag)::value;
 #pragma unroll 2
-      for (int st = 0; st < 16; st++) {
-        const int jl = (li + st) & 15;
-        const SlotData<MIXED> dj = sj[half | jl];
-        T dx, dy, dz;
-        if constexpr (MIXED) {
-          dx = T((int)(dj.p.x - si.p.x)) * sx;
-          dy = T((int)(dj.p.y - si.p.y)) * sy;
-          dz = T((int)(dj.p.z - si.p.z)) * sz;
-        } else {
-          dx = dj.p.x - si.p.x;
-          dy = dj.p.y - si.p.y;
-          dz = dj.p.z - si.p.z;
-          dx -= bx->L[0] * rint(bx->Lr[0] * dx);
-          dy -= bx->L[1] * rint(bx->Lr[1] * dy);
-          dz -= bx->L[2] * rint(bx->Lr[2] * dz);
-        }
-        const T r2 = dx * dx + dy * dy + dz * dz;
-        bool in = ivalid && dj.m.x >= 0 && r2 <= T(p.cut2) && (!diag || jl > li);
-        int ex = 0;
-        if (in && si.m.y == dj.m.y) {
-          ex = excl_check(s, si.m.x, dj.m.x);
-          if (ex == 2) in = false;
-        }
-        T qq, qj;
-        if constexpr (MIXED) qj = __uint_as_float(dj.p.w);
-        else qj = dj.p.w;
-        qq = qi * qj;
-        T2 ab;
-        if constexpr (LSW != NONE) ab = ljab[(ex == 1 ? ntt : 0) + tio + dj.m.z];
-        else ab = T2{T(0), T(0)};
-        T fs = pair_force<MIXED, LSW, CM, CSW>(p, in, ex, r2, qq, ab, a);
-        T fx = dx * fs, fy = dy * fs, fz = dz * fs;
-        if constexpr (VIR) {
-          a.vir[0] += fx * dx; a.vir[1] += fx * dy; a.vir[2] += fx * dz;
-          a.vir[3] += fy * dy; a.vir[4] += fy * dz; a.vir[5] += fz * dz;
-        }
-        if constexpr (CM == 2) {
-          // Lattice images beyond the minimal one (edge below twice the cutoff): the reference
-          // loops myLattice for every pair (NonbondedPMEwaldSystemForce.h:644-650); FULL
-          // exclusions skip only the first image, MODIFIED scaling applies to it only.
-          if (multi) {
-            const bool pv = ivalid && dj.m.x >= 0 && (!diag || jl > li);
-            for (int kk = 1; kk < bx->nlat; kk++) {
-              const double *lv = lat + 3 * (bx->lat0 + kk);
-              T rx = dx + T(lv[0]), ry = dy + T(lv[1]), rz = dz + T(lv[2]);
-              T rr2 = rx * rx + ry * ry + rz * rz;
-              bool inl = pv && rr2 <= T(p.coul_cut2);
-              Acc<T> b2;
-              b2.elj = T(0);
-              b2.ec = T(0);
-              T g = pair_force<MIXED, NONE, 2, CSW>(p, inl, 0, rr2, qq, T2{T(0), T(0)}, b2);
-              a.ec += b2.ec;
-              T gx = rx * g, gy = ry * g, gz = rz * g;
-              fx += gx; fy += gy; fz += gz;
-              if constexpr (VIR) {
-                a.vir[0] += gx * rx; a.vir[1] += gx * ry; a.vir[2] += gx * rz;
-                a.vir[3] += gy * ry; a.vir[4] += gy * rz; a.vir[5] += gz * rz;
+        for (int st = 0; st < 16; st++) {
+          const int jl = (li + st) & 15;
+          const JStage<MIXED> dj = sj[half | jl];
+          T dx = T(dj.p.x) - xi, dy = T(dj.p.y) - yi, dz = T(dj.p.z) - zi;
+          if constexpr (!MIXED) {
+            // the reference's minimal image: d - L rint(d / L) equals its single-wrap result
+            dx -= bx->L[0] * rint(bx->Lr[0] * dx);
+            dy -= bx->L[1] * rint(bx->Lr[1] * dy);
+            dz -= bx->L[2] * rint(bx->Lr[2] * dz);
+          } else if constexpr (WRAP) {
+            dx -= Lf[0] * rintf(Lrf[0] * dx);
+            dy -= Lf[1] * rintf(Lrf[1] * dy);
+            dz -= Lf[2] * rintf(Lrf[2] * dz);
+          }
+          const T r2 = dx * dx + dy * dy + dz * dz;
+          bool in = r2 <= cut2;
+          if constexpr (WRAP) in = in && ivalid && dj.m.x >= 0;  // sentinels do not survive a wrap
+          if constexpr (DIAG) in = in && jl > li;
+          int ex = 0;
+          if (in && im.y == dj.m.x) {
+            ex = excl_check(s, im.x, sorig[half | jl]);
+            if (ex == 2) in = false;
+          }
+          T2 ab;
+          if constexpr (LSW != NONE) ab = ljab[(ex == 1 ? ntt : 0) + tio + dj.m.y];
+          else ab = T2{T(0), T(0)};
+          T fs = pair_force<MIXED, LSW, CM, CSW>(p, in, ex, r2, qi * T(dj.p.w), ab, a);
+          T fx = dx * fs, fy = dy * fs, fz = dz * fs;
+          if constexpr (VIR) {
+            a.vir[0] += fx * dx; a.vir[1] += fx * dy; a.vir[2] += fx * dz;
+            a.vir[3] += fy * dy; a.vir[4] += fy * dz; a.vir[5] += fz * dz;
+          }
+          if constexpr (CM == 2 && MULTI && WRAP) {
+            // Lattice images beyond the minimal one (edge below twice the cutoff): the reference
+            // loops myLattice for every pair (NonbondedPMEwaldSystemForce.h:644-650); FULL
+            // exclusions skip only the first image, MODIFIED scaling applies to it only.
+            if (multi) {
+              bool pv = dj.m.x >= 0 && im.x >= 0;
+              if constexpr (DIAG) pv = pv && jl > li;
+              for (int kk = 1; kk < bx->nlat; kk++) {
+                const double *lv = lat + 3 * (bx->lat0 + kk);
+                T rx = dx + T(lv[0]), ry = dy + T(lv[1]), rz = dz + T(lv[2]);
+                T rr2 = rx * rx + ry * ry + rz * rz;
+                bool inl = pv && rr2 <= T(p.coul_cut2);
+                Acc<T> b2;
+                b2.elj = T(0);
+                b2.ec = T(0);
+                T g = pair_force<MIXED, NONE, 2, CSW>(p, inl, 0, rr2, qi * T(dj.p.w), T2{T(0), T(0)}, b2);
+                a.ec += b2.ec;
+                T gx = rx * g, gy = ry * g, gz = rz * g;
+                fx += gx; fy += gy; fz += gz;
+                if constexpr (VIR) {
+                  a.vir[0] += gx * rx; a.vir[1] += gx * ry; a.vir[2] += gx * rz;
+                  a.vir[3] += gy * ry; a.vir[4] += gy * rz; a.vir[5] += gz * rz;
+                }
               }
             }
           }
+          a.fi[0] -= fx; a.fi[1] -= fy; a.fi[2] -= fz;
+          fj[0] += fx; fj[1] += fy; fj[2] += fz;
+          // rotate j-force accumulators inside the 16-lane segment
+          fj[0] = __shfl_sync(0xffffffffu, fj[0], nxt);
+          fj[1] = __shfl_sync(0xffffffffu, fj[1], nxt);
+          fj[2] = __shfl_sync(0xffffffffu, fj[2], nxt);
         }
-        a.fi[0] -= fx; a.fi[1] -= fy; a.fi[2] -= fz;
-        fj[0] += fx; fj[1] += fy; fj[2] += fz;
-        // rotate j-force accumulators inside the 16-lane segment
-        fj[0] = __shfl_sync(0xffffffffu, fj[0], nxt);
-        fj[1] = __shfl_sync(0xffffffffu, fj[1], nxt);
-        fj[2] = __shfl_sync(0xffffffffu, fj[2], nxt);
+      };
+      bool unwrapped = false;
+      if constexpr (MIXED) {
+        if (!wrap) {
+          unwrapped = true;
+          if (diag) body(std::true_type{}, std::false_type{});
+          else body(std::false_type{}, std::false_type{});
+        }
       }
+      if (!unwrapped) {
+        if (diag) body(std::true_type{}, std::true_type{});
+        else body(std::false_type{}, std::true_type{});
+      }
+
       // after 16 rotations lane l holds the accumulator of j-atom l of the tile
       if (diag) {
         a.fi[0] += fj[0]; a.fi[1] += fj[1]; a.fi[2] += fj[2];
-      } else if (mine.m.x >= 0) {
-        long long *f = s.facc + 3 * (long long)mine.m.x;
+      } else if (jorig >= 0) {
+        long long *f = s.facc + 3 * (long long)jorig;
         long long v0 = f2fix(fj[0], (T)FORCE_SCALE), v1 = f2fix(fj[1], (T)FORCE_SCALE),
                   v2 = f2fix(fj[2], (T)FORCE_SCALE);
         if (v0) red_add(f, v0);
@@ -368,13 +446,16 @@ __global__ void __launch_bounds__(PAIR_THREADS, MIXED ? 3 : 2)
   flush_e();
 }
 
-template <bool MIXED, int LSW, int CM, int CSW, bool VIR>
+template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI = false>
 int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st) {
-  auto kern = k_pair<MIXED, LSW, CM, CSW, VIR>;
+  if constexpr (CM == 2 && !MULTI) {
+    if (pl.multi) return launch_t<MIXED, LSW, CM, CSW, VIR, true>(s, nb, pl, st);
+  }
+  auto kern = k_pair<MIXED, LSW, CM, CSW, VIR, MULTI>;
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
   const int ntt = pl.p.ntypes * pl.p.ntypes;
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  size_t smem = ljbytes + PAIR_WARPS * 32 * sizeof(SlotData<MIXED>);
+  size_t smem = ljbytes + PAIR_WARPS * 32 * (sizeof(JStage<MIXED>) + sizeof(int));
   static int grid = 0;
   static size_t conf_smem = 0;
   if (!grid || conf_smem != smem) {

@@ -404,41 +404,61 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
   return r;
 }
 
-constexpr int PT = 1024;  // plane-kernel threads
+constexpr int LT = 256;          // threads of the y- and x-line kernels
+constexpr int LMAXE = 4096;      // complex elements per line-kernel CTA
 
-template <typename T, int MAXE>
-__global__ void __launch_bounds__(PT) k_fft_plane(PmeDev pm) {
+// y-lines of the half spectrum: rows C[kz][x][0..ny) of one work item are contiguous.
+template <typename T>
+__global__ void __launch_bounds__(LT) k_fft_y(PmeDev pm, int sign) {
   using T2 = typename C2<T>::t;
-  extern __shared__ unsigned char smem_raw[];
-  const int2 wk = pm.pwork[blockIdx.x];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 wk = pm.ywork[blockIdx.x];  // box, kz, x0, rows
   const PmeBoxPlan &pl = pm.plan[wk.x];
-  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], kz = wk.y;
-  double *red = reinterpret_cast<double *>(smem_raw);  // 32 doubles
-  T2 *twx = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
-  T2 *twy = twx + nx;
-  T2 *buf = twy + ny;
-  for (int k = threadIdx.x; k < nx; k += PT) {
-    if constexpr (sizeof(T) == 4) twx[k] = pm.twiddlef[pl.tw0[0] + k];
-    else twx[k] = pm.twiddle[pl.tw0[0] + k];
+  const int nx = pl.n[0], ny = pl.n[1], kz = wk.y, x0 = wk.z, rows = wk.w;
+  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
+  T2 *buf = tw + ny;
+  for (int k = threadIdx.x; k < ny; k += LT) {
+    if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[1] + k];
+    else tw[k] = pm.twiddle[pl.tw0[1] + k];
   }
-  for (int k = threadIdx.x; k < ny; k += PT) {
-    if constexpr (sizeof(T) == 4) twy[k] = pm.twiddlef[pl.tw0[1] + k];
-    else twy[k] = pm.twiddle[pl.tw0[1] + k];
-  }
-  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + (long long)kz * nx * ny;
-  const int ne = nx * ny;
-  for (int e = threadIdx.x; e < ne; e += PT) buf[e] = C[e];
+  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + ((long long)kz * nx + x0) * ny;
+  const int ne = rows * ny;
+  for (int e = threadIdx.x; e < ne; e += LT) buf[e] = C[e];
   __syncthreads();
-  // forward along y (lines = x rows, contiguous) then along x (lines = y columns, stride ny)
-  fft_lines<PT, MAXE>(buf, ny, nx, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], twy, -1);
-  fft_lines<PT, MAXE>(buf, nx, ny, 1, ny, pm.radix + pl.rad0[0], pl.nrad[0], twx, -1);
-  // influence function, energy and virial (Grid.h:236-341) on the half spectrum kz <= nz/2
+  fft_lines<LT, LMAXE>(buf, ny, rows, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], tw, sign);
+  for (int e = threadIdx.x; e < ne; e += LT) C[e] = buf[e];
+}
+
+// x-lines (columns y0..y0+cols of one kz plane): forward FFT, influence function with energy and
+// virial (Grid.h:236-341, half spectrum kz <= nz/2 with the doubling of interior kz), inverse FFT.
+template <typename T>
+__global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 wk = pm.xwork[blockIdx.x];  // box, kz, y0, cols
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], kz = wk.y, y0 = wk.z, cols = wk.w;
+  double *red = reinterpret_cast<double *>(smem_raw);  // 32 doubles
+  T2 *tw = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
+  T2 *buf = tw + nx;  // buf[x * cols + c]
+  for (int k = threadIdx.x; k < nx; k += LT) {
+    if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[0] + k];
+    else tw[k] = pm.twiddle[pl.tw0[0] + k];
+  }
+  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + (long long)kz * nx * ny + y0;
+  const int ne = nx * cols;
+  for (int e = threadIdx.x; e < ne; e += LT) {
+    int x = e / cols, c = e % cols;
+    buf[e] = C[(long long)x * ny + c];
+  }
+  __syncthreads();
+  fft_lines<LT, LMAXE>(buf, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, -1);
   const double *bxt = pm.infl + pl.inf0[0], *byt = pm.infl + pl.inf0[1], *bzt = pm.infl + pl.inf0[2];
   const double mk = kz * pl.mr[2];
   const double wz = (kz > 0 && ((2 * kz != nz) || (nz & 1))) ? 2.0 : 1.0;
   double en = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
-  for (int e = threadIdx.x; e < ne; e += PT) {
-    int i = e / ny, j = e % ny;
+  for (int e = threadIdx.x; e < ne; e += LT) {
+    int i = e / cols, j = y0 + e % cols;
     if (i == 0 && j == 0 && kz == 0) {
       buf[e] = cmk(T(0), T(0));
       continue;
@@ -461,23 +481,25 @@ __global__ void __launch_bounds__(PT) k_fft_plane(PmeDev pm) {
   double part[7] = {en, vxx, vxy, vxz, vyy, vyz, vzz};
   const int np = pm.virial ? 7 : 1;
   for (int c = 0; c < np; c++) {
-    double r = block_sum<PT, T>(part[c], red);
+    double r = block_sum<LT, T>(part[c], red);
     if (threadIdx.x == 0) pm.plane_part[(long long)blockIdx.x * 8 + c] = r;
   }
   __syncthreads();
-  fft_lines<PT, MAXE>(buf, nx, ny, 1, ny, pm.radix + pl.rad0[0], pl.nrad[0], twx, +1);
-  fft_lines<PT, MAXE>(buf, ny, nx, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], twy, +1);
-  for (int e = threadIdx.x; e < ne; e += PT) C[e] = buf[e];
+  fft_lines<LT, LMAXE>(buf, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, +1);
+  for (int e = threadIdx.x; e < ne; e += LT) {
+    int x = e / cols, c = e % cols;
+    C[(long long)x * ny + c] = buf[e];
+  }
 }
 
-// Per box: fixed-order sum of its planes' partials, x 0.5 (Grid.h:319-337), into the box
+// Per box: fixed-order sum of its x-line partials, x 0.5 (Grid.h:319-337), into the box
 // accumulators.
 __global__ void k_pme_energy(const SystemDev s, PmeDev pm) {
   // one warp per box; lane-strided partial sums then a fixed shuffle tree (reproducible)
   int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (b >= pm.nbox) return;
   const PmeBoxPlan &pl = pm.plan[b];
-  int p0 = pl.plane0, np = pl.n[2] / 2 + 1;
+  int p0 = pl.plane0, np = pl.nparts;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const int nc = pm.virial ? 7 : 1;
   for (int p = p0 + lane; p < p0 + np; p += 32)
@@ -544,14 +566,16 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     zconf = true;
   }
   k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
-  constexpr int PMAXE = MIXED ? 16384 : 13312;
-  size_t psmem = 32 * sizeof(double) + sizeof(T2) * (512 + (size_t)pm.max_plane_elems);
-  static size_t pconf = 0;
-  if (pconf != psmem) {
-    cudaFuncSetAttribute(k_fft_plane<T, PMAXE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-    pconf = psmem;
+  const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + (size_t)LMAXE);
+  static bool lconf = false;
+  if (!lconf) {
+    cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
+    cudaFuncSetAttribute(k_fft_x_infl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
+    lconf = true;
   }
-  k_fft_plane<T, PMAXE><<<pm.npwork, PT, psmem, st>>>(pm);
+  k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, -1);
+  k_fft_x_infl<T><<<pm.nxwork, LT, lsmem, st>>>(pm);
+  k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, +1);
   k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   if (mark) mark(mctx, "pme_fft");
   k_gather<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
@@ -563,7 +587,7 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
 
 }  // namespace
 
-int pme_max_plane_elems(int precision) { return precision ? 16384 : 13312; }
+int pme_line_capacity() { return LMAXE; }
 
 int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,
                      StageMark mark, void *mctx) {

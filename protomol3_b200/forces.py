@@ -110,6 +110,9 @@ class Topology:
                 C.cast(descs, C.c_void_p), len(self.boxes), PRECISIONS[self.precision]))
         return self._sys
 
+    def set_skin(self, skin):
+        L.check(L.lib().pmb_system_set_skin(self.system(), float(skin)))
+
     def set_stream(self, stream_handle):
         L.check(L.lib().pmb_system_set_stream(self.system(), C.c_void_p(stream_handle)))
 

@@ -189,3 +189,26 @@ def test_config2_size_mixed_vs_oracle():
     assert rel_rms(f, fo) < 1e-5
     assert energy_ok(e[F.ScalarStructure.COULOMB], eo[O.E_COULOMB],
                      abs(info["terms"][0]) + abs(info["terms"][1]), "mixed", topo.n_atoms)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_list_reuse_with_skin_matches_rebuild_every_step(precision):
+    """A Verlet skin changes which pairs are tested, never which are evaluated."""
+    b = W.water_box(1500, seed=41)
+    grid = W.pme_grid_for(b["box"][0])
+
+    def run(skin):
+        topo = F.Topology(b, precision)
+        topo.set_skin(skin)
+        fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0)),
+              F.NonbondedPMEwaldSystemForce((grid,) * 3, 10.0)]
+        md = F.Integrator(topo, fl, timestep=1.0)
+        md.set_state(b["pos"], b["vel"])
+        md.run(40)
+        pos, vel = md.state()
+        return pos, md.forces_now()
+    p0, f0 = run(0.0)
+    p1, f1 = run(0.6)
+    tol = 1e-9 if precision == "fp64" else 1e-4
+    assert np.abs(p1 - p0).max() < tol
+    assert rel_rms(f1, f0) < (1e-9 if precision == "fp64" else 1e-5)
