@@ -237,9 +237,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
     for (int c = 0; c < 6; c++) vfix[c] = 0;
   };
   // stage one slot (or padding) as this lane's j-atom
+  // (padding slots of a box's last cluster, orig < 0, become sentinels as well: they carry no
+  // charge but an LJ type, and must never meet a real atom)
   auto stage_slot = [&](int sl, JStage<MIXED> &js, int &orig) {
-    if (sl >= 0) {
-      const int4 m = nb.slot_meta[sl];
+    const int4 m = sl >= 0 ? nb.slot_meta[sl] : make_int4(-1, -1, 0, 0);
+    if (m.x >= 0) {
       orig = m.x;
       js.m = make_int2(m.y, m.z);
       if constexpr (MIXED) {
