@@ -165,6 +165,29 @@ int pmb_profile(pmb_system *sys, pmb_force *const *forces, int n_forces, int nre
 /* Measured FP32 FMA issue rate of the device (TFLOP/s), the roofline of the pair kernel. */
 int pmb_fp32_peak(double *tflops);
 
+/* Allocation-free cutoff evaluation (no counterpart in the reference) ------------------------ */
+#define PMB_STATIC_MAX_BOXES 1024
+/* pmb_evaluate_device for one NonbondedCutoff force, for callers that may not allocate device
+ * memory: callers whose HBM is reserved up front (a serving loop that admits boxes against a
+ * fixed memory budget, a host framework whose caching allocator owns the device) and callers
+ * that cannot take the device-wide synchronisation of cudaFree.  pmb_evaluate_device allocates
+ * the neighbour list on its first call and whenever a larger cutoff needs more room; this entry
+ * point makes no cudaMalloc, cudaFree or other allocating call.  It visits all pairs of each box
+ * in FP64 whatever the system's precision (no neighbour list; cost grows as the square of the
+ * atoms per box), so its results equal pmb_evaluate_device's within FP64 rounding.
+ * Scratch: one static device array of fixed-point energy/virial accumulators per device,
+ * PMB_STATIC_MAX_BOXES boxes x PMB_E_STRIDE int64 (128 KiB); a system with more boxes gets
+ * PMB_ERR_CAPACITY and nothing runs.  The call zeroes the scratch itself (cudaMemsetAsync on
+ * the system's stream) before using it, so nothing has to start at zero.
+ * d_positions [3 N], d_forces [3 N] (overwritten) and d_energies [n_boxes * PMB_E_STRIDE]
+ * (overwritten; may be NULL) are device pointers; work is enqueued on the system's stream with
+ * no host synchronisation.  The first call on a device (the current device) looks the scratch
+ * up with cudaGetSymbolAddress, which may load the module: make that first call before any
+ * stream capture.  Calls whose executions overlap on one device (other streams, systems or host
+ * threads) share the scratch and race on it: order them on one stream or synchronise between. */
+int pmb_cutoff_evaluate_static(pmb_force *f, const double *d_positions, double *d_forces,
+                               double *d_energies, int virial);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -74,7 +74,10 @@ _PROTOS = [
     ("pmb_profile", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
                               C.c_int, C.c_void_p, C.c_char_p, C.c_int]),
     ("pmb_fp32_peak", C.c_int, [C.c_void_p]),
+    ("pmb_cutoff_evaluate_static", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_int]),
 ]
+STATIC_MAX_BOXES = 1024
 
 _lib = None
 

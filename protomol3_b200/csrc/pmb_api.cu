@@ -1248,3 +1248,42 @@ int pmb_md_energies(pmb_md *m, double *energies, double *kinetic) {
 }
 
 }  // extern "C"
+
+// Allocation-free NonbondedCutoff evaluation: the only scratch is the static energy/virial array
+// of pmb_pair.cu; topology and LJ tables are the system's, created by pmb_system_create.
+static_assert(STATIC_MAX_BOXES == PMB_STATIC_MAX_BOXES, "static scratch size mismatch");
+
+extern "C" int pmb_cutoff_evaluate_static(pmb_force *f, const double *d_positions, double *d_forces,
+                                          double *d_energies, int virial) {
+  if (!f || !d_positions || !d_forces) return fail(PMB_ERR_ARG, "null argument");
+  if (f->kind != PMB_FORCE_CUTOFF)
+    return fail(PMB_ERR_UNSUPPORTED, "pmb_cutoff_evaluate_static evaluates NonbondedCutoff forces only");
+  pmb_system *s = f->sys;
+  if (s->nbox > PMB_STATIC_MAX_BOXES)
+    return fail(PMB_ERR_CAPACITY, "pmb_cutoff_evaluate_static: " + std::to_string(s->nbox) +
+                                      " boxes exceed its static scratch of PMB_STATIC_MAX_BOXES = " +
+                                      std::to_string(PMB_STATIC_MAX_BOXES) + " boxes");
+  long long *eacc = nullptr;
+  CK(static_eacc_address(&eacc));
+  // the cutoff branch of pair_jobs, without its host vector
+  PairParams p = base_params(s, virial);
+  p.do_lj = f->d.lj;
+  p.coul_mode = f->d.coulomb ? 1 : 0;
+  p.lj_sw = make_switch(f->d.lj_switch, f->d.lj_switchon, f->d.lj_cutoff);
+  p.coul_sw = make_switch(f->d.coulomb_switch, f->d.coulomb_switchon, f->d.coulomb_cutoff);
+  p.lj_cut2 = f->d.lj_cutoff * f->d.lj_cutoff;
+  p.coul_cut2 = f->d.coulomb_cutoff * f->d.coulomb_cutoff;
+  const double rc = force_pair_cutoff(f);
+  p.cut2 = rc * rc;
+  int max_box_atoms = 0;
+  for (const BoxDev &b : s->hbox) max_box_atoms = std::max(max_box_atoms, b.natoms);
+  SystemDev sd = s->dev();
+  sd.eacc = eacc;
+  sd.facc = nullptr;
+  CK(pair_allpairs_launch(sd, p, s->d_lj, d_positions, d_forces, eacc, max_box_atoms, s->stream));
+  if (d_energies) {
+    energies_to_double(sd, nullptr, d_energies, s->stream);
+    CK(cudaGetLastError());
+  }
+  return PMB_OK;
+}

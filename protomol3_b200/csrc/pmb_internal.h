@@ -89,6 +89,15 @@ struct PairLaunch {
 };
 int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st);
 
+// Allocation-free all-pairs variant (FP64): energy/virial accumulators in a static device array
+// of STATIC_MAX_BOXES boxes.  static_eacc_address looks the array up once per device (current
+// device); pair_allpairs_launch zeroes s.nbox boxes of it on st, then writes fout [3 natoms].
+constexpr int STATIC_MAX_BOXES = 1024;
+cudaError_t static_eacc_address(long long **out);
+cudaError_t pair_allpairs_launch(const SystemDev &s, const PairParams &p, const double *ljd,
+                                 const double *pos, double *fout, long long *eacc,
+                                 int max_box_atoms, cudaStream_t st);
+
 // ------------------------------------------------------------------ PME (pme.cu)
 struct PmeBoxPlan {
   int n[3];

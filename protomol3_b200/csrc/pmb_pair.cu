@@ -28,6 +28,7 @@
 //   * mixed: positions as 32-bit fractional fixed point per box edge, so the minimal image is the
 //     wrap-around of an int32 difference and the pair vector keeps full FP32 precision however
 //     large the box; FP32 arithmetic with MUFU rsqrt/exp2/rcp.
+#include <mutex>
 #include <type_traits>
 
 #include "pmb_internal.h"
@@ -499,6 +500,127 @@ int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, c
   if (pl.p.ntypes > MAX_LJ_TYPES) return -1;
   if (pl.precision) return pl.p.virial ? launch_v<true, true>(s, nb, pl, st) : launch_v<true, false>(s, nb, pl, st);
   return pl.p.virial ? launch_v<false, true>(s, nb, pl, st) : launch_v<false, false>(s, nb, pl, st);
+}
+
+// ======================================================================= allocation-free variant
+// All-pairs FP64 variant of the cutoff pair kernel for callers that may not allocate device
+// memory: no neighbour list, every pair of a box visited from both sides (each thread sums the
+// full force on its own atom in registers and stores it, so forces need no accumulator and no
+// atomics); energies and the virial count each pair once (j > i) and are added in fixed point to
+// per-box accumulators that live in a static device array instead of the system's buffers.
+namespace {
+
+constexpr int AP_THREADS = 128;
+
+// Fixed-point energy / virial accumulators of the allocation-free pass,
+// [STATIC_MAX_BOXES][ACC_PER_BOX] int64 = 128 KiB.  Zeroed by every call before use.
+static __device__ __align__(256) long long g_static_eacc[STATIC_MAX_BOXES * ACC_PER_BOX];
+
+template <int CM, bool VIR>
+__global__ void __launch_bounds__(AP_THREADS)
+    k_pair_allpairs(SystemDev s, PairParams p, const double *ljd, const double *pos, double *fout,
+                    long long *eacc) {
+  __shared__ double4 sp[AP_THREADS];  // j-atoms of the tile: x, y, z, q
+  __shared__ int2 sm[AP_THREADS];     // molecule, type
+  const int b = blockIdx.y;
+  const BoxDev &bx = s.box[b];
+  const int n = bx.natoms;
+  if ((int)blockIdx.x * AP_THREADS >= n) return;  // whole block: no atom of this box left
+  const int li = blockIdx.x * AP_THREADS + threadIdx.x;
+  const bool valid = li < n;
+  const int i = bx.atom0 + (valid ? li : 0);
+  const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2], qi = s.charge[i];
+  const int mi = s.molecule[i], ti = s.type[i], nt = p.ntypes;
+  double fi[3] = {0.0, 0.0, 0.0}, elj = 0.0, ec = 0.0, vir[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int j0 = 0; j0 < n; j0 += AP_THREADS) {
+    __syncthreads();
+    const int lj = j0 + threadIdx.x;
+    if (lj < n) {
+      const int j = bx.atom0 + lj;
+      sp[threadIdx.x] = make_double4(pos[3 * j], pos[3 * j + 1], pos[3 * j + 2], s.charge[j]);
+      sm[threadIdx.x] = make_int2(s.molecule[j], s.type[j]);
+    }
+    __syncthreads();
+    const int nj = min(AP_THREADS, n - j0);
+    for (int k = 0; k < nj; k++) {
+      const double4 pj = sp[k];
+      const int2 mj = sm[k];
+      double dx = pj.x - xi, dy = pj.y - yi, dz = pj.z - zi;
+      // the reference's minimal image: d - L rint(d / L) equals its single-wrap result
+      dx -= bx.L[0] * rint(bx.Lr[0] * dx);
+      dy -= bx.L[1] * rint(bx.Lr[1] * dy);
+      dz -= bx.L[2] * rint(bx.Lr[2] * dz);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      bool in = valid && j0 + k != li && r2 <= p.cut2;
+      int ex = 0;
+      if (in && mj.x == mi) {
+        ex = excl_check(s, i, bx.atom0 + j0 + k);
+        if (ex == 2) in = false;
+      }
+      const double *ab = ljd + 4 * (ti * nt + mj.y) + (ex == 1 ? 2 : 0);
+      Acc<double> t;
+      t.elj = t.ec = 0.0;
+      const double fs = pair_force<false, SWR, CM, SWR>(p, in, ex, r2, qi * pj.w, double2{ab[0], ab[1]}, t);
+      const double fx = dx * fs, fy = dy * fs, fz = dz * fs;
+      fi[0] -= fx;
+      fi[1] -= fy;
+      fi[2] -= fz;
+      if (j0 + k > li) {
+        elj += t.elj;
+        ec += t.ec;
+        if constexpr (VIR) {
+          vir[0] += fx * dx; vir[1] += fx * dy; vir[2] += fx * dz;
+          vir[3] += fy * dy; vir[4] += fy * dz; vir[5] += fz * dz;
+        }
+      }
+    }
+  }
+  if (valid) {
+    fout[3 * i] = fi[0];
+    fout[3 * i + 1] = fi[1];
+    fout[3 * i + 2] = fi[2];
+  }
+  box_accumulate(eacc, b, valid, E_LJ, elj, nullptr);
+  box_accumulate(eacc, b, valid, E_COUL, ec, VIR ? vir : nullptr);
+}
+
+}  // namespace
+
+cudaError_t static_eacc_address(long long **out) {
+  constexpr int MAX_DEV = 64;
+  static std::mutex mu;
+  static long long *addr[MAX_DEV] = {};
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_eacc);
+    if (e != cudaSuccess) return e;
+    addr[dev] = static_cast<long long *>(p);
+  }
+  *out = addr[dev];
+  return cudaSuccess;
+}
+
+cudaError_t pair_allpairs_launch(const SystemDev &s, const PairParams &p, const double *ljd,
+                                 const double *pos, double *fout, long long *eacc,
+                                 int max_box_atoms, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(eacc, 0, sizeof(long long) * ACC_PER_BOX * s.nbox, st);
+  if (e != cudaSuccess) return e;
+  if (max_box_atoms > 0) {
+    dim3 grid((max_box_atoms + AP_THREADS - 1) / AP_THREADS, s.nbox);
+    if (p.coul_mode == 1) {
+      if (p.virial) k_pair_allpairs<1, true><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
+      else k_pair_allpairs<1, false><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
+    } else {
+      if (p.virial) k_pair_allpairs<0, true><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
+      else k_pair_allpairs<0, false><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
+    }
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace pmb
