@@ -850,7 +850,7 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
       // z-lines in groups of 16 consecutive y (8 packed complex lines per CTA)
       for (int x = 0; x < pl.n[0]; x++)
         for (int y0 = 0; y0 < pl.n[1]; y0 += 16) zwork.push_back(make_int4(bi, x, y0, std::min(16, pl.n[1] - y0)));
-      const int rows = std::max(1, std::min(32, lcap / pl.n[1])), cols = std::max(1, std::min(32, lcap / pl.n[0]));
+      const int rows = std::max(1, std::min(16, lcap / pl.n[1])), cols = std::max(1, std::min(16, lcap / pl.n[0]));
       for (int kz = 0; kz <= pl.n[2] / 2; kz++) {
         for (int x0 = 0; x0 < pl.n[0]; x0 += rows) ywork.push_back(make_int4(bi, kz, x0, std::min(rows, pl.n[0] - x0)));
         for (int y0 = 0; y0 < pl.n[1]; y0 += cols) xwork.push_back(make_int4(bi, kz, y0, std::min(cols, pl.n[1] - y0)));

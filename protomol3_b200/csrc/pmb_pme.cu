@@ -8,8 +8,10 @@
 //   k_spread      one thread per atom slot, B-spline weights, 64 int64 fixed-point atomics
 //   k_fft_z_fwd   z-lines of the fixed-point grid (cleared as it is read), two real lines packed
 //                 per complex FFT, half spectrum written as [kz][x][y]
-//   k_fft_plane   one CTA per (box, kz) plane in shared memory: forward FFT along y and x,
-//                 influence function multiply with energy and virial, inverse along x and y
+//   k_fft_y       y-lines of the half spectrum (groups of up to 16 rows of one kz plane)
+//   k_fft_x_infl  x-lines (groups of up to 16 columns): forward FFT, influence function multiply
+//                 with energy and virial partials, inverse FFT
+//   k_fft_y       inverse y-lines
 //   k_fft_z_inv   inverse z transform back to the real potential grid [x][y][z]
 //   k_gather      one thread per atom slot, 64-point stencil, fixed-point force atomics
 //   k_pme_energy  fixed-order sum of the per-plane partials into the box accumulators
@@ -87,63 +89,57 @@ __device__ __forceinline__ void dft_small(T2 *v, int sign) {
   }
 }
 
-// One Stockham stage, in place: every thread first reads all of its butterfly inputs into
-// registers, the CTA synchronises, then the outputs are written (so no ping-pong buffer).
-template <int R, int THREADS, int MAXE, typename T2>
-__device__ __forceinline__ void fft_stage(T2 *buf, int n, int nlines, int lstride, int estride,
-                                          int Ns, const T2 *tw, int sign) {
-  constexpr int MB = (MAXE + R * THREADS - 1) / (R * THREADS);
+// One Stockham stage, out of place (src -> dst): each thread takes whole butterflies (R inputs
+// read, twiddled, transformed and written), so only R values are live at a time.
+template <int R, typename T2>
+__device__ __forceinline__ void fft_stage(const T2 *__restrict__ src, T2 *__restrict__ dst, int n,
+                                          int nlines, int lstride, int estride, int Ns,
+                                          const T2 *tw, int sign) {
   const int nb = n / R, total = nb * nlines, step = n / (Ns * R);
-  T2 v[MB][R];
+  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+    // contiguous lines: consecutive threads take consecutive butterflies of one line;
+    // strided lines: consecutive threads take the same butterfly of consecutive lines
+    const int line = estride == 1 ? b / nb : b % nlines, j = estride == 1 ? b % nb : b / nlines;
+    const T2 *Ls = src + line * lstride;
+    T2 *Ld = dst + line * lstride;
+    T2 v[R];
 #pragma unroll
-  for (int mb = 0; mb < MB; mb++) {
-    int b = threadIdx.x + mb * THREADS;
-    if (b < total) {
-      // contiguous lines: consecutive threads take consecutive butterflies of one line;
-      // strided lines: consecutive threads take the same butterfly of consecutive lines
-      int line = estride == 1 ? b / nb : b % nlines, j = estride == 1 ? b % nb : b / nlines;
-      T2 *L = buf + line * lstride;
+    for (int r = 0; r < R; r++) v[r] = Ls[(j + r * nb) * estride];
+    const int k = j % Ns;
 #pragma unroll
-      for (int r = 0; r < R; r++) v[mb][r] = L[(j + r * nb) * estride];
+    for (int r = 1; r < R; r++) {
+      T2 w = tw[r * k * step];
+      if (sign > 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
     }
-  }
-  __syncthreads();
+    dft_small<R>(v, sign);
+    const int out = (j / Ns) * Ns * R + k;
 #pragma unroll
-  for (int mb = 0; mb < MB; mb++) {
-    int b = threadIdx.x + mb * THREADS;
-    if (b < total) {
-      int line = estride == 1 ? b / nb : b % nlines, j = estride == 1 ? b % nb : b / nlines;
-      int k = j % Ns;
-#pragma unroll
-      for (int r = 1; r < R; r++) {
-        T2 w = tw[r * k * step];
-        if (sign > 0) w.y = -w.y;
-        v[mb][r] = cmul(v[mb][r], w);
-      }
-      dft_small<R>(v[mb], sign);
-      int out = (j / Ns) * Ns * R + k;
-      T2 *L = buf + line * lstride;
-#pragma unroll
-      for (int r = 0; r < R; r++) L[(out + r * Ns) * estride] = v[mb][r];
-    }
+    for (int r = 0; r < R; r++) Ld[(out + r * Ns) * estride] = v[r];
   }
   __syncthreads();
 }
 
 // Batched 1-D FFTs of length n over shared memory (element e of line l at
-// buf[l*lstride + e*estride]); radices[0..nrad) multiply to n.
-template <int THREADS, int MAXE, typename T2>
-__device__ void fft_lines(T2 *buf, int n, int nlines, int lstride, int estride, const int *radices,
-                          int nrad, const T2 *tw, int sign) {
+// buf[l*lstride + e*estride]); radices[0..nrad) multiply to n.  Stages alternate between buf
+// and tmp (same layout); returns the buffer holding the result.
+template <typename T2>
+__device__ T2 *fft_lines(T2 *buf, T2 *tmp, int n, int nlines, int lstride, int estride,
+                         const int *radices, int nrad, const T2 *tw, int sign) {
   int Ns = 1;
+  T2 *src = buf, *dst = tmp;
   for (int s = 0; s < nrad; s++) {
-    int R = radices[s];
-    if (R == 4) fft_stage<4, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
-    else if (R == 2) fft_stage<2, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
-    else if (R == 3) fft_stage<3, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
-    else fft_stage<5, THREADS, MAXE>(buf, n, nlines, lstride, estride, Ns, tw, sign);
+    const int R = radices[s];
+    if (R == 4) fft_stage<4>(src, dst, n, nlines, lstride, estride, Ns, tw, sign);
+    else if (R == 2) fft_stage<2>(src, dst, n, nlines, lstride, estride, Ns, tw, sign);
+    else if (R == 3) fft_stage<3>(src, dst, n, nlines, lstride, estride, Ns, tw, sign);
+    else fft_stage<5>(src, dst, n, nlines, lstride, estride, Ns, tw, sign);
     Ns *= R;
+    T2 *t = src;
+    src = dst;
+    dst = t;
   }
+  return src;
 }
 
 // B-spline weights of order P at w (BSpline::set, BSpline.cpp:55-105).
@@ -157,19 +153,23 @@ __device__ __forceinline__ void bspline(int P, T w, T *th, T *dth) {
   th[P - 1] = T(0);
   th[1] = w;
   th[0] = T(1) - w;
+  #pragma unroll
   for (int k = 2; k < P - 1; k++) {
     T div = T(1) / T(k);
     th[k] = div * w * th[k - 1];
+    #pragma unroll
     for (int j = 1; j < k; j++)
       th[k - j] = div * ((w + T(j)) * th[k - j - 1] + (T(k + 1 - j) - w) * th[k - j]);
     th[0] = div * (T(1) - w) * th[0];
   }
   if (dth) {
     dth[0] = -th[0];
+    #pragma unroll
     for (int j = 1; j <= P - 1; j++) dth[j] = th[j - 1] - th[j];
   }
   T div = T(1) / (T(P) - T(1));
   th[P - 1] = div * w * th[P - 2];
+  #pragma unroll
   for (int j = 1; j < P - 1; j++)
     th[P - 1 - j] = div * ((w + T(j)) * th[P - j - 2] + (T(P - j) - w) * th[P - 1 - j]);
   th[0] = div * (T(1) - w) * th[0];
@@ -200,7 +200,8 @@ __device__ __forceinline__ void grid_coord(unsigned fx, double x, double hr, int
   base = iu - (P - 1) / 2 + n;  // myNXOffset = -(order-1)/2 + n
 }
 
-template <bool MIXED>
+// PC > 0: interpolation order fixed at compile time (weights stay in registers); PC = 0: run time.
+template <bool MIXED, int PC>
 __global__ void k_spread(NbListDev nb, PmeDev pm) {
   using T = typename std::conditional<MIXED, float, double>::type;
   int sl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,7 +209,7 @@ __global__ void k_spread(NbListDev nb, PmeDev pm) {
   int4 m = nb.slot_meta[sl];
   if (m.x < 0) return;
   const PmeBoxPlan &pl = pm.plan[m.w];
-  const int P = pm.order;
+  const int P = PC > 0 ? PC : pm.order;
   T th[3][MAXP];
   int base[3];
   T q;
@@ -235,13 +236,16 @@ __global__ void k_spread(NbListDev nb, PmeDev pm) {
   }
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
   long long *g = pm.qgrid + pl.grid0;
+  #pragma unroll
   for (int i = 0; i < P; i++) {
     T a = q * th[0][i];
     int i1 = (i + base[0]) % nx;
+    #pragma unroll
     for (int j = 0; j < P; j++) {
       T ab = a * th[1][j];
       int j1 = (j + base[1]) % ny;
       long long *row = g + ((long long)i1 * ny + j1) * nz;
+      #pragma unroll
       for (int k = 0; k < P; k++) {
         int k1 = (k + base[2]) % nz;
         long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
@@ -251,7 +255,7 @@ __global__ void k_spread(NbListDev nb, PmeDev pm) {
   }
 }
 
-template <bool MIXED>
+template <bool MIXED, int PC>
 __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   using T = typename std::conditional<MIXED, float, double>::type;
   int sl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -259,7 +263,7 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   int4 m = nb.slot_meta[sl];
   if (m.x < 0) return;
   const PmeBoxPlan &pl = pm.plan[m.w];
-  const int P = pm.order;
+  const int P = PC > 0 ? PC : pm.order;
   T th[3][MAXP], dth[3][MAXP];
   int base[3];
   T q;
@@ -287,12 +291,15 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
   const T *g = reinterpret_cast<const T *>(pm.rgrid) + pl.grid0;
   T fx = 0, fy = 0, fz = 0;
+  #pragma unroll
   for (int i = 0; i < P; i++) {
     int i1 = (i + base[0]) % nx;
+    #pragma unroll
     for (int j = 0; j < P; j++) {
       int j1 = (j + base[1]) % ny;
       T xij = dth[0][i] * th[1][j], yij = th[0][i] * dth[1][j], zij = th[0][i] * th[1][j];
       const T *row = g + ((long long)i1 * ny + j1) * nz;
+      #pragma unroll
       for (int k = 0; k < P; k++) {
         int k1 = (k + base[2]) % nz;
         T term = row[k1];
@@ -308,19 +315,19 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   red_add(f + 2, f2fix((double)(fz * T(pl.hr[2]) * q), FORCE_SCALE));
 }
 
-constexpr int ZT = 256;          // threads of the z-line kernels
-constexpr int ZMAXE = 16 * 256;  // 16 packed line pairs x nz <= 256
+constexpr int ZT = 128;         // threads of the z-line kernels
+constexpr int ZMAXE = 8 * 256;  // 8 packed line pairs x nz <= 256, per ping-pong buffer
 
 template <typename T>
-__global__ void __launch_bounds__(ZT) k_fft_z_fwd(PmeDev pm) {
+__global__ void __launch_bounds__(ZT, 8) k_fft_z_fwd(PmeDev pm) {
   using T2 = typename C2<T>::t;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 wk = pm.zwork[blockIdx.x];
   const PmeBoxPlan &pl = pm.plan[wk.x];
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], x = wk.y, y0 = wk.z, cnt = wk.w;
   const int npair = (cnt + 1) / 2;
   T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + nz;
+  T2 *buf = tw + 256, *tmp = buf + ZMAXE;
   for (int k = threadIdx.x; k < nz; k += ZT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[2] + k];
     else tw[k] = pm.twiddle[pl.tw0[2] + k];
@@ -338,12 +345,12 @@ __global__ void __launch_bounds__(ZT) k_fft_z_fwd(PmeDev pm) {
     dst[line & 1] = v;
   }
   __syncthreads();
-  fft_lines<ZT, ZMAXE>(buf, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, -1);
+  const T2 *res = fft_lines(buf, tmp, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, -1);
   const int nh = nz / 2 + 1;
   T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0;
   for (int e = threadIdx.x; e < npair * nh; e += ZT) {
     int pi = e % npair, k = e / npair;
-    T2 zk = buf[pi * nz + k], zn = buf[pi * nz + (nz - k) % nz];
+    T2 zk = res[pi * nz + k], zn = res[pi * nz + (nz - k) % nz];
     // X = (Z_k + conj(Z_{n-k})) / 2, Y = -i/2 (Z_k - conj(Z_{n-k}))
     T2 X = cmk(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
     T2 Y = cmk(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
@@ -354,15 +361,15 @@ __global__ void __launch_bounds__(ZT) k_fft_z_fwd(PmeDev pm) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(ZT) k_fft_z_inv(PmeDev pm) {
+__global__ void __launch_bounds__(ZT, 8) k_fft_z_inv(PmeDev pm) {
   using T2 = typename C2<T>::t;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 wk = pm.zwork[blockIdx.x];
   const PmeBoxPlan &pl = pm.plan[wk.x];
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], x = wk.y, y0 = wk.z, cnt = wk.w;
   const int npair = (cnt + 1) / 2, nh = nz / 2 + 1;
   T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + nz;
+  T2 *buf = tw + 256, *tmp = buf + ZMAXE;
   for (int k = threadIdx.x; k < nz; k += ZT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[2] + k];
     else tw[k] = pm.twiddle[pl.tw0[2] + k];
@@ -381,11 +388,11 @@ __global__ void __launch_bounds__(ZT) k_fft_z_inv(PmeDev pm) {
     if (k > 0 && 2 * k != nz) buf[pi * nz + nz - k] = cmk(X.x + Y.y, Y.x - X.y);
   }
   __syncthreads();
-  fft_lines<ZT, ZMAXE>(buf, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, +1);
+  const T2 *res = fft_lines(buf, tmp, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, +1);
   T *R = reinterpret_cast<T *>(pm.rgrid) + pl.grid0 + ((long long)x * ny + y0) * nz;
   for (int e = threadIdx.x; e < cnt * nz; e += ZT) {
     int line = e / nz, z = e % nz;
-    T2 v = buf[(line >> 1) * nz + z];
+    T2 v = res[(line >> 1) * nz + z];
     R[(long long)line * nz + z] = (line & 1) ? v.y : v.x;
   }
 }
@@ -404,19 +411,19 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
   return r;
 }
 
-constexpr int LT = 256;          // threads of the y- and x-line kernels
-constexpr int LMAXE = 4096;      // complex elements per line-kernel CTA
+constexpr int LT = 128;          // threads of the y- and x-line kernels
+constexpr int LMAXE = 2048;      // complex elements per line-kernel CTA, per ping-pong buffer
 
 // y-lines of the half spectrum: rows C[kz][x][0..ny) of one work item are contiguous.
 template <typename T>
-__global__ void __launch_bounds__(LT) k_fft_y(PmeDev pm, int sign) {
+__global__ void __launch_bounds__(LT, 8) k_fft_y(PmeDev pm, int sign) {
   using T2 = typename C2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 wk = pm.ywork[blockIdx.x];  // box, kz, x0, rows
   const PmeBoxPlan &pl = pm.plan[wk.x];
   const int nx = pl.n[0], ny = pl.n[1], kz = wk.y, x0 = wk.z, rows = wk.w;
-  T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + ny;
+  T2 *tw = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
+  T2 *buf = tw + 256, *tmp = buf + LMAXE;
   for (int k = threadIdx.x; k < ny; k += LT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[1] + k];
     else tw[k] = pm.twiddle[pl.tw0[1] + k];
@@ -425,14 +432,14 @@ __global__ void __launch_bounds__(LT) k_fft_y(PmeDev pm, int sign) {
   const int ne = rows * ny;
   for (int e = threadIdx.x; e < ne; e += LT) buf[e] = C[e];
   __syncthreads();
-  fft_lines<LT, LMAXE>(buf, ny, rows, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], tw, sign);
-  for (int e = threadIdx.x; e < ne; e += LT) C[e] = buf[e];
+  const T2 *res = fft_lines(buf, tmp, ny, rows, ny, 1, pm.radix + pl.rad0[1], pl.nrad[1], tw, sign);
+  for (int e = threadIdx.x; e < ne; e += LT) C[e] = res[e];
 }
 
 // x-lines (columns y0..y0+cols of one kz plane): forward FFT, influence function with energy and
 // virial (Grid.h:236-341, half spectrum kz <= nz/2 with the doubling of interior kz), inverse FFT.
 template <typename T>
-__global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
+__global__ void __launch_bounds__(LT, 8) k_fft_x_infl(PmeDev pm) {
   using T2 = typename C2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 wk = pm.xwork[blockIdx.x];  // box, kz, y0, cols
@@ -440,7 +447,7 @@ __global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], kz = wk.y, y0 = wk.z, cols = wk.w;
   double *red = reinterpret_cast<double *>(smem_raw);  // 32 doubles
   T2 *tw = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
-  T2 *buf = tw + nx;  // buf[x * cols + c]
+  T2 *buf = tw + 256, *tmp = buf + LMAXE;  // buf[x * cols + c]
   for (int k = threadIdx.x; k < nx; k += LT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[0] + k];
     else tw[k] = pm.twiddle[pl.tw0[0] + k];
@@ -452,7 +459,8 @@ __global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
     buf[e] = C[(long long)x * ny + c];
   }
   __syncthreads();
-  fft_lines<LT, LMAXE>(buf, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, -1);
+  T2 *spec = fft_lines(buf, tmp, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, -1);
+  T2 *other = spec == buf ? tmp : buf;
   const double *bxt = pm.infl + pl.inf0[0], *byt = pm.infl + pl.inf0[1], *bzt = pm.infl + pl.inf0[2];
   const double mk = kz * pl.mr[2];
   const double wz = (kz > 0 && ((2 * kz != nz) || (nz & 1))) ? 2.0 : 1.0;
@@ -460,14 +468,14 @@ __global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
   for (int e = threadIdx.x; e < ne; e += LT) {
     int i = e / cols, j = y0 + e % cols;
     if (i == 0 && j == 0 && kz == 0) {
-      buf[e] = cmk(T(0), T(0));
+      spec[e] = cmk(T(0), T(0));
       continue;
     }
     int i0 = i <= nx / 2 ? i : i - nx, j0 = j <= ny / 2 ? j : j - ny;
     double mi = i0 * pl.mr[0], mj = j0 * pl.mr[1];
     double m2 = mi * mi + mj * mj + mk * mk;
     double theta = bxt[i] * byt[j] * bzt[kz] * pl.piVr / m2;
-    T2 c = buf[e];
+    T2 c = spec[e];
     double qq = (double)c.x * (double)c.x + (double)c.y * (double)c.y;
     double ee = wz * qq * theta;
     en += ee;
@@ -476,7 +484,7 @@ __global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
       vxx += ee * (1.0 - v * mi * mi); vxy -= ee * (v * mi * mj); vxz -= ee * (v * mi * mk);
       vyy += ee * (1.0 - v * mj * mj); vyz -= ee * (v * mj * mk); vzz += ee * (1.0 - v * mk * mk);
     }
-    buf[e] = cmk(c.x * T(theta), c.y * T(theta));
+    spec[e] = cmk(c.x * T(theta), c.y * T(theta));
   }
   double part[7] = {en, vxx, vxy, vxz, vyy, vyz, vzz};
   const int np = pm.virial ? 7 : 1;
@@ -485,10 +493,10 @@ __global__ void __launch_bounds__(LT) k_fft_x_infl(PmeDev pm) {
     if (threadIdx.x == 0) pm.plane_part[(long long)blockIdx.x * 8 + c] = r;
   }
   __syncthreads();
-  fft_lines<LT, LMAXE>(buf, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, +1);
+  const T2 *res = fft_lines(spec, other, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, +1);
   for (int e = threadIdx.x; e < ne; e += LT) {
     int x = e / cols, c = e % cols;
-    C[(long long)x * ny + c] = buf[e];
+    C[(long long)x * ny + c] = res[e];
   }
 }
 
@@ -556,9 +564,10 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   using T2 = typename C2<T>::t;
   const int TB = 256;
   constexpr bool MIXED = sizeof(T) == 4;
-  k_spread<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
+  if (pm.order == 4) k_spread<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
+  else k_spread<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
   if (mark) mark(mctx, "pme_spread");
-  size_t zsmem = sizeof(T2) * (256 + ZMAXE);
+  size_t zsmem = sizeof(T2) * (256 + 2 * (size_t)ZMAXE);
   static bool zconf = false;
   if (!zconf) {
     cudaFuncSetAttribute(k_fft_z_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
@@ -566,7 +575,7 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     zconf = true;
   }
   k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
-  const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + (size_t)LMAXE);
+  const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)LMAXE);
   static bool lconf = false;
   if (!lconf) {
     cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
@@ -578,7 +587,8 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, +1);
   k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   if (mark) mark(mctx, "pme_fft");
-  k_gather<MIXED><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
+  if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
+  else k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   if (mark) mark(mctx, "pme_gather");
   k_pme_energy<<<(pm.nbox * 32 + 127) / 128, 128, 0, st>>>(s, pm);
   if (mark) mark(mctx, "pme_energy");

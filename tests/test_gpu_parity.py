@@ -89,6 +89,23 @@ def test_pme_vs_oracle(precision, nw, grid, rc):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("grid,order", [((25, 18, 32), 6), ((27, 16, 30), 8)])
+def test_pme_anisotropic_grid_and_order(precision, grid, order):
+    """Grid lengths of pure radix 5, 3 and 2 in different dimensions and interpolation orders
+    other than 4 (the generic spread/gather instance)."""
+    b = W.water_box(216, seed=11)
+    pme = F.NonbondedPMEwaldSystemForce(grid, 8.0, order=order)
+    f, e, topo = gpu_eval(b, [pme], precision, virial=True)
+    fo, eo, vo, info = O.evaluate(O.System(b), b["pos"], pme=O.pme_params(grid, 8.0, order=order),
+                                  virial=True)
+    assert rel_rms(f, fo) < TOL[precision]
+    real, recip = info["terms"][0], info["terms"][1]
+    assert energy_ok(e[F.ScalarStructure.COULOMB], eo[O.E_COULOMB], abs(real) + abs(recip),
+                     precision, topo.n_atoms)
+    np.testing.assert_allclose(e.virial().ravel(), vo, rtol=0, atol=TOL[precision] * np.abs(vo).max() * 10)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_lj_plus_pme_fused(precision):
     """LJ C2 8->10 with PME real space 10 A, the config-2 force set, on a 1,000-water box."""
     b = W.water_box(1000, seed=9)

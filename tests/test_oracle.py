@@ -73,11 +73,12 @@ needs_ref = pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not bu
 
 
 @needs_ref
-@pytest.mark.parametrize("nw,grid,rc", [(216, 20, 8.0), (60, 12, 9.0)])
-def test_oracle_matches_reference_pme(nw, grid, rc):
+@pytest.mark.parametrize("nw,grid,rc,order", [(216, (20,) * 3, 8.0, 4), (60, (12,) * 3, 9.0, 4),
+                                              (216, (25, 18, 32), 8.0, 6), (216, (27, 16, 30), 8.0, 8)])
+def test_oracle_matches_reference_pme(nw, grid, rc, order):
     b = W.water_box(nw, seed=11)
     s = O.System(b)
-    pm = O.pme_params((grid,) * 3, rc)
+    pm = O.pme_params(grid, rc, order=order)
     f, e, v, _ = O.evaluate(s, b["pos"], pme=pm, virial=True)
     fr, er, vr = O.ref_evaluate(s, b["pos"], pme=pm, virial=True)
     assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) < 1e-12
