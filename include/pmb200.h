@@ -134,7 +134,8 @@ int pmb_force_evaluate(pmb_force *f, const double *positions, double *forces, do
 int pmb_evaluate(pmb_system *sys, pmb_force *const *forces, int n_forces, const double *positions,
                  double *forces_out, double *energies, int virial);
 /* Same, with device pointers and no host synchronisation: d_forces and d_energies are
- * overwritten (not accumulated), on the system's stream. */
+ * overwritten (not accumulated), on the system's stream.  d_positions NULL reuses the positions
+ * of the last evaluation (PMB_ERR_STATE if there was none). */
 int pmb_evaluate_device(pmb_system *sys, pmb_force *const *forces, int n_forces,
                         const double *d_positions, double *d_forces, double *d_energies,
                         int virial);
@@ -158,10 +159,12 @@ int pmb_md_kernels_per_step(pmb_md *md, int *n);
 /* Diagnostics -------------------------------------------------------------------------------- */
 /* Runs the force set nrep times with CUDA events between pipeline stages (TimerStatistic /
  * DEBUG_PME_TIMING of the reference, as device times); flush_l2 writes a 256 MB buffer before
- * each repetition.  stage_ms[i] is the mean time of stage i, names receives the comma-separated
- * stage names. */
-int pmb_profile(pmb_system *sys, pmb_force *const *forces, int n_forces, int nrep, int flush_l2,
-                double *stage_ms, int max_stages, int *n_stages, char *names, int names_len);
+ * each repetition.  positions [3 N] (host) are uploaded first; NULL reuses the positions of the
+ * last evaluation (PMB_ERR_STATE if there was none).  stage_ms[i] is the mean time of stage i,
+ * names receives the comma-separated stage names. */
+int pmb_profile(pmb_system *sys, const double *positions, pmb_force *const *forces, int n_forces,
+                int nrep, int flush_l2, double *stage_ms, int max_stages, int *n_stages,
+                char *names, int names_len);
 /* Measured FP32 FMA issue rate of the device (TFLOP/s), the roofline of the pair kernel. */
 int pmb_fp32_peak(double *tflops);
 

@@ -185,6 +185,7 @@ struct pmb_system {
   BoxDev *d_box = nullptr;
   int *d_atom_box = nullptr, *d_type = nullptr, *d_mol = nullptr;
   double *d_pos = nullptr, *d_charge = nullptr, *d_mass = nullptr, *d_lj = nullptr;
+  bool have_pos = false;  // positions were uploaded at least once (evaluate, profile, set_state)
   int *d_excl_start = nullptr, *d_excl_partner = nullptr, *d_excl_kindc = nullptr;
   int *d_excl_pairs = nullptr, *d_excl_kind = nullptr;
   BondedDev bonded{};
@@ -923,8 +924,11 @@ int pmb_evaluate_device(pmb_system *s, pmb_force *const *fs, int n, const double
   for (int i = 0; i < n; i++)
     if (!fs[i] || fs[i]->sys != s) return fail(PMB_ERR_ARG, "force belongs to another system");
   cudaStream_t st = s->stream;
-  if (d_pos && d_pos != s->d_pos)
+  if (d_pos && d_pos != s->d_pos) {
     CK(cudaMemcpyAsync(s->d_pos, d_pos, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToDevice, st));
+    s->have_pos = true;
+  }
+  if (!s->have_pos) return fail(PMB_ERR_STATE, "no positions on the device yet: pass positions");
   SystemDev sd = s->dev();
   zero_accumulators(sd, st);
   int rc = enqueue_forces(s, fs, n, virial);
@@ -943,6 +947,7 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
   cudaStream_t st = s->stream;
   for (int attempt = 0; attempt < 3; attempt++) {
     CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, st));
+    s->have_pos = true;
     int rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
     if (rc) return rc;
     CK(cudaMemcpyAsync(s->h_fout, s->d_fout, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToHost, st));
@@ -974,11 +979,16 @@ int pmb_force_evaluate(pmb_force *f, const double *pos, double *forces, double *
   return pmb_evaluate(f->sys, &f, 1, pos, forces, energies, virial);
 }
 
-int pmb_profile(pmb_system *s, pmb_force *const *fs, int n, int nrep, int flush_l2, double *stage_ms,
-                int max_stages, int *n_stages, char *names, int names_len) {
+int pmb_profile(pmb_system *s, const double *pos, pmb_force *const *fs, int n, int nrep, int flush_l2,
+                double *stage_ms, int max_stages, int *n_stages, char *names, int names_len) {
   if (!s || (n > 0 && !fs) || nrep < 1 || !stage_ms || !n_stages)
     return fail(PMB_ERR_ARG, "null argument");
   cudaStream_t st = s->stream;
+  if (pos) {
+    CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, st));
+    s->have_pos = true;
+  }
+  if (!s->have_pos) return fail(PMB_ERR_STATE, "no positions on the device yet: pass positions");
   const size_t flush_bytes = 256ull << 20;  // twice the 126 MB L2
   if (flush_l2 && !s->flush_buf) CK(cudaMalloc(&s->flush_buf, flush_bytes));
   SystemDev sd = s->dev();
@@ -1158,6 +1168,7 @@ int pmb_md_set_state(pmb_md *m, const double *pos, const double *vel) {
   for (int i = 0; i < 3 * s->natoms; i++)
     if (!std::isfinite(pos[i]) || (vel && !std::isfinite(vel[i]))) return fail(PMB_ERR_NUMERIC, "non-finite state");
   CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
+  s->have_pos = true;
   if (vel) CK(cudaMemcpyAsync(m->d_vel, vel, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
   else CK(cudaMemsetAsync(m->d_vel, 0, sizeof(double) * 3 * s->natoms, s->stream));
   CK(cudaMemsetAsync(m->d_step, 0, sizeof(long long), s->stream));

@@ -52,9 +52,47 @@ __device__ __forceinline__ int excl_check(const SystemDev &s, int oi, int oj) {
   return 0;
 }
 
+// Pair parameters in the arithmetic type of the kernel, converted once on the host (the same
+// round-to-nearest conversion the device would do), so the inner loop reads FP32 constants
+// directly instead of converting FP64 parameters per pair.
+template <typename T>
+struct SwitchT {
+  int kind;
+  T rc2, ron2, s1, s2, s3, c15_1, c05_3, c15_3;
+};
+template <typename T>
+struct ParamsT {
+  int do_lj, ntypes;
+  int lj_all, coul_all;  // the LJ / Coulomb cutoff covers the pair rejection radius
+  SwitchT<T> lj_sw, coul_sw;
+  T cut2, lj_cut2, coul_cut2, alpha, a2pi, coulomb_scaling;
+};
+
+template <typename T>
+SwitchT<T> switch_t(const SwitchDev &w) {
+  SwitchT<T> o;
+  o.kind = w.kind;
+  o.rc2 = (T)w.rc2; o.ron2 = (T)w.ron2; o.s1 = (T)w.s1; o.s2 = (T)w.s2; o.s3 = (T)w.s3;
+  o.c15_1 = (T)w.c15_1; o.c05_3 = (T)w.c05_3; o.c15_3 = (T)w.c15_3;
+  return o;
+}
+template <typename T>
+ParamsT<T> params_t(const PairParams &p) {
+  ParamsT<T> o;
+  o.do_lj = p.do_lj;
+  o.ntypes = p.ntypes;
+  o.lj_all = p.lj_cut2 >= p.cut2;
+  o.coul_all = p.coul_cut2 >= p.cut2;
+  o.lj_sw = switch_t<T>(p.lj_sw);
+  o.coul_sw = switch_t<T>(p.coul_sw);
+  o.cut2 = (T)p.cut2; o.lj_cut2 = (T)p.lj_cut2; o.coul_cut2 = (T)p.coul_cut2;
+  o.alpha = (T)p.alpha; o.a2pi = (T)p.a2pi; o.coulomb_scaling = (T)p.coulomb_scaling;
+  return o;
+}
+
 // Switching function with compile-time kind K (SWR: run time).  value/derivative on r2 < rc2.
 template <int K, typename T>
-__device__ __forceinline__ void sw_apply(const SwitchDev &w, T r2, T &e, T &f) {
+__device__ __forceinline__ void sw_apply(const SwitchT<T> &w, T r2, T &e, T &f) {
   const int kind = K == SWR ? w.kind : K;
   if (kind == SW_C2) {
     T c2 = T(w.rc2) - r2;
@@ -102,7 +140,8 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // parameters (A = B = q = 0), so every term vanishes without output selects.
 template <bool MIXED, int LSW, int CM, int CSW>
 __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type pair_force(
-    const PairParams &p, bool in, int ex, typename std::conditional<MIXED, float, double>::type r2,
+    const ParamsT<typename std::conditional<MIXED, float, double>::type> &p, bool in, int ex,
+    typename std::conditional<MIXED, float, double>::type r2,
     typename std::conditional<MIXED, float, double>::type qq,
     typename std::conditional<MIXED, float2, double2>::type ab,
     Acc<typename std::conditional<MIXED, float, double>::type> &a) {
@@ -120,7 +159,7 @@ __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type
   if constexpr (LSW != NONE) {
     bool use = LSW != SWR || p.do_lj;
     if (use) {
-      const bool inl = in && (p.lj_cut2 >= p.cut2 || r2s <= T(p.lj_cut2));
+      const bool inl = in && (p.lj_all || r2s <= p.lj_cut2);
       const T A = inl ? ab.x : T(0), B = inl ? ab.y : T(0);
       T r6 = rd2 * rd2 * rd2, r12 = r6 * r6, r6B = B * r6, r12A = A * r12;
       T e = r12A - r6B;
@@ -131,7 +170,7 @@ __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type
     }
   }
   if constexpr (CM != 0) {
-    const bool inc = in && (p.coul_cut2 >= p.cut2 || r2s <= T(p.coul_cut2));
+    const bool inc = in && (p.coul_all || r2s <= p.coul_cut2);
     T q = inc ? qq : T(0);
     if (ex == 1) q *= T(p.coulomb_scaling);
     T e, f;
@@ -177,15 +216,21 @@ struct JStage<false> {
 
 template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI>
 __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 2)
-    k_pair(SystemDev s, NbListDev nb, PairParams p, const double *ljd, const double *lat) {
+    k_pair(SystemDev s, NbListDev nb, PairParams p,
+           ParamsT<typename std::conditional<MIXED, float, double>::type> pt, const double *ljd,
+           const double *lat) {
   using T = typename std::conditional<MIXED, float, double>::type;
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nt = p.ntypes, ntt = nt * nt;
   T2 *ljab = reinterpret_cast<T2 *>(smem_raw);  // [ntt] {A, B} then [ntt] {A14, B14}
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  JStage<MIXED> *stage = reinterpret_cast<JStage<MIXED> *>(smem_raw + ljbytes);
-  int *sorig_all = reinterpret_cast<int *>(stage + PAIR_WARPS * 32);
+  // j-atom staging as separate arrays (positions, metadata, original index): unit-stride
+  // element types, so the per-rotation loads of 32 distinct j-atoms are bank-conflict free
+  using JP = decltype(JStage<MIXED>::p);
+  JP *spos_all = reinterpret_cast<JP *>(smem_raw + ljbytes);
+  int2 *smeta_all = reinterpret_cast<int2 *>(spos_all + PAIR_WARPS * 32);
+  int *sorig_all = reinterpret_cast<int *>(smeta_all + PAIR_WARPS * 32);
   for (int k = threadIdx.x; k < ntt; k += blockDim.x) {
     ljab[k] = T2{T(ljd[4 * k]), T(ljd[4 * k + 1])};
     ljab[ntt + k] = T2{T(ljd[4 * k + 2]), T(ljd[4 * k + 3])};
@@ -194,7 +239,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int half = lane & 16, li = lane & 15;
-  JStage<MIXED> *sj = stage + wib * 32;
+  JP *sjp = spos_all + wib * 32;
+  int2 *sjm = smeta_all + wib * 32;
   int *sorig = sorig_all + wib * 32;
   const int gwarp = blockIdx.x * PAIR_WARPS + wib, nwarps = gridDim.x * PAIR_WARPS;
   int total = nb.tile_off[nb.nblk_total];
@@ -323,7 +369,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
       int jorig;
       stage_slot(jsl, mine, jorig);
       __syncwarp();
-      sj[lane] = mine;
+      sjp[lane] = mine.p;
+      sjm[lane] = mine.m;
       sorig[lane] = jorig;
       __syncwarp();
 
@@ -334,7 +381,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
       T fj[3] = {T(0), T(0), T(0)};
       const int tio = im.z * nt;
       const int nxt = half | ((li + 1) & 15);
-      const T cut2 = T(p.cut2);
+      const T cut2 = pt.cut2;
 
       const bool ivalid = im.x >= 0;
       auto body = [&](auto diag_tag, auto wrap_tag) {
@@ -343,7 +390,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
 #pragma unroll 2
         for (int st = 0; st < 16; st++) {
           const int jl = (li + st) & 15;
-          const JStage<MIXED> dj = sj[half | jl];
+          JStage<MIXED> dj;
+          dj.p = sjp[half | jl];
+          dj.m = sjm[half | jl];
           T dx = T(dj.p.x) - xi, dy = T(dj.p.y) - yi, dz = T(dj.p.z) - zi;
           if constexpr (!MIXED) {
             // the reference's minimal image: d - L rint(d / L) equals its single-wrap result
@@ -367,7 +416,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
           T2 ab;
           if constexpr (LSW != NONE) ab = ljab[(ex == 1 ? ntt : 0) + tio + dj.m.y];
           else ab = T2{T(0), T(0)};
-          T fs = pair_force<MIXED, LSW, CM, CSW>(p, in, ex, r2, qi * T(dj.p.w), ab, a);
+          T fs = pair_force<MIXED, LSW, CM, CSW>(pt, in, ex, r2, qi * T(dj.p.w), ab, a);
           T fx = dx * fs, fy = dy * fs, fz = dz * fs;
           if constexpr (VIR) {
             a.vir[0] += fx * dx; a.vir[1] += fx * dy; a.vir[2] += fx * dz;
@@ -384,11 +433,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
                 const double *lv = lat + 3 * (bx->lat0 + kk);
                 T rx = dx + T(lv[0]), ry = dy + T(lv[1]), rz = dz + T(lv[2]);
                 T rr2 = rx * rx + ry * ry + rz * rz;
-                bool inl = pv && rr2 <= T(p.coul_cut2);
+                bool inl = pv && rr2 <= pt.coul_cut2;
                 Acc<T> b2;
                 b2.elj = T(0);
                 b2.ec = T(0);
-                T g = pair_force<MIXED, NONE, 2, CSW>(p, inl, 0, rr2, qi * T(dj.p.w), T2{T(0), T(0)}, b2);
+                T g = pair_force<MIXED, NONE, 2, CSW>(pt, inl, 0, rr2, qi * T(dj.p.w), T2{T(0), T(0)}, b2);
                 a.ec += b2.ec;
                 T gx = rx * g, gy = ry * g, gz = rz * g;
                 fx += gx; fy += gy; fz += gz;
@@ -458,7 +507,7 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
   const int ntt = pl.p.ntypes * pl.p.ntypes;
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  size_t smem = ljbytes + PAIR_WARPS * 32 * (sizeof(JStage<MIXED>) + sizeof(int));
+  size_t smem = ljbytes + PAIR_WARPS * 32 * (sizeof(decltype(JStage<MIXED>::p)) + sizeof(int2) + sizeof(int));
   static int grid = 0;
   static size_t conf_smem = 0;
   if (!grid || conf_smem != smem) {
@@ -472,7 +521,8 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
     grid = nsm * occ;
     conf_smem = smem;
   }
-  kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, pl.lj, pl.lattice);
+  using T = typename std::conditional<MIXED, float, double>::type;
+  kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, params_t<T>(pl.p), pl.lj, pl.lattice);
   return 0;
 }
 
@@ -518,7 +568,7 @@ static __device__ __align__(256) long long g_static_eacc[STATIC_MAX_BOXES * ACC_
 
 template <int CM, bool VIR>
 __global__ void __launch_bounds__(AP_THREADS)
-    k_pair_allpairs(SystemDev s, PairParams p, const double *ljd, const double *pos, double *fout,
+    k_pair_allpairs(SystemDev s, ParamsT<double> p, const double *ljd, const double *pos, double *fout,
                     long long *eacc) {
   __shared__ double4 sp[AP_THREADS];  // j-atoms of the tile: x, y, z, q
   __shared__ int2 sm[AP_THREADS];     // molecule, type
@@ -611,13 +661,14 @@ cudaError_t pair_allpairs_launch(const SystemDev &s, const PairParams &p, const 
   cudaError_t e = cudaMemsetAsync(eacc, 0, sizeof(long long) * ACC_PER_BOX * s.nbox, st);
   if (e != cudaSuccess) return e;
   if (max_box_atoms > 0) {
+    const ParamsT<double> pd = params_t<double>(p);
     dim3 grid((max_box_atoms + AP_THREADS - 1) / AP_THREADS, s.nbox);
     if (p.coul_mode == 1) {
-      if (p.virial) k_pair_allpairs<1, true><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
-      else k_pair_allpairs<1, false><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
+      if (p.virial) k_pair_allpairs<1, true><<<grid, AP_THREADS, 0, st>>>(s, pd, ljd, pos, fout, eacc);
+      else k_pair_allpairs<1, false><<<grid, AP_THREADS, 0, st>>>(s, pd, ljd, pos, fout, eacc);
     } else {
-      if (p.virial) k_pair_allpairs<0, true><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
-      else k_pair_allpairs<0, false><<<grid, AP_THREADS, 0, st>>>(s, p, ljd, pos, fout, eacc);
+      if (p.virial) k_pair_allpairs<0, true><<<grid, AP_THREADS, 0, st>>>(s, pd, ljd, pos, fout, eacc);
+      else k_pair_allpairs<0, false><<<grid, AP_THREADS, 0, st>>>(s, pd, ljd, pos, fout, eacc);
     }
   }
   return cudaGetLastError();

@@ -237,14 +237,21 @@ def evaluate_all(topo, force_list, positions, forces, energies):
         forces[:] = f
 
 
-def profile(topo, force_list, nrep=10, flush_l2=True):
-    """Mean device time (ms) per pipeline stage of ``force_list``, measured with CUDA events."""
+def profile(topo, force_list, positions=None, nrep=10, flush_l2=True):
+    """Mean device time (ms) per pipeline stage of ``force_list``, measured with CUDA events.
+    ``positions`` (N, 3) are uploaded first; None reuses those of the last evaluation."""
     hs = (C.c_void_p * len(force_list))(*[f.handle(topo) for f in force_list])
     ms = np.zeros(32)
     n = C.c_int(0)
     names = C.create_string_buffer(1024)
-    L.check(L.lib().pmb_profile(topo.system(), C.cast(hs, C.c_void_p), len(force_list), int(nrep),
-                                int(flush_l2), _p(ms), 32, C.byref(n), names, 1024))
+    pos = None
+    if positions is not None:
+        pos = np.ascontiguousarray(positions, np.float64)
+        if pos.shape != (topo.n_atoms, 3):
+            raise ValueError("positions must be (%d, 3)" % topo.n_atoms)
+    L.check(L.lib().pmb_profile(topo.system(), _p(pos) if pos is not None else None,
+                                C.cast(hs, C.c_void_p), len(force_list), int(nrep), int(flush_l2),
+                                _p(ms), 32, C.byref(n), names, 1024))
     return dict(zip(names.value.decode().split(","), ms[:n.value].tolist()))
 
 

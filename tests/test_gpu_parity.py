@@ -236,3 +236,20 @@ def test_list_reuse_with_skin_matches_rebuild_every_step(precision):
     tol = 1e-9 if precision == "fp64" else 2e-3
     assert np.abs(p1 - p0).max() < tol
     assert rel_rms(f1, f0) < (1e-9 if precision == "fp64" else 1e-3)
+
+
+def test_profile_needs_positions():
+    """pmb_profile on a system that never received positions is an error, not a silent run on
+    uninitialised device memory; with positions it reports every pipeline stage."""
+    from protomol3_b200 import _lib as L
+    b = W.water_box(216, seed=4)
+    topo = F.Topology(b, "mixed")
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
+          F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0), F.BondedSystemForce()]
+    with pytest.raises(L.PMBError) as err:
+        F.profile(topo, fl, nrep=2)
+    assert err.value.code == L.PMB_ERR_STATE
+    st = F.profile(topo, fl, positions=topo.positions(), nrep=2)
+    for stage in ("nblist", "pair", "pme_spread", "pme_fft", "pme_gather", "bonded"):
+        assert stage in st and st[stage] >= 0.0
+
