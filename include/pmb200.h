@@ -118,6 +118,11 @@ int pmb_system_n_boxes(const pmb_system *sys);
  * every evaluation like Topology::updateCellLists.  The pair set evaluated is the same either
  * way (every pair within the cutoff). */
 int pmb_system_set_skin(pmb_system *sys, double skin);
+/* Waits for the system's stream and reports whether a neighbour list overflowed since the last
+ * check: PMB_ERR_CAPACITY, with the list storage enlarged so that the next evaluation fits.  The
+ * host-pointer entry points check by themselves and retry; pmb_evaluate_device does not
+ * synchronise, so its callers call this after their evaluations and repeat one that overflowed. */
+int pmb_system_check(pmb_system *sys);
 
 /* Forces ------------------------------------------------------------------------------------- */
 pmb_force *pmb_force_create(pmb_system *sys, const pmb_force_desc *desc);

@@ -261,7 +261,9 @@ int nblist_alloc(pmb_system *s, double rl) {
   long long tiles = 0;
   for (int bi = 0; bi < s->nbox; bi++) {
     const BoxDev &b = s->hbox[bi];
-    double V = b.L[0] * b.L[1] * b.L[2], rho = b.natoms / V;
+    // the box average, but at least a condensed-phase density (0.11 atoms/A^3): the atoms may
+    // form a cluster inside a mostly empty box
+    double V = b.L[0] * b.L[1] * b.L[2], rho = std::max(b.natoms / V, 0.11);
     double est = 1.5 * rho * (4.0 / 3.0) * M_PI * std::pow(rl + 8.0, 3) / 2.0 + 256.0;
     int cap = (int)std::min<double>(((b.natoms + 31) / 32) * 32.0, ((long long)est + 31) / 32 * 32.0);
     if (cap < 32) cap = 32;
@@ -711,6 +713,18 @@ int pmb_system_set_skin(pmb_system *s, double skin) {
   s->skin = skin;
   s->nb_ready = false;  // storage is sized for cutoff + skin
   return PMB_OK;
+}
+
+int pmb_system_check(pmb_system *s) {
+  if (!s) return fail(PMB_ERR_ARG, "null system");
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  const int rc = check_status(s);
+  if (rc == PMB_ERR_CAPACITY) {
+    if (grow_and_retry_needed(s)) return PMB_ERR_CUDA;
+    return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded; the lists were enlarged, evaluate again");
+  }
+  return rc;
 }
 
 pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {

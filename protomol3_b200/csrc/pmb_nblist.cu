@@ -3,7 +3,7 @@
 // (topology/CellListEnumeratorPeriodicBoundaries.h:25-134).
 //
 // Instead of linked cell lists walked pair-of-cells by pair-of-cells, atoms are binned on a fine
-// Morton-ordered grid with a deterministic counting sort, packed into 32-atom blocks ("slots"),
+// Hilbert-ordered grid with a deterministic counting sort, packed into 16-atom blocks of slots,
 // and each block I gets a compacted list of atoms of blocks J > I that lie within the list
 // cutoff of I's bounding box.  The pair kernel then sees (I, 32 j-atoms) tiles; the pair set it
 // evaluates is exactly the reference's: every unordered pair once, minimal image, r^2 <= rc^2.
