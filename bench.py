@@ -307,6 +307,15 @@ def run_b200(args, rank, world, local_rank):
                 "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64)}
         topo64.close()
 
+    batched = None
+    if not args.no_batch:
+        batched = batch_leg(stream, flush)
+        if dist:
+            t = torch.tensor([batched["ms_per_step"]], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            batched["ms_per_step"] = float(t.item())
+            batched["value"] = world * batched["atoms"] / (batched["ms_per_step"] * 1e-3)
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu:
         base = cpu_baseline(box, steps=args.cpu_steps)
@@ -331,9 +340,127 @@ def run_b200(args, rank, world, local_rank):
                      "frac": achieved / peak if achieved and peak else None, "traffic": traffic,
                      "work": "%d FLOP x %d in-cutoff pairs per launch" % (FLOPS_PER_PAIR, npairs),
                      "kernel_ms": t_pair, "peak_source": "measured FP32 FMA issue rate (pmb_fp32_peak)"},
-        "stages_ms": stages, "plain_fp64": fp64, "cpu_baseline": base,
+        "stages_ms": stages, "plain_fp64": fp64, "batched": batched, "cpu_baseline": base,
     }
     print(json.dumps(line), flush=True)
+
+
+BATCH_RC, BATCH_SWITCHON = 9.0, 7.5
+
+
+def batch_leg(stream, flush, steps=20, warmup=3, loop_steps=8, loop_boxes=None):
+    """Ensemble throughput: 256 independent water boxes (100-2000 waters each, ~810k atoms,
+    ~5% of them smaller than twice the cutoff), LJ C2 7.5 -> 9 A, PME at ~1 A grid spacing, order
+    4, leapfrog 1 fs.  All boxes advance together in one mixed-precision system (one launch per
+    force stage, one CUDA graph per step), timed with CUDA events, L2 flushed before each step;
+    against it, the plain FP64 path looped box by box (one system and graph per box, every box
+    timed over ``loop_steps`` steps).  Rates in atom-steps/s."""
+    import torch
+    from protomol3_b200 import forces as F
+    from protomol3_b200 import waterbox as W
+    boxes, grids = W.ensemble()
+    natoms = int(sum(len(b["charge"]) for b in boxes))
+
+    def force_set(bg):
+        return [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", BATCH_SWITCHON, BATCH_RC)),
+                F.NonbondedPMEwaldSystemForce((0, 0, 0), BATCH_RC, box_grids=bg)]
+
+    def timed(topo, fl, pos, vel, nsteps, nwarm, precision_flush=True):
+        md = F.Integrator(topo, fl, timestep=DT_FS)
+        md.set_state(pos, vel)
+        for _ in range(nwarm):
+            md.run(1)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        for a, b in evs:
+            if precision_flush:
+                flush.zero_()
+            a.record(stream)
+            md.run(1)
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        p, _ = md.state()
+        if not np.isfinite(p).all():
+            raise RuntimeError("non-finite positions in the batch leg")
+        md.close()
+        return ms
+
+    topo = F.Topology(boxes, "mixed")
+    topo.set_stream(stream.cuda_stream)
+    pos = np.concatenate([b["pos"] for b in boxes])
+    vel = np.concatenate([b["vel"] for b in boxes])
+    ms = timed(topo, force_set([(g, g, g) for g in grids]), pos, vel, steps, warmup)
+    topo.close()
+    batched = natoms * steps / (ms * 1e-3)
+
+    sel = range(len(boxes)) if loop_boxes is None else range(min(loop_boxes, len(boxes)))
+    loop_ms, loop_atoms = 0.0, 0
+    for k in sel:
+        b = boxes[k]
+        t = F.Topology(b, "fp64")
+        t.set_stream(stream.cuda_stream)
+        loop_ms += timed(t, force_set([(grids[k],) * 3]), b["pos"], b["vel"], loop_steps, 2, False)
+        loop_atoms += len(b["charge"])
+        t.close()
+    looped = loop_atoms * loop_steps / (loop_ms * 1e-3)
+    return {"metric": "atom-steps/s, 256 water boxes of 300-6000 atoms",
+            "value": batched, "unit": "atom-steps/s", "atoms": natoms, "boxes": len(boxes),
+            "steps": steps, "ms_per_step": ms / steps, "precision": "mixed",
+            "plain_fp64_loop": {"value": looped, "boxes_timed": len(sel), "steps_per_box": loop_steps,
+                                "ms_per_step_all_boxes": loop_ms / loop_steps * len(boxes) / len(sel)},
+            "batched_over_loop": batched / looped,
+            "config": "LJ C2 7.5->9 A, PME ~1 A spacing (2/3/5-smooth), order 4, rc 9 A, leapfrog 1 fs; "
+                      "L2 flushed before each batched step"}
+
+
+def nve_run(F, box, precision, stream, steps, chunk):
+    """Leapfrog NVE from the box's state; total energy (potential of the last evaluation plus
+    kinetic at the synchronised velocities) after every ``chunk`` steps."""
+    topo = F.Topology(box, precision)
+    topo.set_stream(stream.cuda_stream)
+    fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", SWITCHON, RC)),
+          F.NonbondedPMEwaldSystemForce((GRID,) * 3, RC)]
+    md = F.Integrator(topo, fl, timestep=DT_FS)
+    md.set_state(box["pos"], box["vel"])
+    t, etot = [], []
+    for k in range(0, steps + 1, chunk):
+        if k:
+            md.run(chunk)
+        e, kin = md.energies()
+        t.append(k * DT_FS * 1e-6)  # ns
+        etot.append(float(e[0, :4].sum() + kin[0]))
+    pos, vel = md.state()
+    md.close()
+    topo.close()
+    return np.array(t), np.array(etot), pos, vel
+
+
+def run_nve(args):
+    """NVE stability of the 98,304-atom box: energy drift (kcal/mol/ns per degree of freedom,
+    least-squares slope of the total energy) in mixed precision and on the plain FP64 path, and
+    whether two mixed runs give bit-identical trajectories."""
+    import torch
+    from protomol3_b200 import forces as F
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    box = workload(0)
+    ndof = 3 * len(box["charge"]) - 3
+    out = {"mode": "nve", "steps": args.steps, "timestep_fs": DT_FS, "dof": ndof,
+           "config": config_dict()}
+    runs = {}
+    for name, prec in (("mixed", "mixed"), ("mixed_repeat", "mixed"), ("fp64", "fp64")):
+        t0 = time.perf_counter()
+        t, e, pos, vel = nve_run(F, box, prec, stream, args.steps, args.chunk)
+        slope = float(np.polyfit(t, e, 1)[0])
+        runs[name] = (pos, vel)
+        out[name] = {"drift_kcal_mol_ns_dof": slope / ndof, "e_start": e[0], "e_end": e[-1],
+                     "e_std": float(e.std()), "wall_s": time.perf_counter() - t0}
+    out["mixed_bit_identical"] = bool(np.array_equal(runs["mixed"][0], runs["mixed_repeat"][0]) and
+                                      np.array_equal(runs["mixed"][1], runs["mixed_repeat"][1]))
+    d = runs["mixed"][0] - runs["fp64"][0]
+    out["mixed_vs_fp64_rms_position_diff_A"] = float(np.sqrt((d ** 2).sum(1).mean()))
+    print(json.dumps(out), flush=True)
 
 
 def run_profile(args):
@@ -384,11 +511,26 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-steps", type=int, default=5)
-    ap.add_argument("--mode", choices=["bench", "profile"], default="bench",
-                    help="profile: only --steps force evaluations (bounded case for ncu)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-box ensemble leg")
+    ap.add_argument("--chunk", type=int, default=500, help="nve: steps between energy reads")
+    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve"], default="bench",
+                    help="profile: only --steps force evaluations (bounded case for ncu); "
+                         "batch: only the 256-box ensemble leg; nve: energy drift and "
+                         "reproducibility over --steps steps")
     args = ap.parse_args()
+    if args.mode == "nve":
+        run_nve(args)
+        return
     if args.mode == "profile":
         run_profile(args)
+        return
+    if args.mode == "batch":
+        import torch
+        torch.cuda.set_device(0)
+        stream = torch.cuda.Stream()
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        print(json.dumps(dict(batch_leg(stream, flush, steps=args.steps, warmup=max(3, args.warmup)),
+                              mode="batch")), flush=True)
         return
     if args.warmup < 3:
         args.warmup = 3

@@ -333,17 +333,18 @@ __global__ void __launch_bounds__(ZT, 8) k_fft_z_fwd(PmeDev pm) {
     else tw[k] = pm.twiddle[pl.tw0[2] + k];
   }
   long long *g = pm.qgrid + pl.grid0 + ((long long)x * ny + y0) * nz;
+  // the work item's lines are one contiguous run of cnt * nz grid values: read them all (no
+  // store in between, so the loads overlap), then clear the charge grid for the next step, each
+  // thread the values it read itself
+  const int nrun = cnt * nz;
+#pragma unroll 4
   for (int e = threadIdx.x; e < npair * 2 * nz; e += ZT) {
-    int line = e / nz, z = e % nz;
-    T v = T(0);
-    if (line < cnt) {
-      long long q = g[(long long)line * nz + z];
-      g[(long long)line * nz + z] = 0;  // the charge grid is cleared as it is consumed
-      v = T((double)q * (1.0 / GRID_SCALE));
-    }
+    const long long q = e < nrun ? __ldcs(g + e) : 0ll;
+    const int line = e / nz, z = e - line * nz;
     T *dst = reinterpret_cast<T *>(buf + (line >> 1) * nz + z);
-    dst[line & 1] = v;
+    dst[line & 1] = T((double)q * (1.0 / GRID_SCALE));
   }
+  for (int e = threadIdx.x; e < nrun; e += ZT) g[e] = 0;
   __syncthreads();
   const T2 *res = fft_lines(buf, tmp, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, -1);
   const int nh = nz / 2 + 1;

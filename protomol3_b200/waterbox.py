@@ -116,3 +116,14 @@ def fft_friendly(n):
 def pme_grid_for(edge, spacing=1.0, minimum=8):
     """PME grid edge at about ``spacing`` A rounded up to a 2/3/5-smooth size."""
     return fft_friendly(max(minimum, edge / spacing))
+
+
+def ensemble(n_boxes=256, lo=100, hi=2000, seed=4321, temperature=300.0):
+    """Independent water boxes of uneven size: water counts uniform on [lo, hi], each box at
+    1.0 g/cm^3 with its own seed.  Returns (boxes, PME grid edge per box at ~1 A spacing)."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(lo, hi + 1, size=n_boxes)
+    boxes = [water_box(int(n), seed=seed + 1 + k, temperature=temperature)
+             for k, n in enumerate(counts)]
+    grids = [pme_grid_for(b["box"][0]) for b in boxes]
+    return boxes, grids
