@@ -307,6 +307,10 @@ def run_b200(args, rank, world, local_rank):
                 "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64)}
         topo64.close()
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serving = serve_leg(n_requests=args.serve_requests)
+
     batched = None
     if not args.no_batch:
         batched = batch_leg(stream, flush)
@@ -340,7 +344,7 @@ def run_b200(args, rank, world, local_rank):
                      "frac": achieved / peak if achieved and peak else None, "traffic": traffic,
                      "work": "%d FLOP x %d in-cutoff pairs per launch" % (FLOPS_PER_PAIR, npairs),
                      "kernel_ms": t_pair, "peak_source": "measured FP32 FMA issue rate (pmb_fp32_peak)"},
-        "stages_ms": stages, "plain_fp64": fp64, "batched": batched, "cpu_baseline": base,
+        "stages_ms": stages, "plain_fp64": fp64, "batched": batched, "serving": serving, "cpu_baseline": base,
     }
     print(json.dumps(line), flush=True)
 
@@ -463,6 +467,46 @@ def run_nve(args):
     print(json.dumps(out), flush=True)
 
 
+def serve_leg(n_requests=24, loads=(0.5, 0.8, 0.95), budget_gb=32.0, max_active=32, chunk=200,
+              seed=2024):
+    """Serving: Poisson streams of Langevin MD segments (water boxes log-uniform on 500-50,000
+    atoms, 1,000-20,000 steps, 300 K, gamma 1/ps, 1 fs, LJ C2 7.5 -> 9 A, PME at ~1 A spacing,
+    mixed precision).  Capacity is measured first with every request of the trace present at
+    t = 0; then the same request mix is offered at each fraction of that capacity.  Latency is
+    arrival to completion (wall clock, includes admission wait); p50/p99 per load."""
+    from protomol3_b200 import serving as S
+    from protomol3_b200 import waterbox as W
+
+    def requests(rate):
+        tr = S.poisson_trace(n_requests, rate, seed=seed)
+        return [S.SegmentRequest(k, W.water_box(w, seed=seed + k), st, seed=sd, arrival=a)
+                for k, (a, w, st, sd) in enumerate(tr)]
+
+    def serve(reqs, precision="mixed"):
+        srv = S.MDServer(hbm_budget_bytes=int(budget_gb * (1 << 30)), max_active=max_active, chunk=chunk,
+                         precision=precision)
+        res = srv.run_trace(reqs)
+        out = S.latency_summary(res)
+        out.update(peak_active=srv.peak_active, peak_device_gb=srv.peak_used / (1 << 30))
+        return out
+
+    # warm-up: module load, first graph captures
+    S.MDServer(max_active=2, chunk=chunk).run_trace(requests(0.0)[:2])
+    cap = serve(requests(0.0))
+    capacity = cap["throughput_req_s"]
+    legs = {"capacity": cap}
+    for f in loads:
+        legs["load_%02d" % round(100 * f)] = dict(serve(requests(f * capacity)), offered_req_s=f * capacity)
+    # the plain FP64 path serving the same request mix, all present at t = 0
+    cap64 = serve(requests(0.0), precision="fp64")
+    return {"metric": "p50/p99 completion latency of Langevin MD segments (500-50,000 atoms, "
+                      "1,000-20,000 steps) under Poisson load",
+            "requests_per_load": n_requests, "capacity_req_s": capacity, "loads": legs,
+            "plain_fp64_capacity": cap64, "capacity_over_fp64": capacity / cap64["throughput_req_s"],
+            "hbm_budget_gb": budget_gb, "max_active": max_active, "chunk_steps": chunk,
+            "precision": "mixed"}
+
+
 def run_profile(args):
     """A bounded case for ncu: builds the box and evaluates the force set ``--steps`` times
     through the C ABI (no MD loop, no CPU legs)."""
@@ -512,12 +556,19 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-steps", type=int, default=5)
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-box ensemble leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--chunk", type=int, default=500, help="nve: steps between energy reads")
-    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve"], default="bench",
+    ap.add_argument("--serve-requests", type=int, default=24, help="serve: requests per load level")
+    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve", "serve"], default="bench",
                     help="profile: only --steps force evaluations (bounded case for ncu); "
                          "batch: only the 256-box ensemble leg; nve: energy drift and "
-                         "reproducibility over --steps steps")
+                         "reproducibility over --steps steps; serve: latency under Poisson load")
     args = ap.parse_args()
+    if args.mode == "serve":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(dict(serve_leg(n_requests=args.serve_requests), mode="serve")), flush=True)
+        return
     if args.mode == "nve":
         run_nve(args)
         return

@@ -160,6 +160,10 @@ int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
 int pmb_md_use_graph(pmb_md *md, int enable);
 /* Kernel launches in one captured MD step (0 before the first graph run). */
 int pmb_md_kernels_per_step(pmb_md *md, int *n);
+/* Device memory held for this MD run: its system (atoms, neighbour lists, accumulators), its
+ * forces (PME grids and tables) and the integrator state, in bytes (for admission by memory
+ * budget; the lists are sized at the first evaluation, pmb_md_set_state). */
+int pmb_md_device_bytes(const pmb_md *md, unsigned long long *bytes);
 
 /* Diagnostics -------------------------------------------------------------------------------- */
 /* Runs the force set nrep times with CUDA events between pipeline stages (TimerStatistic /

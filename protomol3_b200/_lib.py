@@ -72,6 +72,7 @@ _PROTOS = [
     ("pmb_md_energies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_use_graph", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_kernels_per_step", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_md_device_bytes", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_profile", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                               C.c_void_p, C.c_int, C.c_void_p, C.c_char_p, C.c_int]),
     ("pmb_fp32_peak", C.c_int, [C.c_void_p]),

@@ -41,6 +41,7 @@ int fail(int code, const std::string &m) {
 
 struct Allocs {
   std::vector<void *> ptrs;
+  size_t bytes = 0;  // device bytes held
   ~Allocs() {
     for (void *p : ptrs) cudaFree(p);
   }
@@ -51,6 +52,7 @@ struct Allocs {
     if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
     if (zero) cudaMemset(p, 0, n * sizeof(T));
     ptrs.push_back(p);
+    bytes += n * sizeof(T);
     return static_cast<T *>(p);
   }
 };
@@ -1233,6 +1235,15 @@ int pmb_md_run(pmb_md *m, int n) {
   }
   integrate_half_kick(s->dev(), m->in, s->stream);
   CK(cudaGetLastError());
+  return PMB_OK;
+}
+
+int pmb_md_device_bytes(const pmb_md *m, unsigned long long *bytes) {
+  if (!m || !bytes) return fail(PMB_ERR_ARG, "null argument");
+  const pmb_system *s = m->sys;
+  size_t b = s->a.bytes + s->nba.bytes + m->a.bytes + (s->flush_buf ? (256ull << 20) : 0);
+  for (const pmb_force *f : m->forces) b += f->a.bytes;
+  *bytes = (unsigned long long)b;
   return PMB_OK;
 }
 

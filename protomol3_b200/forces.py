@@ -374,6 +374,12 @@ class Integrator:
         L.check(L.lib().pmb_md_kernels_per_step(self._h, C.byref(n)))
         return n.value
 
+    def device_bytes(self):
+        """Device memory held by this run (system, forces, integrator state), in bytes."""
+        b = C.c_ulonglong(0)
+        L.check(L.lib().pmb_md_device_bytes(self._h, C.byref(b)))
+        return b.value
+
     def forces_now(self):
         f = np.zeros((self.topo.n_atoms, 3))
         L.check(L.lib().pmb_md_get_forces(self._h, _p(f)))
