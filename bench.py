@@ -139,6 +139,17 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------- helpers
+def max_over_ranks(x, dist, device):
+    """Largest value of x over the ranks: the slowest replica sets the job's time.  Every rank
+    calls it at the same point (a collective); without a process group it returns x."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def pair_count(box, rc):
     """Exact number of unordered atom pairs within rc (minimal image) minus excluded pairs."""
     from scipy.spatial import cKDTree
@@ -256,10 +267,7 @@ def run_b200(args, rank, world, local_rank):
     clocks.start()
     ms, kps = time_md(topo, fl, args.steps, args.warmup)
     clk = clocks.stop()
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     value = world * ns_per_day(ms)
 
     # stage profile of one force evaluation (cold L2) -> pair-kernel roofline
@@ -289,7 +297,7 @@ def run_b200(args, rank, world, local_rank):
             F.evaluate_all(topo, fl, hpos, hfrc, en)
             vel += hfrc * (h * inv_m)
             hpos += vel * h
-        e2e_ms = (time.perf_counter() - t0) * 1e3 / nsteps
+        e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / nsteps, dist, "cuda")
         e2e = {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": int(hpos.nbytes), "d2h_bytes_per_step": int(hfrc.nbytes + 16 * 8),
                "path": "pmb_evaluate (C ABI) with pinned host positions/forces + host leapfrog"}
@@ -299,10 +307,7 @@ def run_b200(args, rank, world, local_rank):
     if args.precision == "mixed" and not args.no_fp64:
         topo64, fl64 = make("fp64")
         ms64, _ = time_md(topo64, fl64, max(3, args.steps // 2), 3)
-        if dist:
-            t = torch.tensor([ms64], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms64 = float(t.item())
+        ms64 = max_over_ranks(ms64, dist, "cuda")
         fp64 = {"value": world * ns_per_day(ms64), "ms_per_step": ms64,
                 "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64)}
         topo64.close()
@@ -314,11 +319,8 @@ def run_b200(args, rank, world, local_rank):
     batched = None
     if not args.no_batch:
         batched = batch_leg(stream, flush)
-        if dist:
-            t = torch.tensor([batched["ms_per_step"]], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            batched["ms_per_step"] = float(t.item())
-            batched["value"] = world * batched["atoms"] / (batched["ms_per_step"] * 1e-3)
+        batched["ms_per_step"] = max_over_ranks(batched["ms_per_step"], dist, "cuda")
+        batched["value"] = world * batched["atoms"] / (batched["ms_per_step"] * 1e-3)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu:
