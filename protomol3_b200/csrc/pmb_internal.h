@@ -32,6 +32,8 @@ struct NbListDev {
   const int *blk_box;          // [nblk]
   float4 *blk_center;          // [nblk] fractional-fixed centre (as uint bits) and count
   uint4 *blk_lo, *blk_hi;      // [nblk] fixed-point extents (x, y, z)
+  int nsblk;                   // superblocks: runs of 32 consecutive blocks
+  uint4 *sblk_lo, *sblk_hi;    // [nsblk] union of their blocks' extents, .w = atoms
   int *jcap_off;               // [nblk+1] offset of each block's j-slot list region
   int *jcount;                 // [nblk] tiles per block (1 diagonal + list tiles)
   int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding)

@@ -275,6 +275,39 @@ __global__ void k_block_bbox(NbListDev nb) {
   }
 }
 
+// Union extents of each run of 32 consecutive blocks (one warp per superblock).  Blocks of
+// different boxes may share a superblock: the union then only enlarges, which never culls a
+// true candidate.
+__global__ void k_superblock_bbox(NbListDev nb) {
+  if (!nb.ctl[1]) return;
+  const int S = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (S >= nb.nsblk) return;
+  const int J = S * 32 + lane;
+  uint4 lo = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0u), hi = make_uint4(0u, 0u, 0u, 0u);
+  if (J < nb.nblk_total) {
+    const uint4 l = nb.blk_lo[J];
+    if (l.w > 0) {
+      lo = l;
+      hi = nb.blk_hi[J];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = min(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
+    lo.y = min(lo.y, __shfl_xor_sync(0xffffffffu, lo.y, o));
+    lo.z = min(lo.z, __shfl_xor_sync(0xffffffffu, lo.z, o));
+    lo.w += __shfl_xor_sync(0xffffffffu, lo.w, o);
+    hi.x = max(hi.x, __shfl_xor_sync(0xffffffffu, hi.x, o));
+    hi.y = max(hi.y, __shfl_xor_sync(0xffffffffu, hi.y, o));
+    hi.z = max(hi.z, __shfl_xor_sync(0xffffffffu, hi.z, o));
+  }
+  if (lane == 0) {
+    if (lo.w == 0) lo.x = lo.y = lo.z = hi.x = hi.y = hi.z = 0;
+    nb.sblk_lo[S] = lo;
+    nb.sblk_hi[S] = hi;
+  }
+}
+
 // Gap (in A) between a point / box and a box, in fractional fixed-point coordinates with the
 // minimal image taken by 32-bit wrap-around.
 __device__ __forceinline__ double box_gap2(const BoxDev &b, const unsigned c1[3], const unsigned h1[3],
@@ -287,6 +320,24 @@ __device__ __forceinline__ double box_gap2(const BoxDev &b, const unsigned c1[3]
     long long gap = a - (long long)h1[k] - (long long)h2[k];
     if (gap > 0) {
       double ga = (double)gap * b.L[k] * (1.0 / 4294967296.0);
+      g2 += ga * ga;
+    }
+  }
+  return g2;
+}
+
+// The same gap in FP32 for the list culling: the gap is exact in fixed point and its conversion
+// errs by < 1e-5 A, far below the 1e-3 A margin of the list radius over the cutoff.
+__device__ __forceinline__ float box_gap2f(const float sL[3], const unsigned c1[3], const unsigned h1[3],
+                                           const unsigned c2[3], const unsigned h2[3]) {
+  float g2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    long long d = (long long)(int)(c2[k] - c1[k]);
+    long long a = d < 0 ? -d : d;
+    long long gap = a - (long long)h1[k] - (long long)h2[k];
+    if (gap > 0) {
+      float ga = (float)gap * sL[k];
       g2 += ga * ga;
     }
   }
@@ -323,51 +374,74 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   int count = 0;
   bool overflow = false;
   unsigned zero[3] = {0, 0, 0};
-  for (int J0 = I + 1; J0 < jend; J0 += 32) {
-    int J = J0 + lane;
-    bool cand = false;
-    if (J < jend) {
-      uint4 loJ = nb.blk_lo[J], hiJ = nb.blk_hi[J];
-      if (loJ.w > 0) {
-        if (b.multi_image) cand = true;
+  const float sL[3] = {(float)(b.L[0] * (1.0 / 4294967296.0)), (float)(b.L[1] * (1.0 / 4294967296.0)),
+                       (float)(b.L[2] * (1.0 / 4294967296.0))};
+  const float rl2 = (float)rlist2;
+  // superblocks (runs of 32 blocks) first, 32 per ballot; then the blocks of each candidate one
+  const int send = (jend + 31) / 32;
+  for (int S0 = (I + 1) / 32; S0 < send && !overflow; S0 += 32) {
+    const int S = S0 + lane;
+    bool scand = false;
+    if (S < send) {
+      const uint4 loS = nb.sblk_lo[S], hiS = nb.sblk_hi[S];
+      if (loS.w > 0) {
+        if (b.multi_image) scand = true;
         else {
-          unsigned cJ[3], hJ[3];
-          center_half(loJ, hiJ, cJ, hJ);
-          cand = box_gap2(b, cI, hI, cJ, hJ) <= rlist2;
+          unsigned cS[3], hS[3];
+          center_half(loS, hiS, cS, hS);
+          scand = box_gap2f(sL, cI, hI, cS, hS) <= rl2;
         }
       }
     }
-    unsigned m = __ballot_sync(0xffffffffu, cand);
-    while (m) {
-      // two candidate blocks per pass: lanes 0-15 test the atoms of the first, 16-31 the second
-      int srcA = __ffs(m) - 1;
-      m &= m - 1;
-      int srcB = m ? __ffs(m) - 1 : -1;
-      if (m) m &= m - 1;
-      int src = lane < BLOCK ? srcA : srcB;
-      bool take = false;
-      int sl = -1;
-      if (src >= 0) {
-        sl = (J0 + src) * BLOCK + (lane & (BLOCK - 1));
-        if (nb.slot_orig[sl] >= 0) {
-          if (b.multi_image) take = true;
+    unsigned sm = __ballot_sync(0xffffffffu, scand);
+    while (sm) {
+      const int J0 = (S0 + __ffs(sm) - 1) * 32;
+      sm &= sm - 1;
+      int J = J0 + lane;
+      bool cand = false;
+      if (J > I && J < jend) {
+        uint4 loJ = nb.blk_lo[J], hiJ = nb.blk_hi[J];
+        if (loJ.w > 0) {
+          if (b.multi_image) cand = true;
           else {
-            uint4 f = nb.slot_fx[sl];
-            unsigned p[3] = {f.x, f.y, f.z};
-            take = box_gap2(b, cI, hI, p, zero) <= rlist2;
+            unsigned cJ[3], hJ[3];
+            center_half(loJ, hiJ, cJ, hJ);
+            cand = box_gap2f(sL, cI, hI, cJ, hJ) <= rl2;
           }
         }
       }
-      unsigned tm = __ballot_sync(0xffffffffu, take);
-      int n = __popc(tm);
-      if (count + n > cap) {
-        overflow = true;
-        break;
+      unsigned m = __ballot_sync(0xffffffffu, cand);
+      while (m) {
+        // two candidate blocks per pass: lanes 0-15 test the atoms of the first, 16-31 the second
+        int srcA = __ffs(m) - 1;
+        m &= m - 1;
+        int srcB = m ? __ffs(m) - 1 : -1;
+        if (m) m &= m - 1;
+        int src = lane < BLOCK ? srcA : srcB;
+        bool take = false;
+        int sl = -1;
+        if (src >= 0) {
+          sl = (J0 + src) * BLOCK + (lane & (BLOCK - 1));
+          if (nb.slot_orig[sl] >= 0) {
+            if (b.multi_image) take = true;
+            else {
+              uint4 f = nb.slot_fx[sl];
+              unsigned p[3] = {f.x, f.y, f.z};
+              take = box_gap2f(sL, cI, hI, p, zero) <= rl2;
+            }
+          }
+        }
+        unsigned tm = __ballot_sync(0xffffffffu, take);
+        int n = __popc(tm);
+        if (count + n > cap) {
+          overflow = true;
+          break;
+        }
+        if (take) out[count + __popc(tm & ((1u << lane) - 1u))] = sl;
+        count += n;
       }
-      if (take) out[count + __popc(tm & ((1u << lane) - 1u))] = sl;
-      count += n;
+      if (overflow) break;
     }
-    if (overflow) break;
   }
   int padded = (count + 31) & ~31;
   if (!overflow)
@@ -378,16 +452,17 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   }
 }
 
+// One warp per block: its tiles' (block, index) entries, written by consecutive lanes.
 __global__ void k_tile_map(NbListDev nb) {
   if (!nb.ctl[1]) return;
-  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (I >= nb.nblk_total) return;
-  int off = nb.tile_off[I], cnt = nb.jcount[I];
+  const int off = nb.tile_off[I], cnt = nb.jcount[I];
   if (off + cnt > nb.tile_cap) {
-    atomicExch(&nb.status[1], 1);
+    if (lane == 0) atomicExch(&nb.status[1], 1);
     return;
   }
-  for (int k = 0; k < cnt; k++) {
+  for (int k = lane; k < cnt; k += 32) {
     nb.tile_blk[off + k] = I;
     nb.tile_k[off + k] = k;
   }
@@ -417,10 +492,11 @@ int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
                                                    nb.nkeys, nb.slot_orig, nb.ctl);
   k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
   k_block_bbox<<<(nb.nslot + T - 1) / T, T, 0, st>>>(nb);
+  k_superblock_bbox<<<(nb.nsblk * 32 + T - 1) / T, T, 0, st>>>(nb);
   int wthreads = nb.nblk_total * 32;
   k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
   scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st, nb.ctl);
-  k_tile_map<<<(nb.nblk_total + T - 1) / T, T, 0, st>>>(nb);
+  k_tile_map<<<(wthreads + T - 1) / T, T, 0, st>>>(nb);
   return 0;
 }
 
