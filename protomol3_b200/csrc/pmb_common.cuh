@@ -25,7 +25,9 @@ enum { E_COUL = 0, E_LJ = 1, E_BOND = 2, E_ANGLE = 3, E_VIR = 4, ACC_PER_BOX = 1
 
 enum { SW_CUTOFF = 0, SW_C1 = 1, SW_C2 = 2 };
 
-constexpr int BLOCK = 16;          // atoms per i-cluster (half a warp; the j-chunk is 32 atoms)
+constexpr int BLOCK = 8;           // atoms per i-cluster (a lane group; the j-chunk is 32 atoms)
+constexpr int GROUPS = 32 / BLOCK; // lane groups per warp
+static_assert(BLOCK == 8 || BLOCK == 16, "i-cluster of 8 or 16 atoms");
 constexpr int JCHUNK = 32;         // j-atoms per tile
 constexpr int MAX_LJ_TYPES = 32;   // LJ table kept in shared memory up to this many types
 

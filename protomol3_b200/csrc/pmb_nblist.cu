@@ -3,7 +3,7 @@
 // (topology/CellListEnumeratorPeriodicBoundaries.h:25-134).
 //
 // Instead of linked cell lists walked pair-of-cells by pair-of-cells, atoms are binned on a fine
-// Hilbert-ordered grid with a deterministic counting sort, packed into 16-atom blocks of slots,
+// Hilbert-ordered grid with a deterministic counting sort, packed into 8-atom blocks of slots,
 // and each block I gets a compacted list of atoms of blocks J > I that lie within the list
 // cutoff of I's bounding box.  The pair kernel then sees (I, 32 j-atoms) tiles; the pair set it
 // evaluates is exactly the reference's: every unordered pair once, minimal image, r^2 <= rc^2.
@@ -248,7 +248,7 @@ __global__ void k_pack(SystemDev s, NbListDev nb, int want_fp64) {
   if (want_fp64) nb.slot_pq[sl] = make_double4(x, y, z, q);
 }
 
-// Bounding box of every 16-slot block in fractional fixed point; a warp covers two blocks.
+// Bounding box of every BLOCK-slot block in fractional fixed point; a warp covers GROUPS blocks.
 __global__ void k_block_bbox(NbListDev nb) {
   if (!nb.ctl[1]) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -267,7 +267,7 @@ __global__ void k_block_bbox(NbListDev nb) {
       hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
     }
   unsigned bal = __ballot_sync(0xffffffffu, valid);
-  int cnt = __popc(bal & (0xffffu << (lane & 16)));
+  int cnt = __popc(bal & (((1u << BLOCK) - 1u) << (lane & ~(BLOCK - 1))));
   if (inr && (lane & (BLOCK - 1)) == 0) {
     if (cnt == 0) lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
     nb.blk_lo[blk] = make_uint4(lo[0], lo[1], lo[2], (unsigned)cnt);
@@ -412,12 +412,11 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
       }
       unsigned m = __ballot_sync(0xffffffffu, cand);
       while (m) {
-        // two candidate blocks per pass: lanes 0-15 test the atoms of the first, 16-31 the second
-        int srcA = __ffs(m) - 1;
-        m &= m - 1;
-        int srcB = m ? __ffs(m) - 1 : -1;
-        if (m) m &= m - 1;
-        int src = lane < BLOCK ? srcA : srcB;
+        // GROUPS candidate blocks per pass: lane group g tests the atoms of the g-th one
+        unsigned mg = m;
+        for (int t = 0; t < lane / BLOCK; t++) mg &= mg - 1;
+        const int src = mg ? __ffs(mg) - 1 : -1;
+        for (int t = 0; t < GROUPS && m; t++) m &= m - 1;
         bool take = false;
         int sl = -1;
         if (src >= 0) {

@@ -1,5 +1,5 @@
 // Fused nonbonded pair kernel: Lennard-Jones with C1/C2/cutoff switching plus either cutoff
-// Coulomb (switched) or the Ewald real-space term, over the (16-atom i-cluster, 32 j-atoms)
+// Coulomb (switched) or the Ewald real-space term, over the (8-atom i-cluster, 32 j-atoms)
 // tiles built by pmb_nblist.cu.
 //
 // Replaces, per pair, OneAtomPair::doOneAtomPair / OneAtomPairTwo::doOneAtomPair
@@ -7,16 +7,16 @@
 // (force/LennardJonesForce.h:28-60), CoulombForce::operator() (force/CoulombForce.h:29-40) and
 // the PME real-space body (mdl/interface/force/nonbonded/NonbondedPMEwaldSystemForce.h:644-700).
 //
-// Warp tiling: the 16 atoms of cluster I sit twice in the warp (lanes 0-15 and 16-31); the 32
-// j-atoms of the tile are staged in shared memory, lanes 0-15 visit j-atoms 0-15 and lanes 16-31
-// j-atoms 16-31 in 16 rotations; the j-force accumulators travel with the rotation through
-// 16-lane shuffles (Newton's third law inside the tile), the two i-force halves are combined
-// once per tile.  Forces leave as int64 fixed point (one atomic per j-atom per tile, one per
+// Warp tiling: the BLOCK atoms of cluster I sit once in each of the GROUPS lane groups of the
+// warp; the 32 j-atoms of the tile are staged in shared memory, lane group g visits j-atoms
+// [g BLOCK, (g + 1) BLOCK) in BLOCK rotations; the j-force accumulators travel with the rotation
+// through shuffles inside the group (Newton's third law inside the tile), the groups' i-forces
+// are combined once per tile.  Forces leave as int64 fixed point (one atomic per j-atom per tile, one per
 // i-atom per run of tiles of the same cluster); energies and virials are summed per tile in a
 // fixed shuffle order and added in fixed point, so results are bit-identical run to run.
 //
 // The inner loop is branch-free: every lane evaluates the potentials on a clamped distance and
-// the result is masked, because ~60% of the pairs of a tile lie outside the cutoff and a
+// the result is masked, because about half of the pairs of a tile lie outside the cutoff and a
 // divergent branch would cost more than the masked arithmetic.  The switching functions of the
 // common force sets are compile-time template parameters; other combinations use a generic
 // instance with run-time switches.
@@ -39,7 +39,7 @@ namespace {
 
 constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_WARPS = PAIR_THREADS / 32;
-constexpr int CHUNK = 4;  // consecutive tiles per warp assignment
+constexpr int CHUNK = 8;  // consecutive tiles per warp assignment
 
 // switch / potential selectors (template parameters)
 constexpr int SWR = -1;   // read the switching function kind at run time
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
   __syncthreads();
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int half = lane & 16, li = lane & 15;
+  const int gb = lane & ~(BLOCK - 1), li = lane & (BLOCK - 1);  // lane group base, i-atom
   JP *sjp = spos_all + wib * 32;
   int2 *sjm = smeta_all + wib * 32;
   int *sorig = sorig_all + wib * 32;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
   float Lf[3] = {0, 0, 0}, Lrf[3] = {0, 0, 0};
 
   auto flush_i = [&]() {
-    if (curI >= 0 && im.x >= 0 && half == 0) {
+    if (curI >= 0 && im.x >= 0 && gb == 0) {
       long long *f = s.facc + 3 * (long long)im.x;
       if (ifix[0]) red_add(f, ifix[0]);
       if (ifix[1]) red_add(f + 1, ifix[1]);
@@ -363,8 +363,8 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
         }
       }
       const bool diag = (k == 0);
-      // diagonal tile: the cluster against itself (lanes 0-15); other tiles: 32 listed j-atoms
-      const int jsl = diag ? (half ? -1 : I * BLOCK + li) : nb.jlist[nb.jcap_off[I] + (k - 1) * JCHUNK + lane];
+      // diagonal tile: the cluster against itself (lane group 0); other tiles: 32 listed j-atoms
+      const int jsl = diag ? (gb ? -1 : I * BLOCK + li) : nb.jlist[nb.jcap_off[I] + (k - 1) * JCHUNK + lane];
       JStage<MIXED> mine;
       int jorig;
       stage_slot(jsl, mine, jorig);
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
       for (int c = 0; c < 6; c++) a.vir[c] = T(0);
       T fj[3] = {T(0), T(0), T(0)};
       const int tio = im.z * nt;
-      const int nxt = half | ((li + 1) & 15);
+      const int nxt = gb | ((li + 1) & (BLOCK - 1));
       const T cut2 = pt.cut2;
 
       const bool ivalid = im.x >= 0;
@@ -388,11 +388,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
         constexpr bool DIAG = decltype(diag_tag)::value;
         constexpr bool WRAP = decltype(wrap_tag)::value;
 #pragma unroll 2
-        for (int st = 0; st < 16; st++) {
-          const int jl = (li + st) & 15;
+        for (int st = 0; st < BLOCK; st++) {
+          const int jl = (li + st) & (BLOCK - 1);
           JStage<MIXED> dj;
-          dj.p = sjp[half | jl];
-          dj.m = sjm[half | jl];
+          dj.p = sjp[gb | jl];
+          dj.m = sjm[gb | jl];
           T dx = T(dj.p.x) - xi, dy = T(dj.p.y) - yi, dz = T(dj.p.z) - zi;
           if constexpr (!MIXED) {
             // the reference's minimal image: d - L rint(d / L) equals its single-wrap result
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
           if constexpr (DIAG) in = in && jl > li;
           int ex = 0;
           if (in && im.y == dj.m.x) {
-            ex = excl_check(s, im.x, sorig[half | jl]);
+            ex = excl_check(s, im.x, sorig[gb | jl]);
             if (ex == 2) in = false;
           }
           T2 ab;
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
           }
           a.fi[0] -= fx; a.fi[1] -= fy; a.fi[2] -= fz;
           fj[0] += fx; fj[1] += fy; fj[2] += fz;
-          // rotate j-force accumulators inside the 16-lane segment
+          // rotate j-force accumulators inside the lane group
           fj[0] = __shfl_sync(0xffffffffu, fj[0], nxt);
           fj[1] = __shfl_sync(0xffffffffu, fj[1], nxt);
           fj[2] = __shfl_sync(0xffffffffu, fj[2], nxt);
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
         else body(std::false_type{}, std::true_type{});
       }
 
-      // after 16 rotations lane l holds the accumulator of j-atom l of the tile
+      // after BLOCK rotations lane l holds the accumulator of j-atom l of the tile
       if (diag) {
         a.fi[0] += fj[0]; a.fi[1] += fj[1]; a.fi[2] += fj[2];
       } else if (jorig >= 0) {
@@ -480,9 +480,11 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
         if (v1) red_add(f + 1, v1);
         if (v2) red_add(f + 2, v2);
       }
-      // combine the two halves of the i-cluster
+      // combine the lane groups of the i-cluster
 #pragma unroll
-      for (int c = 0; c < 3; c++) a.fi[c] += __shfl_xor_sync(0xffffffffu, a.fi[c], 16);
+      for (int o = BLOCK; o < 32; o <<= 1)
+#pragma unroll
+        for (int c = 0; c < 3; c++) a.fi[c] += __shfl_xor_sync(0xffffffffu, a.fi[c], o);
       ifix[0] += f2fix(a.fi[0], (T)FORCE_SCALE);
       ifix[1] += f2fix(a.fi[1], (T)FORCE_SCALE);
       ifix[2] += f2fix(a.fi[2], (T)FORCE_SCALE);
