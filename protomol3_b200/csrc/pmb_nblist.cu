@@ -421,10 +421,11 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
         int sl = -1;
         if (src >= 0) {
           sl = (J0 + src) * BLOCK + (lane & (BLOCK - 1));
-          if (nb.slot_orig[sl] >= 0) {
+          const int o = nb.slot_orig[sl];
+          const uint4 f = nb.slot_fx[sl];  // loaded with the index, not after it
+          if (o >= 0) {
             if (b.multi_image) take = true;
             else {
-              uint4 f = nb.slot_fx[sl];
               unsigned p[3] = {f.x, f.y, f.z};
               take = box_gap2f(sL, cI, hI, p, zero) <= rl2;
             }

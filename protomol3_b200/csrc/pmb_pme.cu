@@ -5,7 +5,8 @@
 // NonbondedPMEwaldSystemForce.h (reciprocalTerm :812-864, correctionTerm :874-911).
 //
 // Pipeline per step (every kernel batched over the boxes of a system):
-//   k_spread      one thread per atom slot, B-spline weights, 64 int64 fixed-point atomics
+//   k_spread      B-spline weights, 64 int64 fixed-point atomics per atom slot (order 4: four
+//                 threads per slot, one x-plane of the stencil each)
 //   k_fft_z_fwd   z-lines of the fixed-point grid (cleared as it is read), two real lines packed
 //                 per complex FFT, half spectrum written as [kz][x][y]
 //   k_fft_y       y-lines of the half spectrum (groups of up to 16 rows of one kz plane)
@@ -251,6 +252,75 @@ __global__ void k_spread(NbListDev nb, PmeDev pm) {
         long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
         if (v) red_add(row + k1, v);
       }
+    }
+  }
+}
+
+// B-spline weights and grid bases of one slot for order 4 (the common case).
+template <bool MIXED, bool DERIV>
+__device__ __forceinline__ void weights4(const NbListDev &nb, const PmeBoxPlan &pl, int sl,
+                                         typename std::conditional<MIXED, float, double>::type th[3][4],
+                                         typename std::conditional<MIXED, float, double>::type dth[3][4],
+                                         int base[3], typename std::conditional<MIXED, float, double>::type &q) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  if constexpr (MIXED) {
+    const uint4 f = nb.slot_fx[sl];
+    const unsigned fx[3] = {f.x, f.y, f.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T w;
+      grid_coord<true>(fx[d], 0.0, 0.0, pl.n[d], 4, base[d], w);
+      bspline<T>(4, w, th[d], DERIV ? dth[d] : nullptr);
+    }
+    q = __uint_as_float(f.w);
+  } else {
+    const double4 pq = nb.slot_pq[sl];
+    const double x[3] = {pq.x, pq.y, pq.z};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      T w;
+      grid_coord<false>(0u, x[d], pl.hr[d], pl.n[d], 4, base[d], w);
+      bspline<T>(4, w, th[d], DERIV ? dth[d] : nullptr);
+    }
+    q = pq.w;
+  }
+}
+
+// v[p] for a run-time p in [0, 4) without indexing a register array (which would go to local
+// memory).
+template <typename T>
+__device__ __forceinline__ T pick4(const T v[4], int p) {
+  return p == 0 ? v[0] : (p == 1 ? v[1] : (p == 2 ? v[2] : v[3]));
+}
+
+// Order 4 with four threads per atom slot: thread p adds the 16 points of x-plane p of the
+// stencil (the same values, in the same order of products, as the one-thread form).
+template <bool MIXED>
+__global__ void k_spread4(NbListDev nb, PmeDev pm) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int sl = (int)(t >> 2), p = (int)(t & 3);
+  if (sl >= nb.nslot) return;
+  const int4 m = nb.slot_meta[sl];
+  if (m.x < 0) return;
+  const PmeBoxPlan &pl = pm.plan[m.w];
+  T th[3][4];
+  int base[3];
+  T q;
+  weights4<MIXED, false>(nb, pl, sl, th, th, base, q);
+  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
+  long long *g = pm.qgrid + pl.grid0;
+  const T a = q * pick4(th[0], p);
+  const int i1 = (p + base[0]) % nx;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const T ab = a * th[1][j];
+    const int j1 = (j + base[1]) % ny;
+    long long *row = g + ((long long)i1 * ny + j1) * nz;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
+      if (v) red_add(row + (k + base[2]) % nz, v);
     }
   }
 }
@@ -565,7 +635,8 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   using T2 = typename C2<T>::t;
   const int TB = 256;
   constexpr bool MIXED = sizeof(T) == 4;
-  if (pm.order == 4) k_spread<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
+  const long long n4 = 4ll * nb.nslot;
+  if (pm.order == 4) k_spread4<MIXED><<<(unsigned)((n4 + TB - 1) / TB), TB, 0, st>>>(nb, pm);
   else k_spread<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
   if (mark) mark(mctx, "pme_spread");
   size_t zsmem = sizeof(T2) * (256 + 2 * (size_t)ZMAXE);
