@@ -259,6 +259,7 @@ int nblist_alloc(pmb_system *s, double rl) {
   for (auto &b : s->hbox) nblk += b.nblk;
   nb.nblk_total = nblk;
   nb.nslot = nblk * BLOCK;
+  if ((long long)nblk * BLOCK >= JSAME) return fail(PMB_ERR_CAPACITY, "too many atoms for one system");
   std::vector<int> blk_box(nblk), jcap_off(nblk + 1, 0);
   long long tiles = 0;
   for (int bi = 0; bi < s->nbox; bi++) {
@@ -299,6 +300,7 @@ int nblist_alloc(pmb_system *s, double rl) {
   nb.want_fp64 = s->precision == PMB_FP64;
   nb.slot_pq = nb.want_fp64 ? s->nba.get<double4>(nb.nslot) : nullptr;
   nb.slot_meta = s->nba.get<int4>(nb.nslot);
+  nb.fslot = s->nba.get<long long>(3 * (size_t)nb.nslot);
   // sort bins
   std::vector<int> bin_box;
   for (int bi = 0; bi < s->nbox; bi++) {
@@ -323,7 +325,8 @@ int nblist_alloc(pmb_system *s, double rl) {
   const unsigned ctl0[4] = {0u, 0u, 0u, 1u};  // first use builds the list
   CK(cudaMemcpy(nb.ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice));
   s->nb_build_rl = -1.0;
-  if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.scan_tmp || !nb.bin_start)
+  if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.fslot ||
+      !nb.scan_tmp || !nb.bin_start)
     return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
   s->nb_cutoff = rl;
   s->nb_ready = true;
@@ -437,7 +440,8 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     mark(s, "nblist");
   }
   if (!jobs.empty()) {
-    for (auto &j : jobs) {
+    for (size_t q = 0; q < jobs.size(); q++) {
+      const PairJob &j = jobs[q];
       PairLaunch pl;
       pl.precision = s->precision;
       pl.p = j.p;
@@ -447,6 +451,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
       if (j.p.coul_mode == 2 && j.lattice)
         for (const BoxDev &b : s->hbox) pl.multi |= b.multi_image;
       if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+      if (q + 1 == jobs.size()) pair_fold(sd, s->nb, st);  // slot-ordered pair forces -> facc
       mark(s, "pair");
     }
   }

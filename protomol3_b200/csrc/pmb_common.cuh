@@ -2,8 +2,8 @@
 //
 // Layout conventions (all arrays device-resident, one system = a batch of >= 1 periodic boxes):
 //   * atoms of all boxes are concatenated in the caller's order ("original order");
-//   * a box's atoms are re-ordered into "slots" (Morton order of a fine cell grid) grouped in
-//     blocks of 32 slots; a box owns whole blocks, padding slots carry orig = -1;
+//   * a box's atoms are re-ordered into "slots" (Hilbert order of a fine cell grid) grouped in
+//     blocks of BLOCK slots; a box owns whole blocks, padding slots carry orig = -1;
 //   * forces accumulate in int64 fixed point (FORCE_SCALE) in original order, energies and
 //     virials per box in int64 fixed point (ENERGY_SCALE): integer addition is associative, so
 //     every sum is bit-reproducible whatever the launch order or atomic interleaving;
@@ -29,6 +29,7 @@ constexpr int BLOCK = 8;           // atoms per i-cluster (a lane group; the j-c
 constexpr int GROUPS = 32 / BLOCK; // lane groups per warp
 static_assert(BLOCK == 8 || BLOCK == 16, "i-cluster of 8 or 16 atoms");
 constexpr int JCHUNK = 32;         // j-atoms per tile
+constexpr int JSAME = 1 << 30;     // j-list flag: the j-atom shares a molecule with the i-cluster
 constexpr int MAX_LJ_TYPES = 32;   // LJ table kept in shared memory up to this many types
 
 struct BoxDev {

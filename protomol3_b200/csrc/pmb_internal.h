@@ -36,7 +36,7 @@ struct NbListDev {
   uint4 *sblk_lo, *sblk_hi;    // [nsblk] union of their blocks' extents, .w = atoms
   int *jcap_off;               // [nblk+1] offset of each block's j-slot list region
   int *jcount;                 // [nblk] tiles per block (1 diagonal + list tiles)
-  int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding)
+  int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding), JSAME flag bit
   int *tile_off;               // [nblk+1] exclusive scan of jcount
   int *tile_blk;               // [tile_cap] block of each tile
   int *tile_k;                 // [tile_cap] tile index within the block
@@ -48,6 +48,8 @@ struct NbListDev {
   uint4 *slot_fx;              // [nslot] fractional fixed-point x, y, z (2^32 per edge) + q bits
   double4 *slot_pq;            // [nslot] raw double position + q (FP64 path)
   int4 *slot_meta;             // [nslot] orig, molecule, type, box
+  long long *fslot;            // [3][nslot] pair forces by slot (component-major), fixed point;
+                               // folded into facc and cleared after the pair kernels
   // sort
   int nkeys;
   int *key;                    // [natoms]
@@ -90,6 +92,7 @@ struct PairLaunch {
   PairParams p;
 };
 int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st);
+int pair_fold(const SystemDev &s, const NbListDev &nb, cudaStream_t st);
 
 // Allocation-free all-pairs variant (FP64): energy/virial accumulators in a static device array
 // of STATIC_MAX_BOXES boxes.  static_eacc_address looks the array up once per device (current

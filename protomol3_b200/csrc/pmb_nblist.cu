@@ -377,6 +377,15 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   const float sL[3] = {(float)(b.L[0] * (1.0 / 4294967296.0)), (float)(b.L[1] * (1.0 / 4294967296.0)),
                        (float)(b.L[2] * (1.0 / 4294967296.0))};
   const float rl2 = (float)rlist2;
+  // molecules of the cluster's atoms (-2: padding): a listed j-atom of one of them is flagged
+  // JSAME, so the pair kernel runs the exclusion test only on tiles holding such an atom
+  int imol[BLOCK];
+  {
+    const int o = nb.slot_orig[I * BLOCK + (lane & (BLOCK - 1))];
+    const int mine = o >= 0 ? s.molecule[o] : -2;
+#pragma unroll
+    for (int t = 0; t < BLOCK; t++) imol[t] = __shfl_sync(0xffffffffu, mine, t);
+  }
   // superblocks (runs of 32 blocks) first, 32 per ballot; then the blocks of each candidate one
   const int send = (jend + 31) / 32;
   for (int S0 = (I + 1) / 32; S0 < send && !overflow; S0 += 32) {
@@ -418,10 +427,10 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
         const int src = mg ? __ffs(mg) - 1 : -1;
         for (int t = 0; t < GROUPS && m; t++) m &= m - 1;
         bool take = false;
-        int sl = -1;
+        int sl = -1, o = -1;
         if (src >= 0) {
           sl = (J0 + src) * BLOCK + (lane & (BLOCK - 1));
-          const int o = nb.slot_orig[sl];
+          o = nb.slot_orig[sl];
           const uint4 f = nb.slot_fx[sl];  // loaded with the index, not after it
           if (o >= 0) {
             if (b.multi_image) take = true;
@@ -437,7 +446,13 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
           overflow = true;
           break;
         }
-        if (take) out[count + __popc(tm & ((1u << lane) - 1u))] = sl;
+        if (take) {
+          const int mj = s.molecule[o];
+          bool same = false;
+#pragma unroll
+          for (int t = 0; t < BLOCK; t++) same |= mj == imol[t];
+          out[count + __popc(tm & ((1u << lane) - 1u))] = same ? (sl | JSAME) : sl;
+        }
         count += n;
       }
       if (overflow) break;

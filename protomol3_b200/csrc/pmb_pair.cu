@@ -66,6 +66,7 @@ struct ParamsT {
   int lj_all, coul_all;  // the LJ / Coulomb cutoff covers the pair rejection radius
   SwitchT<T> lj_sw, coul_sw;
   T cut2, lj_cut2, coul_cut2, alpha, a2pi, coulomb_scaling;
+  T kexp;  // -alpha^2 log2(e): exp(-alpha^2 r^2) = 2^(kexp r^2)
 };
 
 template <typename T>
@@ -87,6 +88,7 @@ ParamsT<T> params_t(const PairParams &p) {
   o.coul_sw = switch_t<T>(p.coul_sw);
   o.cut2 = (T)p.cut2; o.lj_cut2 = (T)p.lj_cut2; o.coul_cut2 = (T)p.coul_cut2;
   o.alpha = (T)p.alpha; o.a2pi = (T)p.a2pi; o.coulomb_scaling = (T)p.coulomb_scaling;
+  o.kexp = (T)(-p.alpha * p.alpha * 1.4426950408889634);
   return o;
 }
 
@@ -198,9 +200,10 @@ __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type
   return fs;
 }
 
-// Shared-memory image of one j-atom of a tile.  Mixed: coordinates relative to the first atom
-// of the i-cluster (exact fixed-point difference, one rounding to FP32 per tile instead of per
-// pair); padding atoms sit at -1e6 A (i padding at +1e6 A) so the cutoff test masks them.
+// Shared-memory image of one j-atom of a tile (scalar path).  Mixed: coordinates relative to the
+// first atom of the i-cluster (exact fixed-point difference, one rounding to FP32 per tile
+// instead of per pair); padding atoms sit at -1e6 A (i padding at +1e6 A) so the cutoff test
+// masks them.
 template <bool MIXED>
 struct JStage;
 template <>
@@ -214,8 +217,162 @@ struct JStage<false> {
   int2 m;
 };
 
+// ------------------------------------------------------------------ packed FP32 tiles (mixed)
+// Tiles whose j-atoms share no molecule with the i-cluster (no exclusion can apply; the list
+// build flags the others) run on the two-wide FP32 instructions of sm_100 (FADD2 / FMUL2 /
+// FFMA2): every lane evaluates two pairs per step, its i-atom with j-atoms jl and jl + HALF of its
+// lane group, so HALF steps cover the group and each FP32 instruction issues two pairs' work.
+// The j-atoms are staged as pairs {j, j + HALF} (x x' y y' | z z' q q' | type type'), each entry
+// written twice (li and li + BLOCK), so step st reads entry li + st at a constant offset.
+// Masking multiplies the parameters by 0/1 instead of selecting per result, and the C2 switch is
+// evaluated at max(r2, ron2): its value there is 1 and its derivative 0 up to rounding, which
+// removes the inner-radius branch.  Far pairs stay finite (relative coordinates are bounded by
+// the box and the +-1e6 A sentinels), so masked terms are exact zeros.
+constexpr int HALF = BLOCK / 2;
+constexpr int GSTRIDE = 2 * BLOCK + 8;  // entries per lane group; +8 puts groups on other banks
+constexpr int FAST_ENTRIES = GROUPS * GSTRIDE;
+#ifndef PAIR2_UNROLL
+#define PAIR2_UNROLL 4
+#endif
+constexpr int PAIR2_STEPS_UNROLLED = PAIR2_UNROLL;
+#ifndef PAIR_MINB
+#define PAIR_MINB 3  // resident blocks per SM of the mixed kernels
+#endif
+
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sp2(float v) { return make_float2(v, v); }
+// 1.0f where a <= b, else 0.0f (one SET instruction)
+__device__ __forceinline__ float le_mask(float a, float b) {
+  float r;
+  asm("set.le.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+
+template <int K>
+__device__ __forceinline__ void sw_apply2(const SwitchT<float> &w, float2 r2, float2 rinv, float2 &e,
+                                          float2 &f) {
+  const int kind = K == SWR ? w.kind : K;
+  if (kind == SW_C2) {
+    const float2 rc = make_float2(fmaxf(r2.x, w.ron2), fmaxf(r2.y, w.ron2));
+    const float2 c2 = fma2(rc, sp2(-1.f), sp2(w.rc2));
+    const float2 nc4 = mul2(c2, fma2(rc, sp2(-2.f), sp2(-w.s2)));  // -c2 (s2 + 2 r2)
+    const float2 val = mul2(mul2(c2, sp2(-w.s1)), nc4);
+    const float2 nder = mul2(fma2(c2, c2, nc4), sp2(-w.s3));
+    f = fma2(e, nder, mul2(f, val));
+    e = mul2(e, val);
+  } else if (kind == SW_C1) {
+    const float2 dist = mul2(r2, rinv);
+    const float2 t = fma2(r2, sp2(-w.c05_3), sp2(w.c15_1));
+    const float2 val = fma2(mul2(dist, t), sp2(-1.f), sp2(1.f));
+    const float2 nder = fma2(dist, sp2(-w.c15_3), mul2(rinv, sp2(w.c15_1)));
+    f = fma2(e, nder, mul2(f, val));
+    e = mul2(e, val);
+  }
+}
+
+struct Acc2 {
+  float2 fi[3], fj[3], elj, ec, vir[6];
+};
+
+// HALF steps of one lane over its lane group's j-pairs; fi collects +f (the i-force is -fi).
+// sa: this lane's first entry of the packed staging positions (z, charges at + FAST_ENTRIES);
+// sty: its first entry of the packed types.
+template <int LSW, int CM, int CSW, bool VIR>
+__device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float2 *__restrict__ ljab,
+                                            int tio, const float4 *sa, const int2 *sty, int nxt,
+                                            float xi, float yi, float zi, float qi, Acc2 &a) {
+  const float2 nx = sp2(-xi), ny = sp2(-yi), nz = sp2(-zi);
+#pragma unroll PAIR2_STEPS_UNROLLED
+  for (int st = 0; st < HALF; st++) {
+    const float4 u = sa[st], v = sa[FAST_ENTRIES + st];
+    const int2 ty = sty[st];
+    const float2 dx = add2(make_float2(u.x, u.y), nx), dy = add2(make_float2(u.z, u.w), ny),
+                 dz = add2(make_float2(v.x, v.y), nz);
+    const float2 r2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+    const float2 m = make_float2(le_mask(r2.x, p.cut2), le_mask(r2.y, p.cut2));
+    const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+    const float2 rd2 = mul2(rinv, rinv);
+    float2 fs = sp2(0.f);
+    if constexpr (LSW != NONE) {
+      if (LSW != SWR || p.do_lj) {
+        float2 ml = m;
+        if (!p.lj_all) ml = mul2(m, make_float2(le_mask(r2.x, p.lj_cut2), le_mask(r2.y, p.lj_cut2)));
+        const float2 pa = ljab[tio + ty.x], pb = ljab[tio + ty.y];
+        const float2 A = mul2(make_float2(pa.x, pb.x), ml), B = mul2(make_float2(pa.y, pb.y), ml);
+        const float2 r6 = mul2(mul2(rd2, rd2), rd2);
+        const float2 r6B = mul2(B, r6), r12A = mul2(A, mul2(r6, r6));
+        float2 e = fma2(r6B, sp2(-1.f), r12A);
+        float2 f = mul2(fma2(r12A, sp2(12.f), mul2(r6B, sp2(-6.f))), rd2);
+        sw_apply2<LSW>(p.lj_sw, r2, rinv, e, f);
+        a.elj = add2(a.elj, e);
+        fs = f;
+      }
+    }
+    if constexpr (CM != 0) {
+      float2 mc = m;
+      if (!p.coul_all) mc = mul2(m, make_float2(le_mask(r2.x, p.coul_cut2), le_mask(r2.y, p.coul_cut2)));
+      const float2 q = mul2(make_float2(v.z, v.w), mul2(mc, sp2(qi)));
+      float2 e, f;
+      if constexpr (CM == 1) {
+        e = mul2(q, rinv);
+        f = mul2(e, rd2);
+      } else {
+        // erfc(a r) by Abramowitz & Stegun 7.1.26 as the reference evaluates it, exp(-a^2 r^2)
+        // as 2^(r^2 kexp) with kexp = -a^2 log2(e)
+        const float2 ar = mul2(mul2(r2, rinv), sp2(p.alpha));
+        const float2 xe = mul2(r2, sp2(p.kexp));
+        const float2 g = mul2(q, make_float2(ex2_ftz(xe.x), ex2_ftz(xe.y)));
+        const float2 den = fma2(ar, sp2(0.3275911f), sp2(1.f));
+        const float2 t = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
+        float2 h = fma2(t, sp2(1.061405429f), sp2(-1.453152027f));
+        h = fma2(t, h, sp2(1.421413741f));
+        h = fma2(t, h, sp2(-0.284496736f));
+        h = fma2(t, h, sp2(0.254829592f));
+        e = mul2(mul2(mul2(t, h), g), rinv);
+        f = mul2(fma2(g, sp2(p.a2pi), e), rd2);
+      }
+      sw_apply2<CSW>(p.coul_sw, r2, rinv, e, f);
+      a.ec = add2(a.ec, e);
+      fs = add2(fs, f);
+    }
+    const float2 fx = mul2(dx, fs), fy = mul2(dy, fs), fz = mul2(dz, fs);
+    if constexpr (VIR) {
+      a.vir[0] = fma2(fx, dx, a.vir[0]); a.vir[1] = fma2(fx, dy, a.vir[1]);
+      a.vir[2] = fma2(fx, dz, a.vir[2]); a.vir[3] = fma2(fy, dy, a.vir[3]);
+      a.vir[4] = fma2(fy, dz, a.vir[4]); a.vir[5] = fma2(fz, dz, a.vir[5]);
+    }
+    a.fi[0] = add2(a.fi[0], fx); a.fi[1] = add2(a.fi[1], fy); a.fi[2] = add2(a.fi[2], fz);
+    a.fj[0] = add2(a.fj[0], fx); a.fj[1] = add2(a.fj[1], fy); a.fj[2] = add2(a.fj[2], fz);
+    // rotate both j-force accumulators inside the lane group
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      a.fj[c] = make_float2(__shfl_sync(0xffffffffu, a.fj[c].x, nxt), __shfl_sync(0xffffffffu, a.fj[c].y, nxt));
+  }
+}
+
+// Bytes of one warp's j-staging region: the scalar layout (positions, metadata, original index as
+// separate unit-stride arrays, bank-conflict free for 32 distinct j-atoms) or, mixed only, the
+// packed layout; a tile uses one of them.
+template <bool MIXED>
+constexpr size_t warp_stage_bytes() {
+  using JP = decltype(JStage<MIXED>::p);
+  const size_t scalar = 32 * (sizeof(JP) + sizeof(int2) + sizeof(int));
+  const size_t packed = MIXED ? FAST_ENTRIES * (2 * sizeof(float4) + sizeof(int2)) : 0;
+  return ((scalar > packed ? scalar : packed) + 15) & ~(size_t)15;
+}
+
+// Per-warp constants of the current box and i-cluster.
+struct WarpCtx {
+  double s[3];     // box edge / 2^32: fractional fixed point to A
+  float L[3], Lr[3];
+  unsigned r0[3];  // fixed-point position of cluster atom 0 (mixed relative coordinates)
+  int pad_;
+};
+
 template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI>
-__global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 2)
+__global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR_MINB : 2)
     k_pair(SystemDev s, NbListDev nb, PairParams p,
            ParamsT<typename std::conditional<MIXED, float, double>::type> pt, const double *ljd,
            const double *lat) {
@@ -225,12 +382,6 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
   const int nt = p.ntypes, ntt = nt * nt;
   T2 *ljab = reinterpret_cast<T2 *>(smem_raw);  // [ntt] {A, B} then [ntt] {A14, B14}
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  // j-atom staging as separate arrays (positions, metadata, original index): unit-stride
-  // element types, so the per-rotation loads of 32 distinct j-atoms are bank-conflict free
-  using JP = decltype(JStage<MIXED>::p);
-  JP *spos_all = reinterpret_cast<JP *>(smem_raw + ljbytes);
-  int2 *smeta_all = reinterpret_cast<int2 *>(spos_all + PAIR_WARPS * 32);
-  int *sorig_all = reinterpret_cast<int *>(smeta_all + PAIR_WARPS * 32);
   for (int k = threadIdx.x; k < ntt; k += blockDim.x) {
     ljab[k] = T2{T(ljd[4 * k]), T(ljd[4 * k + 1])};
     ljab[ntt + k] = T2{T(ljd[4 * k + 2]), T(ljd[4 * k + 3])};
@@ -239,44 +390,61 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gb = lane & ~(BLOCK - 1), li = lane & (BLOCK - 1);  // lane group base, i-atom
-  JP *sjp = spos_all + wib * 32;
-  int2 *sjm = smeta_all + wib * 32;
-  int *sorig = sorig_all + wib * 32;
+  using JP = decltype(JStage<MIXED>::p);
+  unsigned char *wstage = smem_raw + ljbytes + wib * warp_stage_bytes<MIXED>();
+  JP *sjp = reinterpret_cast<JP *>(wstage);
+  int2 *sjm = reinterpret_cast<int2 *>(sjp + 32);
+  int *sorig = reinterpret_cast<int *>(sjm + 32);
+  // packed layout (mixed): this lane's group and i-atom entry
+  const int qe = (gb / BLOCK) * GSTRIDE + li;
+  float4 *qa = reinterpret_cast<float4 *>(wstage) + qe;
+  float4 *qb = qa + FAST_ENTRIES;
+  int2 *qt = reinterpret_cast<int2 *>(reinterpret_cast<float4 *>(wstage) + 2 * FAST_ENTRIES) + qe;
   const int gwarp = blockIdx.x * PAIR_WARPS + wib, nwarps = gridDim.x * PAIR_WARPS;
   int total = nb.tile_off[nb.nblk_total];
   if (total > nb.tile_cap) total = nb.tile_cap;
 
   int curI = -1, curBox = -1;
   long long ifix[3] = {0, 0, 0};
+  // energies and virials are converted to fixed point per lane and tile, summed over the warp
+  // only when the box changes
   long long efix_lj = 0, efix_c = 0, vfix[6] = {0, 0, 0, 0, 0, 0};
   int4 im = make_int4(-1, -1, 0, 0);   // orig, mol, type, box of this lane's i-atom
   T xi = 0, yi = 0, zi = 0, qi = 0;     // i-atom position (relative for the mixed path)
-  unsigned rx0 = 0, ry0 = 0, rz0 = 0;   // mixed: fixed-point reference (cluster atom 0)
   const BoxDev *bx = nullptr;
-  double sx = 0, sy = 0, sz = 0;
-  bool multi = false, wrap = !MIXED;
-  float Lf[3] = {0, 0, 0}, Lrf[3] = {0, 0, 0};
+  bool wrap = !MIXED;
+  // per-warp constants of the current box and cluster, kept in shared memory rather than in
+  // registers (they are read once per tile)
+  WarpCtx *ctx = reinterpret_cast<WarpCtx *>(smem_raw + ljbytes + PAIR_WARPS * warp_stage_bytes<MIXED>()) + wib;
 
+  // forces accumulate by slot, one component-major array per axis: the j-atoms of a tile come
+  // in runs of consecutive slots, so a lane group's atomics touch two sectors per axis rather than
+  // eight scattered atoms (pair_fold moves them to original order afterwards)
+  const long long nsl = nb.nslot;
   auto flush_i = [&]() {
     if (curI >= 0 && im.x >= 0 && gb == 0) {
-      long long *f = s.facc + 3 * (long long)im.x;
+      long long *f = nb.fslot + (long long)curI * BLOCK + li;
       if (ifix[0]) red_add(f, ifix[0]);
-      if (ifix[1]) red_add(f + 1, ifix[1]);
-      if (ifix[2]) red_add(f + 2, ifix[2]);
+      if (ifix[1]) red_add(f + nsl, ifix[1]);
+      if (ifix[2]) red_add(f + 2 * nsl, ifix[2]);
     }
     ifix[0] = ifix[1] = ifix[2] = 0;
   };
-  auto flush_e = [&]() {
+  auto flush_e = [&]() {  // warp-uniform
+    const long long el = warp_sum_ll(efix_lj), ec = warp_sum_ll(efix_c);
+    long long vs[6] = {0, 0, 0, 0, 0, 0};
+    if constexpr (VIR)
+      for (int c = 0; c < 6; c++) vs[c] = warp_sum_ll(vfix[c]);
     if (curBox >= 0 && lane == 0) {
       long long *e = s.eacc + (long long)curBox * ACC_PER_BOX;
-      if (efix_lj) red_add(e + E_LJ, efix_lj);
-      if (efix_c) red_add(e + E_COUL, efix_c);
+      if (el) red_add(e + E_LJ, el);
+      if (ec) red_add(e + E_COUL, ec);
       if constexpr (VIR) {
         const int map[6][2] = {{0, -1}, {1, 3}, {2, 6}, {4, -1}, {5, 7}, {8, -1}};
         for (int c = 0; c < 6; c++) {
-          if (!vfix[c]) continue;
-          red_add(e + E_VIR + map[c][0], vfix[c]);
-          if (map[c][1] >= 0) red_add(e + E_VIR + map[c][1], vfix[c]);
+          if (!vs[c]) continue;
+          red_add(e + E_VIR + map[c][0], vs[c]);
+          if (map[c][1] >= 0) red_add(e + E_VIR + map[c][1], vs[c]);
         }
       }
     }
@@ -293,8 +461,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
       js.m = make_int2(m.y, m.z);
       if constexpr (MIXED) {
         const uint4 f = nb.slot_fx[sl];
-        js.p = make_float4((float)((double)(int)(f.x - rx0) * sx), (float)((double)(int)(f.y - ry0) * sy),
-                           (float)((double)(int)(f.z - rz0) * sz), __uint_as_float(f.w));
+        js.p = make_float4((float)((double)(int)(f.x - ctx->r0[0]) * ctx->s[0]),
+                           (float)((double)(int)(f.y - ctx->r0[1]) * ctx->s[1]),
+                           (float)((double)(int)(f.z - ctx->r0[2]) * ctx->s[2]), __uint_as_float(f.w));
       } else {
         js.p = nb.slot_pq[sl];
       }
@@ -323,27 +492,34 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
           flush_e();
           curBox = bidx;
           bx = s.box + bidx;
-          multi = bx->multi_image != 0;
-          sx = bx->L[0] * (1.0 / 4294967296.0);
-          sy = bx->L[1] * (1.0 / 4294967296.0);
-          sz = bx->L[2] * (1.0 / 4294967296.0);
-          for (int c = 0; c < 3; c++) {
-            Lf[c] = (float)bx->L[c];
-            Lrf[c] = (float)bx->Lr[c];
-          }
+          __syncwarp();
+          if (lane == 0)
+            for (int c = 0; c < 3; c++) {
+              ctx->s[c] = bx->L[c] * (1.0 / 4294967296.0);
+              ctx->L[c] = (float)bx->L[c];
+              ctx->Lr[c] = (float)bx->Lr[c];
+            }
         }
         if constexpr (MIXED) {
           // coordinates relative to cluster atom 0 are minimal-image differences whenever
           // L/2 > cutoff + cluster extent; otherwise (small boxes) every pair is wrapped again
           const uint4 lo = nb.blk_lo[I], hi = nb.blk_hi[I];
           const double rmax = sqrt(p.cut2) + 1e-3;
-          wrap = multi || (double)(hi.x - lo.x) * sx + rmax >= 0.5 * bx->L[0] ||
+          const double sx = bx->L[0] * (1.0 / 4294967296.0), sy = bx->L[1] * (1.0 / 4294967296.0),
+                       sz = bx->L[2] * (1.0 / 4294967296.0);
+          wrap = bx->multi_image || (double)(hi.x - lo.x) * sx + rmax >= 0.5 * bx->L[0] ||
                  (double)(hi.y - lo.y) * sy + rmax >= 0.5 * bx->L[1] ||
                  (double)(hi.z - lo.z) * sz + rmax >= 0.5 * bx->L[2];
           const uint4 f = nb.slot_fx[sl];
-          rx0 = __shfl_sync(0xffffffffu, f.x, 0);
-          ry0 = __shfl_sync(0xffffffffu, f.y, 0);
-          rz0 = __shfl_sync(0xffffffffu, f.z, 0);
+          const unsigned rx0 = __shfl_sync(0xffffffffu, f.x, 0), ry0 = __shfl_sync(0xffffffffu, f.y, 0),
+                         rz0 = __shfl_sync(0xffffffffu, f.z, 0);
+          __syncwarp();
+          if (lane == 0) {
+            ctx->r0[0] = rx0;
+            ctx->r0[1] = ry0;
+            ctx->r0[2] = rz0;
+          }
+          __syncwarp();
           if (im.x >= 0) {
             xi = (float)((double)(int)(f.x - rx0) * sx);
             yi = (float)((double)(int)(f.y - ry0) * sy);
@@ -363,136 +539,187 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? 3 : 
         }
       }
       const bool diag = (k == 0);
-      // diagonal tile: the cluster against itself (lane group 0); other tiles: 32 listed j-atoms
-      const int jsl = diag ? (gb ? -1 : I * BLOCK + li) : nb.jlist[nb.jcap_off[I] + (k - 1) * JCHUNK + lane];
+      // diagonal tile: the cluster against itself (lane group 0); other tiles: 32 listed j-atoms,
+      // JSAME marking those that share a molecule with the cluster
+      const int jraw = diag ? (gb ? -1 : I * BLOCK + li) : nb.jlist[nb.jcap_off[I] + (k - 1) * JCHUNK + lane];
+      const int jsl = jraw < 0 ? -1 : (jraw & ~JSAME);
+      const bool same = diag || __any_sync(0xffffffffu, jraw >= 0 && (jraw & JSAME));
       JStage<MIXED> mine;
       int jorig;
       stage_slot(jsl, mine, jorig);
-      __syncwarp();
-      sjp[lane] = mine.p;
-      sjm[lane] = mine.m;
-      sorig[lane] = jorig;
-      __syncwarp();
-
-      Acc<T> a;
-      a.fi[0] = a.fi[1] = a.fi[2] = T(0);
-      a.elj = a.ec = T(0);
-      for (int c = 0; c < 6; c++) a.vir[c] = T(0);
-      T fj[3] = {T(0), T(0), T(0)};
       const int tio = im.z * nt;
       const int nxt = gb | ((li + 1) & (BLOCK - 1));
-      const T cut2 = pt.cut2;
+      // per-lane results of the tile: i-force, own j-force, energies, virial
+      T tfi[3], tfj[3], tel, tec, tvir[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
 
-      const bool ivalid = im.x >= 0;
-      auto body = [&](auto diag_tag, auto wrap_tag) {
-        constexpr bool DIAG = decltype(diag_tag)::value;
-        constexpr bool WRAP = decltype(wrap_tag)::value;
+      bool packed = false;
+      if constexpr (MIXED) {
+        if (!wrap && !same) {
+          packed = true;
+          // the pair partner (j + HALF) of this lane's j-atom, then two copies of the entry
+          const float4 P = mine.p;
+          const float px = __shfl_xor_sync(0xffffffffu, P.x, HALF), py = __shfl_xor_sync(0xffffffffu, P.y, HALF),
+                      pz = __shfl_xor_sync(0xffffffffu, P.z, HALF), pq = __shfl_xor_sync(0xffffffffu, P.w, HALF);
+          const int ptype = __shfl_xor_sync(0xffffffffu, mine.m.y, HALF);
+          const float4 ea = make_float4(P.x, px, P.y, py), eb = make_float4(P.z, pz, P.w, pq);
+          const int2 et = make_int2(mine.m.y, ptype);
+          __syncwarp();
+          qa[0] = ea; qa[BLOCK] = ea;
+          qb[0] = eb; qb[BLOCK] = eb;
+          qt[0] = et; qt[BLOCK] = et;
+          __syncwarp();
+          Acc2 a2;
+#pragma unroll
+          for (int c = 0; c < 3; c++) a2.fi[c] = a2.fj[c] = sp2(0.f);
+          a2.elj = a2.ec = sp2(0.f);
+#pragma unroll
+          for (int c = 0; c < 6; c++) a2.vir[c] = sp2(0.f);
+          tile_pairs2<LSW, CM, CSW, VIR>(pt, reinterpret_cast<const float2 *>(ljab), tio, qa, qt, nxt, xi,
+                                         yi, zi, qi, a2);
+          // after HALF rotations: .y holds this lane's j-atom, .x that of the lane HALF away
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            tfj[c] = a2.fj[c].y + __shfl_xor_sync(0xffffffffu, a2.fj[c].x, HALF);
+            tfi[c] = -(a2.fi[c].x + a2.fi[c].y);
+          }
+          tel = a2.elj.x + a2.elj.y;
+          tec = a2.ec.x + a2.ec.y;
+          if constexpr (VIR)
+            for (int c = 0; c < 6; c++) tvir[c] = a2.vir[c].x + a2.vir[c].y;
+        }
+      }
+      if (!packed) {
+        __syncwarp();
+        sjp[lane] = mine.p;
+        sjm[lane] = mine.m;
+        sorig[lane] = jorig;
+        __syncwarp();
+
+        Acc<T> a;
+        a.fi[0] = a.fi[1] = a.fi[2] = T(0);
+        a.elj = a.ec = T(0);
+        for (int c = 0; c < 6; c++) a.vir[c] = T(0);
+        T fj[3] = {T(0), T(0), T(0)};
+        const T cut2 = pt.cut2;
+
+        const bool ivalid = im.x >= 0;
+        auto body = [&](auto diag_tag, auto wrap_tag) {
+          constexpr bool DIAG = decltype(diag_tag)::value;
+          constexpr bool WRAP = decltype(wrap_tag)::value;
 #pragma unroll 2
-        for (int st = 0; st < BLOCK; st++) {
-          const int jl = (li + st) & (BLOCK - 1);
-          JStage<MIXED> dj;
-          dj.p = sjp[gb | jl];
-          dj.m = sjm[gb | jl];
-          T dx = T(dj.p.x) - xi, dy = T(dj.p.y) - yi, dz = T(dj.p.z) - zi;
-          if constexpr (!MIXED) {
-            // the reference's minimal image: d - L rint(d / L) equals its single-wrap result
-            dx -= bx->L[0] * rint(bx->Lr[0] * dx);
-            dy -= bx->L[1] * rint(bx->Lr[1] * dy);
-            dz -= bx->L[2] * rint(bx->Lr[2] * dz);
-          } else if constexpr (WRAP) {
-            dx -= Lf[0] * rintf(Lrf[0] * dx);
-            dy -= Lf[1] * rintf(Lrf[1] * dy);
-            dz -= Lf[2] * rintf(Lrf[2] * dz);
-          }
-          const T r2 = dx * dx + dy * dy + dz * dz;
-          bool in = r2 <= cut2;
-          if constexpr (WRAP) in = in && ivalid && dj.m.x >= 0;  // sentinels do not survive a wrap
-          if constexpr (DIAG) in = in && jl > li;
-          int ex = 0;
-          if (in && im.y == dj.m.x) {
-            ex = excl_check(s, im.x, sorig[gb | jl]);
-            if (ex == 2) in = false;
-          }
-          T2 ab;
-          if constexpr (LSW != NONE) ab = ljab[(ex == 1 ? ntt : 0) + tio + dj.m.y];
-          else ab = T2{T(0), T(0)};
-          T fs = pair_force<MIXED, LSW, CM, CSW>(pt, in, ex, r2, qi * T(dj.p.w), ab, a);
-          T fx = dx * fs, fy = dy * fs, fz = dz * fs;
-          if constexpr (VIR) {
-            a.vir[0] += fx * dx; a.vir[1] += fx * dy; a.vir[2] += fx * dz;
-            a.vir[3] += fy * dy; a.vir[4] += fy * dz; a.vir[5] += fz * dz;
-          }
-          if constexpr (CM == 2 && MULTI && WRAP) {
-            // Lattice images beyond the minimal one (edge below twice the cutoff): the reference
-            // loops myLattice for every pair (NonbondedPMEwaldSystemForce.h:644-650); FULL
-            // exclusions skip only the first image, MODIFIED scaling applies to it only.
-            if (multi) {
-              bool pv = dj.m.x >= 0 && im.x >= 0;
-              if constexpr (DIAG) pv = pv && jl > li;
-              for (int kk = 1; kk < bx->nlat; kk++) {
-                const double *lv = lat + 3 * (bx->lat0 + kk);
-                T rx = dx + T(lv[0]), ry = dy + T(lv[1]), rz = dz + T(lv[2]);
-                T rr2 = rx * rx + ry * ry + rz * rz;
-                bool inl = pv && rr2 <= pt.coul_cut2;
-                Acc<T> b2;
-                b2.elj = T(0);
-                b2.ec = T(0);
-                T g = pair_force<MIXED, NONE, 2, CSW>(pt, inl, 0, rr2, qi * T(dj.p.w), T2{T(0), T(0)}, b2);
-                a.ec += b2.ec;
-                T gx = rx * g, gy = ry * g, gz = rz * g;
-                fx += gx; fy += gy; fz += gz;
-                if constexpr (VIR) {
-                  a.vir[0] += gx * rx; a.vir[1] += gx * ry; a.vir[2] += gx * rz;
-                  a.vir[3] += gy * ry; a.vir[4] += gy * rz; a.vir[5] += gz * rz;
+          for (int st = 0; st < BLOCK; st++) {
+            const int jl = (li + st) & (BLOCK - 1);
+            JStage<MIXED> dj;
+            dj.p = sjp[gb | jl];
+            dj.m = sjm[gb | jl];
+            T dx = T(dj.p.x) - xi, dy = T(dj.p.y) - yi, dz = T(dj.p.z) - zi;
+            if constexpr (!MIXED) {
+              // the reference's minimal image: d - L rint(d / L) equals its single-wrap result
+              dx -= bx->L[0] * rint(bx->Lr[0] * dx);
+              dy -= bx->L[1] * rint(bx->Lr[1] * dy);
+              dz -= bx->L[2] * rint(bx->Lr[2] * dz);
+            } else if constexpr (WRAP) {
+              dx -= ctx->L[0] * rintf(ctx->Lr[0] * dx);
+              dy -= ctx->L[1] * rintf(ctx->Lr[1] * dy);
+              dz -= ctx->L[2] * rintf(ctx->Lr[2] * dz);
+            }
+            const T r2 = dx * dx + dy * dy + dz * dz;
+            bool in = r2 <= cut2;
+            if constexpr (WRAP) in = in && ivalid && dj.m.x >= 0;  // sentinels do not survive a wrap
+            if constexpr (DIAG) in = in && jl > li;
+            int ex = 0;
+            if (in && im.y == dj.m.x) {
+              ex = excl_check(s, im.x, sorig[gb | jl]);
+              if (ex == 2) in = false;
+            }
+            T2 ab;
+            if constexpr (LSW != NONE) ab = ljab[(ex == 1 ? ntt : 0) + tio + dj.m.y];
+            else ab = T2{T(0), T(0)};
+            T fs = pair_force<MIXED, LSW, CM, CSW>(pt, in, ex, r2, qi * T(dj.p.w), ab, a);
+            T fx = dx * fs, fy = dy * fs, fz = dz * fs;
+            if constexpr (VIR) {
+              a.vir[0] += fx * dx; a.vir[1] += fx * dy; a.vir[2] += fx * dz;
+              a.vir[3] += fy * dy; a.vir[4] += fy * dz; a.vir[5] += fz * dz;
+            }
+            if constexpr (CM == 2 && MULTI && WRAP) {
+              // Lattice images beyond the minimal one (edge below twice the cutoff): the reference
+              // loops myLattice for every pair (NonbondedPMEwaldSystemForce.h:644-650); FULL
+              // exclusions skip only the first image, MODIFIED scaling applies to it only.
+              if (bx->multi_image) {
+                bool pv = dj.m.x >= 0 && im.x >= 0;
+                if constexpr (DIAG) pv = pv && jl > li;
+                for (int kk = 1; kk < bx->nlat; kk++) {
+                  const double *lv = lat + 3 * (bx->lat0 + kk);
+                  T rx = dx + T(lv[0]), ry = dy + T(lv[1]), rz = dz + T(lv[2]);
+                  T rr2 = rx * rx + ry * ry + rz * rz;
+                  bool inl = pv && rr2 <= pt.coul_cut2;
+                  Acc<T> b2;
+                  b2.elj = T(0);
+                  b2.ec = T(0);
+                  T g = pair_force<MIXED, NONE, 2, CSW>(pt, inl, 0, rr2, qi * T(dj.p.w), T2{T(0), T(0)}, b2);
+                  a.ec += b2.ec;
+                  T gx = rx * g, gy = ry * g, gz = rz * g;
+                  fx += gx; fy += gy; fz += gz;
+                  if constexpr (VIR) {
+                    a.vir[0] += gx * rx; a.vir[1] += gx * ry; a.vir[2] += gx * rz;
+                    a.vir[3] += gy * ry; a.vir[4] += gy * rz; a.vir[5] += gz * rz;
+                  }
                 }
               }
             }
+            a.fi[0] -= fx; a.fi[1] -= fy; a.fi[2] -= fz;
+            fj[0] += fx; fj[1] += fy; fj[2] += fz;
+            // rotate j-force accumulators inside the lane group
+            fj[0] = __shfl_sync(0xffffffffu, fj[0], nxt);
+            fj[1] = __shfl_sync(0xffffffffu, fj[1], nxt);
+            fj[2] = __shfl_sync(0xffffffffu, fj[2], nxt);
           }
-          a.fi[0] -= fx; a.fi[1] -= fy; a.fi[2] -= fz;
-          fj[0] += fx; fj[1] += fy; fj[2] += fz;
-          // rotate j-force accumulators inside the lane group
-          fj[0] = __shfl_sync(0xffffffffu, fj[0], nxt);
-          fj[1] = __shfl_sync(0xffffffffu, fj[1], nxt);
-          fj[2] = __shfl_sync(0xffffffffu, fj[2], nxt);
+        };
+        bool unwrapped = false;
+        if constexpr (MIXED) {
+          if (!wrap) {
+            unwrapped = true;
+            if (diag) body(std::true_type{}, std::false_type{});
+            else body(std::false_type{}, std::false_type{});
+          }
         }
-      };
-      bool unwrapped = false;
-      if constexpr (MIXED) {
-        if (!wrap) {
-          unwrapped = true;
-          if (diag) body(std::true_type{}, std::false_type{});
-          else body(std::false_type{}, std::false_type{});
+        if (!unwrapped) {
+          if (diag) body(std::true_type{}, std::true_type{});
+          else body(std::false_type{}, std::true_type{});
         }
-      }
-      if (!unwrapped) {
-        if (diag) body(std::true_type{}, std::true_type{});
-        else body(std::false_type{}, std::true_type{});
+        // after BLOCK rotations lane l holds the accumulator of j-atom l of the tile
+        for (int c = 0; c < 3; c++) {
+          tfi[c] = a.fi[c];
+          tfj[c] = fj[c];
+        }
+        tel = a.elj;
+        tec = a.ec;
+        if constexpr (VIR)
+          for (int c = 0; c < 6; c++) tvir[c] = a.vir[c];
       }
 
-      // after BLOCK rotations lane l holds the accumulator of j-atom l of the tile
       if (diag) {
-        a.fi[0] += fj[0]; a.fi[1] += fj[1]; a.fi[2] += fj[2];
+        tfi[0] += tfj[0]; tfi[1] += tfj[1]; tfi[2] += tfj[2];
       } else if (jorig >= 0) {
-        long long *f = s.facc + 3 * (long long)jorig;
-        long long v0 = f2fix(fj[0], (T)FORCE_SCALE), v1 = f2fix(fj[1], (T)FORCE_SCALE),
-                  v2 = f2fix(fj[2], (T)FORCE_SCALE);
+        long long *f = nb.fslot + jsl;
+        long long v0 = f2fix(tfj[0], (T)FORCE_SCALE), v1 = f2fix(tfj[1], (T)FORCE_SCALE),
+                  v2 = f2fix(tfj[2], (T)FORCE_SCALE);
         if (v0) red_add(f, v0);
-        if (v1) red_add(f + 1, v1);
-        if (v2) red_add(f + 2, v2);
+        if (v1) red_add(f + nsl, v1);
+        if (v2) red_add(f + 2 * nsl, v2);
       }
       // combine the lane groups of the i-cluster
 #pragma unroll
       for (int o = BLOCK; o < 32; o <<= 1)
 #pragma unroll
-        for (int c = 0; c < 3; c++) a.fi[c] += __shfl_xor_sync(0xffffffffu, a.fi[c], o);
-      ifix[0] += f2fix(a.fi[0], (T)FORCE_SCALE);
-      ifix[1] += f2fix(a.fi[1], (T)FORCE_SCALE);
-      ifix[2] += f2fix(a.fi[2], (T)FORCE_SCALE);
-      double el = (double)warp_sum(a.elj), ecc = (double)warp_sum(a.ec);
-      efix_lj += f2fix(el, ENERGY_SCALE);
-      efix_c += f2fix(ecc, ENERGY_SCALE);
+        for (int c = 0; c < 3; c++) tfi[c] += __shfl_xor_sync(0xffffffffu, tfi[c], o);
+      ifix[0] += f2fix(tfi[0], (T)FORCE_SCALE);
+      ifix[1] += f2fix(tfi[1], (T)FORCE_SCALE);
+      ifix[2] += f2fix(tfi[2], (T)FORCE_SCALE);
+      efix_lj += f2fix(tel, (T)ENERGY_SCALE);
+      efix_c += f2fix(tec, (T)ENERGY_SCALE);
       if constexpr (VIR) {
-        for (int c = 0; c < 6; c++) vfix[c] += f2fix((double)warp_sum(a.vir[c]), ENERGY_SCALE);
+        for (int c = 0; c < 6; c++) vfix[c] += f2fix(tvir[c], (T)ENERGY_SCALE);
       }
     }
   }
@@ -509,7 +736,7 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
   const int ntt = pl.p.ntypes * pl.p.ntypes;
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  size_t smem = ljbytes + PAIR_WARPS * 32 * (sizeof(decltype(JStage<MIXED>::p)) + sizeof(int2) + sizeof(int));
+  size_t smem = ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx));
   static int grid = 0;
   static size_t conf_smem = 0;
   if (!grid || conf_smem != smem) {
@@ -547,6 +774,29 @@ int launch_v(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
 }
 
 }  // namespace
+
+// Adds the slot-ordered pair forces to the original-order accumulator and clears them (one thread
+// per slot; each atom owns one slot, so the read-modify-write needs no atomics).
+__global__ void k_pair_fold(SystemDev s, NbListDev nb) {
+  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nb.nslot) return;
+  const int o = nb.slot_orig[sl];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    long long *p = nb.fslot + (long long)c * nb.nslot + sl;
+    const long long v = *p;
+    if (v) {
+      *p = 0;
+      if (o >= 0) s.facc[3 * (long long)o + c] += v;
+    }
+  }
+}
+
+int pair_fold(const SystemDev &s, const NbListDev &nb, cudaStream_t st) {
+  const int T = 256;
+  if (nb.nslot > 0) k_pair_fold<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb);
+  return 0;
+}
 
 int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st) {
   if (pl.p.ntypes > MAX_LJ_TYPES) return -1;
