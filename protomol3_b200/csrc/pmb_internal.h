@@ -35,7 +35,7 @@ struct NbListDev {
   int nsblk;                   // superblocks: runs of 32 consecutive blocks
   uint4 *sblk_lo, *sblk_hi;    // [nsblk] union of their blocks' extents, .w = atoms
   int *jcap_off;               // [nblk+1] offset of each block's j-slot list region
-  int *jcount;                 // [nblk] tiles per block (1 diagonal + list tiles)
+  int *jcount;                 // [nblk] tiles per block (its j-list, own slots first, in 32s)
   int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding), JSAME flag bit
   int *tile_off;               // [nblk+1] exclusive scan of jcount
   int *tile_blk;               // [tile_cap] block of each tile

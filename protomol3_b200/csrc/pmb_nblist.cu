@@ -353,8 +353,9 @@ __device__ __forceinline__ void center_half(uint4 lo, uint4 hi, unsigned c[3], u
   }
 }
 
-// One warp per block I: candidate blocks J > I of the same box by bounding-box gap, then the
-// atoms of each candidate within the list cutoff of I's box, compacted into I's j-list.
+// One warp per block I: its own slots, then the candidate blocks J > I of the same box by
+// bounding-box gap and the atoms of each candidate within the list cutoff of I's box, compacted
+// into I's j-list (tiles of 32 entries).
 __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   if (!nb.ctl[1]) return;
   int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -371,7 +372,12 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   int jend = b.blk0 + b.nblk;
   int cap = nb.jcap_off[I + 1] - nb.jcap_off[I];
   int *out = nb.jlist + nb.jcap_off[I];
-  int count = 0;
+  // the block's own slots open its list (flagged JSAME: the pair kernel takes j > i among them)
+  if (lane < BLOCK) {
+    const int sl = I * BLOCK + lane;
+    out[lane] = nb.slot_orig[sl] >= 0 ? (sl | JSAME) : -1;
+  }
+  int count = BLOCK;
   bool overflow = false;
   unsigned zero[3] = {0, 0, 0};
   const float sL[3] = {(float)(b.L[0] * (1.0 / 4294967296.0)), (float)(b.L[1] * (1.0 / 4294967296.0)),
@@ -463,7 +469,7 @@ __global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
     for (int k = count + lane; k < padded; k += 32) out[k] = -1;
   if (lane == 0) {
     if (overflow) atomicExch(&nb.status[0], 1);
-    nb.jcount[I] = overflow ? 1 : 1 + padded / 32;
+    nb.jcount[I] = overflow ? 0 : padded / 32;
   }
 }
 

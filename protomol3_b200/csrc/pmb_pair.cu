@@ -9,11 +9,12 @@
 //
 // Warp tiling: the BLOCK atoms of cluster I sit once in each of the GROUPS lane groups of the
 // warp; the 32 j-atoms of the tile are staged in shared memory, lane group g visits j-atoms
-// [g BLOCK, (g + 1) BLOCK) in BLOCK rotations; the j-force accumulators travel with the rotation
+// [g BLOCK, (g + 1) BLOCK) in rotations; the j-force accumulators travel with the rotation
 // through shuffles inside the group (Newton's third law inside the tile), the groups' i-forces
-// are combined once per tile.  Forces leave as int64 fixed point (one atomic per j-atom per tile, one per
-// i-atom per run of tiles of the same cluster); energies and virials are summed per tile in a
-// fixed shuffle order and added in fixed point, so results are bit-identical run to run.
+// are combined once per tile.  A cluster's j-list opens with its own atoms (pairs j > i of lane
+// group 0 in its first tile).  Forces leave as int64 fixed point by slot (one atomic per j-atom
+// and per i-atom per tile); energies and virials are summed per lane and added in fixed point,
+// so results are bit-identical run to run.
 //
 // The inner loop is branch-free: every lane evaluates the potentials on a clamped distance and
 // the result is masked, because about half of the pairs of a tile lie outside the cutoff and a
@@ -239,15 +240,64 @@ constexpr int PAIR2_STEPS_UNROLLED = PAIR2_UNROLL;
 #define PAIR_MINB 3  // resident blocks per SM of the mixed kernels
 #endif
 
+// Operations whose operands are all per-pair values use the two-wide instructions; those with a
+// constant operand (kernel parameters, polynomial coefficients) are issued as two scalar
+// instructions, which read the constant bank directly instead of materialising a register pair
+// per use (PAIR2_CONST_MODE 0: two-wide for those too; 2: everything scalar).
+#ifndef PAIR2_CONST_MODE
+#define PAIR2_CONST_MODE 0
+#endif
+__device__ __forceinline__ float2 sp2(float v) { return make_float2(v, v); }
+#if PAIR2_CONST_MODE == 2
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+}
+#else
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 sp2(float v) { return make_float2(v, v); }
+#endif
+#if PAIR2_CONST_MODE == 0
+__device__ __forceinline__ float2 mulk(float2 a, float k) { return mul2(a, sp2(k)); }
+__device__ __forceinline__ float2 fmak(float2 a, float k, float2 b) { return fma2(a, sp2(k), b); }
+__device__ __forceinline__ float2 fmakk(float2 a, float k, float c) { return fma2(a, sp2(k), sp2(c)); }
+__device__ __forceinline__ float2 fmaK(float2 a, float2 b, float c) { return fma2(a, b, sp2(c)); }
+#else
+// a k, a k + b, a k + c, a b + c with scalar constants k, c
+__device__ __forceinline__ float2 mulk(float2 a, float k) { return make_float2(a.x * k, a.y * k); }
+__device__ __forceinline__ float2 fmak(float2 a, float k, float2 b) {
+  return make_float2(fmaf(a.x, k, b.x), fmaf(a.y, k, b.y));
+}
+__device__ __forceinline__ float2 fmakk(float2 a, float k, float c) {
+  return make_float2(fmaf(a.x, k, c), fmaf(a.y, k, c));
+}
+__device__ __forceinline__ float2 fmaK(float2 a, float2 b, float c) {
+  return make_float2(fmaf(a.x, b.x, c), fmaf(a.y, b.y, c));
+}
+#endif
 // 1.0f where a <= b, else 0.0f (one SET instruction)
 __device__ __forceinline__ float le_mask(float a, float b) {
   float r;
   asm("set.le.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
   return r;
+}
+
+// Asynchronous global -> shared copies (cp.async, L1-allocating) used to prefetch the next tile's
+// j-list entries and slot records while the current tile computes.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 template <int K>
@@ -256,17 +306,17 @@ __device__ __forceinline__ void sw_apply2(const SwitchT<float> &w, float2 r2, fl
   const int kind = K == SWR ? w.kind : K;
   if (kind == SW_C2) {
     const float2 rc = make_float2(fmaxf(r2.x, w.ron2), fmaxf(r2.y, w.ron2));
-    const float2 c2 = fma2(rc, sp2(-1.f), sp2(w.rc2));
-    const float2 nc4 = mul2(c2, fma2(rc, sp2(-2.f), sp2(-w.s2)));  // -c2 (s2 + 2 r2)
-    const float2 val = mul2(mul2(c2, sp2(-w.s1)), nc4);
-    const float2 nder = mul2(fma2(c2, c2, nc4), sp2(-w.s3));
+    const float2 c2 = fmakk(rc, -1.f, w.rc2);
+    const float2 nc4 = mul2(c2, fmakk(rc, -2.f, -w.s2));  // -c2 (s2 + 2 r2)
+    const float2 val = mul2(mulk(c2, -w.s1), nc4);
+    const float2 nder = mulk(fma2(c2, c2, nc4), -w.s3);
     f = fma2(e, nder, mul2(f, val));
     e = mul2(e, val);
   } else if (kind == SW_C1) {
     const float2 dist = mul2(r2, rinv);
-    const float2 t = fma2(r2, sp2(-w.c05_3), sp2(w.c15_1));
-    const float2 val = fma2(mul2(dist, t), sp2(-1.f), sp2(1.f));
-    const float2 nder = fma2(dist, sp2(-w.c15_3), mul2(rinv, sp2(w.c15_1)));
+    const float2 t = fmakk(r2, -w.c05_3, w.c15_1);
+    const float2 val = fmakk(mul2(dist, t), -1.f, 1.f);
+    const float2 nder = fmak(dist, -w.c15_3, mulk(rinv, w.c15_1));
     f = fma2(e, nder, mul2(f, val));
     e = mul2(e, val);
   }
@@ -283,7 +333,7 @@ template <int LSW, int CM, int CSW, bool VIR>
 __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float2 *__restrict__ ljab,
                                             int tio, const float4 *sa, const int2 *sty, int nxt,
                                             float xi, float yi, float zi, float qi, Acc2 &a) {
-  const float2 nx = sp2(-xi), ny = sp2(-yi), nz = sp2(-zi);
+  const float2 nx = sp2(-xi), ny = sp2(-yi), nz = sp2(-zi), qi2 = sp2(qi);
 #pragma unroll PAIR2_STEPS_UNROLLED
   for (int st = 0; st < HALF; st++) {
     const float4 u = sa[st], v = sa[FAST_ENTRIES + st];
@@ -303,8 +353,8 @@ __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float
         const float2 A = mul2(make_float2(pa.x, pb.x), ml), B = mul2(make_float2(pa.y, pb.y), ml);
         const float2 r6 = mul2(mul2(rd2, rd2), rd2);
         const float2 r6B = mul2(B, r6), r12A = mul2(A, mul2(r6, r6));
-        float2 e = fma2(r6B, sp2(-1.f), r12A);
-        float2 f = mul2(fma2(r12A, sp2(12.f), mul2(r6B, sp2(-6.f))), rd2);
+        float2 e = fmak(r6B, -1.f, r12A);
+        float2 f = mul2(fmak(r12A, 12.f, mulk(r6B, -6.f)), rd2);
         sw_apply2<LSW>(p.lj_sw, r2, rinv, e, f);
         a.elj = add2(a.elj, e);
         fs = f;
@@ -313,7 +363,7 @@ __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float
     if constexpr (CM != 0) {
       float2 mc = m;
       if (!p.coul_all) mc = mul2(m, make_float2(le_mask(r2.x, p.coul_cut2), le_mask(r2.y, p.coul_cut2)));
-      const float2 q = mul2(make_float2(v.z, v.w), mul2(mc, sp2(qi)));
+      const float2 q = mul2(make_float2(v.z, v.w), mul2(mc, qi2));
       float2 e, f;
       if constexpr (CM == 1) {
         e = mul2(q, rinv);
@@ -321,17 +371,17 @@ __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float
       } else {
         // erfc(a r) by Abramowitz & Stegun 7.1.26 as the reference evaluates it, exp(-a^2 r^2)
         // as 2^(r^2 kexp) with kexp = -a^2 log2(e)
-        const float2 ar = mul2(mul2(r2, rinv), sp2(p.alpha));
-        const float2 xe = mul2(r2, sp2(p.kexp));
+        const float2 ar = mulk(mul2(r2, rinv), p.alpha);
+        const float2 xe = mulk(r2, p.kexp);
         const float2 g = mul2(q, make_float2(ex2_ftz(xe.x), ex2_ftz(xe.y)));
-        const float2 den = fma2(ar, sp2(0.3275911f), sp2(1.f));
+        const float2 den = fmakk(ar, 0.3275911f, 1.f);
         const float2 t = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
-        float2 h = fma2(t, sp2(1.061405429f), sp2(-1.453152027f));
-        h = fma2(t, h, sp2(1.421413741f));
-        h = fma2(t, h, sp2(-0.284496736f));
-        h = fma2(t, h, sp2(0.254829592f));
+        float2 h = fmakk(t, 1.061405429f, -1.453152027f);
+        h = fmaK(t, h, 1.421413741f);
+        h = fmaK(t, h, -0.284496736f);
+        h = fmaK(t, h, 0.254829592f);
         e = mul2(mul2(mul2(t, h), g), rinv);
-        f = mul2(fma2(g, sp2(p.a2pi), e), rd2);
+        f = mul2(fmak(g, p.a2pi, e), rd2);
       }
       sw_apply2<CSW>(p.coul_sw, r2, rinv, e, f);
       a.ec = add2(a.ec, e);
@@ -371,6 +421,14 @@ struct WarpCtx {
   int pad_;
 };
 
+// Bytes of one warp's prefetch region: the j-list entries of a chunk of tiles, and two buffers of
+// slot records (position, metadata) and raw j-list words for the tile in flight and the next.
+template <bool MIXED>
+constexpr size_t warp_pref_bytes() {
+  return 2 * 32 * (MIXED ? sizeof(uint4) : sizeof(double4)) + 2 * 32 * sizeof(int4) + CHUNK * 32 * sizeof(int) +
+         2 * 32 * sizeof(int);
+}
+
 template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI>
 __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR_MINB : 2)
     k_pair(SystemDev s, NbListDev nb, PairParams p,
@@ -405,10 +463,15 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
   if (total > nb.tile_cap) total = nb.tile_cap;
 
   int curI = -1, curBox = -1;
-  long long ifix[3] = {0, 0, 0};
-  // energies and virials are converted to fixed point per lane and tile, summed over the warp
-  // only when the box changes
-  long long efix_lj = 0, efix_c = 0, vfix[6] = {0, 0, 0, 0, 0, 0};
+  // energies (and virials) per lane: summed in the arithmetic type over a chunk of tiles, then
+  // added in fixed point to this lane's slots in shared memory; summed over the warp and added to
+  // the box accumulators when the box changes
+  T el_acc = T(0), ec_acc = T(0), v_acc[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  constexpr int NE = VIR ? 8 : 2;
+  long long *wsum = reinterpret_cast<long long *>(
+      smem_raw + ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx))) + wib * NE * 32;
+#pragma unroll
+  for (int c = 0; c < NE; c++) wsum[c * 32 + lane] = 0;
   int4 im = make_int4(-1, -1, 0, 0);   // orig, mol, type, box of this lane's i-atom
   T xi = 0, yi = 0, zi = 0, qi = 0;     // i-atom position (relative for the mixed path)
   const BoxDev *bx = nullptr;
@@ -421,20 +484,24 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
   // in runs of consecutive slots, so a lane group's atomics touch two sectors per axis rather than
   // eight scattered atoms (pair_fold moves them to original order afterwards)
   const long long nsl = nb.nslot;
-  auto flush_i = [&]() {
-    if (curI >= 0 && im.x >= 0 && gb == 0) {
-      long long *f = nb.fslot + (long long)curI * BLOCK + li;
-      if (ifix[0]) red_add(f, ifix[0]);
-      if (ifix[1]) red_add(f + nsl, ifix[1]);
-      if (ifix[2]) red_add(f + 2 * nsl, ifix[2]);
+  auto spill_e = [&]() {
+    wsum[lane] += f2fix(el_acc, (T)ENERGY_SCALE);
+    wsum[32 + lane] += f2fix(ec_acc, (T)ENERGY_SCALE);
+    el_acc = ec_acc = T(0);
+    if constexpr (VIR) {
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        wsum[(2 + c) * 32 + lane] += f2fix(v_acc[c], (T)ENERGY_SCALE);
+        v_acc[c] = T(0);
+      }
     }
-    ifix[0] = ifix[1] = ifix[2] = 0;
   };
   auto flush_e = [&]() {  // warp-uniform
-    const long long el = warp_sum_ll(efix_lj), ec = warp_sum_ll(efix_c);
+    spill_e();
+    const long long el = warp_sum_ll(wsum[lane]), ec = warp_sum_ll(wsum[32 + lane]);
     long long vs[6] = {0, 0, 0, 0, 0, 0};
     if constexpr (VIR)
-      for (int c = 0; c < 6; c++) vs[c] = warp_sum_ll(vfix[c]);
+      for (int c = 0; c < 6; c++) vs[c] = warp_sum_ll(wsum[(2 + c) * 32 + lane]);
     if (curBox >= 0 && lane == 0) {
       long long *e = s.eacc + (long long)curBox * ACC_PER_BOX;
       if (el) red_add(e + E_LJ, el);
@@ -448,24 +515,55 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
         }
       }
     }
-    efix_lj = efix_c = 0;
-    for (int c = 0; c < 6; c++) vfix[c] = 0;
+#pragma unroll
+    for (int c = 0; c < NE; c++) wsum[c * 32 + lane] = 0;
   };
   // stage one slot (or padding) as this lane's j-atom
   // (padding slots of a box's last cluster, orig < 0, become sentinels as well: they carry no
   // charge but an LJ type, and must never meet a real atom)
-  auto stage_slot = [&](int sl, JStage<MIXED> &js, int &orig) {
-    const int4 m = sl >= 0 ? nb.slot_meta[sl] : make_int4(-1, -1, 0, 0);
+  // prefetch region: slot records [2][32], metadata [2][32], a chunk's j-list words [CHUNK][32],
+  // raw j-list words of the buffered tiles [2][32]
+  using RawP = typename std::conditional<MIXED, uint4, double4>::type;
+  unsigned char *wpref = smem_raw + ljbytes +
+                         PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx) + NE * 32 * sizeof(long long)) +
+                         wib * warp_pref_bytes<MIXED>();
+  RawP *rawP = reinterpret_cast<RawP *>(wpref);
+  int4 *rawM = reinterpret_cast<int4 *>(rawP + 64);
+  int *jbuf = reinterpret_cast<int *>(rawM + 64);
+  int *rawJ = jbuf + CHUNK * 32;
+  int tI = -1, tk = -1, tjb = 0;  // lane t < CHUNK: block, index and j-list offset of chunk tile t
+  // issues the copies of tile t's slot records into buffer b (warp-uniform; one commit group)
+  auto prefetch = [&](int t, int b) {
+    const int It = __shfl_sync(0xffffffffu, tI, t), kt = __shfl_sync(0xffffffffu, tk, t);
+    int jr = -1;
+    if (It >= 0) jr = jbuf[t * 32 + lane];
+    rawJ[b * 32 + lane] = jr;
+    const int sl = jr < 0 ? -1 : (jr & ~JSAME);
+    if (sl >= 0) {
+      if constexpr (MIXED) {
+        cp_async16(rawP + b * 32 + lane, nb.slot_fx + sl);
+      } else {
+        cp_async16(rawP + b * 32 + lane, nb.slot_pq + sl);
+        cp_async16(reinterpret_cast<unsigned char *>(rawP + b * 32 + lane) + 16,
+                   reinterpret_cast<const unsigned char *>(nb.slot_pq + sl) + 16);
+      }
+      cp_async16(rawM + b * 32 + lane, nb.slot_meta + sl);
+    }
+    cp_async_commit();
+  };
+  // stage this lane's j-atom of buffer b (or padding)
+  auto stage_slot = [&](int sl, int b, JStage<MIXED> &js, int &orig) {
+    const int4 m = sl >= 0 ? rawM[b * 32 + lane] : make_int4(-1, -1, 0, 0);
     if (m.x >= 0) {
       orig = m.x;
       js.m = make_int2(m.y, m.z);
       if constexpr (MIXED) {
-        const uint4 f = nb.slot_fx[sl];
+        const uint4 f = rawP[b * 32 + lane];
         js.p = make_float4((float)((double)(int)(f.x - ctx->r0[0]) * ctx->s[0]),
                            (float)((double)(int)(f.y - ctx->r0[1]) * ctx->s[1]),
                            (float)((double)(int)(f.z - ctx->r0[2]) * ctx->s[2]), __uint_as_float(f.w));
       } else {
-        js.p = nb.slot_pq[sl];
+        js.p = rawP[b * 32 + lane];
       }
     } else {
       orig = -1;
@@ -475,15 +573,42 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
     }
   };
 
+  // Tiles go to warps in chunks of CHUNK consecutive tiles.  Per chunk the tile records and their
+  // j-list words are fetched once (one round trip each); each tile's slot records are copied one
+  // tile ahead into the other buffer, so only the first tile of a chunk waits for them.
   for (int c0 = gwarp * CHUNK; c0 < total; c0 += nwarps * CHUNK) {
-    const int cend = min(c0 + CHUNK, total);
-    for (int u = c0; u < cend; u++) {
-      const int I = nb.tile_blk[u], k = nb.tile_k[u];
-      if (I < 0 || I >= nb.nblk_total || k < 0 ||
-          (k > 0 && (k - 1) * JCHUNK >= nb.jcap_off[I + 1] - nb.jcap_off[I]))
-        continue;  // unreachable with a consistent tile map; keeps every access in bounds
+    const int nc = min(CHUNK, total - c0);
+    tI = -1;
+    tk = -1;
+    tjb = 0;
+    if (lane < nc) {
+      const int I = nb.tile_blk[c0 + lane], k = nb.tile_k[c0 + lane];
+      // an inconsistent tile record is skipped (unreachable; keeps every access in bounds)
+      if (I >= 0 && I < nb.nblk_total && k >= 0) {
+        const int j0 = nb.jcap_off[I], j1 = nb.jcap_off[I + 1];
+        if (k * JCHUNK < j1 - j0) {
+          tI = I;
+          tk = k;
+          tjb = j0 + k * JCHUNK;
+        }
+      }
+    }
+    for (int t = 0; t < nc; t++) {
+      const int It = __shfl_sync(0xffffffffu, tI, t), kt = __shfl_sync(0xffffffffu, tk, t),
+                jb = __shfl_sync(0xffffffffu, tjb, t);
+      if (It >= 0) cp_async4(jbuf + t * 32 + lane, nb.jlist + jb + lane);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    prefetch(0, 0);
+    for (int t = 0; t < nc; t++) {
+      if (t + 1 < nc) prefetch(t + 1, (t + 1) & 1);
+      else cp_async_commit();  // an empty group keeps the wait count below uniform
+      cp_async_wait<1>();      // tile t's copies (all but the newest group) have landed
+      const int buf = t & 1;
+      const int I = __shfl_sync(0xffffffffu, tI, t), k = __shfl_sync(0xffffffffu, tk, t);
+      if (I < 0) continue;
       if (I != curI) {
-        flush_i();
         curI = I;
         const int sl = I * BLOCK + li;
         im = nb.slot_meta[sl];
@@ -538,15 +663,15 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
           qi = q4.w;
         }
       }
+      // 32 listed j-atoms, JSAME marking those that share a molecule with the cluster; the first
+      // tile opens with the cluster's own atoms (lane group 0, pairs j > i only)
       const bool diag = (k == 0);
-      // diagonal tile: the cluster against itself (lane group 0); other tiles: 32 listed j-atoms,
-      // JSAME marking those that share a molecule with the cluster
-      const int jraw = diag ? (gb ? -1 : I * BLOCK + li) : nb.jlist[nb.jcap_off[I] + (k - 1) * JCHUNK + lane];
+      const int jraw = rawJ[buf * 32 + lane];
       const int jsl = jraw < 0 ? -1 : (jraw & ~JSAME);
       const bool same = diag || __any_sync(0xffffffffu, jraw >= 0 && (jraw & JSAME));
       JStage<MIXED> mine;
       int jorig;
-      stage_slot(jsl, mine, jorig);
+      stage_slot(jsl, buf, mine, jorig);
       const int tio = im.z * nt;
       const int nxt = gb | ((li + 1) & (BLOCK - 1));
       // per-lane results of the tile: i-force, own j-force, energies, virial
@@ -626,7 +751,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
             const T r2 = dx * dx + dy * dy + dz * dz;
             bool in = r2 <= cut2;
             if constexpr (WRAP) in = in && ivalid && dj.m.x >= 0;  // sentinels do not survive a wrap
-            if constexpr (DIAG) in = in && jl > li;
+            if constexpr (DIAG) in = in && (gb != 0 || jl > li);
             int ex = 0;
             if (in && im.y == dj.m.x) {
               ex = excl_check(s, im.x, sorig[gb | jl]);
@@ -647,7 +772,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
               // exclusions skip only the first image, MODIFIED scaling applies to it only.
               if (bx->multi_image) {
                 bool pv = dj.m.x >= 0 && im.x >= 0;
-                if constexpr (DIAG) pv = pv && jl > li;
+                if constexpr (DIAG) pv = pv && (gb != 0 || jl > li);
                 for (int kk = 1; kk < bx->nlat; kk++) {
                   const double *lv = lat + 3 * (bx->lat0 + kk);
                   T rx = dx + T(lv[0]), ry = dy + T(lv[1]), rz = dz + T(lv[2]);
@@ -698,7 +823,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
           for (int c = 0; c < 6; c++) tvir[c] = a.vir[c];
       }
 
-      if (diag) {
+      if (diag && gb == 0) {  // own atom li: its j-side force joins its i-side force
         tfi[0] += tfj[0]; tfi[1] += tfj[1]; tfi[2] += tfj[2];
       } else if (jorig >= 0) {
         long long *f = nb.fslot + jsl;
@@ -713,17 +838,21 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
       for (int o = BLOCK; o < 32; o <<= 1)
 #pragma unroll
         for (int c = 0; c < 3; c++) tfi[c] += __shfl_xor_sync(0xffffffffu, tfi[c], o);
-      ifix[0] += f2fix(tfi[0], (T)FORCE_SCALE);
-      ifix[1] += f2fix(tfi[1], (T)FORCE_SCALE);
-      ifix[2] += f2fix(tfi[2], (T)FORCE_SCALE);
-      efix_lj += f2fix(tel, (T)ENERGY_SCALE);
-      efix_c += f2fix(tec, (T)ENERGY_SCALE);
-      if constexpr (VIR) {
-        for (int c = 0; c < 6; c++) vfix[c] += f2fix(tvir[c], (T)ENERGY_SCALE);
+      if (gb == 0 && im.x >= 0) {  // the i-cluster's forces of this tile, by slot
+        long long *f = nb.fslot + (long long)I * BLOCK + li;
+        const long long v0 = f2fix(tfi[0], (T)FORCE_SCALE), v1 = f2fix(tfi[1], (T)FORCE_SCALE),
+                        v2 = f2fix(tfi[2], (T)FORCE_SCALE);
+        if (v0) red_add(f, v0);
+        if (v1) red_add(f + nsl, v1);
+        if (v2) red_add(f + 2 * nsl, v2);
       }
+      el_acc += tel;
+      ec_acc += tec;
+      if constexpr (VIR)
+        for (int c = 0; c < 6; c++) v_acc[c] += tvir[c];
     }
+    spill_e();
   }
-  flush_i();
   flush_e();
 }
 
@@ -736,7 +865,8 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
   const int ntt = pl.p.ntypes * pl.p.ntypes;
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
-  size_t smem = ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx));
+  size_t smem = ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx) +
+                                        (VIR ? 8 : 2) * 32 * sizeof(long long) + warp_pref_bytes<MIXED>());
   static int grid = 0;
   static size_t conf_smem = 0;
   if (!grid || conf_smem != smem) {
