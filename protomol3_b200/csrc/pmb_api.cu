@@ -13,6 +13,17 @@
 #include <string>
 #include <vector>
 
+// PME transform work items per CTA (z-lines <= 16; rows / columns capped by the line buffer).
+#ifndef PME_ZLINES
+#define PME_ZLINES 8
+#endif
+#ifndef PME_YROWS
+#define PME_YROWS 4
+#endif
+#ifndef PME_XCOLS
+#define PME_XCOLS 8
+#endif
+
 #include "../../include/pmb200.h"
 #include "pmb_internal.h"
 
@@ -826,6 +837,8 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     std::vector<int4> ywork, xwork;
     long long g0 = 0, c0 = 0;
     const int lcap = pme_line_capacity();
+    int zbuf = 1, lbuf = 1;
+    std::vector<double> theta;
     double th0[8];
     bspline_h(P, 0.0, th0);
     for (int bi = 0; bi < nbox; bi++) {
@@ -869,18 +882,43 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
       pl.cgrid0 = c0;
       pl.piVr = 1.0 / (M_PI * b.L[0] * b.L[1] * b.L[2]);
       pl.fac = M_PI * M_PI / (f->alpha * f->alpha);
-      pl.plane0 = (int)xwork.size();
       g0 += (long long)pl.n[0] * pl.n[1] * pl.n[2];
       c0 += (long long)(pl.n[2] / 2 + 1) * pl.n[0] * pl.n[1];
-      // z-lines in groups of 16 consecutive y (8 packed complex lines per CTA)
+      // small work items (PME_ZLINES z-lines = PME_ZLINES / 2 packed complex lines, PME_YROWS
+      // y-lines, PME_XCOLS x-lines per CTA): many CTAs in flight hide the latency of the
+      // shared-memory stages
       for (int x = 0; x < pl.n[0]; x++)
-        for (int y0 = 0; y0 < pl.n[1]; y0 += 16) zwork.push_back(make_int4(bi, x, y0, std::min(16, pl.n[1] - y0)));
-      const int rows = std::max(1, std::min(16, lcap / pl.n[1])), cols = std::max(1, std::min(16, lcap / pl.n[0]));
+        for (int y0 = 0; y0 < pl.n[1]; y0 += PME_ZLINES) {
+          const int cnt = std::min(PME_ZLINES, pl.n[1] - y0);
+          zwork.push_back(make_int4(bi, x, y0, cnt));
+          zbuf = std::max(zbuf, (cnt + 1) / 2 * pl.n[2]);
+        }
+      const int rows = std::max(1, std::min(PME_YROWS, lcap / pl.n[1])),
+                cols = std::max(1, std::min(PME_XCOLS, lcap / pl.n[0]));
+      lbuf = std::max(lbuf, std::max(rows * pl.n[1], cols * pl.n[0]));
       for (int kz = 0; kz <= pl.n[2] / 2; kz++) {
         for (int x0 = 0; x0 < pl.n[0]; x0 += rows) ywork.push_back(make_int4(bi, kz, x0, std::min(rows, pl.n[0] - x0)));
         for (int y0 = 0; y0 < pl.n[1]; y0 += cols) xwork.push_back(make_int4(bi, kz, y0, std::min(cols, pl.n[1] - y0)));
       }
-      pl.nparts = (int)xwork.size() - pl.plane0;
+      // influence function per half-spectrum point [kz][x][y] (Grid.h:236-341): B(m)
+      // exp(-pi^2 m^2/alpha^2) / (pi V m^2), 0 at m = 0
+      {
+        const int nx = pl.n[0], ny = pl.n[1], nh = pl.n[2] / 2 + 1;
+        const double *bx = infl.data() + pl.inf0[0], *by = infl.data() + pl.inf0[1],
+                     *bz = infl.data() + pl.inf0[2];
+        for (int kz = 0; kz < nh; kz++)
+          for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++) {
+              double th = 0.0;
+              if (i || j || kz) {
+                const int i0 = i <= nx / 2 ? i : i - nx, j0 = j <= ny / 2 ? j : j - ny;
+                const double mi = i0 * pl.mr[0], mj = j0 * pl.mr[1], mk = kz * pl.mr[2];
+                const double m2 = mi * mi + mj * mj + mk * mk;
+                th = bx[i] * by[j] * bz[kz] * pl.piVr / m2;
+              }
+              theta.push_back(th);
+            }
+      }
       f->plans.push_back(pl);
     }
     PmeDev &pm = f->pm;
@@ -900,6 +938,16 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     rc |= upload(f->a, dtw, tw);
     rc |= upload(f->a, dtwf, twf);
     rc |= upload(f->a, dinf, infl);
+    if (s->precision) {
+      std::vector<float> thf(theta.begin(), theta.end());
+      float *dth;
+      rc |= upload(f->a, dth, thf);
+      pm.theta = dth;
+    } else {
+      double *dth;
+      rc |= upload(f->a, dth, theta);
+      pm.theta = dth;
+    }
     rc |= upload(f->a, drad, radix);
     rc |= upload(f->a, dz, zwork);
     rc |= upload(f->a, dy, ywork);
@@ -915,11 +963,12 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     pm.nywork = (int)ywork.size();
     pm.xwork = dx;
     pm.nxwork = (int)xwork.size();
+    pm.zbuf = zbuf;
+    pm.lbuf = lbuf;
     pm.qgrid = f->a.get<long long>(g0);
     pm.rgrid = s->precision ? (void *)f->a.get<float>(g0) : (void *)f->a.get<double>(g0);
     pm.cgrid = s->precision ? (void *)f->a.get<float2>(c0) : (void *)f->a.get<double2>(c0);
-    pm.plane_part = f->a.get<double>(8 * (size_t)xwork.size());
-    if (rc || !pm.qgrid || !pm.rgrid || !pm.cgrid || !pm.plane_part) return bad(PMB_ERR_CUDA, "PME allocation failed");
+    if (rc || !pm.qgrid || !pm.rgrid || !pm.cgrid) return bad(PMB_ERR_CUDA, "PME allocation failed");
   } else {
     f->pm.alpha = f->alpha;
     f->pm.a2pi = 2.0 * f->alpha / std::sqrt(M_PI);

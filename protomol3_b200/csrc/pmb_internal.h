@@ -111,8 +111,6 @@ struct PmeBoxPlan {
   int tw0[3];         // offsets of twiddle tables (complex elements)
   int inf0[3];        // offsets of influence tables
   int rad0[3], nrad[3];
-  int plane0;         // first energy-partial slot (x-line work item) of this box
-  int nparts;         // number of x-line work items of this box
   double hr[3];       // n / L
   double mr[3];       // 1 / L
   double piVr, fac;   // 1/(pi V), pi^2 / alpha^2
@@ -127,6 +125,8 @@ struct PmeDev {
   const double2 *twiddle;     // per dim tables exp(-2 pi i k / n)
   const float2 *twiddlef;
   const double *infl;         // per dim influence factor B(m) exp(-pi^2 m^2/alpha^2)
+  const void *theta;          // influence function per half-spectrum point (float / double,
+                              // layout as cgrid), 0 at m = 0
   const int *radix;           // radices per dim
   const int4 *zwork;          // z-pass work items: box, x, y0, count
   int nzwork;
@@ -134,7 +134,7 @@ struct PmeDev {
   int nywork;
   const int4 *xwork;          // x-line work items: box, kz, y0, columns
   int nxwork;
-  double *plane_part;         // [nxwork * 8] energy + virial partials
+  int zbuf, lbuf;             // complex elements per ping-pong buffer of the z / line kernels
   double alpha, a2pi;
   int virial;
 };

@@ -11,11 +11,10 @@
 //                 per complex FFT, half spectrum written as [kz][x][y]
 //   k_fft_y       y-lines of the half spectrum (groups of up to 16 rows of one kz plane)
 //   k_fft_x_infl  x-lines (groups of up to 16 columns): forward FFT, influence function multiply
-//                 with energy and virial partials, inverse FFT
+//                 with energy and virial partials added to the box accumulators, inverse FFT
 //   k_fft_y       inverse y-lines
 //   k_fft_z_inv   inverse z transform back to the real potential grid [x][y][z]
 //   k_gather      one thread per atom slot, 64-point stencil, fixed-point force atomics
-//   k_pme_energy  fixed-order sum of the per-plane partials into the box accumulators
 // The transforms are unnormalised, as the reference's ZFFT/FFTW calls; r2c/c2r replace the
 // reference's full complex transform of a real grid (identical result: the spectrum is Hermitian
 // and the influence function even in m).
@@ -90,6 +89,11 @@ __device__ __forceinline__ void dft_small(T2 *v, int sign) {
   }
 }
 
+// floor(a / d) for 0 <= a < 2^21 from r ~ 1/d (a few ulp suffice: (a + 1/2) / d stays at least
+// 1/(2d) away from an integer), without an integer division.
+__device__ __forceinline__ int divf(int a, float r) { return __float2int_rz(((float)a + 0.5f) * r); }
+__device__ __forceinline__ float rcpf(int d) { return __fdividef(1.0f, (float)d); }
+
 // One Stockham stage, out of place (src -> dst): each thread takes whole butterflies (R inputs
 // read, twiddled, transformed and written), so only R values are live at a time.
 template <int R, typename T2>
@@ -97,16 +101,24 @@ __device__ __forceinline__ void fft_stage(const T2 *__restrict__ src, T2 *__rest
                                           int nlines, int lstride, int estride, int Ns,
                                           const T2 *tw, int sign) {
   const int nb = n / R, total = nb * nlines, step = n / (Ns * R);
+  const float rnb = rcpf(nb), rnl = rcpf(nlines), rns = rcpf(Ns);
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
     // contiguous lines: consecutive threads take consecutive butterflies of one line;
     // strided lines: consecutive threads take the same butterfly of consecutive lines
-    const int line = estride == 1 ? b / nb : b % nlines, j = estride == 1 ? b % nb : b / nlines;
+    int line, j;
+    if (estride == 1) {
+      line = divf(b, rnb);
+      j = b - line * nb;
+    } else {
+      j = divf(b, rnl);
+      line = b - j * nlines;
+    }
     const T2 *Ls = src + line * lstride;
     T2 *Ld = dst + line * lstride;
     T2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = Ls[(j + r * nb) * estride];
-    const int k = j % Ns;
+    const int jq = divf(j, rns), k = j - jq * Ns;
 #pragma unroll
     for (int r = 1; r < R; r++) {
       T2 w = tw[r * k * step];
@@ -114,7 +126,7 @@ __device__ __forceinline__ void fft_stage(const T2 *__restrict__ src, T2 *__rest
       v[r] = cmul(v[r], w);
     }
     dft_small<R>(v, sign);
-    const int out = (j / Ns) * Ns * R + k;
+    const int out = jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; r++) Ld[(out + r * Ns) * estride] = v[r];
   }
@@ -397,7 +409,7 @@ __global__ void __launch_bounds__(ZT, 8) k_fft_z_fwd(PmeDev pm) {
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], x = wk.y, y0 = wk.z, cnt = wk.w;
   const int npair = (cnt + 1) / 2;
   T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + 256, *tmp = buf + ZMAXE;
+  T2 *buf = tw + 256, *tmp = buf + pm.zbuf;
   for (int k = threadIdx.x; k < nz; k += ZT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[2] + k];
     else tw[k] = pm.twiddle[pl.tw0[2] + k];
@@ -407,10 +419,11 @@ __global__ void __launch_bounds__(ZT, 8) k_fft_z_fwd(PmeDev pm) {
   // store in between, so the loads overlap), then clear the charge grid for the next step, each
   // thread the values it read itself
   const int nrun = cnt * nz;
+  const float rnz = rcpf(nz), rnp = rcpf(npair);
 #pragma unroll 4
   for (int e = threadIdx.x; e < npair * 2 * nz; e += ZT) {
     const long long q = e < nrun ? __ldcs(g + e) : 0ll;
-    const int line = e / nz, z = e - line * nz;
+    const int line = divf(e, rnz), z = e - line * nz;
     T *dst = reinterpret_cast<T *>(buf + (line >> 1) * nz + z);
     dst[line & 1] = T((double)q * (1.0 / GRID_SCALE));
   }
@@ -420,8 +433,8 @@ __global__ void __launch_bounds__(ZT, 8) k_fft_z_fwd(PmeDev pm) {
   const int nh = nz / 2 + 1;
   T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0;
   for (int e = threadIdx.x; e < npair * nh; e += ZT) {
-    int pi = e % npair, k = e / npair;
-    T2 zk = res[pi * nz + k], zn = res[pi * nz + (nz - k) % nz];
+    const int k = divf(e, rnp), pi = e - k * npair;
+    T2 zk = res[pi * nz + k], zn = res[pi * nz + (k == 0 ? 0 : nz - k)];
     // X = (Z_k + conj(Z_{n-k})) / 2, Y = -i/2 (Z_k - conj(Z_{n-k}))
     T2 X = cmk(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
     T2 Y = cmk(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
@@ -440,14 +453,15 @@ __global__ void __launch_bounds__(ZT, 8) k_fft_z_inv(PmeDev pm) {
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], x = wk.y, y0 = wk.z, cnt = wk.w;
   const int npair = (cnt + 1) / 2, nh = nz / 2 + 1;
   T2 *tw = reinterpret_cast<T2 *>(smem_raw);
-  T2 *buf = tw + 256, *tmp = buf + ZMAXE;
+  T2 *buf = tw + 256, *tmp = buf + pm.zbuf;
   for (int k = threadIdx.x; k < nz; k += ZT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[2] + k];
     else tw[k] = pm.twiddle[pl.tw0[2] + k];
   }
   const T2 *C = reinterpret_cast<const T2 *>(pm.cgrid) + pl.cgrid0;
+  const float rnz = rcpf(nz), rnp = rcpf(npair);
   for (int e = threadIdx.x; e < npair * nh; e += ZT) {
-    int pi = e % npair, k = e / npair;
+    const int k = divf(e, rnp), pi = e - k * npair;
     const T2 *row = C + ((long long)k * nx + x) * ny + y0 + 2 * pi;
     T2 X = row[0];
     T2 Y = (2 * pi + 1 < cnt) ? row[1] : cmk(T(0), T(0));
@@ -462,7 +476,7 @@ __global__ void __launch_bounds__(ZT, 8) k_fft_z_inv(PmeDev pm) {
   const T2 *res = fft_lines(buf, tmp, nz, npair, nz, 1, pm.radix + pl.rad0[2], pl.nrad[2], tw, +1);
   T *R = reinterpret_cast<T *>(pm.rgrid) + pl.grid0 + ((long long)x * ny + y0) * nz;
   for (int e = threadIdx.x; e < cnt * nz; e += ZT) {
-    int line = e / nz, z = e % nz;
+    const int line = divf(e, rnz), z = e - line * nz;
     T2 v = res[(line >> 1) * nz + z];
     R[(long long)line * nz + z] = (line & 1) ? v.y : v.x;
   }
@@ -494,7 +508,7 @@ __global__ void __launch_bounds__(LT, 8) k_fft_y(PmeDev pm, int sign) {
   const PmeBoxPlan &pl = pm.plan[wk.x];
   const int nx = pl.n[0], ny = pl.n[1], kz = wk.y, x0 = wk.z, rows = wk.w;
   T2 *tw = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
-  T2 *buf = tw + 256, *tmp = buf + LMAXE;
+  T2 *buf = tw + 256, *tmp = buf + pm.lbuf;
   for (int k = threadIdx.x; k < ny; k += LT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[1] + k];
     else tw[k] = pm.twiddle[pl.tw0[1] + k];
@@ -510,7 +524,7 @@ __global__ void __launch_bounds__(LT, 8) k_fft_y(PmeDev pm, int sign) {
 // x-lines (columns y0..y0+cols of one kz plane): forward FFT, influence function with energy and
 // virial (Grid.h:236-341, half spectrum kz <= nz/2 with the doubling of interior kz), inverse FFT.
 template <typename T>
-__global__ void __launch_bounds__(LT, 8) k_fft_x_infl(PmeDev pm) {
+__global__ void __launch_bounds__(LT, 8) k_fft_x_infl(const SystemDev s, PmeDev pm) {
   using T2 = typename C2<T>::t;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 wk = pm.xwork[blockIdx.x];  // box, kz, y0, cols
@@ -518,83 +532,67 @@ __global__ void __launch_bounds__(LT, 8) k_fft_x_infl(PmeDev pm) {
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2], kz = wk.y, y0 = wk.z, cols = wk.w;
   double *red = reinterpret_cast<double *>(smem_raw);  // 32 doubles
   T2 *tw = reinterpret_cast<T2 *>(smem_raw + 32 * sizeof(double));
-  T2 *buf = tw + 256, *tmp = buf + LMAXE;  // buf[x * cols + c]
+  T2 *buf = tw + 256, *tmp = buf + pm.lbuf;  // buf[x * cols + c]
   for (int k = threadIdx.x; k < nx; k += LT) {
     if constexpr (sizeof(T) == 4) tw[k] = pm.twiddlef[pl.tw0[0] + k];
     else tw[k] = pm.twiddle[pl.tw0[0] + k];
   }
   T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + (long long)kz * nx * ny + y0;
   const int ne = nx * cols;
+  const float rcols = rcpf(cols);
   for (int e = threadIdx.x; e < ne; e += LT) {
-    int x = e / cols, c = e % cols;
+    const int x = divf(e, rcols), c = e - x * cols;
     buf[e] = C[(long long)x * ny + c];
   }
   __syncthreads();
   T2 *spec = fft_lines(buf, tmp, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, -1);
   T2 *other = spec == buf ? tmp : buf;
-  const double *bxt = pm.infl + pl.inf0[0], *byt = pm.infl + pl.inf0[1], *bzt = pm.infl + pl.inf0[2];
+  // influence function of this plane's columns (precomputed per plan, 0 at m = 0)
+  const T *th = reinterpret_cast<const T *>(pm.theta) + pl.cgrid0 + (long long)kz * nx * ny + y0;
   const double mk = kz * pl.mr[2];
   const double wz = (kz > 0 && ((2 * kz != nz) || (nz & 1))) ? 2.0 : 1.0;
   double en = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
   for (int e = threadIdx.x; e < ne; e += LT) {
-    int i = e / cols, j = y0 + e % cols;
-    if (i == 0 && j == 0 && kz == 0) {
-      spec[e] = cmk(T(0), T(0));
-      continue;
-    }
-    int i0 = i <= nx / 2 ? i : i - nx, j0 = j <= ny / 2 ? j : j - ny;
-    double mi = i0 * pl.mr[0], mj = j0 * pl.mr[1];
-    double m2 = mi * mi + mj * mj + mk * mk;
-    double theta = bxt[i] * byt[j] * bzt[kz] * pl.piVr / m2;
+    const int i = divf(e, rcols), cc = e - i * cols;
+    const T theta = th[(long long)i * ny + cc];
     T2 c = spec[e];
     double qq = (double)c.x * (double)c.x + (double)c.y * (double)c.y;
-    double ee = wz * qq * theta;
+    double ee = wz * qq * (double)theta;
     en += ee;
-    if (pm.virial) {
+    if (pm.virial && theta != T(0)) {
+      const int j = y0 + cc;
+      int i0 = i <= nx / 2 ? i : i - nx, j0 = j <= ny / 2 ? j : j - ny;
+      double mi = i0 * pl.mr[0], mj = j0 * pl.mr[1];
+      double m2 = mi * mi + mj * mj + mk * mk;
       double v = 2.0 * (1.0 / m2 + pl.fac);
       vxx += ee * (1.0 - v * mi * mi); vxy -= ee * (v * mi * mj); vxz -= ee * (v * mi * mk);
       vyy += ee * (1.0 - v * mj * mj); vyz -= ee * (v * mj * mk); vzz += ee * (1.0 - v * mk * mk);
     }
-    spec[e] = cmk(c.x * T(theta), c.y * T(theta));
+    spec[e] = cmk(c.x * theta, c.y * theta);
   }
+  // the CTA's energy (x 0.5, Grid.h:319-337) and virial partials go to the box accumulators in
+  // fixed point (a fixed reduction order per CTA, integer sums across CTAs)
   double part[7] = {en, vxx, vxy, vxz, vyy, vyz, vzz};
   const int np = pm.virial ? 7 : 1;
+  long long *eb = s.eacc + (long long)wk.x * ACC_PER_BOX;
+  const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};  // xx xy xz yy yz zz
   for (int c = 0; c < np; c++) {
-    double r = block_sum<LT, T>(part[c], red);
-    if (threadIdx.x == 0) pm.plane_part[(long long)blockIdx.x * 8 + c] = r;
+    const double r = block_sum<LT, T>(part[c], red);
+    if (threadIdx.x == 0) {
+      const long long v = f2fix(r * 0.5, ENERGY_SCALE);
+      if (c == 0) {
+        red_add(eb + E_COUL, v);
+      } else {
+        red_add(eb + E_VIR + slot[c - 1][0], v);
+        if (slot[c - 1][1] != slot[c - 1][0]) red_add(eb + E_VIR + slot[c - 1][1], v);
+      }
+    }
   }
   __syncthreads();
   const T2 *res = fft_lines(spec, other, nx, cols, 1, cols, pm.radix + pl.rad0[0], pl.nrad[0], tw, +1);
   for (int e = threadIdx.x; e < ne; e += LT) {
-    int x = e / cols, c = e % cols;
+    const int x = divf(e, rcols), c = e - x * cols;
     C[(long long)x * ny + c] = res[e];
-  }
-}
-
-// Per box: fixed-order sum of its x-line partials, x 0.5 (Grid.h:319-337), into the box
-// accumulators.
-__global__ void k_pme_energy(const SystemDev s, PmeDev pm) {
-  // one warp per box; lane-strided partial sums then a fixed shuffle tree (reproducible)
-  int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (b >= pm.nbox) return;
-  const PmeBoxPlan &pl = pm.plan[b];
-  int p0 = pl.plane0, np = pl.nparts;
-  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  const int nc = pm.virial ? 7 : 1;
-  for (int p = p0 + lane; p < p0 + np; p += 32)
-    for (int c = 0; c < nc; c++) acc[c] += pm.plane_part[(long long)p * 8 + c];
-  for (int c = 0; c < nc; c++) acc[c] = warp_sum(acc[c]);
-  if (lane != 0) return;
-  long long *e = s.eacc + (long long)b * ACC_PER_BOX;
-  red_add(e + E_COUL, f2fix(acc[0] * 0.5, ENERGY_SCALE));
-  if (pm.virial) {
-    // xx xy xz yy yz zz -> row-major 3x3
-    const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
-    for (int c = 0; c < 6; c++) {
-      long long v = f2fix(acc[1 + c] * 0.5, ENERGY_SCALE);
-      red_add(e + E_VIR + slot[c][0], v);
-      if (slot[c][1] != slot[c][0]) red_add(e + E_VIR + slot[c][1], v);
-    }
   }
 }
 
@@ -639,31 +637,32 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   if (pm.order == 4) k_spread4<MIXED><<<(unsigned)((n4 + TB - 1) / TB), TB, 0, st>>>(nb, pm);
   else k_spread<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
   if (mark) mark(mctx, "pme_spread");
-  size_t zsmem = sizeof(T2) * (256 + 2 * (size_t)ZMAXE);
+  // shared memory sized to the largest work item of the plan (caps ZMAXE / LMAXE)
+  const size_t zsmem = sizeof(T2) * (256 + 2 * (size_t)pm.zbuf);
   static bool zconf = false;
   if (!zconf) {
-    cudaFuncSetAttribute(k_fft_z_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
-    cudaFuncSetAttribute(k_fft_z_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem);
+    const int zcap = (int)(sizeof(T2) * (256 + 2 * (size_t)ZMAXE));
+    cudaFuncSetAttribute(k_fft_z_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, zcap);
+    cudaFuncSetAttribute(k_fft_z_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, zcap);
     zconf = true;
   }
   k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
-  const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)LMAXE);
+  const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)pm.lbuf);
   static bool lconf = false;
   if (!lconf) {
-    cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
-    cudaFuncSetAttribute(k_fft_x_infl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
+    const int lcap = (int)(32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)LMAXE));
+    cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lcap);
+    cudaFuncSetAttribute(k_fft_x_infl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lcap);
     lconf = true;
   }
   k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, -1);
-  k_fft_x_infl<T><<<pm.nxwork, LT, lsmem, st>>>(pm);
+  k_fft_x_infl<T><<<pm.nxwork, LT, lsmem, st>>>(s, pm);
   k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, +1);
   k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   if (mark) mark(mctx, "pme_fft");
   if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   else k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   if (mark) mark(mctx, "pme_gather");
-  k_pme_energy<<<(pm.nbox * 32 + 127) / 128, 128, 0, st>>>(s, pm);
-  if (mark) mark(mctx, "pme_energy");
   return 0;
 }
 
