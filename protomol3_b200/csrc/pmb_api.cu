@@ -299,6 +299,10 @@ int nblist_alloc(pmb_system *s, double rl) {
   nb.nsblk = (nblk + 31) / 32;
   nb.sblk_lo = s->nba.get<uint4>(nb.nsblk);
   nb.sblk_hi = s->nba.get<uint4>(nb.nsblk);
+  nb.blk_c = s->nba.get<uint4>(nblk);
+  nb.blk_h = s->nba.get<uint4>(nblk);
+  nb.sblk_c = s->nba.get<uint4>(nb.nsblk);
+  nb.sblk_h = s->nba.get<uint4>(nb.nsblk);
   nb.jcount = s->nba.get<int>(nblk + 1);
   nb.jlist = s->nba.get<int>((size_t)jcap_off[nblk], false);
   nb.tile_off = s->nba.get<int>(nblk + 1);
@@ -336,7 +340,7 @@ int nblist_alloc(pmb_system *s, double rl) {
   const unsigned ctl0[4] = {0u, 0u, 0u, 1u};  // first use builds the list
   CK(cudaMemcpy(nb.ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice));
   s->nb_build_rl = -1.0;
-  if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.fslot ||
+  if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.blk_c || !nb.blk_h || !nb.sblk_c || !nb.sblk_h || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.fslot ||
       !nb.scan_tmp || !nb.bin_start)
     return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
   s->nb_cutoff = rl;

@@ -32,8 +32,10 @@ struct NbListDev {
   const int *blk_box;          // [nblk]
   float4 *blk_center;          // [nblk] fractional-fixed centre (as uint bits) and count
   uint4 *blk_lo, *blk_hi;      // [nblk] fixed-point extents (x, y, z)
+  uint4 *blk_c, *blk_h;        // [nblk] the same as centre (.w = atoms) and half extent
   int nsblk;                   // superblocks: runs of 32 consecutive blocks
   uint4 *sblk_lo, *sblk_hi;    // [nsblk] union of their blocks' extents, .w = atoms
+  uint4 *sblk_c, *sblk_h;      // [nsblk] the same as centre (.w = atoms) and half extent
   int *jcap_off;               // [nblk+1] offset of each block's j-slot list region
   int *jcount;                 // [nblk] tiles per block (its j-list, own slots first, in 32s)
   int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding), JSAME flag bit

@@ -272,6 +272,9 @@ __global__ void k_block_bbox(NbListDev nb) {
     if (cnt == 0) lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
     nb.blk_lo[blk] = make_uint4(lo[0], lo[1], lo[2], (unsigned)cnt);
     nb.blk_hi[blk] = make_uint4(hi[0], hi[1], hi[2], 0u);
+    nb.blk_c[blk] = make_uint4(lo[0] + (hi[0] - lo[0]) / 2u, lo[1] + (hi[1] - lo[1]) / 2u,
+                               lo[2] + (hi[2] - lo[2]) / 2u, (unsigned)cnt);
+    nb.blk_h[blk] = make_uint4((hi[0] - lo[0]) / 2u + 1u, (hi[1] - lo[1]) / 2u + 1u, (hi[2] - lo[2]) / 2u + 1u, 0u);
   }
 }
 
@@ -305,166 +308,138 @@ __global__ void k_superblock_bbox(NbListDev nb) {
     if (lo.w == 0) lo.x = lo.y = lo.z = hi.x = hi.y = hi.z = 0;
     nb.sblk_lo[S] = lo;
     nb.sblk_hi[S] = hi;
+    nb.sblk_c[S] = make_uint4(lo.x + (hi.x - lo.x) / 2u, lo.y + (hi.y - lo.y) / 2u, lo.z + (hi.z - lo.z) / 2u, lo.w);
+    nb.sblk_h[S] = make_uint4((hi.x - lo.x) / 2u + 1u, (hi.y - lo.y) / 2u + 1u, (hi.z - lo.z) / 2u + 1u, 0u);
   }
 }
 
-// Gap (in A) between a point / box and a box, in fractional fixed-point coordinates with the
-// minimal image taken by 32-bit wrap-around.
-__device__ __forceinline__ double box_gap2(const BoxDev &b, const unsigned c1[3], const unsigned h1[3],
-                                           const unsigned c2[3], const unsigned h2[3]) {
-  double g2 = 0.0;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    long long d = (long long)(int)(c2[k] - c1[k]);
-    long long a = d < 0 ? -d : d;
-    long long gap = a - (long long)h1[k] - (long long)h2[k];
-    if (gap > 0) {
-      double ga = (double)gap * b.L[k] * (1.0 / 4294967296.0);
-      g2 += ga * ga;
-    }
-  }
-  return g2;
-}
-
-// The same gap in FP32 for the list culling: the gap is exact in fixed point and its conversion
-// errs by < 1e-5 A, far below the 1e-3 A margin of the list radius over the cutoff.
-__device__ __forceinline__ float box_gap2f(const float sL[3], const unsigned c1[3], const unsigned h1[3],
-                                           const unsigned c2[3], const unsigned h2[3]) {
+// Gap^2 (A^2) between the box (c1, h1 half extents in A) and the box (c2, h2 fixed-point half
+// extents) in FP32: the fixed-point difference (minimal image by 32-bit wrap-around) converts
+// with an error of < 1e-5 A, far below the 1e-3 A margin of the list radius over the cutoff.
+__device__ __forceinline__ float gap2f(const float sL[3], const unsigned c1[3], const float h1[3],
+                                       uint4 c2, uint4 h2) {
+  const unsigned c[3] = {c2.x, c2.y, c2.z}, h[3] = {h2.x, h2.y, h2.z};
   float g2 = 0.f;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    long long d = (long long)(int)(c2[k] - c1[k]);
-    long long a = d < 0 ? -d : d;
-    long long gap = a - (long long)h1[k] - (long long)h2[k];
-    if (gap > 0) {
-      float ga = (float)gap * sL[k];
-      g2 += ga * ga;
-    }
+    const float d = fmaxf((fabsf((float)(int)(c[k] - c1[k])) - (float)h[k]) * sL[k] - h1[k], 0.f);
+    g2 = fmaf(d, d, g2);
   }
   return g2;
 }
 
-__device__ __forceinline__ void center_half(uint4 lo, uint4 hi, unsigned c[3], unsigned h[3]) {
-  unsigned l[3] = {lo.x, lo.y, lo.z}, u[3] = {hi.x, hi.y, hi.z};
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    h[k] = (u[k] - l[k]) / 2u + 1u;
-    c[k] = l[k] + (u[k] - l[k]) / 2u;
-  }
-}
+constexpr int BL_THREADS = 256;
+constexpr int BL_CAP = 128;  // candidate blocks buffered per warp before their atoms are tested
 
 // One warp per block I: its own slots, then the candidate blocks J > I of the same box by
-// bounding-box gap and the atoms of each candidate within the list cutoff of I's box, compacted
-// into I's j-list (tiles of 32 entries).
-__global__ void k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
+// bounding-box gap (superblocks of 32 blocks first), compacted into a shared-memory list, then
+// the atoms of GROUPS listed blocks per pass within the list cutoff of I's box, compacted into
+// I's j-list (tiles of 32 entries).  The loads of the next pass are issued before the current
+// pass is tested.
+__global__ void __launch_bounds__(BL_THREADS) k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
+  __shared__ int cand_all[BL_THREADS / 32][BL_CAP];
   if (!nb.ctl[1]) return;
-  int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (I >= nb.nblk_total) return;
-  int bi = nb.blk_box[I];
+  int *cl = cand_all[threadIdx.x >> 5];
+  const int bi = nb.blk_box[I];
   const BoxDev &b = s.box[bi];
-  uint4 loI = nb.blk_lo[I], hiI = nb.blk_hi[I];
-  if (loI.w == 0) {
+  const uint4 cIv = nb.blk_c[I], hIv = nb.blk_h[I];
+  if (cIv.w == 0) {
     if (lane == 0) nb.jcount[I] = 0;
     return;
   }
-  unsigned cI[3], hI[3];
-  center_half(loI, hiI, cI, hI);
-  int jend = b.blk0 + b.nblk;
-  int cap = nb.jcap_off[I + 1] - nb.jcap_off[I];
-  int *out = nb.jlist + nb.jcap_off[I];
-  // the block's own slots open its list (flagged JSAME: the pair kernel takes j > i among them)
-  if (lane < BLOCK) {
-    const int sl = I * BLOCK + lane;
-    out[lane] = nb.slot_orig[sl] >= 0 ? (sl | JSAME) : -1;
-  }
-  int count = BLOCK;
-  bool overflow = false;
-  unsigned zero[3] = {0, 0, 0};
   const float sL[3] = {(float)(b.L[0] * (1.0 / 4294967296.0)), (float)(b.L[1] * (1.0 / 4294967296.0)),
                        (float)(b.L[2] * (1.0 / 4294967296.0))};
+  const unsigned cI[3] = {cIv.x, cIv.y, cIv.z};
+  const float hI[3] = {(float)hIv.x * sL[0], (float)hIv.y * sL[1], (float)hIv.z * sL[2]};
+  const int jend = b.blk0 + b.nblk;
+  const int cap = nb.jcap_off[I + 1] - nb.jcap_off[I];
+  int *out = nb.jlist + nb.jcap_off[I];
+  const bool multi = b.multi_image != 0;
   const float rl2 = (float)rlist2;
+  const int g = lane / BLOCK, li = lane & (BLOCK - 1);
   // molecules of the cluster's atoms (-2: padding): a listed j-atom of one of them is flagged
-  // JSAME, so the pair kernel runs the exclusion test only on tiles holding such an atom
+  // JSAME, so the pair kernel runs the exclusion test only on tiles holding such an atom; the
+  // block's own slots open its list (the pair kernel takes j > i among them)
   int imol[BLOCK];
   {
-    const int o = nb.slot_orig[I * BLOCK + (lane & (BLOCK - 1))];
-    const int mine = o >= 0 ? s.molecule[o] : -2;
+    const int4 m = nb.slot_meta[I * BLOCK + li];
+    if (lane < BLOCK) out[lane] = m.x >= 0 ? ((I * BLOCK + lane) | JSAME) : -1;
+    const int mine = m.x >= 0 ? m.y : -2;
 #pragma unroll
     for (int t = 0; t < BLOCK; t++) imol[t] = __shfl_sync(0xffffffffu, mine, t);
   }
-  // superblocks (runs of 32 blocks) first, 32 per ballot; then the blocks of each candidate one
+  int count = BLOCK, ncand = 0;
+  bool overflow = false;
+
+  // atoms of the listed candidate blocks, GROUPS blocks (32 slots) per pass
+  auto atoms = [&]() {
+    __syncwarp();
+    int sl = g < ncand ? cl[g] * BLOCK + li : -1;
+    int4 m = make_int4(-1, -1, 0, 0);
+    uint4 f = make_uint4(0, 0, 0, 0);
+    if (sl >= 0) {
+      m = nb.slot_meta[sl];
+      f = nb.slot_fx[sl];
+    }
+    for (int p = 0; p < ncand; p += GROUPS) {
+      const int q = p + GROUPS + g;
+      const int sl2 = q < ncand ? cl[q] * BLOCK + li : -1;
+      int4 m2 = make_int4(-1, -1, 0, 0);
+      uint4 f2 = make_uint4(0, 0, 0, 0);
+      if (sl2 >= 0) {
+        m2 = nb.slot_meta[sl2];
+        f2 = nb.slot_fx[sl2];
+      }
+      const bool take = m.x >= 0 && (multi || gap2f(sL, cI, hI, f, make_uint4(0, 0, 0, 0)) <= rl2);
+      const unsigned tm = __ballot_sync(0xffffffffu, take);
+      const int n = __popc(tm);
+      if (count + n > cap) {
+        overflow = true;
+        break;
+      }
+      if (take) {
+        bool same = false;
+#pragma unroll
+        for (int t = 0; t < BLOCK; t++) same |= m.y == imol[t];
+        out[count + __popc(tm & ((1u << lane) - 1u))] = same ? (sl | JSAME) : sl;
+      }
+      count += n;
+      sl = sl2;
+      m = m2;
+      f = f2;
+    }
+    ncand = 0;
+    __syncwarp();
+  };
+
+  // superblocks (runs of 32 blocks), 32 per ballot; then the 32 blocks of each candidate one
   const int send = (jend + 31) / 32;
   for (int S0 = (I + 1) / 32; S0 < send && !overflow; S0 += 32) {
     const int S = S0 + lane;
     bool scand = false;
     if (S < send) {
-      const uint4 loS = nb.sblk_lo[S], hiS = nb.sblk_hi[S];
-      if (loS.w > 0) {
-        if (b.multi_image) scand = true;
-        else {
-          unsigned cS[3], hS[3];
-          center_half(loS, hiS, cS, hS);
-          scand = box_gap2f(sL, cI, hI, cS, hS) <= rl2;
-        }
-      }
+      const uint4 cS = nb.sblk_c[S];
+      if (cS.w > 0) scand = multi || gap2f(sL, cI, hI, cS, nb.sblk_h[S]) <= rl2;
     }
     unsigned sm = __ballot_sync(0xffffffffu, scand);
-    while (sm) {
-      const int J0 = (S0 + __ffs(sm) - 1) * 32;
+    while (sm && !overflow) {
+      const int J = (S0 + __ffs(sm) - 1) * 32 + lane;
       sm &= sm - 1;
-      int J = J0 + lane;
       bool cand = false;
       if (J > I && J < jend) {
-        uint4 loJ = nb.blk_lo[J], hiJ = nb.blk_hi[J];
-        if (loJ.w > 0) {
-          if (b.multi_image) cand = true;
-          else {
-            unsigned cJ[3], hJ[3];
-            center_half(loJ, hiJ, cJ, hJ);
-            cand = box_gap2f(sL, cI, hI, cJ, hJ) <= rl2;
-          }
-        }
+        const uint4 cJ = nb.blk_c[J];
+        if (cJ.w > 0) cand = multi || gap2f(sL, cI, hI, cJ, nb.blk_h[J]) <= rl2;
       }
-      unsigned m = __ballot_sync(0xffffffffu, cand);
-      while (m) {
-        // GROUPS candidate blocks per pass: lane group g tests the atoms of the g-th one
-        unsigned mg = m;
-        for (int t = 0; t < lane / BLOCK; t++) mg &= mg - 1;
-        const int src = mg ? __ffs(mg) - 1 : -1;
-        for (int t = 0; t < GROUPS && m; t++) m &= m - 1;
-        bool take = false;
-        int sl = -1, o = -1;
-        if (src >= 0) {
-          sl = (J0 + src) * BLOCK + (lane & (BLOCK - 1));
-          o = nb.slot_orig[sl];
-          const uint4 f = nb.slot_fx[sl];  // loaded with the index, not after it
-          if (o >= 0) {
-            if (b.multi_image) take = true;
-            else {
-              unsigned p[3] = {f.x, f.y, f.z};
-              take = box_gap2f(sL, cI, hI, p, zero) <= rl2;
-            }
-          }
-        }
-        unsigned tm = __ballot_sync(0xffffffffu, take);
-        int n = __popc(tm);
-        if (count + n > cap) {
-          overflow = true;
-          break;
-        }
-        if (take) {
-          const int mj = s.molecule[o];
-          bool same = false;
-#pragma unroll
-          for (int t = 0; t < BLOCK; t++) same |= mj == imol[t];
-          out[count + __popc(tm & ((1u << lane) - 1u))] = same ? (sl | JSAME) : sl;
-        }
-        count += n;
-      }
-      if (overflow) break;
+      const unsigned m = __ballot_sync(0xffffffffu, cand);
+      if (ncand + __popc(m) > BL_CAP) atoms();
+      if (cand) cl[ncand + __popc(m & ((1u << lane) - 1u))] = J;
+      ncand += __popc(m);
     }
   }
-  int padded = (count + 31) & ~31;
+  if (!overflow && ncand > 0) atoms();
+  const int padded = (count + 31) & ~31;
   if (!overflow)
     for (int k = count + lane; k < padded; k += 32) out[k] = -1;
   if (lane == 0) {
