@@ -242,6 +242,7 @@ def run_b200(args, rank, world, local_rank):
             flush.zero_()
             md.run(1)
         torch.cuda.synchronize()
+        builds0 = topo.list_builds()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         if dist:
             dist.barrier()
@@ -255,17 +256,19 @@ def run_b200(args, rank, world, local_rank):
         if dist:
             dist.barrier()
         ms = sum(a.elapsed_time(b) for a, b in evs) / steps
-        kps = md.kernels_per_step()
+        # launches: each step's graph plus the closing half kick of run(1)
+        rebuilds = topo.list_builds() - builds0
+        kps = (md.kernels_per_step() + 1) * steps
         pos, vel = md.state()
         if not np.isfinite(pos).all():
             raise RuntimeError("non-finite positions after the timed run")
         md.close()
-        return ms, kps
+        return ms, kps, rebuilds
 
     clocks = ClockSampler(local_rank)
     topo, fl = make(args.precision)
     clocks.start()
-    ms, kps = time_md(topo, fl, args.steps, args.warmup)
+    ms, kps, rebuilds = time_md(topo, fl, args.steps, args.warmup)
     clk = clocks.stop()
     ms = max_over_ranks(ms, dist, "cuda")
     value = world * ns_per_day(ms)
@@ -306,7 +309,7 @@ def run_b200(args, rank, world, local_rank):
     fp64 = None
     if args.precision == "mixed" and not args.no_fp64:
         topo64, fl64 = make("fp64")
-        ms64, _ = time_md(topo64, fl64, max(3, args.steps // 2), 3)
+        ms64, _, _ = time_md(topo64, fl64, max(3, args.steps // 2), 3)
         ms64 = max_over_ranks(ms64, dist, "cuda")
         fp64 = {"value": world * ns_per_day(ms64), "ms_per_step": ms64,
                 "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64)}
@@ -340,7 +343,7 @@ def run_b200(args, rank, world, local_rank):
         "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": dict(config_dict(), precision=args.precision,
                        parallelism="replicas" if world > 1 else "single"),
-        "clocks": clk, "gpu_launches": (kps + 1) * args.steps, "e2e": e2e,
+        "clocks": clk, "gpu_launches": kps, "list_rebuilds": rebuilds, "e2e": e2e,
         "roofline": {"bound": "fp32", "kernel": "k_pair (LJ C2 + Ewald real space)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved and peak else None, "traffic": traffic,

@@ -123,6 +123,10 @@ int pmb_system_set_skin(pmb_system *sys, double skin);
  * host-pointer entry points check by themselves and retry; pmb_evaluate_device does not
  * synchronise, so its callers call this after their evaluations and repeat one that overflowed. */
 int pmb_system_check(pmb_system *sys);
+/* Neighbour-list builds so far (the first evaluation builds; later ones rebuild once an atom has
+ * moved more than half the skin).  Synchronises the system stream.  No counterpart in the
+ * reference, which rebuilds its cell lists at every evaluation. */
+int pmb_system_list_builds(pmb_system *sys, long long *n);
 
 /* Forces ------------------------------------------------------------------------------------- */
 pmb_force *pmb_force_create(pmb_system *sys, const pmb_force_desc *desc);
@@ -158,7 +162,8 @@ int pmb_md_run(pmb_md *md, int n_steps);
 /* Energies of the last force evaluation [n_boxes * PMB_E_STRIDE] and kinetic energy per box. */
 int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
 int pmb_md_use_graph(pmb_md *md, int enable);
-/* Kernel launches in one captured MD step (0 before the first graph run). */
+/* Kernel launches in one captured MD step (0 before the first graph run); the list-rebuild
+ * kernels are launched every step and return at once when no rebuild is due. */
 int pmb_md_kernels_per_step(pmb_md *md, int *n);
 /* Device memory held for this MD run: its system (atoms, neighbour lists, accumulators), its
  * forces (PME grids and tables) and the integrator state, in bytes (for admission by memory

@@ -55,6 +55,7 @@ _PROTOS = [
     ("pmb_system_n_boxes", C.c_int, [C.c_void_p]),
     ("pmb_system_set_skin", C.c_int, [C.c_void_p, C.c_double]),
     ("pmb_system_check", C.c_int, [C.c_void_p]),
+    ("pmb_system_list_builds", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_force_create", C.c_void_p, [C.c_void_p, C.c_void_p]),
     ("pmb_force_destroy", C.c_int, [C.c_void_p]),
     ("pmb_force_alpha", C.c_int, [C.c_void_p, C.c_void_p]),

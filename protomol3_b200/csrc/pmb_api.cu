@@ -334,10 +334,10 @@ int nblist_alloc(pmb_system *s, double rl) {
   int maxn = std::max(nb.nkeys, nblk) + 1;
   nb.scan_tmp = s->nba.get<int>(maxn / 4096 + 2);
   nb.xref = s->nba.get<double>(3 * (size_t)s->natoms);
-  nb.ctl = s->nba.get<unsigned>(4);
+  nb.ctl = s->nba.get<unsigned>(8);
   nb.half_skin2 = (float)(0.25 * s->skin * s->skin);
   if (!nb.xref || !nb.ctl) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
-  const unsigned ctl0[4] = {0u, 0u, 0u, 1u};  // first use builds the list
+  const unsigned ctl0[8] = {0u, 0u, 0u, 1u, 0u, 0u, 0u, 0u};  // first use builds the list
   CK(cudaMemcpy(nb.ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice));
   s->nb_build_rl = -1.0;
   if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.blk_c || !nb.blk_h || !nb.sblk_c || !nb.sblk_h || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.fslot ||
@@ -750,6 +750,17 @@ int pmb_system_check(pmb_system *s) {
     return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded; the lists were enlarged, evaluate again");
   }
   return rc;
+}
+
+int pmb_system_list_builds(pmb_system *s, long long *n) {
+  if (!s || !n) return fail(PMB_ERR_ARG, "null argument");
+  *n = 0;
+  if (!s->nb_ready) return PMB_OK;
+  unsigned long long v = 0;
+  CK(cudaMemcpyAsync(&v, s->nb.ctl + 4, sizeof(v), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *n = (long long)v;
+  return PMB_OK;
 }
 
 pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
@@ -1238,6 +1249,7 @@ int pmb_md_kernels_per_step(pmb_md *m, int *n) {
   *n = m->kernels_per_step;
   return PMB_OK;
 }
+
 
 int pmb_md_set_state(pmb_md *m, const double *pos, const double *vel) {
   if (!m || !pos) return fail(PMB_ERR_ARG, "null argument");

@@ -64,7 +64,8 @@ struct NbListDev {
   // list reuse: the list is built with cutoff + skin and rebuilt only once some atom moved more
   // than skin/2 since the last build (decided on the device, every step)
   double *xref;                // [3 natoms] positions at the last build
-  unsigned *ctl;               // [4] max displacement^2 (float bits), rebuild flag, block counter, force
+  unsigned *ctl;               // [8] max displacement^2 (float bits), rebuild flag, block counter,
+                               // force flag, list builds (64-bit counter in [4..5])
   float half_skin2;
 };
 

@@ -164,7 +164,9 @@ __global__ void k_disp_check(SystemDev s, NbListDev nb) {
     if (done == gridDim.x - 1) {
       __threadfence();
       float mx = __uint_as_float(atomicAdd(&nb.ctl[0], 0u));
-      nb.ctl[1] = (nb.ctl[3] != 0u || mx > nb.half_skin2) ? 1u : 0u;
+      const unsigned rebuild = (nb.ctl[3] != 0u || mx > nb.half_skin2) ? 1u : 0u;
+      nb.ctl[1] = rebuild;
+      if (rebuild) ++*reinterpret_cast<unsigned long long *>(nb.ctl + 4);
       nb.ctl[0] = 0u;
       nb.ctl[2] = 0u;
       nb.ctl[3] = 0u;
@@ -479,6 +481,9 @@ int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   const int T = 256;
   int na = s.natoms;
   if (na <= 0) return 0;
+  // every kernel after the displacement check exits at once unless ctl[1] asks for a rebuild
+  // (inside a CUDA graph such a launch costs about a microsecond)
+  const int wthreads = nb.nblk_total * 32;
   k_disp_check<<<(na + T - 1) / T, T, 0, st>>>(s, nb);
   k_zero_bins<<<(nb.nkeys + T) / T, T, 0, st>>>(nb.bin_count, nb.nkeys, nb.ctl);
   k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count, nb.ctl);
@@ -489,7 +494,6 @@ int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
   k_block_bbox<<<(nb.nslot + T - 1) / T, T, 0, st>>>(nb);
   k_superblock_bbox<<<(nb.nsblk * 32 + T - 1) / T, T, 0, st>>>(nb);
-  int wthreads = nb.nblk_total * 32;
   k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
   scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st, nb.ctl);
   k_tile_map<<<(wthreads + T - 1) / T, T, 0, st>>>(nb);

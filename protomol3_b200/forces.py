@@ -113,6 +113,12 @@ class Topology:
     def set_skin(self, skin):
         L.check(L.lib().pmb_system_set_skin(self.system(), float(skin)))
 
+    def list_builds(self):
+        """Neighbour-list builds so far (waits for the system's stream)."""
+        n = C.c_longlong(0)
+        L.check(L.lib().pmb_system_list_builds(self.system(), C.byref(n)))
+        return n.value
+
     def set_stream(self, stream_handle):
         L.check(L.lib().pmb_system_set_stream(self.system(), C.c_void_p(stream_handle)))
 
@@ -370,6 +376,8 @@ class Integrator:
         return pos, vel
 
     def kernels_per_step(self):
+        """Kernel launches of one MD step (the list-rebuild kernels exit at once when no rebuild
+        is due)."""
         n = C.c_int(0)
         L.check(L.lib().pmb_md_kernels_per_step(self._h, C.byref(n)))
         return n.value
