@@ -484,7 +484,54 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
   // in runs of consecutive slots, so a lane group's atomics touch two sectors per axis rather than
   // eight scattered atoms (pair_fold moves them to original order afterwards)
   const long long nsl = nb.nslot;
+  // i-forces of the current cluster per lane: the scalar path's in fi_acc, the packed path's
+  // (+f, the i-force is -fi) in a2p.fi; combined over the lane groups and added by slot when the
+  // cluster changes.  The packed path's energies and virial also accumulate in a2p over a chunk.
+  T fi_acc[3] = {T(0), T(0), T(0)};
+  Acc2 a2p;
+#pragma unroll
+  for (int c = 0; c < 3; c++) a2p.fi[c] = a2p.fj[c] = sp2(0.f);
+  a2p.elj = a2p.ec = sp2(0.f);
+#pragma unroll
+  for (int c = 0; c < 6; c++) a2p.vir[c] = sp2(0.f);
+  auto flush_fi = [&]() {  // warp-uniform
+    T f[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      f[c] = fi_acc[c];
+      if constexpr (MIXED) f[c] -= a2p.fi[c].x + a2p.fi[c].y;
+    }
+#pragma unroll
+    for (int o = BLOCK; o < 32; o <<= 1)
+#pragma unroll
+      for (int c = 0; c < 3; c++) f[c] += __shfl_xor_sync(0xffffffffu, f[c], o);
+    if (curI >= 0 && gb == 0 && im.x >= 0) {
+      long long *fs = nb.fslot + (long long)curI * BLOCK + li;
+      const long long v0 = f2fix(f[0], (T)FORCE_SCALE), v1 = f2fix(f[1], (T)FORCE_SCALE),
+                      v2 = f2fix(f[2], (T)FORCE_SCALE);
+      if (v0) red_add(fs, v0);
+      if (v1) red_add(fs + nsl, v1);
+      if (v2) red_add(fs + 2 * nsl, v2);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      fi_acc[c] = T(0);
+      a2p.fi[c] = sp2(0.f);
+    }
+  };
   auto spill_e = [&]() {
+    if constexpr (MIXED) {
+      el_acc += a2p.elj.x + a2p.elj.y;
+      ec_acc += a2p.ec.x + a2p.ec.y;
+      a2p.elj = a2p.ec = sp2(0.f);
+      if constexpr (VIR) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+          v_acc[c] += a2p.vir[c].x + a2p.vir[c].y;
+          a2p.vir[c] = sp2(0.f);
+        }
+      }
+    }
     wsum[lane] += f2fix(el_acc, (T)ENERGY_SCALE);
     wsum[32 + lane] += f2fix(ec_acc, (T)ENERGY_SCALE);
     el_acc = ec_acc = T(0);
@@ -609,6 +656,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
       const int I = __shfl_sync(0xffffffffu, tI, t), k = __shfl_sync(0xffffffffu, tk, t);
       if (I < 0) continue;
       if (I != curI) {
+        flush_fi();
         curI = I;
         const int sl = I * BLOCK + li;
         im = nb.slot_meta[sl];
@@ -674,8 +722,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
       stage_slot(jsl, buf, mine, jorig);
       const int tio = im.z * nt;
       const int nxt = gb | ((li + 1) & (BLOCK - 1));
-      // per-lane results of the tile: i-force, own j-force, energies, virial
-      T tfi[3], tfj[3], tel, tec, tvir[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+      T tfj[3];  // this lane's j-atom force of the tile
 
       bool packed = false;
       if constexpr (MIXED) {
@@ -693,24 +740,13 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
           qb[0] = eb; qb[BLOCK] = eb;
           qt[0] = et; qt[BLOCK] = et;
           __syncwarp();
-          Acc2 a2;
 #pragma unroll
-          for (int c = 0; c < 3; c++) a2.fi[c] = a2.fj[c] = sp2(0.f);
-          a2.elj = a2.ec = sp2(0.f);
-#pragma unroll
-          for (int c = 0; c < 6; c++) a2.vir[c] = sp2(0.f);
+          for (int c = 0; c < 3; c++) a2p.fj[c] = sp2(0.f);
           tile_pairs2<LSW, CM, CSW, VIR>(pt, reinterpret_cast<const float2 *>(ljab), tio, qa, qt, nxt, xi,
-                                         yi, zi, qi, a2);
+                                         yi, zi, qi, a2p);
           // after HALF rotations: .y holds this lane's j-atom, .x that of the lane HALF away
 #pragma unroll
-          for (int c = 0; c < 3; c++) {
-            tfj[c] = a2.fj[c].y + __shfl_xor_sync(0xffffffffu, a2.fj[c].x, HALF);
-            tfi[c] = -(a2.fi[c].x + a2.fi[c].y);
-          }
-          tel = a2.elj.x + a2.elj.y;
-          tec = a2.ec.x + a2.ec.y;
-          if constexpr (VIR)
-            for (int c = 0; c < 6; c++) tvir[c] = a2.vir[c].x + a2.vir[c].y;
+          for (int c = 0; c < 3; c++) tfj[c] = a2p.fj[c].y + __shfl_xor_sync(0xffffffffu, a2p.fj[c].x, HALF);
         }
       }
       if (!packed) {
@@ -813,18 +849,20 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
           else body(std::false_type{}, std::true_type{});
         }
         // after BLOCK rotations lane l holds the accumulator of j-atom l of the tile
+#pragma unroll
         for (int c = 0; c < 3; c++) {
-          tfi[c] = a.fi[c];
+          fi_acc[c] += a.fi[c];
           tfj[c] = fj[c];
         }
-        tel = a.elj;
-        tec = a.ec;
+        el_acc += a.elj;
+        ec_acc += a.ec;
         if constexpr (VIR)
-          for (int c = 0; c < 6; c++) tvir[c] = a.vir[c];
+          for (int c = 0; c < 6; c++) v_acc[c] += a.vir[c];
       }
 
       if (diag && gb == 0) {  // own atom li: its j-side force joins its i-side force
-        tfi[0] += tfj[0]; tfi[1] += tfj[1]; tfi[2] += tfj[2];
+#pragma unroll
+        for (int c = 0; c < 3; c++) fi_acc[c] += tfj[c];
       } else if (jorig >= 0) {
         long long *f = nb.fslot + jsl;
         long long v0 = f2fix(tfj[0], (T)FORCE_SCALE), v1 = f2fix(tfj[1], (T)FORCE_SCALE),
@@ -833,26 +871,10 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
         if (v1) red_add(f + nsl, v1);
         if (v2) red_add(f + 2 * nsl, v2);
       }
-      // combine the lane groups of the i-cluster
-#pragma unroll
-      for (int o = BLOCK; o < 32; o <<= 1)
-#pragma unroll
-        for (int c = 0; c < 3; c++) tfi[c] += __shfl_xor_sync(0xffffffffu, tfi[c], o);
-      if (gb == 0 && im.x >= 0) {  // the i-cluster's forces of this tile, by slot
-        long long *f = nb.fslot + (long long)I * BLOCK + li;
-        const long long v0 = f2fix(tfi[0], (T)FORCE_SCALE), v1 = f2fix(tfi[1], (T)FORCE_SCALE),
-                        v2 = f2fix(tfi[2], (T)FORCE_SCALE);
-        if (v0) red_add(f, v0);
-        if (v1) red_add(f + nsl, v1);
-        if (v2) red_add(f + 2 * nsl, v2);
-      }
-      el_acc += tel;
-      ec_acc += tec;
-      if constexpr (VIR)
-        for (int c = 0; c < 6; c++) v_acc[c] += tvir[c];
     }
     spill_e();
   }
+  flush_fi();
   flush_e();
 }
 
