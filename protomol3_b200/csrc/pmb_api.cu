@@ -188,6 +188,10 @@ int valid_switch(int k) { return k == SW_CUTOFF || k == SW_C1 || k == SW_C2; }
 struct pmb_system {
   int precision = 0, nbox = 0, natoms = 0, ntypes = 0;
   cudaStream_t stream = nullptr;
+  // second stream (higher priority) for the forces that run beside the pair kernel, with the
+  // events that fork it from and join it to the system stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool own_stream = false;
   Allocs a;
   std::vector<BoxDev> hbox;
@@ -241,6 +245,9 @@ struct pmb_system {
     if (h_eout) cudaFreeHost(h_eout);
     if (h_status) cudaFreeHost(h_status);
     if (own_stream && stream) cudaStreamDestroy(stream);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 };
 
@@ -454,41 +461,69 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     nblist_build(sd, s->nb, rlist, st);
     mark(s, "nblist");
   }
-  if (!jobs.empty()) {
-    for (size_t q = 0; q < jobs.size(); q++) {
-      const PairJob &j = jobs[q];
-      PairLaunch pl;
-      pl.precision = s->precision;
-      pl.p = j.p;
-      pl.lj = s->d_lj;
-      pl.lattice = j.lattice;
-      pl.multi = 0;
-      if (j.p.coul_mode == 2 && j.lattice)
-        for (const BoxDev &b : s->hbox) pl.multi |= b.multi_image;
-      if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
-      if (q + 1 == jobs.size()) pair_fold(sd, s->nb, st);  // slot-ordered pair forces -> facc
-      mark(s, "pair");
+  // PME, exclusion corrections and bonded terms run on the side stream beside the pair kernel
+  // (every sum is an integer atomic, so the interleaving does not change a bit); the stage
+  // profiler keeps them in one stream to time each stage
+  bool others = false;
+  for (int i = 0; i < n; i++) others |= fs[i]->kind == PMB_FORCE_PME || fs[i]->kind == PMB_FORCE_BONDED;
+  bool split = !s->prof && !jobs.empty() && others && st != cudaStreamLegacy;
+  if (split && !s->side) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      split = false;  // created outside a capture only
+    } else {
+      int lo = 0, hi = 0;
+      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      CK(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi));
+      CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     }
+  }
+  cudaStream_t so = st;
+  if (split) {
+    CK(cudaEventRecord(s->ev_fork, st));
+    CK(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+    so = s->side;
   }
   for (int i = 0; i < n; i++) {
     pmb_force *f = fs[i];
     if (f->kind == PMB_FORCE_PME) {
       f->pm.virial = virial;
       if (f->d.reciprocal) {
-        pme_recip_launch(sd, s->nb, f->pm, st, mark, s);
+        pme_recip_launch(sd, s->nb, f->pm, so, mark, s);
       }
       if (f->d.correction) {
         pme_correction_launch(sd, f->pm, s->d_excl_pairs, s->d_excl_kind, (int)s->h_excl_kind.size(),
-                              s->coulomb_scaling, st);
+                              s->coulomb_scaling, so);
         mark(s, "pme_correction");
       }
     } else if (f->kind == PMB_FORCE_BONDED) {
       BondedDev b = s->bonded;
       b.virial = virial;
-      bonded_launch(sd, b, st);
+      bonded_launch(sd, b, so);
       mark(s, "bonded");
     }
   }
+  for (size_t q = 0; q < jobs.size(); q++) {
+    const PairJob &j = jobs[q];
+    PairLaunch pl;
+    pl.precision = s->precision;
+    pl.p = j.p;
+    pl.lj = s->d_lj;
+    pl.lattice = j.lattice;
+    pl.multi = 0;
+    if (j.p.coul_mode == 2 && j.lattice)
+      for (const BoxDev &b : s->hbox) pl.multi |= b.multi_image;
+    if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+    mark(s, "pair");
+  }
+  if (split) {
+    CK(cudaEventRecord(s->ev_join, so));
+    CK(cudaStreamWaitEvent(st, s->ev_join, 0));
+  }
+  // slot-ordered pair forces -> facc (a plain read-modify-write: after the join)
+  if (!jobs.empty()) pair_fold(sd, s->nb, st);
   CK(cudaGetLastError());
   return PMB_OK;
 }

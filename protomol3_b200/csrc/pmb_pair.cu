@@ -889,9 +889,9 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
   size_t smem = ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx) +
                                         (VIR ? 8 : 2) * 32 * sizeof(long long) + warp_pref_bytes<MIXED>());
-  static int grid = 0;
+  static int resident = 0;
   static size_t conf_smem = 0;
-  if (!grid || conf_smem != smem) {
+  if (!resident || conf_smem != smem) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, nsm = 0, occ = 0;
@@ -899,9 +899,10 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, PAIR_THREADS, smem);
     if (occ < 1) occ = 1;
-    grid = nsm * occ;
+    resident = nsm * occ;
     conf_smem = smem;
   }
+  const int grid = resident;  // persistent: every resident CTA walks its share of the tiles
   using T = typename std::conditional<MIXED, float, double>::type;
   kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, params_t<T>(pl.p), pl.lj, pl.lattice);
   return 0;
