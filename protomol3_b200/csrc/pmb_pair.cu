@@ -202,9 +202,9 @@ __device__ __forceinline__ typename std::conditional<MIXED, float, double>::type
 }
 
 // Shared-memory image of one j-atom of a tile (scalar path).  Mixed: coordinates relative to the
-// first atom of the i-cluster (exact fixed-point difference, one rounding to FP32 per tile
-// instead of per pair); padding atoms sit at -1e6 A (i padding at +1e6 A) so the cutoff test
-// masks them.
+// first atom of the i-cluster (exact fixed-point difference converted to FP32 and scaled once per
+// tile, not per pair: about 1 ulp at 13 A, 1e-6 A); padding atoms sit at -1e6 A (i padding at
+// +1e6 A) so the cutoff test masks them.
 template <bool MIXED>
 struct JStage;
 template <>
@@ -416,6 +416,7 @@ constexpr size_t warp_stage_bytes() {
 // Per-warp constants of the current box and i-cluster.
 struct WarpCtx {
   double s[3];     // box edge / 2^32: fractional fixed point to A
+  float sf[3];     // the same in FP32 (j-atom staging: one conversion and one product per axis)
   float L[3], Lr[3];
   unsigned r0[3];  // fixed-point position of cluster atom 0 (mixed relative coordinates)
   int pad_;
@@ -606,9 +607,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
       js.m = make_int2(m.y, m.z);
       if constexpr (MIXED) {
         const uint4 f = rawP[b * 32 + lane];
-        js.p = make_float4((float)((double)(int)(f.x - ctx->r0[0]) * ctx->s[0]),
-                           (float)((double)(int)(f.y - ctx->r0[1]) * ctx->s[1]),
-                           (float)((double)(int)(f.z - ctx->r0[2]) * ctx->s[2]), __uint_as_float(f.w));
+        js.p = make_float4((float)(int)(f.x - ctx->r0[0]) * ctx->sf[0],
+                           (float)(int)(f.y - ctx->r0[1]) * ctx->sf[1],
+                           (float)(int)(f.z - ctx->r0[2]) * ctx->sf[2], __uint_as_float(f.w));
       } else {
         js.p = rawP[b * 32 + lane];
       }
@@ -669,6 +670,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
           if (lane == 0)
             for (int c = 0; c < 3; c++) {
               ctx->s[c] = bx->L[c] * (1.0 / 4294967296.0);
+              ctx->sf[c] = (float)(bx->L[c] * (1.0 / 4294967296.0));
               ctx->L[c] = (float)bx->L[c];
               ctx->Lr[c] = (float)bx->Lr[c];
             }
@@ -867,9 +869,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
         long long *f = nb.fslot + jsl;
         long long v0 = f2fix(tfj[0], (T)FORCE_SCALE), v1 = f2fix(tfj[1], (T)FORCE_SCALE),
                   v2 = f2fix(tfj[2], (T)FORCE_SCALE);
-        if (v0) red_add(f, v0);
-        if (v1) red_add(f + nsl, v1);
-        if (v2) red_add(f + 2 * nsl, v2);
+        red_add(f, v0);
+        red_add(f + nsl, v1);
+        red_add(f + 2 * nsl, v2);
       }
     }
     spill_e();
