@@ -283,23 +283,26 @@ def run_b200(args, rank, world, local_rank):
     e2e = None
     if rank == 0 or world > 1:
         n = topo.n_atoms
-        hpos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-        hfrc = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        # pinned host buffers; the caller's leapfrog runs in place on the host (torch CPU ops on
+        # the same memory, multi-threaded, as a C++ integrator loop of the caller would)
+        tpos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+        tfrc = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+        hpos, hfrc = tpos.numpy(), tfrc.numpy()
         hpos[:] = box["pos"]
-        vel = box["vel"].copy()
-        inv_m = (1.0 / box["mass"])[:, None]
         h = DT_FS * 0.02045482828087295
+        tvel = torch.from_numpy(box["vel"].copy())
+        thinv = torch.from_numpy(h / box["mass"])[:, None]
         en = F.ScalarStructure(1)
         nsteps = max(3, args.steps // 2)
         for it in range(nsteps + 2):
             if it == 2:
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-            hfrc[:] = 0.0
+            tfrc.zero_()
             en.clear()
             F.evaluate_all(topo, fl, hpos, hfrc, en)
-            vel += hfrc * (h * inv_m)
-            hpos += vel * h
+            tvel.addcmul_(tfrc, thinv)
+            tpos.add_(tvel, alpha=h)
         e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / nsteps, dist, "cuda")
         e2e = {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": int(hpos.nbytes), "d2h_bytes_per_step": int(hfrc.nbytes + 16 * 8),
