@@ -338,7 +338,7 @@ constexpr int BL_CAP = 128;  // candidate blocks buffered per warp before their 
 // the atoms of GROUPS listed blocks per pass within the list cutoff of I's box, compacted into
 // I's j-list (tiles of 32 entries).  The loads of the next pass are issued before the current
 // pass is tested.
-__global__ void __launch_bounds__(BL_THREADS) k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
+__global__ void __launch_bounds__(BL_THREADS, 4) k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   __shared__ int cand_all[BL_THREADS / 32][BL_CAP];
   if (!nb.ctl[1]) return;
   const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -364,14 +364,78 @@ __global__ void __launch_bounds__(BL_THREADS) k_build_lists(SystemDev s, NbListD
   // molecules of the cluster's atoms (-2: padding): a listed j-atom of one of them is flagged
   // JSAME, so the pair kernel runs the exclusion test only on tiles holding such an atom; the
   // block's own slots open its list (the pair kernel takes j > i among them)
+  // and the block's atom positions (fixed point; padding atoms far away): a candidate atom is
+  // listed when it is within the list radius of one of them, the exact Verlet condition per
+  // pair (the bounding-box gap alone would list about a third more atoms)
+  // (in shared memory, FP32 relative to the block's first atom; padding atoms far away)
+  // stored as pairs of atoms {t, t + BLOCK/2}: x x' y y' | z z' (two-wide FP32 tests)
+  __shared__ float4 ipos_all[BL_THREADS / 32][BLOCK];
+  float4 *ipos = ipos_all[threadIdx.x >> 5];
   int imol[BLOCK];
+  unsigned r0[3];
   {
     const int4 m = nb.slot_meta[I * BLOCK + li];
+    const uint4 f = nb.slot_fx[I * BLOCK + li];
     if (lane < BLOCK) out[lane] = m.x >= 0 ? ((I * BLOCK + lane) | JSAME) : -1;
     const int mine = m.x >= 0 ? m.y : -2;
 #pragma unroll
     for (int t = 0; t < BLOCK; t++) imol[t] = __shfl_sync(0xffffffffu, mine, t);
+    r0[0] = __shfl_sync(0xffffffffu, f.x, 0);
+    r0[1] = __shfl_sync(0xffffffffu, f.y, 0);
+    r0[2] = __shfl_sync(0xffffffffu, f.z, 0);
+    float px = 1e6f, py = 1e6f, pz = 1e6f;
+    if (m.x >= 0) {
+      px = (float)(int)(f.x - r0[0]) * sL[0];
+      py = (float)(int)(f.y - r0[1]) * sL[1];
+      pz = (float)(int)(f.z - r0[2]) * sL[2];
+    }
+    const float qx = __shfl_down_sync(0xffffffffu, px, BLOCK / 2), qy = __shfl_down_sync(0xffffffffu, py, BLOCK / 2),
+                qz = __shfl_down_sync(0xffffffffu, pz, BLOCK / 2);
+    if (lane < BLOCK / 2) {
+      ipos[2 * lane] = make_float4(px, qx, py, qy);
+      ipos[2 * lane + 1] = make_float4(pz, qz, 0.f, 0.f);
+    }
+    __syncwarp();
   }
+  // offsets from the first atom are minimal images of candidate-atom differences unless the box
+  // is under about twice the list radius plus the block's extent: then each difference is
+  // wrapped again
+  const float rlf = sqrtf(rl2);
+  const bool rewrap = rlf + 2.f * hI[0] >= 0.5f * (float)b.L[0] || rlf + 2.f * hI[1] >= 0.5f * (float)b.L[1] ||
+                      rlf + 2.f * hI[2] >= 0.5f * (float)b.L[2];
+  const float Lf[3] = {(float)b.L[0], (float)b.L[1], (float)b.L[2]},
+              Lrf[3] = {(float)b.Lr[0], (float)b.Lr[1], (float)b.Lr[2]};
+  auto near_any = [&](uint4 f) {
+    const float px = (float)(int)(f.x - r0[0]) * sL[0], py = (float)(int)(f.y - r0[1]) * sL[1],
+                pz = (float)(int)(f.z - r0[2]) * sL[2];
+    bool near = false;
+    if (rewrap) {
+#pragma unroll
+      for (int t = 0; t < BLOCK / 2; t++) {
+        const float4 a = ipos[2 * t], c = ipos[2 * t + 1];
+        const float qx[2] = {a.x, a.y}, qy[2] = {a.z, a.w}, qz[2] = {c.x, c.y};
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          float dx = px - qx[u], dy = py - qy[u], dz = pz - qz[u];
+          dx -= Lf[0] * rintf(dx * Lrf[0]);
+          dy -= Lf[1] * rintf(dy * Lrf[1]);
+          dz -= Lf[2] * rintf(dz * Lrf[2]);
+          near |= fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= rl2;
+        }
+      }
+      return near;
+    }
+    const float2 nx2 = make_float2(-px, -px), ny2 = make_float2(-py, -py), nz2 = make_float2(-pz, -pz);
+#pragma unroll
+    for (int t = 0; t < BLOCK / 2; t++) {
+      const float4 a = ipos[2 * t], c = ipos[2 * t + 1];
+      const float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx2), dy = __fadd2_rn(make_float2(a.z, a.w), ny2),
+                   dz = __fadd2_rn(make_float2(c.x, c.y), nz2);
+      const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      near |= (r2.x <= rl2) | (r2.y <= rl2);
+    }
+    return near;
+  };
   int count = BLOCK, ncand = 0;
   bool overflow = false;
 
@@ -394,7 +458,7 @@ __global__ void __launch_bounds__(BL_THREADS) k_build_lists(SystemDev s, NbListD
         m2 = nb.slot_meta[sl2];
         f2 = nb.slot_fx[sl2];
       }
-      const bool take = m.x >= 0 && (multi || gap2f(sL, cI, hI, f, make_uint4(0, 0, 0, 0)) <= rl2);
+      const bool take = m.x >= 0 && (multi || (gap2f(sL, cI, hI, f, make_uint4(0, 0, 0, 0)) <= rl2 && near_any(f)));
       const unsigned tm = __ballot_sync(0xffffffffu, take);
       const int n = __popc(tm);
       if (count + n > cap) {
