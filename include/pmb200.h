@@ -113,7 +113,7 @@ int pmb_system_destroy(pmb_system *sys);
 int pmb_system_set_stream(pmb_system *sys, void *cuda_stream);
 int pmb_system_n_atoms(const pmb_system *sys);
 int pmb_system_n_boxes(const pmb_system *sys);
-/* Verlet skin (A, default 0.4): the cell/neighbour list is built for cutoff + skin and rebuilt
+/* Verlet skin (A, default 0.8): the cell/neighbour list is built for cutoff + skin and rebuilt
  * on the device only when some atom moved more than skin/2 since the last build; 0 rebuilds at
  * every evaluation like Topology::updateCellLists.  The pair set evaluated is the same either
  * way (every pair within the cutoff). */

@@ -214,7 +214,7 @@ struct pmb_system {
   bool nb_ready = false;
   double nb_cutoff = 0.0;    // radius the list storage is sized for
   double nb_build_rl = -1.0; // radius the current list was built with
-  double skin = 0.4;         // list radius = pair cutoff + skin
+  double skin = 0.8;         // list radius = pair cutoff + skin
   NbListDev nb{};
   Allocs nba;
   int n_bonded = 0;

@@ -35,9 +35,11 @@ def test_each_result_alone_equals_result_in_the_mix():
 
 def test_staggered_arrivals_and_budget():
     """A budget that holds one segment serialises them; staggered arrivals are served in order
-    and every segment frees its device memory when it completes."""
+    and every segment frees its device memory when it completes.  The budget is the smallest
+    request's estimate, so no request fits beside a resident one whatever the timing (a request
+    above the budget still runs, alone)."""
     reqs = _reqs(arrivals=(0.0, 0.05, 0.1))
-    one = max(S.estimate_bytes(r.n_atoms, r.grid) for r in reqs)
+    one = min(S.estimate_bytes(r.n_atoms, r.grid) for r in reqs)
     srv = S.MDServer(hbm_budget_bytes=one, max_active=8, chunk=100)
     res = srv.run_trace(reqs)
     assert [r.req.rid for r in res] == [0, 1, 2]
