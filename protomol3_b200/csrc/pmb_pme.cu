@@ -213,6 +213,13 @@ __device__ __forceinline__ void grid_coord(unsigned fx, double x, double hr, int
   base = iu - (P - 1) / 2 + n;  // myNXOffset = -(order-1)/2 + n
 }
 
+// x mod n for 0 <= x < 3n (a stencil index: base in [n - (p-1)/2, 2n) plus an offset below p,
+// with n >= p), without an integer division.
+__device__ __forceinline__ int wrap3(int x, int n) {
+  x = x >= n ? x - n : x;
+  return x >= n ? x - n : x;
+}
+
 // PC > 0: interpolation order fixed at compile time (weights stay in registers); PC = 0: run time.
 template <bool MIXED, int PC>
 __global__ void k_spread(NbListDev nb, PmeDev pm) {
@@ -252,15 +259,15 @@ __global__ void k_spread(NbListDev nb, PmeDev pm) {
   #pragma unroll
   for (int i = 0; i < P; i++) {
     T a = q * th[0][i];
-    int i1 = (i + base[0]) % nx;
+    int i1 = wrap3(i + base[0], nx);
     #pragma unroll
     for (int j = 0; j < P; j++) {
       T ab = a * th[1][j];
-      int j1 = (j + base[1]) % ny;
+      int j1 = wrap3(j + base[1], ny);
       long long *row = g + ((long long)i1 * ny + j1) * nz;
       #pragma unroll
       for (int k = 0; k < P; k++) {
-        int k1 = (k + base[2]) % nz;
+        int k1 = wrap3(k + base[2], nz);
         long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
         if (v) red_add(row + k1, v);
       }
@@ -270,13 +277,12 @@ __global__ void k_spread(NbListDev nb, PmeDev pm) {
 
 // B-spline weights and grid bases of one slot for order 4 (the common case).
 template <bool MIXED, bool DERIV>
-__device__ __forceinline__ void weights4(const NbListDev &nb, const PmeBoxPlan &pl, int sl,
+__device__ __forceinline__ void weights4(const PmeBoxPlan &pl, uint4 f, double4 pq,
                                          typename std::conditional<MIXED, float, double>::type th[3][4],
                                          typename std::conditional<MIXED, float, double>::type dth[3][4],
                                          int base[3], typename std::conditional<MIXED, float, double>::type &q) {
   using T = typename std::conditional<MIXED, float, double>::type;
   if constexpr (MIXED) {
-    const uint4 f = nb.slot_fx[sl];
     const unsigned fx[3] = {f.x, f.y, f.z};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -286,7 +292,6 @@ __device__ __forceinline__ void weights4(const NbListDev &nb, const PmeBoxPlan &
     }
     q = __uint_as_float(f.w);
   } else {
-    const double4 pq = nb.slot_pq[sl];
     const double x[3] = {pq.x, pq.y, pq.z};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -313,26 +318,31 @@ __global__ void k_spread4(NbListDev nb, PmeDev pm) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int sl = (int)(t >> 2), p = (int)(t & 3);
   if (sl >= nb.nslot) return;
+  // the slot's metadata and position are loaded together (one round trip)
   const int4 m = nb.slot_meta[sl];
+  uint4 f4 = make_uint4(0, 0, 0, 0);
+  double4 p4 = make_double4(0, 0, 0, 0);
+  if constexpr (MIXED) f4 = nb.slot_fx[sl];
+  else p4 = nb.slot_pq[sl];
   if (m.x < 0) return;
   const PmeBoxPlan &pl = pm.plan[m.w];
   T th[3][4];
   int base[3];
   T q;
-  weights4<MIXED, false>(nb, pl, sl, th, th, base, q);
+  weights4<MIXED, false>(pl, f4, p4, th, th, base, q);
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
   long long *g = pm.qgrid + pl.grid0;
   const T a = q * pick4(th[0], p);
-  const int i1 = (p + base[0]) % nx;
+  const int i1 = wrap3(p + base[0], nx);
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     const T ab = a * th[1][j];
-    const int j1 = (j + base[1]) % ny;
+    const int j1 = wrap3(j + base[1], ny);
     long long *row = g + ((long long)i1 * ny + j1) * nz;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
-      if (v) red_add(row + (k + base[2]) % nz, v);
+      if (v) red_add(row + wrap3(k + base[2], nz), v);
     }
   }
 }
@@ -342,7 +352,12 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   using T = typename std::conditional<MIXED, float, double>::type;
   int sl = blockIdx.x * blockDim.x + threadIdx.x;
   if (sl >= nb.nslot) return;
+  // the slot's metadata and position are loaded together (one round trip)
   int4 m = nb.slot_meta[sl];
+  uint4 f4 = make_uint4(0, 0, 0, 0);
+  double4 pq = make_double4(0, 0, 0, 0);
+  if constexpr (MIXED) f4 = nb.slot_fx[sl];
+  else pq = nb.slot_pq[sl];
   if (m.x < 0) return;
   const PmeBoxPlan &pl = pm.plan[m.w];
   const int P = PC > 0 ? PC : pm.order;
@@ -350,17 +365,15 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   int base[3];
   T q;
   if constexpr (MIXED) {
-    uint4 f = nb.slot_fx[sl];
-    unsigned fx[3] = {f.x, f.y, f.z};
+    unsigned fx[3] = {f4.x, f4.y, f4.z};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       T w;
       grid_coord<true>(fx[d], 0.0, 0.0, pl.n[d], P, base[d], w);
       bspline<T>(P, w, th[d], dth[d]);
     }
-    q = __uint_as_float(f.w);
+    q = __uint_as_float(f4.w);
   } else {
-    double4 pq = nb.slot_pq[sl];
     double x[3] = {pq.x, pq.y, pq.z};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -375,15 +388,15 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   T fx = 0, fy = 0, fz = 0;
   #pragma unroll
   for (int i = 0; i < P; i++) {
-    int i1 = (i + base[0]) % nx;
+    int i1 = wrap3(i + base[0], nx);
     #pragma unroll
     for (int j = 0; j < P; j++) {
-      int j1 = (j + base[1]) % ny;
+      int j1 = wrap3(j + base[1], ny);
       T xij = dth[0][i] * th[1][j], yij = th[0][i] * dth[1][j], zij = th[0][i] * th[1][j];
       const T *row = g + ((long long)i1 * ny + j1) * nz;
       #pragma unroll
       for (int k = 0; k < P; k++) {
-        int k1 = (k + base[2]) % nz;
+        int k1 = wrap3(k + base[2], nz);
         T term = row[k1];
         fx -= term * xij * th[2][k];
         fy -= term * yij * th[2][k];
