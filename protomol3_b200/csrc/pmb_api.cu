@@ -191,7 +191,7 @@ struct pmb_system {
   // second stream (higher priority) for the forces that run beside the pair kernel, with the
   // events that fork it from and join it to the system stream
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_slots = nullptr, ev_join = nullptr;
   bool own_stream = false;
   Allocs a;
   std::vector<BoxDev> hbox;
@@ -247,6 +247,7 @@ struct pmb_system {
     if (own_stream && stream) cudaStreamDestroy(stream);
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_slots) cudaEventDestroy(ev_slots);
     if (ev_join) cudaEventDestroy(ev_join);
   }
 };
@@ -449,21 +450,11 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   std::vector<PairJob> jobs = pair_jobs(s, fs, n, virial);
   bool need_pme_slots = false;
   for (int i = 0; i < n; i++) need_pme_slots |= fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal;
-  if (!jobs.empty() || need_pme_slots) {
-    // list radius: pair cutoff + skin (+ a margin for the fixed-point culling)
-    const double rlist = std::max(rl, 1.0) + s->skin + 1e-3;
-    int rc = ensure_nblist(s, rlist);
-    if (rc) return rc;
-    if (rlist != s->nb_build_rl) {  // a list built for another radius cannot be reused
-      CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, st));
-      s->nb_build_rl = rlist;
-    }
-    nblist_build(sd, s->nb, rlist, st);
-    mark(s, "nblist");
-  }
-  // PME, exclusion corrections and bonded terms run on the side stream beside the pair kernel
-  // (every sum is an integer atomic, so the interleaving does not change a bit); the stage
-  // profiler keeps them in one stream to time each stage
+  const bool need_list = !jobs.empty() || need_pme_slots;
+  // PME, exclusion corrections and bonded terms run on the side stream beside the list build and
+  // the pair kernel (every sum is an integer atomic, so the interleaving does not change a bit):
+  // the corrections and bonded terms from the start, the PME chain once this step's slot records
+  // are packed.  The stage profiler keeps everything in one stream to time each stage.
   bool others = false;
   for (int i = 0; i < n; i++) others |= fs[i]->kind == PMB_FORCE_PME || fs[i]->kind == PMB_FORCE_BONDED;
   bool split = !s->prof && !jobs.empty() && others && st != cudaStreamLegacy;
@@ -477,6 +468,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
       CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
       CK(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi));
       CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&s->ev_slots, cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     }
   }
@@ -486,25 +478,49 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     CK(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
     so = s->side;
   }
-  for (int i = 0; i < n; i++) {
-    pmb_force *f = fs[i];
-    if (f->kind == PMB_FORCE_PME) {
+  auto launch_recip = [&](pmb_force *f) {
+    f->pm.virial = virial;
+    pme_recip_launch(sd, s->nb, f->pm, so, mark, s);
+  };
+  auto launch_atom_terms = [&](pmb_force *f) {  // exclusion corrections, bonded: no list needed
+    if (f->kind == PMB_FORCE_PME && f->d.correction) {
       f->pm.virial = virial;
-      if (f->d.reciprocal) {
-        pme_recip_launch(sd, s->nb, f->pm, so, mark, s);
-      }
-      if (f->d.correction) {
-        pme_correction_launch(sd, f->pm, s->d_excl_pairs, s->d_excl_kind, (int)s->h_excl_kind.size(),
-                              s->coulomb_scaling, so);
-        mark(s, "pme_correction");
-      }
+      pme_correction_launch(sd, f->pm, s->d_excl_pairs, s->d_excl_kind, (int)s->h_excl_kind.size(),
+                            s->coulomb_scaling, so);
+      mark(s, "pme_correction");
     } else if (f->kind == PMB_FORCE_BONDED) {
       BondedDev b = s->bonded;
       b.virial = virial;
       bonded_launch(sd, b, so);
       mark(s, "bonded");
     }
+  };
+  if (split)
+    for (int i = 0; i < n; i++) launch_atom_terms(fs[i]);
+  if (need_list) {
+    // list radius: pair cutoff + skin (+ a margin for the fixed-point culling)
+    const double rlist = std::max(rl, 1.0) + s->skin + 1e-3;
+    int rc = ensure_nblist(s, rlist);
+    if (rc) return rc;
+    if (rlist != s->nb_build_rl) {  // a list built for another radius cannot be reused
+      CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, st));
+      s->nb_build_rl = rlist;
+    }
+    nblist_sort(sd, s->nb, st);
+    if (split && need_pme_slots) {
+      CK(cudaEventRecord(s->ev_slots, st));
+      CK(cudaStreamWaitEvent(s->side, s->ev_slots, 0));
+      for (int i = 0; i < n; i++)
+        if (fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal) launch_recip(fs[i]);
+    }
+    nblist_lists(sd, s->nb, rlist, st);
+    mark(s, "nblist");
   }
+  if (!split)
+    for (int i = 0; i < n; i++) {
+      if (fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal) launch_recip(fs[i]);
+      launch_atom_terms(fs[i]);
+    }
   for (size_t q = 0; q < jobs.size(); q++) {
     const PairJob &j = jobs[q];
     PairLaunch pl;

@@ -65,7 +65,8 @@ struct NbListDev {
   // than skin/2 since the last build (decided on the device, every step)
   double *xref;                // [3 natoms] positions at the last build
   unsigned *ctl;               // [8] max displacement^2 (float bits), rebuild flag, block counter,
-                               // force flag, list builds (64-bit counter in [4..5])
+                               // force flag, list builds (64-bit counter in [4..5]), the pair
+                               // kernel's next chunk and finished warps ([6], [7]; zero between launches)
   float half_skin2;
 };
 
@@ -81,7 +82,8 @@ struct SystemDev {
   long long *eacc;             // [nbox * ACC_PER_BOX]
 };
 
-int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st);
+int nblist_sort(const SystemDev &s, NbListDev &nb, cudaStream_t st);
+int nblist_lists(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st);
 int fp32_peak_probe(double *tflops);
 
 // ------------------------------------------------------------------ pair kernel (pair.cu)

@@ -541,13 +541,14 @@ int scan_exclusive(const int *in, int *out, int n, int *tmp, cudaStream_t st, co
 
 }  // namespace
 
-int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st) {
+// First half of a build: displacement check, sort into slots and the slot records of this step's
+// positions (the PME kernels need no more than these).
+int nblist_sort(const SystemDev &s, NbListDev &nb, cudaStream_t st) {
   const int T = 256;
   int na = s.natoms;
   if (na <= 0) return 0;
   // every kernel after the displacement check exits at once unless ctl[1] asks for a rebuild
   // (inside a CUDA graph such a launch costs about a microsecond)
-  const int wthreads = nb.nblk_total * 32;
   k_disp_check<<<(na + T - 1) / T, T, 0, st>>>(s, nb);
   k_zero_bins<<<(nb.nkeys + T) / T, T, 0, st>>>(nb.bin_count, nb.nkeys, nb.ctl);
   k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count, nb.ctl);
@@ -556,6 +557,14 @@ int nblist_build(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   k_sort_bins<<<(nb.nkeys + T - 1) / T, T, 0, st>>>(s, nb.bin_box, nb.bin_start, nb.bin_count,
                                                    nb.nkeys, nb.slot_orig, nb.ctl);
   k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
+  return 0;
+}
+
+// Second half: cluster boxes, the cluster j-lists and the tile map of the pair kernel.
+int nblist_lists(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStream_t st) {
+  const int T = 256;
+  if (s.natoms <= 0) return 0;
+  const int wthreads = nb.nblk_total * 32;
   k_block_bbox<<<(nb.nslot + T - 1) / T, T, 0, st>>>(nb);
   k_superblock_bbox<<<(nb.nsblk * 32 + T - 1) / T, T, 0, st>>>(nb);
   k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);

@@ -621,10 +621,19 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
     }
   };
 
-  // Tiles go to warps in chunks of CHUNK consecutive tiles.  Per chunk the tile records and their
-  // j-list words are fetched once (one round trip each); each tile's slot records are copied one
-  // tile ahead into the other buffer, so only the first tile of a chunk waits for them.
-  for (int c0 = gwarp * CHUNK; c0 < total; c0 += nwarps * CHUNK) {
+  // Tiles go to warps in chunks of CHUNK consecutive tiles: chunk gwarp first, then the next
+  // unclaimed chunk from a counter (ctl[6]), so warps that start late (SMs busy with the PME
+  // kernels beside this one) take fewer chunks.  The floating-point partial sums (i-forces,
+  // energies, virial) are closed at every chunk end, so the result does not depend on which warp
+  // took which chunk.  Per chunk the tile records and their j-list words are fetched once (one
+  // round trip each); each tile's slot records are copied one tile ahead into the other buffer,
+  // so only the first tile of a chunk waits for them.
+  unsigned *wq = nb.ctl + 6;
+  const int nchunk = (total + CHUNK - 1) / CHUNK;
+  for (int ci = gwarp; ci < nchunk;) {
+    int tnext = 0;
+    if (lane == 0) tnext = nwarps + (int)atomicAdd(wq, 1u);  // claimed now, read at chunk end
+    const int c0 = ci * CHUNK;
     const int nc = min(CHUNK, total - c0);
     tI = -1;
     tk = -1;
@@ -875,9 +884,17 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
       }
     }
     spill_e();
+    flush_fi();
+    ci = __shfl_sync(0xffffffffu, tnext, 0);
   }
   flush_fi();
   flush_e();
+  // the last warp to finish resets the chunk counter for the next launch (every warp has made
+  // its last claim before it counts itself here)
+  if (lane == 0 && atomicAdd(wq + 1, 1u) == (unsigned)nwarps - 1u) {
+    atomicExch(wq, 0u);
+    atomicExch(wq + 1, 0u);
+  }
 }
 
 template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI = false>
