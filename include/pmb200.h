@@ -162,6 +162,30 @@ int pmb_md_run(pmb_md *md, int n_steps);
 /* Energies of the last force evaluation [n_boxes * PMB_E_STRIDE] and kinetic energy per box. */
 int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
 int pmb_md_use_graph(pmb_md *md, int enable);
+/* Bond constraints of a leapfrog run (replaces ModifierShake / ModifierRattle as
+ * module/ModifierModule.cpp:106-128 installs them): SHAKE after every drift, RATTLE after every
+ * step, on a constraint list in the reference's order (topology/TopologyUtilities.cpp:695-775,
+ * buildRattleShakeBondConstraintList).  A modifier is on when its flag is set, epsilon > 0 and
+ * max_iter > 0 (the reference's defaults: 1e-5 and 30).  Each application sweeps the list as the
+ * reference does until the mean error is at most epsilon, at most max_iter + 1 sweeps; the
+ * constraint virial is not accumulated.  Constrained groups (atoms linked by constraints) hold at
+ * most 8 atoms and 16 constraints; max_iter below 256.  The SHAKE reference positions are the
+ * positions at pmb_md_set_state, or the current ones when this is called after it.
+ * PMB_ERR_UNSUPPORTED for the Langevin integrator. */
+typedef struct {
+  int n_constraints;
+  const int *atom1, *atom2;   /* [n_constraints] */
+  const double *rest_length;  /* [n_constraints] A */
+  int shake;
+  double shake_epsilon;
+  int shake_max_iter;
+  int rattle;
+  double rattle_epsilon;
+  int rattle_max_iter;
+} pmb_constraint_desc;
+int pmb_md_set_constraints(pmb_md *md, const pmb_constraint_desc *desc);
+/* Sweeps of the last SHAKE and RATTLE application (max_iter + 1: not converged). */
+int pmb_md_constraint_sweeps(pmb_md *md, int *shake_sweeps, int *rattle_sweeps);
 /* Kernel launches in one captured MD step (0 before the first graph run); the list-rebuild
  * kernels are launched every step and return at once when no rebuild is due. */
 int pmb_md_kernels_per_step(pmb_md *md, int *n);

@@ -47,6 +47,12 @@ class OrcPME(C.Structure):
                 ("do_corr", C.c_int)]
 
 
+class OrcConstraints(C.Structure):
+    _fields_ = [("n", C.c_int), ("a1", C.c_void_p), ("a2", C.c_void_p), ("len", C.c_void_p),
+                ("shake_eps", C.c_double), ("shake_maxiter", C.c_int),
+                ("rattle_eps", C.c_double), ("rattle_maxiter", C.c_int)]
+
+
 _lib = None
 
 
@@ -55,7 +61,8 @@ def lib():
     if _lib is None:
         build()
         _lib = C.CDLL(LIB)
-        for fn in ("orc_cutoff", "orc_pme", "orc_bonded", "orc_leapfrog"):
+        for fn in ("orc_cutoff", "orc_pme", "orc_bonded", "orc_leapfrog",
+                   "orc_leapfrog_constrained", "orc_shake", "orc_rattle"):
             getattr(_lib, fn).restype = C.c_int
         _lib.orc_pme_alpha.restype = C.c_double
         _lib.orc_pme_alpha.argtypes = [C.c_double, C.c_double]
@@ -166,6 +173,30 @@ def leapfrog(system, pos, vel, dt, nsteps, cutoff=None, pme=None, bonded=True):
     return pos, vel, f, e
 
 
+def leapfrog_constrained(system, pos, vel, dt, nsteps, constraints, shake=(1e-5, 30),
+                         rattle=(1e-5, 30), cutoff=None, pme=None, bonded=False, last_pos=None):
+    """LeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step) as
+    orc_leapfrog_constrained restates them.  constraints = (atom1, atom2, rest_length);
+    shake / rattle = (epsilon, max_iter) or None.  Returns pos, vel, forces, energies."""
+    L = lib()
+    pos = np.ascontiguousarray(pos, np.float64).copy()
+    vel = np.ascontiguousarray(vel, np.float64).copy()
+    last = pos.copy() if last_pos is None else np.ascontiguousarray(last_pos, np.float64).copy()
+    keep = [np.ascontiguousarray(constraints[0], np.int32), np.ascontiguousarray(constraints[1], np.int32),
+            np.ascontiguousarray(constraints[2], np.float64)]
+    c = OrcConstraints()
+    c.n = len(keep[0])
+    c.a1, c.a2, c.len = _p(keep[0]), _p(keep[1]), _p(keep[2])
+    c.shake_eps, c.shake_maxiter = shake if shake is not None else (0.0, 0)
+    c.rattle_eps, c.rattle_maxiter = rattle if rattle is not None else (0.0, 0)
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    L.orc_leapfrog_constrained(C.byref(system.s), C.byref(cutoff) if cutoff is not None else None,
+                               C.byref(pme) if pme is not None else None, int(bonded), C.byref(c),
+                               C.c_double(dt), int(nsteps), _p(pos), _p(vel), _p(last), _p(f), _p(e))
+    return pos, vel, f, e
+
+
 def pme_alpha(cutoff, accuracy):
     return lib().orc_pme_alpha(cutoff, accuracy)
 
@@ -258,3 +289,41 @@ def ref_evaluate(system, pos, cutoff=None, pme=None, bonded=False, virial=False,
         p.cutoff, p.accuracy, p.alpha, p.real_switch = pme.cutoff, pme.accuracy, pme.alpha, pme.real_switch
         L.ref_pme_eval(C.byref(r), C.byref(p), _p(f), _p(e), vp)
     return f, e, v
+
+
+# ProtoMol's own leapfrog integrator with its SHAKE/RATTLE modifiers (oracle/_ref/libpmref_md.so).
+REF_MD_LIB = os.path.join(HERE, "_ref", "libpmref_md.so")
+_ref_md = None
+
+
+def ref_md_available():
+    return os.path.exists(REF_MD_LIB)
+
+
+def ref_leapfrog_constrained(system, elem, pos, vel, dt, nsteps, shake=(1e-5, 30),
+                             rattle=(1e-5, 30), all_bonds=True):
+    """The reference run with no force terms: returns pos, vel and the reference's constraint
+    list (atom1, atom2, rest_length)."""
+    global _ref_md
+    if _ref_md is None:
+        ref_lib()  # its force path library first (the md library links against it)
+        _ref_md = C.CDLL(REF_MD_LIB)
+    pos = np.ascontiguousarray(pos, np.float64).copy()
+    vel = np.ascontiguousarray(vel, np.float64).copy()
+    r = _ref_input(system, pos, 5.0)
+    el = C.create_string_buffer(elem.encode() if isinstance(elem, str) else bytes(elem))
+    cap = 4 * system.n + 16
+    cons = np.zeros(3 * cap, np.int32)
+    lens = np.zeros(cap)
+    ncon = C.c_int(0)
+    se, sm = shake if shake is not None else (0.0, 0)
+    re_, rm = rattle if rattle is not None else (0.0, 0)
+    rc = _ref_md.ref_leapfrog_constrained(
+        C.byref(r), el, int(shake is not None), C.c_double(se), int(sm), int(rattle is not None),
+        C.c_double(re_), int(rm), int(all_bonds), C.c_double(dt), int(nsteps), _p(pos), _p(vel),
+        C.byref(ncon), _p(cons), _p(lens), cap)
+    if rc:
+        raise RuntimeError("reference run failed")
+    n = min(ncon.value, cap)
+    cons = cons[:3 * n].reshape(-1, 3)
+    return pos, vel, (cons[:, 0].copy(), cons[:, 1].copy(), lens[:n].copy())

@@ -785,3 +785,141 @@ int orc_leapfrog(const orc_system *s, const orc_cutoff_params *cp, const orc_pme
   memcpy(energies_out, e, sizeof(e));
   return 0;
 }
+
+/* ------------------------------------------------------------------ SHAKE / RATTLE */
+static const double TIMEFACTOR = 48.88821290839616; /* base/PMConstants.cpp:53 */
+
+/* ModifierMetaShake::calcError (ModifierMetaShake.cpp:12-33): mean over the constraints of
+ * |d^2 - l^2| / (2 l^2), with d = x[a2] - x[a1]. */
+static double shake_error(const orc_constraints *c, const double *x) {
+  double error = 0;
+  for (int i = 0; i < c->n; i++) {
+    const double *p1 = x + 3 * c->a1[i], *p2 = x + 3 * c->a2[i];
+    const double l2 = c->len[i] * c->len[i];
+    const double dx = p2[0] - p1[0], dy = p2[1] - p1[1], dz = p2[2] - p1[2];
+    error += fabs(dx * dx + dy * dy + dz * dz - l2) / (2.0 * l2);
+  }
+  return error / c->n;
+}
+
+int orc_shake(const orc_constraints *c, const double *mass, int n_atoms, double dt_fs, double *pos,
+              double *vel, double *last_pos) {
+  /* ModifierShake::doExecute (ModifierShake.cpp:17-75); the virial term is not accumulated */
+  double error = shake_error(c, pos);
+  const double dt = dt_fs / TIMEFACTOR;
+  int iter = 0;
+  while (error > c->shake_eps) {
+    for (int i = 0; i < c->n; i++) {
+      const int a1 = c->a1[i], a2 = c->a2[i];
+      double *p1 = pos + 3 * a1, *p2 = pos + 3 * a2, *v1 = vel + 3 * a1, *v2 = vel + 3 * a2;
+      const double *q1 = last_pos + 3 * a1, *q2 = last_pos + 3 * a2;
+      const double pab[3] = {p1[0] - p2[0], p1[1] - p2[1], p1[2] - p2[2]};
+      const double pabsq = pab[0] * pab[0] + pab[1] * pab[1] + pab[2] * pab[2];
+      const double rabsq = c->len[i] * c->len[i];
+      const double diffsq = rabsq - pabsq;
+      const double rab[3] = {q1[0] - q2[0], q1[1] - q2[1], q1[2] - q2[2]};
+      const double rpab = rab[0] * pab[0] + rab[1] * pab[1] + rab[2] * pab[2];
+      const double rM1 = 1 / mass[a1], rM2 = 1 / mass[a2];
+      const double gab = diffsq / (2 * (rM1 + rM2) * rpab);
+      double dp[3];
+      for (int q = 0; q < 3; q++) dp[q] = rab[q] * gab;
+      for (int q = 0; q < 3; q++) {
+        p1[q] += dp[q] * rM1;
+        p2[q] -= dp[q] * rM2;
+      }
+      for (int q = 0; q < 3; q++) dp[q] /= dt;
+      for (int q = 0; q < 3; q++) {
+        v1[q] += dp[q] * rM1;
+        v2[q] -= dp[q] * rM2;
+      }
+    }
+    error = shake_error(c, pos);
+    iter++;
+    if (iter > c->shake_maxiter) break;
+  }
+  memcpy(last_pos, pos, sizeof(double) * 3 * (size_t)n_atoms);
+  return iter;
+}
+
+/* ModifierMetaRattle::calcError (ModifierMetaRattle.cpp:12-31): mean |(x1 - x2).(v1 - v2)|. */
+static double rattle_error(const orc_constraints *c, const double *x, const double *v) {
+  double error = 0;
+  for (int i = 0; i < c->n; i++) {
+    const int a1 = c->a1[i], a2 = c->a2[i];
+    const double vab[3] = {v[3 * a1] - v[3 * a2], v[3 * a1 + 1] - v[3 * a2 + 1], v[3 * a1 + 2] - v[3 * a2 + 2]};
+    const double rab[3] = {x[3 * a1] - x[3 * a2], x[3 * a1 + 1] - x[3 * a2 + 1], x[3 * a1 + 2] - x[3 * a2 + 2]};
+    error += fabs(rab[0] * vab[0] + rab[1] * vab[1] + rab[2] * vab[2]);
+  }
+  return error / c->n;
+}
+
+int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const double *pos,
+               double *vel) {
+  /* ModifierRattle::doExecute (ModifierRattle.cpp:17-64); the virial term is not accumulated */
+  double error = rattle_error(c, pos, vel);
+  const double dt = dt_fs / TIMEFACTOR;
+  int iter = 0;
+  while (error > c->rattle_eps) {
+    for (int i = 0; i < c->n; i++) {
+      const int a1 = c->a1[i], a2 = c->a2[i];
+      const double rM1 = 1 / mass[a1], rM2 = 1 / mass[a2];
+      const double *p1 = pos + 3 * a1, *p2 = pos + 3 * a2;
+      double *v1 = vel + 3 * a1, *v2 = vel + 3 * a2;
+      const double rab[3] = {p1[0] - p2[0], p1[1] - p2[1], p1[2] - p2[2]};
+      const double rabsq = rab[0] * rab[0] + rab[1] * rab[1] + rab[2] * rab[2];
+      const double vab[3] = {v1[0] - v2[0], v1[1] - v2[1], v1[2] - v2[2]};
+      const double rvab = rab[0] * vab[0] + rab[1] * vab[1] + rab[2] * vab[2];
+      const double gab = -rvab / (dt * (rM1 + rM2) * rabsq);
+      for (int q = 0; q < 3; q++) {
+        const double dp = rab[q] * gab;
+        v1[q] += dp * dt * rM1;
+        v2[q] -= dp * dt * rM2;
+      }
+    }
+    error = rattle_error(c, pos, vel);
+    iter++;
+    if (iter > c->rattle_maxiter) break;
+  }
+  return iter;
+}
+
+int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
+                             const orc_pme_params *pme, int do_bonded, const orc_constraints *c,
+                             double dt_fs, int nsteps, double *pos, double *vel, double *last_pos,
+                             double *forces_out, double *energies_out) {
+  const int n = s->n;
+  const int shake = c && c->n > 0 && c->shake_eps > 0 && c->shake_maxiter > 0;
+  const int rattle = c && c->n > 0 && c->rattle_eps > 0 && c->rattle_maxiter > 0;
+  double *f = forces_out, e[ORC_E_COUNT];
+  const double h = dt_fs * INV_TIMEFACTOR;
+  all_forces(s, cp, pme, do_bonded, pos, f, e);
+  if (nsteps >= 1) {
+    /* doHalfKickdoDrift, fast path (no pre-drift modifier), then the post-drift SHAKE */
+    for (int i = 0; i < n; i++)
+      for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h * 0.5 / s->mass[i];
+    for (int i = 0; i < 3 * n; i++) pos[i] += vel[i] * h;
+    if (shake) orc_shake(c, s->mass, n, dt_fs, pos, vel, last_pos);
+    all_forces(s, cp, pme, do_bonded, pos, f, e);
+    for (int st = 1; st < nsteps; st++) {
+      if (rattle) {
+        /* doKickdoDrift with a post-step modifier: half kick, RATTLE, half kick, drift */
+        for (int i = 0; i < n; i++)
+          for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h * 0.5 / s->mass[i];
+        orc_rattle(c, s->mass, dt_fs, pos, vel);
+        for (int i = 0; i < n; i++)
+          for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h * 0.5 / s->mass[i];
+      } else {
+        for (int i = 0; i < n; i++)
+          for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h / s->mass[i];
+      }
+      for (int i = 0; i < 3 * n; i++) pos[i] += vel[i] * h;
+      if (shake) orc_shake(c, s->mass, n, dt_fs, pos, vel, last_pos);
+      all_forces(s, cp, pme, do_bonded, pos, f, e);
+    }
+    for (int i = 0; i < n; i++)
+      for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h * 0.5 / s->mass[i];
+    if (rattle) orc_rattle(c, s->mass, dt_fs, pos, vel);
+  }
+  memcpy(energies_out, e, sizeof(e));
+  return 0;
+}

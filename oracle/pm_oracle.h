@@ -81,6 +81,38 @@ int orc_leapfrog(const orc_system *s, const orc_cutoff_params *cp, const orc_pme
                  int do_bonded, double dt_fs, int nsteps, double *pos, double *vel,
                  double *forces_out, double *energies_out);
 
+/* SHAKE / RATTLE bond constraints (modifier/ModifierShake.cpp, ModifierRattle.cpp): the
+ * constraint list in the reference's order (topology/TopologyUtilities.cpp:695-775).  A sweep
+ * applies every constraint in list order (Gauss-Seidel); sweeps repeat while the mean error over
+ * all constraints exceeds epsilon, at most max_iter + 1 of them.  epsilon <= 0 or max_iter <= 0
+ * switches a modifier off (ModifierModule.cpp:111, 124). */
+typedef struct {
+  int n;
+  const int *a1, *a2;
+  const double *len;
+  double shake_eps;
+  int shake_maxiter;
+  double rattle_eps;
+  int rattle_maxiter;
+} orc_constraints;
+
+/* One SHAKE application after a drift: moves pos and vel, then last_pos = pos.  Returns the
+ * number of sweeps (ModifierShake::doExecute). */
+int orc_shake(const orc_constraints *c, const double *mass, int n_atoms, double dt_fs, double *pos,
+              double *vel, double *last_pos);
+/* One RATTLE application (velocities only; ModifierRattle::doExecute).  Returns the sweeps. */
+int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const double *pos,
+               double *vel);
+
+/* LeapfrogIntegrator::run(nsteps) with SHAKE as a post-drift modifier and RATTLE as a post-step
+ * modifier (LeapfrogIntegrator.cpp:56-87,89-102; ModifierModule.cpp:106-128).  last_pos holds
+ * the SHAKE reference positions (the initial positions before the first run).  cp/pme may be
+ * NULL; with no force terms the forces are zero. */
+int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
+                             const orc_pme_params *pme, int do_bonded, const orc_constraints *c,
+                             double dt_fs, int nsteps, double *pos, double *vel, double *last_pos,
+                             double *forces_out, double *energies_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,13 @@ class IntegratorDesc(C.Structure):
                 ("gamma_ps", C.c_double), ("seed", C.c_ulonglong)]
 
 
+class ConstraintDesc(C.Structure):
+    _fields_ = [("n_constraints", C.c_int), ("atom1", C.c_void_p), ("atom2", C.c_void_p),
+                ("rest_length", C.c_void_p), ("shake", C.c_int), ("shake_epsilon", C.c_double),
+                ("shake_max_iter", C.c_int), ("rattle", C.c_int), ("rattle_epsilon", C.c_double),
+                ("rattle_max_iter", C.c_int)]
+
+
 # (name, restype, argtypes)
 _PROTOS = [
     ("pmb_last_error", C.c_char_p, []),
@@ -72,6 +79,8 @@ _PROTOS = [
     ("pmb_md_run", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_energies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_use_graph", C.c_int, [C.c_void_p, C.c_int]),
+    ("pmb_md_set_constraints", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_md_constraint_sweeps", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_kernels_per_step", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_device_bytes", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_profile", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,

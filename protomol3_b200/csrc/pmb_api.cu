@@ -1196,18 +1196,38 @@ struct pmb_md {
   cudaGraphExec_t g_first = nullptr, g_next = nullptr;
   int kernels_per_step = 0;
   std::vector<double> h_e, h_k;
-  ~pmb_md() {
+  // SHAKE after every drift, RATTLE after every step (absent: ngroup == 0)
+  ConstraintDev con{};
+  bool shake = false, rattle = false;
+  Allocs *con_a = nullptr;
+  void drop_graphs() {
     if (g_first) cudaGraphExecDestroy(g_first);
     if (g_next) cudaGraphExecDestroy(g_next);
+    g_first = g_next = nullptr;
+  }
+  ~pmb_md() {
+    drop_graphs();
+    delete con_a;
   }
 };
 
 namespace {
 
+// One step of LeapfrogIntegrator::run: kick (the opening half kick for kick = 0.5), drift, and
+// the step's forces.  With constraints, as the reference's modifier hooks place them
+// (LeapfrogIntegrator.cpp:56-87): a full kick becomes half kick, RATTLE, half kick when RATTLE
+// is on, and SHAKE follows every drift.
 int md_step_enqueue(pmb_md *m, double kick) {
   pmb_system *s = m->sys;
   SystemDev sd = s->dev();
-  integrate_kick_drift(sd, m->in, kick, s->stream);
+  if (kick == 1.0 && m->rattle) {
+    integrate_half_kick(sd, m->in, s->stream);
+    if (constraints_apply(m->con, m->in, 1, s->stream)) return fail(PMB_ERR_CUDA, "RATTLE launch");
+    integrate_kick_drift(sd, m->in, 0.5, s->stream);
+  } else {
+    integrate_kick_drift(sd, m->in, kick, s->stream);
+  }
+  if (m->shake && constraints_apply(m->con, m->in, 0, s->stream)) return fail(PMB_ERR_CUDA, "SHAKE launch");
   return enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
 }
 
@@ -1302,6 +1322,127 @@ int pmb_md_kernels_per_step(pmb_md *m, int *n) {
 }
 
 
+int pmb_md_set_constraints(pmb_md *m, const pmb_constraint_desc *d) {
+  if (!m || !d) return fail(PMB_ERR_ARG, "null argument");
+  pmb_system *s = m->sys;
+  const int nc = d->n_constraints;
+  if (nc < 0 || (nc > 0 && (!d->atom1 || !d->atom2 || !d->rest_length)))
+    return fail(PMB_ERR_ARG, "constraint arrays");
+  // ModifierModule::addModifiers: a modifier is added only with epsilon > 0 and max_iter > 0
+  const bool shake = d->shake && d->shake_epsilon > 0 && d->shake_max_iter > 0 && nc > 0;
+  const bool rattle = d->rattle && d->rattle_epsilon > 0 && d->rattle_max_iter > 0 && nc > 0;
+  if ((shake && d->shake_max_iter >= CON_MAX_SWEEPS) || (rattle && d->rattle_max_iter >= CON_MAX_SWEEPS))
+    return fail(PMB_ERR_ARG, "max_iter must be below 256");
+  if ((shake || rattle) && m->d.kind != PMB_LEAPFROG)
+    return fail(PMB_ERR_UNSUPPORTED, "constraints are supported with the leapfrog integrator");
+  for (int k = 0; k < nc; k++) {
+    const int a = d->atom1[k], b = d->atom2[k];
+    if (a < 0 || b < 0 || a >= s->natoms || b >= s->natoms || a == b)
+      return fail(PMB_ERR_ARG, "constraint atom out of range");
+    if (!(d->rest_length[k] > 0) || !std::isfinite(d->rest_length[k]))
+      return fail(PMB_ERR_ARG, "constraint rest length must be positive");
+  }
+  // groups: connected components of the constraint graph (union-find), constraints of a group in
+  // list order, atoms in order of first use
+  std::vector<int> parent(s->natoms);
+  for (int i = 0; i < s->natoms; i++) parent[i] = i;
+  auto find = [&](int x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  };
+  for (int k = 0; k < nc; k++) {
+    int ra = find(d->atom1[k]), rb = find(d->atom2[k]);
+    if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+  }
+  std::vector<int> gid(s->natoms, -1), group_of_con(nc);
+  int ng = 0;
+  for (int k = 0; k < nc; k++) {
+    int r = find(d->atom1[k]);
+    if (gid[r] < 0) gid[r] = ng++;
+    group_of_con[k] = gid[r];
+  }
+  std::vector<std::vector<int>> gcons(ng), gatoms(ng);
+  for (int k = 0; k < nc; k++) gcons[group_of_con[k]].push_back(k);
+  std::vector<int> group_con(ng + 1, 0), group_atom(ng + 1, 0), atoms;
+  std::vector<int2> local;
+  std::vector<double> len;
+  int max_atoms = 0, max_cons = 0;
+  for (int g = 0; g < ng; g++) {
+    std::vector<int> &ga = gatoms[g];
+    auto local_of = [&](int a) {
+      for (size_t i = 0; i < ga.size(); i++)
+        if (ga[i] == a) return (int)i;
+      ga.push_back(a);
+      return (int)ga.size() - 1;
+    };
+    for (int k : gcons[g]) {
+      const int la = local_of(d->atom1[k]), lb = local_of(d->atom2[k]);
+      local.push_back(make_int2(la, lb));
+      len.push_back(d->rest_length[k]);
+    }
+    if ((int)ga.size() > CON_MAX_ATOMS || (int)gcons[g].size() > CON_MAX_CONS)
+      return fail(PMB_ERR_UNSUPPORTED, "a constrained group has more than 8 atoms or 16 constraints");
+    max_atoms = std::max(max_atoms, (int)ga.size());
+    max_cons = std::max(max_cons, (int)gcons[g].size());
+    atoms.insert(atoms.end(), ga.begin(), ga.end());
+    group_con[g + 1] = group_con[g] + (int)gcons[g].size();
+    group_atom[g + 1] = (int)atoms.size();
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  m->drop_graphs();
+  delete m->con_a;
+  m->con_a = nullptr;
+  m->con = ConstraintDev{};
+  m->shake = shake;
+  m->rattle = rattle;
+  if (!shake && !rattle) return PMB_OK;
+  Allocs *a = m->con_a = new Allocs();
+  ConstraintDev &c = m->con;
+  int *d_gc = nullptr, *d_ga = nullptr, *d_atoms = nullptr;
+  int2 *d_local = nullptr;
+  double *d_len = nullptr;
+  if (upload(*a, d_gc, group_con) || upload(*a, d_ga, group_atom) || upload(*a, d_atoms, atoms) ||
+      upload(*a, d_local, local) || upload(*a, d_len, len))
+    return PMB_ERR_CUDA;
+  c.rab = a->get<double>(3 * (size_t)nc);
+  c.err = a->get<long long>(2 * (CON_MAX_SWEEPS + 1));
+  c.sweeps = a->get<int>(2);
+  if (!c.rab || !c.err || !c.sweeps) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the constraints");
+  c.ngroup = ng;
+  c.ncons = nc;
+  c.max_atoms = max_atoms;
+  c.max_cons = max_cons;
+  c.group_con = d_gc;
+  c.group_atom = d_ga;
+  c.atoms = d_atoms;
+  c.con_local = d_local;
+  c.len = d_len;
+  // a group error above this is clamped in the sums (ng * clamp * 2^40 stays below 2^62); such a
+  // sum already exceeds any epsilon below clamp / n_constraints
+  c.clamp = std::min(1e6, 4611686018427387904.0 / (CON_ERR_SCALE * std::max(ng, 1)));
+  const double TIMEFACTOR = 48.88821290839616;  // base/PMConstants.cpp:53
+  c.dt = m->d.timestep_fs / TIMEFACTOR;  // ModifierShake.cpp:22, ModifierRattle.cpp:22
+  c.shake_eps = d->shake_epsilon;
+  c.shake_max = shake ? d->shake_max_iter : 0;
+  c.rattle_eps = d->rattle_epsilon;
+  c.rattle_max = rattle ? d->rattle_max_iter : 0;
+  if (m->have_state) constraints_init(c, m->in, s->stream);
+  CK(cudaGetLastError());
+  return PMB_OK;
+}
+
+int pmb_md_constraint_sweeps(pmb_md *m, int *shake_sweeps, int *rattle_sweeps) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  int h[2] = {0, 0};
+  if (m->con.sweeps) {
+    CK(cudaMemcpyAsync(h, m->con.sweeps, sizeof(h), cudaMemcpyDeviceToHost, m->sys->stream));
+    CK(cudaStreamSynchronize(m->sys->stream));
+  }
+  if (shake_sweeps) *shake_sweeps = h[0];
+  if (rattle_sweeps) *rattle_sweeps = h[1];
+  return PMB_OK;
+}
+
 int pmb_md_set_state(pmb_md *m, const double *pos, const double *vel) {
   if (!m || !pos) return fail(PMB_ERR_ARG, "null argument");
   pmb_system *s = m->sys;
@@ -1312,6 +1453,7 @@ int pmb_md_set_state(pmb_md *m, const double *pos, const double *vel) {
   if (vel) CK(cudaMemcpyAsync(m->d_vel, vel, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
   else CK(cudaMemsetAsync(m->d_vel, 0, sizeof(double) * 3 * s->natoms, s->stream));
   CK(cudaMemsetAsync(m->d_step, 0, sizeof(long long), s->stream));
+  constraints_init(m->con, m->in, s->stream);  // the new positions are SHAKE's last ones
   SystemDev sd = s->dev();
   for (int attempt = 0; attempt < 3; attempt++) {
     zero_accumulators(sd, s->stream);
@@ -1358,6 +1500,7 @@ int pmb_md_run(pmb_md *m, int n) {
     }
   }
   integrate_half_kick(s->dev(), m->in, s->stream);
+  if (m->rattle && constraints_apply(m->con, m->in, 1, s->stream)) return fail(PMB_ERR_CUDA, "RATTLE launch");
   CK(cudaGetLastError());
   return PMB_OK;
 }
@@ -1365,7 +1508,8 @@ int pmb_md_run(pmb_md *m, int n) {
 int pmb_md_device_bytes(const pmb_md *m, unsigned long long *bytes) {
   if (!m || !bytes) return fail(PMB_ERR_ARG, "null argument");
   const pmb_system *s = m->sys;
-  size_t b = s->a.bytes + s->nba.bytes + m->a.bytes + (s->flush_buf ? (256ull << 20) : 0);
+  size_t b = s->a.bytes + s->nba.bytes + m->a.bytes + (m->con_a ? m->con_a->bytes : 0) +
+             (s->flush_buf ? (256ull << 20) : 0);
   for (const pmb_force *f : m->forces) b += f->a.bytes;
   *bytes = (unsigned long long)b;
   return PMB_OK;

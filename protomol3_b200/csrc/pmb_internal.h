@@ -174,6 +174,30 @@ struct IntegratorDev {
   double *pos, *vel;
   long long *step;     // device step counter
 };
+// SHAKE / RATTLE bond constraints, one thread per connected group of constraints (a rigid water:
+// 3 constraints on 3 atoms).  A group's constraints keep their order in the reference's list.
+constexpr int CON_MAX_ATOMS = 8;    // atoms of one group
+constexpr int CON_MAX_CONS = 16;    // constraints of one group
+constexpr double CON_ERR_SCALE = 1099511627776.0;  // 2^40: fixed point of the per-sweep error sums
+struct ConstraintDev {
+  int ngroup, ncons;
+  int max_atoms, max_cons;  // largest group (selects the kernel: rigid waters have 3 and 3)
+  const int *group_con;    // [ngroup + 1] constraint offsets of each group
+  const int *group_atom;   // [ngroup + 1] offsets into atoms
+  const int *atoms;        // group atoms (global indices), each group's first-use order
+  const int2 *con_local;   // [ncons] the two atoms of a constraint as indices into its group
+  const double *len;       // [ncons] rest lengths
+  double *rab;             // [3 ncons] SHAKE reference vectors x[a1] - x[a2] of the last SHAKE
+  long long *err;          // [2][CON_MAX_SWEEPS + 1] per-sweep error sums (SHAKE, RATTLE)
+  int *sweeps;             // [2] sweeps of the last SHAKE and RATTLE
+  double clamp;            // largest group error added to a sum (keeps the int64 sums in range)
+  double dt;               // timestep / TIMEFACTOR, as the modifiers use it
+  double shake_eps, rattle_eps;
+  int shake_max, rattle_max;
+};
+constexpr int CON_MAX_SWEEPS = 256;  // max_iter + 1 bound
+int constraints_init(const ConstraintDev &c, const IntegratorDev &in, cudaStream_t st);
+int constraints_apply(const ConstraintDev &c, const IntegratorDev &in, int rattle, cudaStream_t st);
 int integrate_kick_drift(const SystemDev &s, const IntegratorDev &in, double kick, cudaStream_t st);
 int integrate_half_kick(const SystemDev &s, const IntegratorDev &in, cudaStream_t st);
 int kinetic_energy(const SystemDev &s, const IntegratorDev &in, double *out_per_box, cudaStream_t st);

@@ -151,7 +151,7 @@ __global__ void k_kick_drift(const SystemDev s, IntegratorDev in, double kick) {
       fa[c] = 0;
       // (F * h * 0.5) / m for the half kick, (F * h) / m for the full kick, as the reference
       v[c] += kick == 1.0 ? f * h / m : f * h * 0.5 / m;
-      x[c] += v[c] * h;
+      x[c] = __dadd_rn(x[c], __dmul_rn(v[c], h));  // rounded like the reference's x += v * h
     }
   } else {
     // Langevin (StandardIntegrator::run, StandardIntegrator.cpp:27-37): per step a noisy half
@@ -172,7 +172,7 @@ __global__ void k_kick_drift(const SystemDev s, IntegratorDev in, double kick) {
       fa[c] = 0;
       if (kick == 1.0) v[c] = v[c] * vdt + f * fdt / m + rb[c] * sq * ndt;
       v[c] = v[c] * vdt + f * fdt / m + ra[c] * sq * ndt;
-      x[c] += v[c] * h;
+      x[c] = __dadd_rn(x[c], __dmul_rn(v[c], h));
     }
   }
 }
@@ -233,6 +233,296 @@ __global__ void k_fma_probe(float *out, int iters, float a, float b) {
 #pragma unroll
   for (int c = 0; c < 8; c++) r += x[c];
   if (r == 1234.5f) out[0] = r;
+}
+
+// ------------------------------------------------------------------ SHAKE / RATTLE
+// ModifierShake::doExecute (modifier/ModifierShake.cpp:17-75), ModifierRattle::doExecute
+// (modifier/ModifierRattle.cpp:17-64) and their error estimates (ModifierMetaShake.cpp:12-33,
+// ModifierMetaRattle.cpp:12-31).  The reference sweeps its whole constraint list in order and
+// repeats while the mean error over all constraints exceeds epsilon (at most max_iter + 1
+// sweeps).  Constraints of different groups share no atom, so a sweep of the list is a sweep of
+// every group in list order, and the number of sweeps is the same for all groups.  One thread
+// per group, two passes: the first sweeps its group max_iter times without writing anything back
+// and adds the group's error before each sweep to that sweep's sum (integer atomics, so the sums
+// and the count do not depend on the order of the additions); the second reads the count off
+// the sums and replays exactly that many sweeps from the same state, with the same arithmetic,
+// then writes positions, velocities and (SHAKE) the reference vectors for the next application.
+// Every operation is rounded as the reference's C++ rounds it (no fused multiply-adds).  The
+// virial term of the modifiers is not accumulated.
+template <int MA, int MC>
+struct ConGroup {
+  int nc;
+  double x[MA][3], v[MA][3], rm[MA];
+  int2 ij[MC];
+  double len[MC], rab[MC][3];
+};
+
+// register-resident access to a small array by a run-time index
+template <int MA>
+__device__ __forceinline__ void pick3(const double (&a)[MA][3], int i, double o[3]) {
+  o[0] = a[0][0]; o[1] = a[0][1]; o[2] = a[0][2];
+#pragma unroll
+  for (int k = 1; k < MA; k++)
+    if (i == k) { o[0] = a[k][0]; o[1] = a[k][1]; o[2] = a[k][2]; }
+}
+template <int MA>
+__device__ __forceinline__ double pick1(const double (&a)[MA], int i) {
+  double o = a[0];
+#pragma unroll
+  for (int k = 1; k < MA; k++)
+    if (i == k) o = a[k];
+  return o;
+}
+template <int MA>
+__device__ __forceinline__ void put3(double (&a)[MA][3], int i, const double o[3]) {
+#pragma unroll
+  for (int k = 0; k < MA; k++)
+    if (i == k) { a[k][0] = o[0]; a[k][1] = o[1]; a[k][2] = o[2]; }
+}
+__device__ __forceinline__ double dot3_rn(const double *a, const double *b) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1])), __dmul_rn(a[2], b[2]));
+}
+
+template <int MA, int MC>
+__device__ void con_load(const ConstraintDev &c, const IntegratorDev &in, int gi, bool shake,
+                         ConGroup<MA, MC> &g) {
+  const int c0 = c.group_con[gi], a0 = c.group_atom[gi];
+  const int na = c.group_atom[gi + 1] - a0;
+  g.nc = c.group_con[gi + 1] - c0;
+#pragma unroll
+  for (int i = 0; i < MA; i++) {
+    if (i < na) {
+      const int a = c.atoms[a0 + i];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        g.x[i][q] = in.pos[3 * (long long)a + q];
+        g.v[i][q] = in.vel[3 * (long long)a + q];
+      }
+      g.rm[i] = 1.0 / in.mass[a];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 3; q++) g.x[i][q] = g.v[i][q] = 0.0;
+      g.rm[i] = 0.0;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < MC; k++) {
+    if (k < g.nc) {
+      g.ij[k] = c.con_local[c0 + k];
+      g.len[k] = c.len[c0 + k];
+#pragma unroll
+      for (int q = 0; q < 3; q++) g.rab[k][q] = shake ? c.rab[3 * (long long)(c0 + k) + q] : 0.0;
+    } else {
+      g.ij[k] = make_int2(0, 0);
+      g.len[k] = 1.0;
+#pragma unroll
+      for (int q = 0; q < 3; q++) g.rab[k][q] = 0.0;
+    }
+  }
+}
+
+// sum over the group's constraints of |d^2 - l^2| / (2 l^2), d = x[a2] - x[a1]
+template <int MA, int MC>
+__device__ double shake_group_error(const ConGroup<MA, MC> &g) {
+  double e = 0.0;
+#pragma unroll
+  for (int k = 0; k < MC; k++) {
+    if (k < g.nc) {
+      double p1[3], p2[3], d[3];
+      pick3(g.x, g.ij[k].x, p1);
+      pick3(g.x, g.ij[k].y, p2);
+#pragma unroll
+      for (int q = 0; q < 3; q++) d[q] = __dsub_rn(p2[q], p1[q]);
+      const double l2 = __dmul_rn(g.len[k], g.len[k]);
+      e = __dadd_rn(e, __ddiv_rn(fabs(__dsub_rn(dot3_rn(d, d), l2)), __dmul_rn(2.0, l2)));
+    }
+  }
+  return e;
+}
+
+// sum over the group's constraints of |(x1 - x2).(v1 - v2)|
+template <int MA, int MC>
+__device__ double rattle_group_error(const ConGroup<MA, MC> &g) {
+  double e = 0.0;
+#pragma unroll
+  for (int k = 0; k < MC; k++) {
+    if (k < g.nc) {
+      double p1[3], p2[3], v1[3], v2[3], r[3], w[3];
+      pick3(g.x, g.ij[k].x, p1);
+      pick3(g.x, g.ij[k].y, p2);
+      pick3(g.v, g.ij[k].x, v1);
+      pick3(g.v, g.ij[k].y, v2);
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        w[q] = __dsub_rn(v1[q], v2[q]);
+        r[q] = __dsub_rn(p1[q], p2[q]);
+      }
+      e = __dadd_rn(e, fabs(dot3_rn(r, w)));
+    }
+  }
+  return e;
+}
+
+template <int MA, int MC>
+__device__ void shake_sweep(ConGroup<MA, MC> &g, double dt) {
+#pragma unroll
+  for (int k = 0; k < MC; k++) {
+    if (k < g.nc) {
+      const int a1 = g.ij[k].x, a2 = g.ij[k].y;
+      double p1[3], p2[3], v1[3], v2[3], pab[3];
+      pick3(g.x, a1, p1);
+      pick3(g.x, a2, p2);
+      pick3(g.v, a1, v1);
+      pick3(g.v, a2, v2);
+#pragma unroll
+      for (int q = 0; q < 3; q++) pab[q] = __dsub_rn(p1[q], p2[q]);
+      const double pabsq = dot3_rn(pab, pab);
+      const double rabsq = __dmul_rn(g.len[k], g.len[k]);
+      const double diffsq = __dsub_rn(rabsq, pabsq);
+      const double rpab = dot3_rn(g.rab[k], pab);
+      const double rM1 = pick1(g.rm, a1), rM2 = pick1(g.rm, a2);
+      const double gab = __ddiv_rn(diffsq, __dmul_rn(__dmul_rn(2.0, __dadd_rn(rM1, rM2)), rpab));
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        double dp = __dmul_rn(g.rab[k][q], gab);
+        p1[q] = __dadd_rn(p1[q], __dmul_rn(dp, rM1));
+        p2[q] = __dsub_rn(p2[q], __dmul_rn(dp, rM2));
+        dp = __ddiv_rn(dp, dt);
+        v1[q] = __dadd_rn(v1[q], __dmul_rn(dp, rM1));
+        v2[q] = __dsub_rn(v2[q], __dmul_rn(dp, rM2));
+      }
+      put3(g.x, a1, p1);
+      put3(g.x, a2, p2);
+      put3(g.v, a1, v1);
+      put3(g.v, a2, v2);
+    }
+  }
+}
+
+template <int MA, int MC>
+__device__ void rattle_sweep(ConGroup<MA, MC> &g, double dt) {
+#pragma unroll
+  for (int k = 0; k < MC; k++) {
+    if (k < g.nc) {
+      const int a1 = g.ij[k].x, a2 = g.ij[k].y;
+      double p1[3], p2[3], v1[3], v2[3], rab[3], vab[3];
+      pick3(g.x, a1, p1);
+      pick3(g.x, a2, p2);
+      pick3(g.v, a1, v1);
+      pick3(g.v, a2, v2);
+      const double rM1 = pick1(g.rm, a1), rM2 = pick1(g.rm, a2);
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        rab[q] = __dsub_rn(p1[q], p2[q]);
+        vab[q] = __dsub_rn(v1[q], v2[q]);
+      }
+      const double rabsq = dot3_rn(rab, rab);
+      const double rvab = dot3_rn(rab, vab);
+      const double gab = __ddiv_rn(-rvab, __dmul_rn(__dmul_rn(dt, __dadd_rn(rM1, rM2)), rabsq));
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const double dp = __dmul_rn(rab[q], gab);
+        v1[q] = __dadd_rn(v1[q], __dmul_rn(__dmul_rn(dp, dt), rM1));
+        v2[q] = __dsub_rn(v2[q], __dmul_rn(__dmul_rn(dp, dt), rM2));
+      }
+      put3(g.v, a1, v1);
+      put3(g.v, a2, v2);
+    }
+  }
+}
+
+constexpr int CON_THREADS = 128;
+
+// SHAKE reference vectors from the current positions (ModifierMetaRattleShake::doInitialize
+// takes the positions at initialisation as the last ones)
+template <int MA, int MC>
+__global__ void k_constraint_init(ConstraintDev c, IntegratorDev in) {
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= c.ngroup) return;
+  ConGroup<MA, MC> g;
+  con_load<MA, MC>(c, in, gi, false, g);
+  const int c0 = c.group_con[gi];
+#pragma unroll
+  for (int k = 0; k < MC; k++) {
+    if (k < g.nc) {
+      double p1[3], p2[3];
+      pick3(g.x, g.ij[k].x, p1);
+      pick3(g.x, g.ij[k].y, p2);
+#pragma unroll
+      for (int q = 0; q < 3; q++) c.rab[3 * (long long)(c0 + k) + q] = __dsub_rn(p1[q], p2[q]);
+    }
+  }
+}
+
+template <int MA, int MC, bool RATTLE, bool APPLY>
+__global__ void __launch_bounds__(CON_THREADS) k_constrain(ConstraintDev c, IntegratorDev in) {
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = gi < c.ngroup;
+  ConGroup<MA, MC> g;
+  if (valid) {
+    con_load<MA, MC>(c, in, gi, !RATTLE, g);
+  } else {
+    g.nc = 0;
+#pragma unroll
+    for (int i = 0; i < MA; i++) {
+#pragma unroll
+      for (int q = 0; q < 3; q++) g.x[i][q] = g.v[i][q] = 0.0;
+      g.rm[i] = 0.0;
+    }
+  }
+  const int maxit = RATTLE ? c.rattle_max : c.shake_max;
+  long long *E = c.err + (RATTLE ? CON_MAX_SWEEPS + 1 : 0);
+  if constexpr (!APPLY) {
+    // error before sweep k (k = 0 .. max_iter) into sum k; the warp's sum goes in one atomic
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k <= maxit; k++) {
+      if (k > 0) {
+        if constexpr (RATTLE) rattle_sweep(g, c.dt);
+        else shake_sweep(g, c.dt);
+      }
+      const double e = RATTLE ? rattle_group_error(g) : shake_group_error(g);
+      long long qv = __double2ll_rn(fmin(e, c.clamp) * CON_ERR_SCALE);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) qv += __shfl_xor_sync(0xffffffffu, qv, o);
+      if (lane == 0 && qv) atomicAdd(reinterpret_cast<unsigned long long *>(E + k), (unsigned long long)qv);
+    }
+  } else {
+    // the reference's loop: sweep while the mean error exceeds epsilon, at most max_iter + 1
+    const double eps = RATTLE ? c.rattle_eps : c.shake_eps;
+    int K = 0;
+    while (K <= maxit && (double)E[K] / CON_ERR_SCALE / c.ncons > eps) K++;
+    if (!valid) return;
+    for (int k = 0; k < K; k++) {
+      if constexpr (RATTLE) rattle_sweep(g, c.dt);
+      else shake_sweep(g, c.dt);
+    }
+    const int a0 = c.group_atom[gi], na = c.group_atom[gi + 1] - a0;
+#pragma unroll
+    for (int i = 0; i < MA; i++) {
+      if (i < na) {
+        const long long a = c.atoms[a0 + i];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          if constexpr (!RATTLE) in.pos[3 * a + q] = g.x[i][q];
+          in.vel[3 * a + q] = g.v[i][q];
+        }
+      }
+    }
+    if constexpr (!RATTLE) {
+      const int c0 = c.group_con[gi];
+#pragma unroll
+      for (int k = 0; k < MC; k++) {
+        if (k < g.nc) {
+          double p1[3], p2[3];
+          pick3(g.x, g.ij[k].x, p1);
+          pick3(g.x, g.ij[k].y, p2);
+#pragma unroll
+          for (int q = 0; q < 3; q++) c.rab[3 * (long long)(c0 + k) + q] = __dsub_rn(p1[q], p2[q]);
+        }
+      }
+    }
+    if (gi == 0) c.sweeps[RATTLE ? 1 : 0] = K;
+  }
 }
 
 }  // namespace
@@ -309,6 +599,41 @@ int integrate_half_kick(const SystemDev &s, const IntegratorDev &in, cudaStream_
 
 int kinetic_energy(const SystemDev &s, const IntegratorDev &in, double *out, cudaStream_t st) {
   k_kinetic<<<s.nbox, 256, 0, st>>>(s, in, out);
+  return 0;
+}
+
+template <int MA, int MC>
+static void constraints_apply_t(const ConstraintDev &c, const IntegratorDev &in, int rattle, cudaStream_t st) {
+  const int blocks = (c.ngroup + CON_THREADS - 1) / CON_THREADS;
+  if (rattle) {
+    k_constrain<MA, MC, true, false><<<blocks, CON_THREADS, 0, st>>>(c, in);
+    k_constrain<MA, MC, true, true><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  } else {
+    k_constrain<MA, MC, false, false><<<blocks, CON_THREADS, 0, st>>>(c, in);
+    k_constrain<MA, MC, false, true><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  }
+}
+
+int constraints_init(const ConstraintDev &c, const IntegratorDev &in, cudaStream_t st) {
+  if (c.ngroup <= 0) return 0;
+  const int blocks = (c.ngroup + CON_THREADS - 1) / CON_THREADS;
+  if (c.max_atoms <= 3 && c.max_cons <= 3)
+    k_constraint_init<3, 3><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  else
+    k_constraint_init<CON_MAX_ATOMS, CON_MAX_CONS><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  return 0;
+}
+
+// One SHAKE (rattle = 0) or RATTLE (rattle = 1) application: clear the per-sweep sums, then the
+// two passes.
+int constraints_apply(const ConstraintDev &c, const IntegratorDev &in, int rattle, cudaStream_t st) {
+  if (c.ngroup <= 0) return 0;
+  const int maxit = rattle ? c.rattle_max : c.shake_max;
+  cudaError_t e = cudaMemsetAsync(c.err + (rattle ? CON_MAX_SWEEPS + 1 : 0), 0,
+                                  sizeof(long long) * (maxit + 1), st);
+  if (e != cudaSuccess) return 1;
+  if (c.max_atoms <= 3 && c.max_cons <= 3) constraints_apply_t<3, 3>(c, in, rattle, st);
+  else constraints_apply_t<CON_MAX_ATOMS, CON_MAX_CONS>(c, in, rattle, st);
   return 0;
 }
 

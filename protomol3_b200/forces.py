@@ -361,6 +361,28 @@ class Integrator:
                                                       len(self.forces), C.byref(d)))
         L.check(L.lib().pmb_md_use_graph(self._h, int(use_graph)))
 
+    def set_constraints(self, constraints, shake=True, shake_epsilon=1e-5, shake_max_iter=30,
+                        rattle=True, rattle_epsilon=1e-5, rattle_max_iter=30):
+        """SHAKE after every drift and RATTLE after every step (``shake``/``rattle`` and their
+        ``-epsilon``/``-maxIter`` options of module/ModifierModule.cpp:41-48,106-128) on
+        ``constraints`` = (atom1, atom2, rest_length) arrays in the reference's list order, e.g.
+        from ``constraints.rattle_shake_constraints``."""
+        a1, a2, ln = constraints
+        self._con = (np.ascontiguousarray(a1, np.int32), np.ascontiguousarray(a2, np.int32),
+                     np.ascontiguousarray(ln, np.float64))
+        d = L.ConstraintDesc()
+        d.n_constraints = len(self._con[0])
+        d.atom1, d.atom2, d.rest_length = (_p(a) for a in self._con)
+        d.shake, d.shake_epsilon, d.shake_max_iter = int(shake), shake_epsilon, int(shake_max_iter)
+        d.rattle, d.rattle_epsilon, d.rattle_max_iter = int(rattle), rattle_epsilon, int(rattle_max_iter)
+        L.check(L.lib().pmb_md_set_constraints(self._h, C.byref(d)))
+
+    def constraint_sweeps(self):
+        """(SHAKE, RATTLE) sweeps of the last application; max_iter + 1 means not converged."""
+        a, b = C.c_int(0), C.c_int(0)
+        L.check(L.lib().pmb_md_constraint_sweeps(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def set_state(self, positions, velocities=None):
         pos = np.ascontiguousarray(positions, np.float64)
         vel = None if velocities is None else np.ascontiguousarray(velocities, np.float64)

@@ -97,7 +97,7 @@ def water_box(n_waters, seed=1234, temperature=300.0, edge=None):
         angles=np.stack([h1, o, h2], 1).astype(np.int32),
         angle_k=np.full(n_waters, 55.0), angle_theta0=np.full(n_waters, np.deg2rad(THETA_HOH)),
         ub_k=np.zeros(n_waters), ub_r0=np.zeros(n_waters), coulomb_scaling=1.0,
-        seed=seed)
+        elem="OHH" * n_waters, seed=seed)
 
 
 def fft_friendly(n):

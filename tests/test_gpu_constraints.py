@@ -1,0 +1,109 @@
+"""SHAKE / RATTLE on the device (two-pass group kernels of pmb_md.cu) against the reference's
+own integrator and modifiers (golden fixture) and the oracle's restatement.
+
+With no force terms every operation is the reference's, in its order, so the device state must
+equal the reference's bit for bit; with forces, the fixed-point force accumulation separates
+the trajectories by rounding only (tolerance 1e-9 A on positions after 10 steps)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from protomol3_b200 import _lib as L
+from protomol3_b200 import constraints as CS
+from protomol3_b200 import forces as F
+from protomol3_b200 import waterbox as W
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "water64_rigid_ref.npz")
+
+
+def _opt(a):
+    return None if a[1] == 0 else (float(a[0]), int(a[1]))
+
+
+def _device_run(box, cons, dt, steps, shake, rattle, precision="fp64", forces=(), chunks=None,
+                use_graph=True):
+    topo = F.Topology(box, precision)
+    md = F.Integrator(topo, list(forces), timestep=dt, use_graph=use_graph)
+    md.set_constraints(cons, shake=shake is not None, shake_epsilon=(shake or (0, 0))[0],
+                       shake_max_iter=(shake or (0, 0))[1], rattle=rattle is not None,
+                       rattle_epsilon=(rattle or (0, 0))[0], rattle_max_iter=(rattle or (0, 0))[1])
+    md.set_state(box["pos"], box["vel"])
+    for n in (chunks or [steps]):
+        md.run(n)
+    pos, vel = md.state()
+    sweeps = md.constraint_sweeps()
+    md.close()
+    topo.close()
+    return pos, vel, sweeps
+
+
+@pytest.mark.parametrize("case", ["sr", "s", "r", "tight"])
+def test_device_equals_reference_golden(case):
+    g = np.load(GOLD)
+    box = W.water_box(64, seed=7)
+    cons = CS.rattle_shake_constraints(box)
+    pos, vel, _ = _device_run(box, cons, float(g["dt"]), int(g[case + "_steps"]),
+                              _opt(g[case + "_shake"]), _opt(g[case + "_rattle"]))
+    assert np.array_equal(pos, g[case + "_pos"])
+    assert np.array_equal(vel, g[case + "_vel"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_equals_oracle_many_groups(precision):
+    """2,000 waters (63 warps of groups), runs split over several calls (the closing RATTLE of
+    each call, then the next call's opening half kick), with and without the CUDA graph."""
+    box = W.water_box(2000, seed=21)
+    cons = CS.rattle_shake_constraints(box)
+    ref_pos, ref_vel, _, _ = O.leapfrog_constrained(O.System(box), box["pos"], box["vel"], 2.0, 4, cons)
+    ref_pos, ref_vel, _, _ = O.leapfrog_constrained(O.System(box), ref_pos, ref_vel, 2.0, 6, cons,
+                                                    last_pos=ref_pos)
+    for graph in (True, False):
+        pos, vel, sweeps = _device_run(box, cons, 2.0, 10, (1e-5, 30), (1e-5, 30), precision,
+                                       chunks=[4, 6], use_graph=graph)
+        assert np.array_equal(pos, ref_pos) and np.array_equal(vel, ref_vel)
+        assert 1 <= sweeps[0] <= 31 and 1 <= sweeps[1] <= 31
+
+
+def test_device_general_groups():
+    """Groups other than single waters take the general kernel: every tenth water is linked to
+    the next one by an extra H-O bond, which joins the two into one group of 6 atoms and 7
+    constraints.  Still the oracle's result exactly."""
+    box = dict(W.water_box(300, seed=5))
+    extra = np.array([[3 * w + 2, 3 * w + 3] for w in range(0, 290, 10)], np.int32)
+    box["bonds"] = np.concatenate([box["bonds"], extra])
+    p = box["pos"].reshape(-1, 3)
+    box["bond_r0"] = np.concatenate([box["bond_r0"], np.linalg.norm(p[extra[:, 0]] - p[extra[:, 1]], axis=1)])
+    box["bond_k"] = np.concatenate([box["bond_k"], np.zeros(len(extra))])
+    cons = CS.rattle_shake_constraints(box)
+    assert len(cons[0]) == 3 * 300 + len(extra)
+    ref_pos, ref_vel, _, _ = O.leapfrog_constrained(O.System(box), box["pos"], box["vel"], 1.0, 8, cons)
+    pos, vel, _ = _device_run(box, cons, 1.0, 8, (1e-5, 30), (1e-5, 30))
+    assert np.array_equal(pos, ref_pos) and np.array_equal(vel, ref_vel)
+
+
+def test_device_with_forces_close_to_oracle():
+    """Bonded + LJ/Coulomb C2 cutoff forces, FP64 path, 10 steps of 2 fs on 216 rigid waters."""
+    box = W.water_box(216, seed=9)
+    cons = CS.rattle_shake_constraints(box)
+    cp = O.cutoff_params(lj=("C2", 7.0, 8.0), coul=("C2", 7.0, 8.0))
+    ref_pos, ref_vel, _, _ = O.leapfrog_constrained(O.System(box), box["pos"], box["vel"], 2.0, 10, cons,
+                                                    cutoff=cp, bonded=True)
+    forces = [F.BondedSystemForce(),
+              F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0), coulomb=("C2", 7.0, 8.0))]
+    pos, vel, _ = _device_run(box, cons, 2.0, 10, (1e-5, 30), (1e-5, 30), "fp64", forces)
+    assert np.abs(pos - ref_pos).max() < 1e-9
+    assert np.abs(vel - ref_vel).max() < 1e-9
+
+
+def test_langevin_with_constraints_is_refused():
+    box = W.water_box(27, seed=1)
+    topo = F.Topology(box, "fp64")
+    md = F.Integrator(topo, [], kind="langevin")
+    with pytest.raises(RuntimeError):
+        md.set_constraints(CS.rattle_shake_constraints(box))
+    md.close()
+    topo.close()
+    assert L.lib() is not None
