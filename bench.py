@@ -475,6 +475,68 @@ def run_nve(args):
     print(json.dumps(out), flush=True)
 
 
+def run_rigid(args):
+    """Rigid water at 2 fs: the 98,304-atom box with the same force set, SHAKE after every drift
+    and RATTLE after every step (the reference's defaults: epsilon 1e-5, 30 iterations), in mixed
+    precision and on the plain FP64 path.  Steps are timed one by one with CUDA events and an L2
+    flush before each, as in the main bench."""
+    import torch
+    from protomol3_b200 import constraints as CS
+    from protomol3_b200 import forces as F
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    box = workload(0)
+    cons = CS.rattle_shake_constraints(box)
+    dt = 2.0
+    out = {"mode": "rigid", "metric": "ns/day at 98k atoms, rigid TIP3P (SHAKE + RATTLE), 2 fs leapfrog",
+           "unit": "ns/day", "timestep_fs": dt, "constraints": int(len(cons[0])), "steps": args.steps,
+           "warmup": max(3, args.warmup),
+           "config": dict(config_dict(), timestep_fs=dt, workload=config_dict()["workload"].replace(
+               "leapfrog 1 fs", "rigid waters (SHAKE + RATTLE), leapfrog 2 fs"))}
+    clocks = ClockSampler(0)
+    for prec in ("mixed", "fp64"):
+        topo = F.Topology(box, prec)
+        topo.set_stream(stream.cuda_stream)
+        fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", SWITCHON, RC)),
+              F.NonbondedPMEwaldSystemForce((GRID,) * 3, RC)]
+        md = F.Integrator(topo, fl, timestep=dt)
+        md.set_constraints(cons)
+        md.set_state(box["pos"], box["vel"])
+        for _ in range(max(3, args.warmup)):
+            flush.zero_()
+            md.run(1)
+        torch.cuda.synchronize()
+        b0 = topo.list_builds()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        if prec == "mixed":
+            clocks.start()
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            md.run(1)
+            b.record(stream)
+        torch.cuda.synchronize()
+        if prec == "mixed":
+            out["clocks"] = clocks.stop()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        sweeps = md.constraint_sweeps()
+        pos, vel = md.state()
+        p = pos.reshape(-1, 3)
+        d2 = ((p[cons[1]] - p[cons[0]]) ** 2).sum(1)
+        err = float(np.mean(np.abs(d2 - cons[2] ** 2) / (2 * cons[2] ** 2)))
+        out[prec] = {"value": 86400.0 * dt * 1e-6 / (ms * 1e-3), "ms_per_step": ms,
+                     "list_rebuilds": topo.list_builds() - b0, "last_sweeps_shake_rattle": list(sweeps),
+                     "mean_constraint_error": err, "finite": bool(np.isfinite(pos).all())}
+        md.close()
+        topo.close()
+    out["value"] = out["mixed"]["value"]
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    print(json.dumps(out), flush=True)
+
+
 def serve_leg(n_requests=24, loads=(0.5, 0.8, 0.95), budget_gb=32.0, max_active=32, chunk=200,
               seed=2024):
     """Serving: Poisson streams of Langevin MD segments (water boxes log-uniform on 500-50,000
@@ -567,11 +629,15 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--chunk", type=int, default=500, help="nve: steps between energy reads")
     ap.add_argument("--serve-requests", type=int, default=24, help="serve: requests per load level")
-    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve", "serve"], default="bench",
+    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve", "serve", "rigid"], default="bench",
                     help="profile: only --steps force evaluations (bounded case for ncu); "
                          "batch: only the 256-box ensemble leg; nve: energy drift and "
-                         "reproducibility over --steps steps; serve: latency under Poisson load")
+                         "reproducibility over --steps steps; serve: latency under Poisson load; "
+                         "rigid: SHAKE + RATTLE at 2 fs")
     args = ap.parse_args()
+    if args.mode == "rigid":
+        run_rigid(args)
+        return
     if args.mode == "serve":
         import torch
         torch.cuda.set_device(0)

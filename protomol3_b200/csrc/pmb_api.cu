@@ -1405,9 +1405,13 @@ int pmb_md_set_constraints(pmb_md *m, const pmb_constraint_desc *d) {
       upload(*a, d_local, local) || upload(*a, d_len, len))
     return PMB_ERR_CUDA;
   c.rab = a->get<double>(3 * (size_t)nc);
-  c.err = a->get<long long>(2 * (CON_MAX_SWEEPS + 1));
+  c.err = a->get<long long>(2 * (size_t)CON_ERR_BLOCK);
   c.sweeps = a->get<int>(2);
-  if (!c.rab || !c.err || !c.sweeps) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the constraints");
+  c.win = a->get<double>((size_t)CON_WINDOW * 6 * max_atoms * ng, false);
+  if (!c.rab || !c.err || !c.sweeps || !c.win) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the constraints");
+  // the first application scans every sweep up to the cap
+  const int first[2] = {shake ? d->shake_max_iter : 0, rattle ? d->rattle_max_iter : 0};
+  CK(cudaMemcpy(c.sweeps, first, sizeof(first), cudaMemcpyHostToDevice));
   c.ngroup = ng;
   c.ncons = nc;
   c.max_atoms = max_atoms;

@@ -188,14 +188,20 @@ struct ConstraintDev {
   const int2 *con_local;   // [ncons] the two atoms of a constraint as indices into its group
   const double *len;       // [ncons] rest lengths
   double *rab;             // [3 ncons] SHAKE reference vectors x[a1] - x[a2] of the last SHAKE
-  long long *err;          // [2][CON_MAX_SWEEPS + 1] per-sweep error sums (SHAKE, RATTLE)
-  int *sweeps;             // [2] sweeps of the last SHAKE and RATTLE
+  long long *err;          // [2][CON_ERR_BLOCK]: per modifier, the per-sweep error sums of the
+                           // two rounds and the hand-over words (continue flag, first-round sweeps)
+  int *sweeps;             // [2] sweeps of the last SHAKE and RATTLE (the next first round scans
+                           // up to two more)
+  double *win;             // [CON_WINDOW][6][max_atoms][ngroup] group states at the sweep counts
+                           // around the last one, written by the first scan
   double clamp;            // largest group error added to a sum (keeps the int64 sums in range)
   double dt;               // timestep / TIMEFACTOR, as the modifiers use it
   double shake_eps, rattle_eps;
   int shake_max, rattle_max;
 };
 constexpr int CON_MAX_SWEEPS = 256;  // max_iter + 1 bound
+constexpr int CON_ERR_BLOCK = 2 * (CON_MAX_SWEEPS + 1) + 2;
+constexpr int CON_WINDOW = 3;
 int constraints_init(const ConstraintDev &c, const IntegratorDev &in, cudaStream_t st);
 int constraints_apply(const ConstraintDev &c, const IntegratorDev &in, int rattle, cudaStream_t st);
 int integrate_kick_drift(const SystemDev &s, const IntegratorDev &in, double kick, cudaStream_t st);

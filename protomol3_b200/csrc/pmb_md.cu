@@ -242,11 +242,14 @@ __global__ void k_fma_probe(float *out, int iters, float a, float b) {
 // repeats while the mean error over all constraints exceeds epsilon (at most max_iter + 1
 // sweeps).  Constraints of different groups share no atom, so a sweep of the list is a sweep of
 // every group in list order, and the number of sweeps is the same for all groups.  One thread
-// per group, two passes: the first sweeps its group max_iter times without writing anything back
-// and adds the group's error before each sweep to that sweep's sum (integer atomics, so the sums
-// and the count do not depend on the order of the additions); the second reads the count off
-// the sums and replays exactly that many sweeps from the same state, with the same arithmetic,
-// then writes positions, velocities and (SHAKE) the reference vectors for the next application.
+// per group, two passes: the scan sweeps its group without writing the state back and adds the
+// group's error before each sweep to that sweep's sum (integer atomics, so the sums and the
+// count do not depend on the order of the additions); the apply reads the count off the sums and
+// takes the state after exactly that many sweeps, from the states the scan kept for the counts
+// next to the last application's, or by replaying the sweeps with the same arithmetic, then
+// writes positions, velocities and (SHAKE) the reference vectors for the next application.  The
+// scan stops two sweeps past the last count; when that is not enough a second scan and apply
+// continue from there up to the cap.
 // Every operation is rounded as the reference's C++ rounds it (no fused multiply-adds).  The
 // virial term of the modifiers is not accumulated.
 template <int MA, int MC>
@@ -254,7 +257,7 @@ struct ConGroup {
   int nc;
   double x[MA][3], v[MA][3], rm[MA];
   int2 ij[MC];
-  double len[MC], rab[MC][3];
+  double len[MC], ie[MC], rab[MC][3];  // ie = 1 / (2 l^2), for the SHAKE error estimate
 };
 
 // register-resident access to a small array by a run-time index
@@ -310,18 +313,22 @@ __device__ void con_load(const ConstraintDev &c, const IntegratorDev &in, int gi
     if (k < g.nc) {
       g.ij[k] = c.con_local[c0 + k];
       g.len[k] = c.len[c0 + k];
+      g.ie[k] = 1.0 / (2.0 * g.len[k] * g.len[k]);
 #pragma unroll
       for (int q = 0; q < 3; q++) g.rab[k][q] = shake ? c.rab[3 * (long long)(c0 + k) + q] : 0.0;
     } else {
       g.ij[k] = make_int2(0, 0);
       g.len[k] = 1.0;
+      g.ie[k] = 0.5;
 #pragma unroll
       for (int q = 0; q < 3; q++) g.rab[k][q] = 0.0;
     }
   }
 }
 
-// sum over the group's constraints of |d^2 - l^2| / (2 l^2), d = x[a2] - x[a1]
+// sum over the group's constraints of |d^2 - l^2| / (2 l^2), d = x[a2] - x[a1] (the division as a
+// product with 1 / (2 l^2): the estimate only feeds the stopping test, whose sums are rounded to
+// 2^-40 anyway)
 template <int MA, int MC>
 __device__ double shake_group_error(const ConGroup<MA, MC> &g) {
   double e = 0.0;
@@ -334,7 +341,7 @@ __device__ double shake_group_error(const ConGroup<MA, MC> &g) {
 #pragma unroll
       for (int q = 0; q < 3; q++) d[q] = __dsub_rn(p2[q], p1[q]);
       const double l2 = __dmul_rn(g.len[k], g.len[k]);
-      e = __dadd_rn(e, __ddiv_rn(fabs(__dsub_rn(dot3_rn(d, d), l2)), __dmul_rn(2.0, l2)));
+      e += fabs(dot3_rn(d, d) - l2) * g.ie[k];
     }
   }
   return e;
@@ -454,13 +461,23 @@ __global__ void k_constraint_init(ConstraintDev c, IntegratorDev in) {
   }
 }
 
-template <int MA, int MC, bool RATTLE, bool APPLY>
-__global__ void __launch_bounds__(CON_THREADS) k_constrain(ConstraintDev c, IntegratorDev in) {
-  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = gi < c.ngroup;
-  ConGroup<MA, MC> g;
+template <int MA, int MC, bool RATTLE>
+__device__ __forceinline__ void con_sweep(ConGroup<MA, MC> &g, double dt) {
+  if constexpr (RATTLE) rattle_sweep(g, dt);
+  else shake_sweep(g, dt);
+}
+
+template <int MA, int MC, bool RATTLE>
+__device__ __forceinline__ double con_error(const ConGroup<MA, MC> &g) {
+  if constexpr (RATTLE) return rattle_group_error(g);
+  else return shake_group_error(g);
+}
+
+template <int MA, int MC>
+__device__ __forceinline__ void con_load_or_zero(const ConstraintDev &c, const IntegratorDev &in, int gi,
+                                                 bool valid, bool shake, ConGroup<MA, MC> &g) {
   if (valid) {
-    con_load<MA, MC>(c, in, gi, !RATTLE, g);
+    con_load<MA, MC>(c, in, gi, shake, g);
   } else {
     g.nc = 0;
 #pragma unroll
@@ -470,58 +487,148 @@ __global__ void __launch_bounds__(CON_THREADS) k_constrain(ConstraintDev c, Inte
       g.rm[i] = 0.0;
     }
   }
+}
+
+// window slot w, component q (x, y, z, vx, vy, vz), group atom i of group gi
+__device__ __forceinline__ long long win_at(const ConstraintDev &c, int w, int q, int i, int gi) {
+  return (((long long)w * 6 + q) * c.max_atoms + i) * c.ngroup + gi;
+}
+
+// Hand-over words after the two rounds of sums in a modifier's error block
+constexpr int CON_FLAG = 2 * (CON_MAX_SWEEPS + 1), CON_K1 = CON_FLAG + 1;
+
+// First round: sweeps up to S = min(max_iter, last count + 2); states at the counts around the
+// last one go to the window.  Second round (only when the first found no sweep count that meets
+// epsilon below the cap): from the state the first apply wrote, up to the remaining budget.
+template <int MA, int MC, bool RATTLE, int ROUND>
+__global__ void __launch_bounds__(CON_THREADS) k_con_scan(ConstraintDev c, IntegratorDev in) {
+  long long *blk = c.err + (RATTLE ? CON_ERR_BLOCK : 0);
   const int maxit = RATTLE ? c.rattle_max : c.shake_max;
-  long long *E = c.err + (RATTLE ? CON_MAX_SWEEPS + 1 : 0);
-  if constexpr (!APPLY) {
-    // error before sweep k (k = 0 .. max_iter) into sum k; the warp's sum goes in one atomic
-    const int lane = threadIdx.x & 31;
-    for (int k = 0; k <= maxit; k++) {
-      if (k > 0) {
-        if constexpr (RATTLE) rattle_sweep(g, c.dt);
-        else shake_sweep(g, c.dt);
-      }
-      const double e = RATTLE ? rattle_group_error(g) : shake_group_error(g);
-      long long qv = __double2ll_rn(fmin(e, c.clamp) * CON_ERR_SCALE);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) qv += __shfl_xor_sync(0xffffffffu, qv, o);
-      if (lane == 0 && qv) atomicAdd(reinterpret_cast<unsigned long long *>(E + k), (unsigned long long)qv);
-    }
+  int S, wlo = 0;
+  if constexpr (ROUND == 1) {
+    const int prev = c.sweeps[RATTLE ? 1 : 0];
+    S = min(maxit, prev + 2);
+    wlo = max(0, prev - 1);
   } else {
-    // the reference's loop: sweep while the mean error exceeds epsilon, at most max_iter + 1
-    const double eps = RATTLE ? c.rattle_eps : c.shake_eps;
-    int K = 0;
-    while (K <= maxit && (double)E[K] / CON_ERR_SCALE / c.ncons > eps) K++;
-    if (!valid) return;
-    for (int k = 0; k < K; k++) {
-      if constexpr (RATTLE) rattle_sweep(g, c.dt);
-      else shake_sweep(g, c.dt);
+    if (!blk[CON_FLAG]) return;
+    S = maxit - (int)blk[CON_K1];
+  }
+  long long *E = blk + (ROUND == 1 ? 0 : CON_MAX_SWEEPS + 1);
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = gi < c.ngroup;
+  ConGroup<MA, MC> g;
+  con_load_or_zero<MA, MC>(c, in, gi, valid, !RATTLE, g);
+  const int na = valid ? c.group_atom[gi + 1] - c.group_atom[gi] : 0;
+  const int lane = threadIdx.x & 31;
+  for (int k = 0; k <= S; k++) {
+    if (k > 0) con_sweep<MA, MC, RATTLE>(g, c.dt);
+    if (ROUND == 1 && k > 0 && k >= wlo && k < wlo + CON_WINDOW) {
+#pragma unroll
+      for (int i = 0; i < MA; i++) {
+        if (i < na) {
+#pragma unroll
+          for (int q = 0; q < 3; q++) {
+            if constexpr (!RATTLE) c.win[win_at(c, k - wlo, q, i, gi)] = g.x[i][q];
+            c.win[win_at(c, k - wlo, 3 + q, i, gi)] = g.v[i][q];
+          }
+        }
+      }
     }
-    const int a0 = c.group_atom[gi], na = c.group_atom[gi + 1] - a0;
+    // error before sweep k + 1 into sum k; the warp's sum goes in one atomic
+    long long qv = __double2ll_rn(fmin(con_error<MA, MC, RATTLE>(g), c.clamp) * CON_ERR_SCALE);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) qv += __shfl_xor_sync(0xffffffffu, qv, o);
+    if (lane == 0 && qv) atomicAdd(reinterpret_cast<unsigned long long *>(E + k), (unsigned long long)qv);
+  }
+}
+
+// The reference's loop: sweep while the mean error exceeds epsilon, at most max_iter + 1 sweeps.
+// The first apply takes the count off the first round's sums; when none of them meets epsilon
+// below the cap it applies S sweeps and hands over to the second round.
+template <int MA, int MC, bool RATTLE, int ROUND>
+__global__ void __launch_bounds__(CON_THREADS) k_con_apply(ConstraintDev c, IntegratorDev in) {
+  long long *blk = c.err + (RATTLE ? CON_ERR_BLOCK : 0);
+  const int maxit = RATTLE ? c.rattle_max : c.shake_max;
+  const double eps = RATTLE ? c.rattle_eps : c.shake_eps;
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = gi < c.ngroup;
+  int K, wlo = 0, S;
+  bool from_window = false, handover = false;
+  if constexpr (ROUND == 1) {
+    const int prev = c.sweeps[RATTLE ? 1 : 0];
+    S = min(maxit, prev + 2);
+    wlo = max(0, prev - 1);
+    K = 0;
+    while (K <= S && (double)blk[K] / CON_ERR_SCALE / c.ncons > eps) K++;
+    int cont = 0;
+    if (K > S) {
+      if (S == maxit) K = maxit + 1;
+      else {
+        K = S;
+        cont = 1;
+      }
+    }
+    if (gi == 0) {
+      blk[CON_FLAG] = cont;
+      blk[CON_K1] = K;
+    }
+    handover = cont != 0;
+    from_window = K > 0 && K <= S && K >= wlo && K < wlo + CON_WINDOW;
+  } else {
+    if (!blk[CON_FLAG]) {
+      if (gi == 0) c.sweeps[RATTLE ? 1 : 0] = (int)blk[CON_K1];
+      return;
+    }
+    const int s1 = (int)blk[CON_K1];
+    S = maxit - s1;
+    const long long *E = blk + CON_MAX_SWEEPS + 1;
+    K = 0;
+    while (K <= S && (double)E[K] / CON_ERR_SCALE / c.ncons > eps) K++;
+    if (gi == 0) c.sweeps[RATTLE ? 1 : 0] = s1 + K;
+  }
+  if (!valid) return;
+  ConGroup<MA, MC> g;
+  con_load<MA, MC>(c, in, gi, !RATTLE, g);
+  const int a0 = c.group_atom[gi], na = c.group_atom[gi + 1] - a0;
+  if (from_window) {
 #pragma unroll
     for (int i = 0; i < MA; i++) {
       if (i < na) {
-        const long long a = c.atoms[a0 + i];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-          if constexpr (!RATTLE) in.pos[3 * a + q] = g.x[i][q];
-          in.vel[3 * a + q] = g.v[i][q];
+          if constexpr (!RATTLE) g.x[i][q] = c.win[win_at(c, K - wlo, q, i, gi)];
+          g.v[i][q] = c.win[win_at(c, K - wlo, 3 + q, i, gi)];
         }
       }
     }
-    if constexpr (!RATTLE) {
-      const int c0 = c.group_con[gi];
+  } else {
+    for (int k = 0; k < K; k++) con_sweep<MA, MC, RATTLE>(g, c.dt);
+  }
 #pragma unroll
-      for (int k = 0; k < MC; k++) {
-        if (k < g.nc) {
-          double p1[3], p2[3];
-          pick3(g.x, g.ij[k].x, p1);
-          pick3(g.x, g.ij[k].y, p2);
+  for (int i = 0; i < MA; i++) {
+    if (i < na) {
+      const long long a = c.atoms[a0 + i];
 #pragma unroll
-          for (int q = 0; q < 3; q++) c.rab[3 * (long long)(c0 + k) + q] = __dsub_rn(p1[q], p2[q]);
-        }
+      for (int q = 0; q < 3; q++) {
+        if constexpr (!RATTLE) in.pos[3 * a + q] = g.x[i][q];
+        in.vel[3 * a + q] = g.v[i][q];
       }
     }
-    if (gi == 0) c.sweeps[RATTLE ? 1 : 0] = K;
+  }
+  // the next SHAKE's reference vectors; not yet when the second round still sweeps against the
+  // current ones
+  if (!RATTLE && !handover) {
+    const int c0 = c.group_con[gi];
+#pragma unroll
+    for (int k = 0; k < MC; k++) {
+      if (k < g.nc) {
+        double p1[3], p2[3];
+        pick3(g.x, g.ij[k].x, p1);
+        pick3(g.x, g.ij[k].y, p2);
+#pragma unroll
+        for (int q = 0; q < 3; q++) c.rab[3 * (long long)(c0 + k) + q] = __dsub_rn(p1[q], p2[q]);
+      }
+    }
   }
 }
 
@@ -602,16 +709,13 @@ int kinetic_energy(const SystemDev &s, const IntegratorDev &in, double *out, cud
   return 0;
 }
 
-template <int MA, int MC>
-static void constraints_apply_t(const ConstraintDev &c, const IntegratorDev &in, int rattle, cudaStream_t st) {
+template <int MA, int MC, bool RATTLE>
+static void constraints_apply_t(const ConstraintDev &c, const IntegratorDev &in, cudaStream_t st) {
   const int blocks = (c.ngroup + CON_THREADS - 1) / CON_THREADS;
-  if (rattle) {
-    k_constrain<MA, MC, true, false><<<blocks, CON_THREADS, 0, st>>>(c, in);
-    k_constrain<MA, MC, true, true><<<blocks, CON_THREADS, 0, st>>>(c, in);
-  } else {
-    k_constrain<MA, MC, false, false><<<blocks, CON_THREADS, 0, st>>>(c, in);
-    k_constrain<MA, MC, false, true><<<blocks, CON_THREADS, 0, st>>>(c, in);
-  }
+  k_con_scan<MA, MC, RATTLE, 1><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  k_con_apply<MA, MC, RATTLE, 1><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  k_con_scan<MA, MC, RATTLE, 2><<<blocks, CON_THREADS, 0, st>>>(c, in);
+  k_con_apply<MA, MC, RATTLE, 2><<<blocks, CON_THREADS, 0, st>>>(c, in);
 }
 
 int constraints_init(const ConstraintDev &c, const IntegratorDev &in, cudaStream_t st) {
@@ -624,16 +728,21 @@ int constraints_init(const ConstraintDev &c, const IntegratorDev &in, cudaStream
   return 0;
 }
 
-// One SHAKE (rattle = 0) or RATTLE (rattle = 1) application: clear the per-sweep sums, then the
-// two passes.
+// One SHAKE (rattle = 0) or RATTLE (rattle = 1) application: clear the modifier's sums and
+// hand-over words, then scan and apply, twice (the second round returns at once unless the first
+// stopped short of both epsilon and the cap).
 int constraints_apply(const ConstraintDev &c, const IntegratorDev &in, int rattle, cudaStream_t st) {
   if (c.ngroup <= 0) return 0;
-  const int maxit = rattle ? c.rattle_max : c.shake_max;
-  cudaError_t e = cudaMemsetAsync(c.err + (rattle ? CON_MAX_SWEEPS + 1 : 0), 0,
-                                  sizeof(long long) * (maxit + 1), st);
+  cudaError_t e = cudaMemsetAsync(c.err + (rattle ? CON_ERR_BLOCK : 0), 0, sizeof(long long) * CON_ERR_BLOCK, st);
   if (e != cudaSuccess) return 1;
-  if (c.max_atoms <= 3 && c.max_cons <= 3) constraints_apply_t<3, 3>(c, in, rattle, st);
-  else constraints_apply_t<CON_MAX_ATOMS, CON_MAX_CONS>(c, in, rattle, st);
+  const bool water = c.max_atoms <= 3 && c.max_cons <= 3;
+  if (rattle) {
+    if (water) constraints_apply_t<3, 3, true>(c, in, st);
+    else constraints_apply_t<CON_MAX_ATOMS, CON_MAX_CONS, true>(c, in, st);
+  } else {
+    if (water) constraints_apply_t<3, 3, false>(c, in, st);
+    else constraints_apply_t<CON_MAX_ATOMS, CON_MAX_CONS, false>(c, in, st);
+  }
   return 0;
 }
 

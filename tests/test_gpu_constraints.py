@@ -67,6 +67,32 @@ def test_device_equals_oracle_many_groups(precision):
         assert 1 <= sweeps[0] <= 31 and 1 <= sweeps[1] <= 31
 
 
+def test_device_second_round_when_the_sweep_count_jumps():
+    """The first scan of an application covers up to two sweeps more than the last one took;
+    velocities scaled up between two runs make the next applications need more, which the
+    second round supplies.  Still the oracle's result exactly."""
+    box = W.water_box(500, seed=33)
+    cons = CS.rattle_shake_constraints(box)
+    topo = F.Topology(box, "fp64")
+    md = F.Integrator(topo, [], timestep=2.0)
+    md.set_constraints(cons)
+    md.set_state(box["pos"], box["vel"])
+    md.run(3)
+    p1, v1 = md.state()
+    k1 = md.constraint_sweeps()
+    md.set_state(p1, 6.0 * v1)
+    md.run(3)
+    p2, v2 = md.state()
+    k2 = md.constraint_sweeps()
+    md.close()
+    topo.close()
+    r1, w1, _, _ = O.leapfrog_constrained(O.System(box), box["pos"], box["vel"], 2.0, 3, cons)
+    r2, w2, _, _ = O.leapfrog_constrained(O.System(box), r1, 6.0 * w1, 2.0, 3, cons, last_pos=r1)
+    assert np.array_equal(p1, r1) and np.array_equal(v1, w1)
+    assert np.array_equal(p2, r2) and np.array_equal(v2, w2)
+    assert k2[0] > k1[0] + 2 or k2[1] > k1[1] + 2, (k1, k2)
+
+
 def test_device_general_groups():
     """Groups other than single waters take the general kernel: every tenth water is linked to
     the next one by an extra H-O bond, which joins the two into one group of 6 atoms and 7
