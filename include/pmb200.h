@@ -186,6 +186,32 @@ typedef struct {
 int pmb_md_set_constraints(pmb_md *md, const pmb_constraint_desc *desc);
 /* Sweeps of the last SHAKE and RATTLE application (max_iter + 1: not converged). */
 int pmb_md_constraint_sweeps(pmb_md *md, int *shake_sweeps, int *rattle_sweeps);
+
+/* Trajectory output -------------------------------------------------------------------------- */
+typedef struct pmb_traj pmb_traj;
+/* A DCD trajectory in the format of DCDTrajectoryWriter (io/DCDTrajectoryWriter.cpp:75-233), as
+ * OutputDCDTrajectory opens it (output/OutputDCDTrajectory.cpp:27-43; the reference passes
+ * timestep 1.0): header written with the first frame, frame count updated with every frame,
+ * float32 coordinates.  little_endian selects the byte order of the file.  The first title line
+ * names the file and this library's build, like the reference's. */
+pmb_traj *pmb_traj_open_dcd(const char *path, int n_atoms, double timestep, int first_step, int little_endian,
+                            const char *comment);
+/* An XYZ file in the format of XYZWriter::write (io/XYZWriter.cpp:28-53); every frame rewrites
+ * it (final positions, as OutputFinalXYZPos).  names: one string per atom. */
+pmb_traj *pmb_traj_open_xyz(const char *path, int n_atoms, const char *const *names);
+/* A frame from host positions [3 n_atoms]; written before the call returns. */
+int pmb_traj_write_host(pmb_traj *t, const double *positions);
+/* A frame of the MD run's current positions, taken without stopping the device: an asynchronous
+ * copy into one of three pinned staging buffers on the system's stream and a writer thread that
+ * appends the frame once the copy has landed (OutputDCDTrajectory::doRun without the
+ * synchronisation).  Waits only when all three buffers are in flight.  Not during a stream
+ * capture. */
+int pmb_md_write_frame(pmb_md *md, pmb_traj *t);
+/* Waits until every frame handed over is in the file; the first write error, if any. */
+int pmb_traj_flush(pmb_traj *t);
+int pmb_traj_frames(pmb_traj *t, long long *frames);
+/* Flushes, closes the file and frees the trajectory. */
+int pmb_traj_close(pmb_traj *t);
 /* Kernel launches in one captured MD step (0 before the first graph run); the list-rebuild
  * kernels are launched every step and return at once when no rebuild is due. */
 int pmb_md_kernels_per_step(pmb_md *md, int *n);

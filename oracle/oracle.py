@@ -327,3 +327,30 @@ def ref_leapfrog_constrained(system, elem, pos, vel, dt, nsteps, shake=(1e-5, 30
     n = min(ncon.value, cap)
     cons = cons[:3 * n].reshape(-1, 3)
     return pos, vel, (cons[:, 0].copy(), cons[:, 1].copy(), lens[:n].copy())
+
+
+def _ref_md_lib():
+    global _ref_md
+    if _ref_md is None:
+        ref_lib()
+        _ref_md = C.CDLL(REF_MD_LIB)
+    return _ref_md
+
+
+def ref_write_dcd(path, frames, timestep=1.0, first_step=0):
+    """The reference's DCDTrajectoryWriter, opened as OutputDCDTrajectory opens it, writing
+    ``frames`` [n_frames, n_atoms, 3]."""
+    fr = np.ascontiguousarray(frames, np.float64)
+    rc = _ref_md_lib().ref_write_dcd(str(path).encode(), int(fr.shape[1]), int(fr.shape[0]), _p(fr),
+                                     C.c_double(timestep), int(first_step))
+    if rc:
+        raise RuntimeError("reference DCD writer failed")
+
+
+def ref_write_xyz(path, pos, names):
+    """The reference's XYZWriter::write(coords, names)."""
+    p = np.ascontiguousarray(pos, np.float64)
+    arr = (C.c_char_p * len(names))(*[str(n).encode() for n in names])
+    rc = _ref_md_lib().ref_write_xyz(str(path).encode(), len(names), _p(p), arr)
+    if rc:
+        raise RuntimeError("reference XYZ writer failed")

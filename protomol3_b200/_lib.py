@@ -81,6 +81,13 @@ _PROTOS = [
     ("pmb_md_use_graph", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_set_constraints", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_constraint_sweeps", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pmb_traj_open_dcd", C.c_void_p, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]),
+    ("pmb_traj_open_xyz", C.c_void_p, [C.c_char_p, C.c_int, C.c_void_p]),
+    ("pmb_traj_write_host", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_md_write_frame", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_traj_flush", C.c_int, [C.c_void_p]),
+    ("pmb_traj_frames", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_traj_close", C.c_int, [C.c_void_p]),
     ("pmb_md_kernels_per_step", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_device_bytes", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_profile", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,

@@ -1435,6 +1435,21 @@ int pmb_md_set_constraints(pmb_md *m, const pmb_constraint_desc *d) {
   return PMB_OK;
 }
 
+}  // extern "C"
+
+namespace pmb {
+int md_frame_source(pmb_md *m, const double **d_pos, int *n_atoms, cudaStream_t *stream, int *device) {
+  if (!m->have_state) return fail(PMB_ERR_STATE, "pmb_md_set_state must come first");
+  *d_pos = m->sys->d_pos;
+  *n_atoms = m->sys->natoms;
+  *stream = m->sys->stream;
+  CK(cudaGetDevice(device));
+  return PMB_OK;
+}
+}  // namespace pmb
+
+extern "C" {
+
 int pmb_md_constraint_sweeps(pmb_md *m, int *shake_sweeps, int *rattle_sweeps) {
   if (!m) return fail(PMB_ERR_ARG, "null md");
   int h[2] = {0, 0};

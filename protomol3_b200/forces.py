@@ -383,6 +383,11 @@ class Integrator:
         L.check(L.lib().pmb_md_constraint_sweeps(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def write_frame(self, traj):
+        """Appends the current positions to ``traj`` without stopping the device (an
+        asynchronous copy and a writer thread; ``traj.flush()`` waits for the file)."""
+        L.check(L.lib().pmb_md_write_frame(self._h, traj.handle()))
+
     def set_state(self, positions, velocities=None):
         pos = np.ascontiguousarray(positions, np.float64)
         vel = None if velocities is None else np.ascontiguousarray(velocities, np.float64)
@@ -425,6 +430,57 @@ class Integrator:
         if self._h is not None:
             L.lib().pmb_md_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Trajectory:
+    """Trajectory files in the reference's formats: ``Trajectory.dcd`` (``DCDFile``,
+    output/OutputDCDTrajectory.cpp; io/DCDTrajectoryWriter.cpp) and ``Trajectory.xyz``
+    (``finXYZPosFile``, io/XYZWriter.cpp).  Frames come from host positions (``write``) or from
+    a device MD run (``Integrator.write_frame``)."""
+
+    def __init__(self, handle, n_atoms):
+        self._h = L.checked_ptr(handle)
+        self.n_atoms = n_atoms
+
+    @classmethod
+    def dcd(cls, path, n_atoms, timestep=1.0, first_step=0, little_endian=True, comment=""):
+        return cls(L.lib().pmb_traj_open_dcd(str(path).encode(), int(n_atoms), float(timestep),
+                                             int(first_step), int(little_endian), comment.encode()),
+                   n_atoms)
+
+    @classmethod
+    def xyz(cls, path, names):
+        arr = (C.c_char_p * len(names))(*[str(n).encode() for n in names])
+        return cls(L.lib().pmb_traj_open_xyz(str(path).encode(), len(names), C.cast(arr, C.c_void_p)),
+                   len(names))
+
+    def handle(self):
+        return self._h
+
+    def write(self, positions):
+        pos = np.ascontiguousarray(positions, np.float64).reshape(-1)
+        if pos.size != 3 * self.n_atoms:
+            raise ValueError("positions must be [n_atoms, 3]")
+        L.check(L.lib().pmb_traj_write_host(self._h, _p(pos)))
+
+    def flush(self):
+        L.check(L.lib().pmb_traj_flush(self._h))
+
+    def frames(self):
+        n = C.c_longlong(0)
+        L.check(L.lib().pmb_traj_frames(self._h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if self._h is not None:
+            h, self._h = self._h, None
+            L.check(L.lib().pmb_traj_close(h))
 
     def __del__(self):
         try:
