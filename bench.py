@@ -537,6 +537,65 @@ def run_rigid(args):
     print(json.dumps(out), flush=True)
 
 
+def run_frames(args):
+    """Trajectory output during the run: the 98,304-atom MD step (mixed, 1 fs) timed one by one
+    as in the main bench, without output and with a DCD frame taken off the device after every
+    step (device snapshot, host copy on the trajectory's own stream, writer thread), plus the
+    wall time until the file holds every frame."""
+    import tempfile
+    import torch
+    from protomol3_b200 import forces as F
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    box = workload(0)
+    out = {"mode": "frames", "metric": "ms per MD step with a DCD frame every step (98k atoms, mixed)",
+           "steps": args.steps, "warmup": max(3, args.warmup), "config": config_dict()}
+    tmp = tempfile.mkdtemp()
+    for leg in ("no_output", "dcd_every_step"):
+        topo = F.Topology(box, "mixed")
+        topo.set_stream(stream.cuda_stream)
+        fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", SWITCHON, RC)),
+              F.NonbondedPMEwaldSystemForce((GRID,) * 3, RC)]
+        md = F.Integrator(topo, fl, timestep=DT_FS)
+        md.set_state(box["pos"], box["vel"])
+        traj = F.Trajectory.dcd(os.path.join(tmp, "t.dcd"), topo.n_atoms) if leg != "no_output" else None
+        for _ in range(max(3, args.warmup)):
+            flush.zero_()
+            md.run(1)
+            if traj:
+                md.write_frame(traj)
+        if traj:
+            traj.flush()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        t0 = time.perf_counter()
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            md.run(1)
+            if traj:
+                md.write_frame(traj)
+            b.record(stream)
+        torch.cuda.synchronize()
+        t_dev = time.perf_counter() - t0
+        if traj:
+            traj.flush()
+        t_all = time.perf_counter() - t0
+        ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        out[leg] = {"ms_per_step": ms, "wall_s_device_done": t_dev, "wall_s_file_done": t_all}
+        if traj:
+            out[leg]["frames_in_file"] = traj.frames()
+            out[leg]["file_bytes"] = os.path.getsize(os.path.join(tmp, "t.dcd"))
+            traj.close()
+        md.close()
+        topo.close()
+    out["frame_cost_ms_per_step"] = out["dcd_every_step"]["ms_per_step"] - out["no_output"]["ms_per_step"]
+    print(json.dumps(out), flush=True)
+
+
 def serve_leg(n_requests=24, loads=(0.5, 0.8, 0.95), budget_gb=32.0, max_active=32, chunk=200,
               seed=2024):
     """Serving: Poisson streams of Langevin MD segments (water boxes log-uniform on 500-50,000
@@ -629,14 +688,17 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--chunk", type=int, default=500, help="nve: steps between energy reads")
     ap.add_argument("--serve-requests", type=int, default=24, help="serve: requests per load level")
-    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve", "serve", "rigid"], default="bench",
+    ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve", "serve", "rigid", "frames"], default="bench",
                     help="profile: only --steps force evaluations (bounded case for ncu); "
                          "batch: only the 256-box ensemble leg; nve: energy drift and "
                          "reproducibility over --steps steps; serve: latency under Poisson load; "
-                         "rigid: SHAKE + RATTLE at 2 fs")
+                         "rigid: SHAKE + RATTLE at 2 fs; frames: DCD output every step")
     args = ap.parse_args()
     if args.mode == "rigid":
         run_rigid(args)
+        return
+    if args.mode == "frames":
+        run_frames(args)
         return
     if args.mode == "serve":
         import torch

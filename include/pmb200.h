@@ -201,11 +201,11 @@ pmb_traj *pmb_traj_open_dcd(const char *path, int n_atoms, double timestep, int 
 pmb_traj *pmb_traj_open_xyz(const char *path, int n_atoms, const char *const *names);
 /* A frame from host positions [3 n_atoms]; written before the call returns. */
 int pmb_traj_write_host(pmb_traj *t, const double *positions);
-/* A frame of the MD run's current positions, taken without stopping the device: an asynchronous
- * copy into one of three pinned staging buffers on the system's stream and a writer thread that
- * appends the frame once the copy has landed (OutputDCDTrajectory::doRun without the
- * synchronisation).  Waits only when all three buffers are in flight.  Not during a stream
- * capture. */
+/* A frame of the MD run's current positions, taken without stopping the device: a device
+ * snapshot on the system's stream, its copy into one of three pinned host buffers on a stream of
+ * the trajectory's own, and a writer thread that appends the frame once the copy has landed
+ * (OutputDCDTrajectory::doRun without the synchronisation).  Waits only when all three buffers
+ * are in flight; the first frame allocates the buffers.  Not during a stream capture. */
 int pmb_md_write_frame(pmb_md *md, pmb_traj *t);
 /* Waits until every frame handed over is in the file; the first write error, if any. */
 int pmb_traj_flush(pmb_traj *t);

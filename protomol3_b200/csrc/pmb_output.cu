@@ -11,10 +11,11 @@
 //   tab and the three coordinates in 24-wide fields at 15 significant digits; every frame
 //   rewrites the file (final-position output).
 //
-// pmb_md_write_frame takes a frame off the device without stopping it: an asynchronous copy of
-// the positions into one of three pinned staging buffers on the system's stream, an event behind
-// it, and a writer thread per trajectory that waits for the event and appends the frame.  The
-// caller waits only when all three buffers are still in flight.
+// pmb_md_write_frame takes a frame off the device without stopping it: a device-to-device
+// snapshot of the positions on the system's stream (the next step waits only for that), the
+// snapshot's copy into one of three pinned host buffers on the trajectory's own stream, and a
+// writer thread per trajectory that waits for the copy and appends the frame.  The caller waits
+// only when all three buffers are still in flight.
 #include <cuda_runtime.h>
 
 #include <condition_variable>
@@ -77,10 +78,13 @@ struct pmb_traj {
   std::vector<float> fx, fy, fz;
   // asynchronous frames
   struct Stage {
-    double *host = nullptr;
-    cudaEvent_t ev = nullptr;
+    double *host = nullptr;       // pinned
+    double *dev = nullptr;        // device snapshot of the positions
+    cudaEvent_t taken = nullptr;  // snapshot done (system stream)
+    cudaEvent_t ev = nullptr;     // host copy done (copy stream)
     bool busy = false;
   } stage[STAGES];
+  cudaStream_t copy = nullptr;
   std::deque<int> queue;
   std::mutex mu;
   std::condition_variable cv;
@@ -155,7 +159,7 @@ struct pmb_traj {
     }
     std::fflush(f);
     frames++;
-    return std::ferror(f) ? PMB_ERR_CUDA : PMB_OK;
+    return std::ferror(f) ? PMB_ERR_ARG : PMB_OK;
   }
 
   int write_xyz(const double *pos) {
@@ -197,7 +201,7 @@ struct pmb_traj {
       stage[k].busy = false;
       if (rc != PMB_OK && err == PMB_OK) {
         err = rc;
-        err_msg = rc == PMB_ERR_CUDA ? "trajectory frame copy or write failed" : "cannot write " + path;
+        err_msg = rc == PMB_ERR_CUDA ? "trajectory frame copy failed" : "cannot write " + path;
       }
       cv.notify_all();
     }
@@ -226,8 +230,11 @@ struct pmb_traj {
     }
     for (Stage &s : stage) {
       if (s.host) cudaFreeHost(s.host);
+      if (s.dev) cudaFree(s.dev);
+      if (s.taken) cudaEventDestroy(s.taken);
       if (s.ev) cudaEventDestroy(s.ev);
     }
+    if (copy) cudaStreamDestroy(copy);
     if (f) std::fclose(f);
   }
 };
@@ -283,10 +290,14 @@ int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
   if (n != t->n_atoms) return set_error("trajectory atom count differs from the MD run's"), PMB_ERR_ARG;
   if (!t->started) {
     t->device = dev;
+    const size_t bytes = sizeof(double) * 3 * (size_t)n;
+    if (cudaStreamCreateWithFlags(&t->copy, cudaStreamNonBlocking) != cudaSuccess)
+      return set_error("copy stream for the trajectory"), PMB_ERR_CUDA;
     for (pmb_traj::Stage &s : t->stage) {
-      if (cudaMallocHost(&s.host, sizeof(double) * 3 * (size_t)n) != cudaSuccess ||
+      if (cudaMallocHost(&s.host, bytes) != cudaSuccess || cudaMalloc(&s.dev, bytes) != cudaSuccess ||
+          cudaEventCreateWithFlags(&s.taken, cudaEventDisableTiming) != cudaSuccess ||
           cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess)
-        return set_error("pinned staging buffers for the trajectory"), PMB_ERR_CUDA;
+        return set_error("staging buffers for the trajectory"), PMB_ERR_CUDA;
     }
     t->th = std::thread([t] { t->writer_loop(); });
     t->started = true;
@@ -304,9 +315,14 @@ int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
       if (!t->stage[i].busy) k = i;
     t->stage[k].busy = true;
   }
-  if (cudaMemcpyAsync(t->stage[k].host, d_pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, st) !=
-          cudaSuccess ||
-      cudaEventRecord(t->stage[k].ev, st) != cudaSuccess) {
+  // a device snapshot on the run's stream (microseconds), then the host copy on the trajectory's
+  // own stream, beside the steps that follow
+  pmb_traj::Stage &sg = t->stage[k];
+  const size_t bytes = sizeof(double) * 3 * (size_t)n;
+  if (cudaMemcpyAsync(sg.dev, d_pos, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      cudaEventRecord(sg.taken, st) != cudaSuccess || cudaStreamWaitEvent(t->copy, sg.taken, 0) != cudaSuccess ||
+      cudaMemcpyAsync(sg.host, sg.dev, bytes, cudaMemcpyDeviceToHost, t->copy) != cudaSuccess ||
+      cudaEventRecord(sg.ev, t->copy) != cudaSuccess) {
     std::lock_guard<std::mutex> lk(t->mu);
     t->stage[k].busy = false;
     return set_error("trajectory frame copy"), PMB_ERR_CUDA;
