@@ -118,6 +118,16 @@ int pmb_system_n_boxes(const pmb_system *sys);
  * every evaluation like Topology::updateCellLists.  The pair set evaluated is the same either
  * way (every pair within the cutoff). */
 int pmb_system_set_skin(pmb_system *sys, double skin);
+/* Vacuum (VacuumBoundaryConditions, topology/VacuumBoundaryConditions.h: the plain difference,
+ * no images; cell pairs of CellListEnumerator_standard) for the cutoff forces: a box whose edges
+ * are more than twice the extent of its atoms stands in for vacuum, because every minimal-image
+ * difference is then the plain difference.  pmb_vacuum_box gives such edges for positions
+ * [3 n_atoms]: 2 (extent + margin) + 1 per axis (margin: room for the atoms to move, e.g. the
+ * list radius).  With pmb_system_set_vacuum on, pmb_evaluate and pmb_force_evaluate check the
+ * extent of every box's atoms and return PMB_ERR_STATE once it reaches half an edge (device
+ * positions and MD runs are not checked). */
+int pmb_vacuum_box(const double *positions, int n_atoms, double margin, double edges[3]);
+int pmb_system_set_vacuum(pmb_system *sys, int on);
 /* Waits for the system's stream and reports whether a neighbour list overflowed since the last
  * check: PMB_ERR_CAPACITY, with the list storage enlarged so that the next evaluation fits.  The
  * host-pointer entry points check by themselves and retry; pmb_evaluate_device does not

@@ -354,3 +354,18 @@ def ref_write_xyz(path, pos, names):
     rc = _ref_md_lib().ref_write_xyz(str(path).encode(), len(names), _p(p), arr)
     if rc:
         raise RuntimeError("reference XYZ writer failed")
+
+
+def ref_evaluate_vacuum(system, pos, cutoff, cellsize=5.0):
+    """The reference's cutoff forces with VacuumBoundaryConditions (oracle/ref_vacuum.cpp):
+    forces (n, 3), energies[4] (Coulomb, LJ, bond, angle), virial (9,)."""
+    L = _ref_md_lib()
+    pos = np.ascontiguousarray(pos, np.float64)
+    r = _ref_input(system, pos, cellsize)
+    c = RefCutoff()
+    C.memmove(C.byref(c), C.byref(cutoff), C.sizeof(c))
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    v = np.zeros(9)
+    L.ref_cutoff_eval_vacuum(C.byref(r), C.byref(c), _p(f), _p(e), _p(v))
+    return f, e, v

@@ -39,12 +39,24 @@ struct ref_pme {
 
 }  // extern "C"
 
+// The atoms, parameters, exclusions, bonds and angles of any Topology<BC, CubicCellManager>.
+template <class T>
+static inline void fill_topo(T *t, const ref_input *in);
+
+#ifndef PMB_REF_VACUUM
 static inline Topo *make_topo(const ref_input *in) {
   Topo *t = new Topo(in->coulomb_scaling, ExclusionType(ExclusionType::ONE4),
                      PBC(Vector3D(in->box[0], 0, 0), Vector3D(0, in->box[1], 0),
                          Vector3D(0, 0, in->box[2]),
                          Vector3D(in->origin[0], in->origin[1], in->origin[2])),
                      CubicCellManager(in->cellsize), 16.0f);
+  fill_topo(t, in);
+  return t;
+}
+#endif
+
+template <class T>
+static inline void fill_topo(T *t, const ref_input *in) {
   t->atoms.resize(in->n);
   int nmol = 0;
   for (int i = 0; i < in->n; i++) {
@@ -86,7 +98,6 @@ static inline Topo *make_topo(const ref_input *in) {
     a.ureyBradleyRestLength = in->ub_r0[k];
     t->angles.push_back(a);
   }
-  return t;
 }
 
 #endif

@@ -215,6 +215,7 @@ struct pmb_system {
   double nb_cutoff = 0.0;    // radius the list storage is sized for
   double nb_build_rl = -1.0; // radius the current list was built with
   double skin = 0.8;         // list radius = pair cutoff + skin
+  bool vacuum = false;       // boxes stand in for vacuum: evaluations check the extent
   NbListDev nb{};
   Allocs nba;
   int n_bonded = 0;
@@ -1078,11 +1079,46 @@ int pmb_evaluate_device(pmb_system *s, pmb_force *const *fs, int n, const double
   return PMB_OK;
 }
 
+int pmb_vacuum_box(const double *pos, int n_atoms, double margin, double edges[3]) {
+  if (!pos || !edges || n_atoms <= 0 || !(margin >= 0)) return fail(PMB_ERR_ARG, "positions, atom count, margin >= 0");
+  for (int c = 0; c < 3; c++) {
+    double lo = pos[c], hi = pos[c];
+    for (int i = 1; i < n_atoms; i++) {
+      lo = std::min(lo, pos[3 * i + c]);
+      hi = std::max(hi, pos[3 * i + c]);
+    }
+    if (!std::isfinite(lo) || !std::isfinite(hi)) return fail(PMB_ERR_NUMERIC, "non-finite position");
+    edges[c] = 2.0 * (hi - lo + margin) + 1.0;
+  }
+  return PMB_OK;
+}
+
+int pmb_system_set_vacuum(pmb_system *s, int on) {
+  if (!s) return fail(PMB_ERR_ARG, "null system");
+  s->vacuum = on != 0;
+  return PMB_OK;
+}
+
 int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, double *forces,
                  double *energies, int virial) {
   if (!s || !pos) return fail(PMB_ERR_ARG, "null argument");
   for (int i = 0; i < 3 * s->natoms; i++)
     if (!std::isfinite(pos[i])) return fail(PMB_ERR_NUMERIC, "non-finite position");
+  if (s->vacuum) {
+    // the periodic box stands in for vacuum only while no two atoms of a box are half an edge
+    // apart: then every minimal-image difference is the plain difference
+    for (const BoxDev &b : s->hbox)
+      for (int c = 0; c < 3; c++) {
+        double lo = pos[3 * b.atom0 + c], hi = lo;
+        for (int i = b.atom0 + 1; i < b.atom0 + b.natoms; i++) {
+          lo = std::min(lo, pos[3 * i + c]);
+          hi = std::max(hi, pos[3 * i + c]);
+        }
+        if (!(hi - lo < 0.5 * b.L[c]))
+          return fail(PMB_ERR_STATE, "vacuum: the atoms spread over half a box edge; make the system "
+                                     "again with edges from pmb_vacuum_box");
+      }
+  }
   cudaStream_t st = s->stream;
   for (int attempt = 0; attempt < 3; attempt++) {
     CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, st));

@@ -113,6 +113,12 @@ class Topology:
     def set_skin(self, skin):
         L.check(L.lib().pmb_system_set_skin(self.system(), float(skin)))
 
+    def set_vacuum(self, on=True):
+        """Vacuum boundary conditions for the cutoff forces: the box (edges from
+        ``vacuum_box``) stands in for vacuum, and evaluations refuse positions spread over half
+        an edge."""
+        L.check(L.lib().pmb_system_set_vacuum(self.system(), int(on)))
+
     def list_builds(self):
         """Neighbour-list builds so far (waits for the system's stream)."""
         n = C.c_longlong(0)
@@ -436,6 +442,15 @@ class Integrator:
             self.close()
         except Exception:
             pass
+
+
+def vacuum_box(positions, margin=0.0):
+    """Box edges that make a periodic box stand in for vacuum (VacuumBoundaryConditions):
+    2 (extent + margin) + 1 per axis, so no two atoms are half an edge apart."""
+    pos = np.ascontiguousarray(positions, np.float64).reshape(-1)
+    e = np.zeros(3)
+    L.check(L.lib().pmb_vacuum_box(_p(pos), pos.size // 3, float(margin), _p(e)))
+    return e
 
 
 class Trajectory:
