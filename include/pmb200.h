@@ -127,6 +127,15 @@ int pmb_system_set_skin(pmb_system *sys, double skin);
  * extent of every box's atoms and return PMB_ERR_STATE once it reaches half an edge (device
  * positions and MD runs are not checked). */
 int pmb_vacuum_box(const double *positions, int n_atoms, double margin, double edges[3]);
+/* Exact Ewald reciprocal sum, the check path for the PME reciprocal term: what
+ * NonbondedFullEwaldSystemForce with only -reciprocal adds (reciprocalTerm,
+ * force/nonbonded/NonbondedFullEwaldSystemForce.h:873-1083), over the k-vectors |k| < kc of its
+ * initialize (:590-660): kc = 2 alpha sqrt(-ln accuracy), alpha <= 0 takes the reference's
+ * default sqrt(pi) (5.5 N / V^2)^(1/6) per box.  Host positions [3 N]; forces +=, energies +=
+ * (PMB_E_COULOMB and, with virial, the virial slots of each box).  Allocates its k-vector
+ * scratch per call; cost N x (number of k-vectors) per box. */
+int pmb_ewald_reciprocal(pmb_system *sys, const double *positions, double alpha, double accuracy, double *forces,
+                         double *energies, int virial);
 int pmb_system_set_vacuum(pmb_system *sys, int on);
 /* Waits for the system's stream and reports whether a neighbour list overflowed since the last
  * check: PMB_ERR_CAPACITY, with the list storage enlarged so that the next evaluation fits.  The

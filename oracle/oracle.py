@@ -369,3 +369,16 @@ def ref_evaluate_vacuum(system, pos, cutoff, cellsize=5.0):
     v = np.zeros(9)
     L.ref_cutoff_eval_vacuum(C.byref(r), C.byref(c), _p(f), _p(e), _p(v))
     return f, e, v
+
+
+def ref_ewald_reciprocal(system, pos, alpha, accuracy, virial=False):
+    """The reference's NonbondedFullEwaldSystemForce with only the reciprocal term
+    (oracle/ref_ewald.cpp): forces (n, 3), Coulomb energy, virial (9,)."""
+    L = _ref_md_lib()
+    pos = np.ascontiguousarray(pos, np.float64)
+    r = _ref_input(system, pos, 5.0)
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    v = np.zeros(9)
+    L.ref_ewald_reciprocal(C.byref(r), C.c_double(alpha), C.c_double(accuracy), _p(f), _p(e), _p(v), int(virial))
+    return f, e[0], v

@@ -63,6 +63,8 @@ _PROTOS = [
     ("pmb_system_set_skin", C.c_int, [C.c_void_p, C.c_double]),
     ("pmb_vacuum_box", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     ("pmb_system_set_vacuum", C.c_int, [C.c_void_p, C.c_int]),
+    ("pmb_ewald_reciprocal", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p,
+                                       C.c_void_p, C.c_int]),
     ("pmb_system_check", C.c_int, [C.c_void_p]),
     ("pmb_system_list_builds", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_force_create", C.c_void_p, [C.c_void_p, C.c_void_p]),

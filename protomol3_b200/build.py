@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpmb200.so")
-SOURCES = ["pmb_api.cu", "pmb_nblist.cu", "pmb_pair.cu", "pmb_pme.cu", "pmb_md.cu", "pmb_output.cu"]
+SOURCES = ["pmb_api.cu", "pmb_nblist.cu", "pmb_pair.cu", "pmb_pme.cu", "pmb_md.cu", "pmb_output.cu", "pmb_ewald.cu"]
 HEADERS = ["pmb_common.cuh", "pmb_internal.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1079,6 +1079,97 @@ int pmb_evaluate_device(pmb_system *s, pmb_force *const *fs, int n, const double
   return PMB_OK;
 }
 
+int pmb_ewald_reciprocal(pmb_system *s, const double *pos, double alpha, double accuracy, double *forces,
+                         double *energies, int virial) {
+  if (!s || !pos) return fail(PMB_ERR_ARG, "null argument");
+  if (!(accuracy > 0 && accuracy < 1)) return fail(PMB_ERR_ARG, "accuracy must lie in (0, 1)");
+  for (int i = 0; i < 3 * s->natoms; i++)
+    if (!std::isfinite(pos[i])) return fail(PMB_ERR_NUMERIC, "non-finite position");
+  cudaStream_t st = s->stream;
+  CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, st));
+  s->have_pos = true;
+  Allocs tmp;  // a check path: scratch per call
+  double *d_f = tmp.get<double>(3 * (size_t)s->natoms);
+  if (!d_f) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the Ewald sum");
+  std::vector<double> hf(3 * (size_t)s->natoms, 0.0);
+  for (int bi = 0; bi < s->nbox; bi++) {
+    const BoxDev &b = s->hbox[bi];
+    // NonbondedFullEwaldSystemForce::initialize (NonbondedFullEwaldSystemForce.h:590-660), with the
+    // box's volume and reciprocal edges as PeriodicBoundaryConditions::set forms them
+    const double lx = b.L[0], ly = b.L[1], lz = b.L[2];
+    const double V = (lx * ly) * lz, Vr = 1.0 / V;
+    const double lxr = (ly * lz) / (lx * (ly * lz)), lyr = (lz * lx) / (ly * (lz * lx)),
+                 lzr = (lx * ly) / (lz * (lx * ly));
+    const double a = alpha > 0 ? alpha : std::sqrt(M_PI) * std::pow(5.5 * b.natoms / (V * V), 1.0 / 6.0);
+    const double a2r = 1.0 / (a * a), fac = 1.0 / (4.0 * a * a);
+    const double p = -std::log(accuracy);
+    const double kc = 2.0 * a * std::sqrt(p), kc2 = kc * kc;
+    const int hmax = (int)std::floor(kc / (2.0 * M_PI) * lx), kmax = (int)std::floor(kc / (2.0 * M_PI) * ly),
+              lmax = (int)std::floor(kc / (2.0 * M_PI) * lz);
+    std::vector<double3> kv;
+    std::vector<double> ksq, bk, ak;
+    for (int h = 0; h <= hmax; h++) {
+      const double kx = 2.0 * M_PI * h * lxr;
+      for (int k = (h == 0 ? 0 : -kmax); k <= kmax; k++) {
+        const double ky = 2.0 * M_PI * k * lyr;
+        for (int l = (h == 0 && k == 0 ? 1 : -lmax); l <= lmax; l++) {
+          const double kz = 2.0 * M_PI * l * lzr;
+          const double q2 = kx * kx + ky * ky + kz * kz;
+          if (q2 < kc2) {
+            kv.push_back(make_double3(kx, ky, kz));
+            ksq.push_back(q2);
+            const double bb = 1.0 / q2 * std::exp(-q2 * a2r / 4.0);
+            bk.push_back(bb);
+            ak.push_back(8.0 * M_PI * Vr * bb);
+          }
+        }
+      }
+    }
+    const int nk = (int)kv.size();
+    if (nk == 0 || b.natoms == 0) continue;
+    Allocs kt;
+    double3 *d_kv = kt.get<double3>(nk);
+    double *d_a = kt.get<double>(nk), *d_S = kt.get<double>(nk), *d_C = kt.get<double>(nk);
+    if (!d_kv || !d_a || !d_S || !d_C) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the Ewald sum");
+    CK(cudaMemcpyAsync(d_kv, kv.data(), sizeof(double3) * nk, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_a, ak.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st));
+    if (ewald_recip_launch(s->d_pos, s->d_charge, b.atom0, b.natoms, d_kv, d_a, nk, d_S, d_C, d_f, st))
+      return fail(PMB_ERR_CUDA, "Ewald kernels");
+    std::vector<double> S(nk), Cc(nk);
+    CK(cudaMemcpyAsync(S.data(), d_S, sizeof(double) * nk, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(Cc.data(), d_C, sizeof(double) * nk, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hf.data() + 3 * (size_t)b.atom0, d_f + 3 * (size_t)b.atom0, sizeof(double) * 3 * b.natoms,
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // energy and virial in the reference's k order (NonbondedFullEwaldSystemForce.h:1031-1083)
+    double energy = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+    for (int k = 0; k < nk; k++) {
+      const double e = bk[k] * (S[k] * S[k] + Cc[k] * Cc[k]);
+      energy += e;
+      const double c = 2.0 * (1.0 / ksq[k] + fac);
+      const double3 q = kv[k];
+      vxx += e * (1.0 - c * q.x * q.x);
+      vxy -= e * c * q.x * q.y;
+      vxz -= e * c * q.x * q.z;
+      vyy += e * (1.0 - c * q.y * q.y);
+      vyz -= e * c * q.y * q.z;
+      vzz += e * (1.0 - c * q.z * q.z);
+    }
+    const double c = 4.0 * M_PI * Vr;
+    if (energies) {
+      double *eb = energies + (size_t)bi * PMB_E_STRIDE;
+      eb[PMB_E_COULOMB] += c * energy;
+      if (virial) {
+        const double vv[9] = {vxx, vxy, vxz, vxy, vyy, vyz, vxz, vyz, vzz};
+        for (int k = 0; k < 9; k++) eb[PMB_E_VIRIAL + k] += c * vv[k];
+      }
+    }
+  }
+  if (forces)
+    for (size_t i = 0; i < hf.size(); i++) forces[i] += hf[i];
+  return PMB_OK;
+}
+
 int pmb_vacuum_box(const double *pos, int n_atoms, double margin, double edges[3]) {
   if (!pos || !edges || n_atoms <= 0 || !(margin >= 0)) return fail(PMB_ERR_ARG, "positions, atom count, margin >= 0");
   for (int c = 0; c < 3; c++) {

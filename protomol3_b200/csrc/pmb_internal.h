@@ -148,6 +148,9 @@ typedef void (*StageMark)(void *ctx, const char *stage);
 int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,
                      StageMark mark = nullptr, void *mark_ctx = nullptr);
 int pme_line_capacity();
+// Exact Ewald reciprocal sum of one box (pmb_ewald.cu): S, C [nk] and the box's forces in fout.
+int ewald_recip_launch(const double *pos, const double *charge, int atom0, int n, const double3 *kv,
+                       const double *a, int nk, double *S, double *Cc, double *fout, cudaStream_t st);
 int pme_correction_launch(const SystemDev &s, const PmeDev &pm, const int *excl_pairs,
                           const int *excl_kind, int nexcl, double coulomb_scaling, cudaStream_t st);
 

@@ -444,6 +444,17 @@ class Integrator:
             pass
 
 
+def ewald_reciprocal(topo, positions, forces, energies, alpha=-1.0, accuracy=1e-6):
+    """The exact Ewald reciprocal sum (NonbondedFullEwaldSystemForce, reciprocal term only),
+    the check path for PME: forces (N, 3) and energies (ScalarStructure) are accumulated into."""
+    pos = np.ascontiguousarray(positions, np.float64)
+    f = np.ascontiguousarray(forces)
+    L.check(L.lib().pmb_ewald_reciprocal(topo.system(), _p(pos), float(alpha), float(accuracy), _p(f),
+                                         _p(energies.table), int(energies.do_virial)))
+    if f is not forces:
+        forces[:] = f
+
+
 def vacuum_box(positions, margin=0.0):
     """Box edges that make a periodic box stand in for vacuum (VacuumBoundaryConditions):
     2 (extent + margin) + 1 per axis, so no two atoms are half an edge apart."""
