@@ -291,12 +291,14 @@ int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
   if (!t->started) {
     t->device = dev;
     const size_t bytes = sizeof(double) * 3 * (size_t)n;
-    if (cudaStreamCreateWithFlags(&t->copy, cudaStreamNonBlocking) != cudaSuccess)
+    // what a failed attempt obtained is kept (and freed with the trajectory); a retry fills the rest
+    if (!t->copy && cudaStreamCreateWithFlags(&t->copy, cudaStreamNonBlocking) != cudaSuccess)
       return set_error("copy stream for the trajectory"), PMB_ERR_CUDA;
     for (pmb_traj::Stage &s : t->stage) {
-      if (cudaMallocHost(&s.host, bytes) != cudaSuccess || cudaMalloc(&s.dev, bytes) != cudaSuccess ||
-          cudaEventCreateWithFlags(&s.taken, cudaEventDisableTiming) != cudaSuccess ||
-          cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess)
+      if ((!s.host && cudaMallocHost(&s.host, bytes) != cudaSuccess) ||
+          (!s.dev && cudaMalloc(&s.dev, bytes) != cudaSuccess) ||
+          (!s.taken && cudaEventCreateWithFlags(&s.taken, cudaEventDisableTiming) != cudaSuccess) ||
+          (!s.ev && cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming) != cudaSuccess))
         return set_error("staging buffers for the trajectory"), PMB_ERR_CUDA;
     }
     t->th = std::thread([t] { t->writer_loop(); });
