@@ -162,6 +162,22 @@ def pair_count(box, rc):
     return (n_ordered - n) // 2 - len(box["excl_pairs"])
 
 
+def force_errors(f, e, f_ref, e_ref):
+    """Error of forces f / energies e [Coulomb, LJ, ...] against FP64 references: RMS relative
+    force error sqrt(sum |F - F_ref|^2 / sum |F_ref|^2), the largest per-atom error relative to
+    that atom's force and relative to the RMS force, and the relative error of each energy term."""
+    d = np.linalg.norm(f - f_ref, axis=1)
+    fr = np.linalg.norm(f_ref, axis=1)
+    rms = float(np.sqrt((fr ** 2).mean()))
+    out = {"rms_rel_force": float(np.sqrt((d ** 2).sum() / (fr ** 2).sum())),
+           "max_rel_force_per_atom": float((d / np.maximum(fr, 1e-300)).max()),
+           "max_force_err_over_rms_force": float(d.max() / rms)}
+    for k, name in ((0, "coulomb"), (1, "lj")):
+        out["energy_rel_" + name] = float(abs(e[k] - e_ref[k]) / abs(e_ref[k]))
+        out["energy_abs_" + name] = float(abs(e[k] - e_ref[k]))
+    return out
+
+
 def read_profile_traffic():
     """DRAM bytes per launch of the pair kernel from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "pair_kernel_config2.md")
@@ -176,9 +192,43 @@ def read_profile_traffic():
     return None
 
 
-def cpu_baseline(box, steps=1):
-    """The reference's own force classes (compiled from its sources into oracle/_ref) on one
-    core; falls back to the C restatement (oracle/) when the compiled reference is absent."""
+def cpu_facts():
+    """The host CPU the baseline runs on: model name, logical CPUs, CPUs this process may use."""
+    model = None
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    return {"cpu_model": model, "nproc": os.cpu_count(), "usable_cpus": usable}
+
+
+class stdout_to_stderr:
+    """File-descriptor level redirection of stdout to stderr while the reference's code runs: its
+    report stream prints to stdout, where only the JSON line belongs."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def ref_force_step(box, rc, switchon, grid, steps):
+    """``steps`` evaluations of LJ C2 (switchon -> rc) + PME (grid^3, order 4, accuracy 1e-6,
+    real-space rc) on one core: the reference's own force classes compiled from its sources
+    (oracle/_ref), else the C restatement (oracle/).  Returns (s per step, forces of the last
+    evaluation, energies [Coulomb, LJ, bond, angle], kind)."""
     import ctypes as C
     from oracle import oracle as O
     s = O.System(box)
@@ -189,26 +239,68 @@ def cpu_baseline(box, steps=1):
         L = O.ref_lib()
         r = O._ref_input(s, pos, 5.0)
         c = O.RefCutoff()
-        cp = O.cutoff_params(lj=("C2", SWITCHON, RC))
+        cp = O.cutoff_params(lj=("C2", switchon, rc))
         C.memmove(C.byref(c), C.byref(cp), C.sizeof(c))
         p = O.RefPME()
-        p.nx = p.ny = p.nz = GRID
-        p.order, p.cutoff, p.accuracy, p.alpha, p.real_switch = 4, RC, 1e-6, -1.0, 0
-        t0 = time.perf_counter()
-        L.ref_time_step(C.byref(r), C.byref(c), C.byref(p), int(steps), O._p(f), O._p(e))
-        dt = (time.perf_counter() - t0) / steps
-        kind = "reference"
-    else:
-        cp = O.cutoff_params(lj=("C2", SWITCHON, RC))
-        pm = O.pme_params((GRID,) * 3, RC)
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            O.evaluate(s, pos, cutoff=cp, pme=pm, bonded=True)
-        dt = (time.perf_counter() - t0) / steps
-        kind = "port"
-    return {"value": ns_per_day(dt * 1e3), "unit": "ns/day", "cores": 1, "kind": kind,
-            "sample": "%d full force evaluation(s) (LJ C2 + PME 96^3 + corrections) of the 98,304-atom "
-                      "box, single-threaded; %.2f s per step" % (steps, dt)}
+        p.nx = p.ny = p.nz = grid
+        p.order, p.cutoff, p.accuracy, p.alpha, p.real_switch = 4, rc, 1e-6, -1.0, 0
+        with stdout_to_stderr():
+            t0 = time.perf_counter()
+            L.ref_time_step(C.byref(r), C.byref(c), C.byref(p), int(steps), O._p(f), O._p(e))
+            dt = (time.perf_counter() - t0) / steps
+        return dt, f, e, "reference"
+    cp = O.cutoff_params(lj=("C2", switchon, rc))
+    pm = O.pme_params((grid,) * 3, rc)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f, e, _, _ = O.evaluate(s, pos, cutoff=cp, pme=pm)
+    return (time.perf_counter() - t0) / steps, f, e, "port"
+
+
+def cpu_baseline(box, steps=1):
+    """The reference's own force classes (compiled from its sources into oracle/_ref) on one
+    core; falls back to the C restatement (oracle/) when the compiled reference is absent.
+    Also returns the forces and energies of that evaluation, the FP64 reference the accuracy of
+    the timed configuration is stated against."""
+    dt, f, e, kind = ref_force_step(box, RC, SWITCHON, GRID, steps)
+    out = {"value": ns_per_day(dt * 1e3), "unit": "ns/day", "cores": 1, "kind": kind,
+           "sample": "%d force evaluation(s) (LJ C2 + PME 96^3 with real, reciprocal and correction "
+                     "terms) of the 98,304-atom box, single-threaded; %.2f s per step" % (steps, dt)}
+    out.update(cpu_facts())
+    return out, f, e
+
+
+def _ensemble_box_step(args):
+    """One box of the ensemble workload through the reference's force classes, one evaluation;
+    run in a spawned worker process (no CUDA)."""
+    k, n_waters, seed, grid = args
+    from protomol3_b200 import waterbox as W
+    box = W.water_box(n_waters, seed=seed)
+    dt, _, _, kind = ref_force_step(box, BATCH_RC, BATCH_SWITCHON, grid, 1)
+    return len(box["charge"]), dt, kind
+
+
+def cpu_ensemble(processes=None):
+    """The ensemble workload on the host the way the reference would run it: one single-threaded
+    process per box, ``nproc`` of them at a time, every box evaluated once (LJ C2 7.5 -> 9 A +
+    PME ~1 A spacing, order 4).  Aggregate atom-steps/s = atoms of all boxes / wall time."""
+    import multiprocessing as mp
+    from protomol3_b200 import waterbox as W
+    # the same water counts, seeds and grids as waterbox.ensemble() gives the GPU leg
+    counts = np.random.default_rng(4321).integers(100, 2001, size=256)
+    work = [(k, int(n), 4321 + 1 + k, W.pme_grid_for(W.box_edge(int(n)))) for k, n in enumerate(counts)]
+    nproc = processes or cpu_facts()["usable_cpus"] or 1
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_ensemble_box_step, work, chunksize=1)
+    wall = time.perf_counter() - t0
+    atoms = sum(r[0] for r in res)
+    return {"value": atoms / wall, "unit": "atom-steps/s", "processes": nproc, "boxes": len(res),
+            "atoms": atoms, "wall_s": wall, "kind": res[0][2],
+            "single_core_atom_steps_s": atoms / sum(r[1] for r in res),
+            "sample": "every box evaluated once, one single-threaded process per box, %d at a time "
+                      "(process start-up included in the wall time)" % nproc}
 
 
 # ------------------------------------------------------------------------------- B200 arm
@@ -280,8 +372,7 @@ def run_b200(args, rank, world, local_rank):
     npairs = pair_count(box, RC) if rank == 0 else None
 
     # end-to-end through the C ABI with pinned host buffers
-    e2e = None
-    if rank == 0 or world > 1:
+    def e2e_leg(topo, fl):
         n = topo.n_atoms
         # pinned host buffers; the caller's leapfrog runs in place on the host (torch CPU ops on
         # the same memory, multi-threaded, as a C++ integrator loop of the caller would)
@@ -294,19 +385,36 @@ def run_b200(args, rank, world, local_rank):
         thinv = torch.from_numpy(h / box["mass"])[:, None]
         en = F.ScalarStructure(1)
         nsteps = max(3, args.steps // 2)
+        parts = {"enqueue": 0.0, "wait_device": 0.0, "accumulate": 0.0, "host_leapfrog": 0.0}
         for it in range(nsteps + 2):
             if it == 2:
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
+                parts = dict.fromkeys(parts, 0.0)
             tfrc.zero_()
             en.clear()
             F.evaluate_all(topo, fl, hpos, hfrc, en)
+            t1 = time.perf_counter()
             tvel.addcmul_(tfrc, thinv)
             tpos.add_(tvel, alpha=h)
+            parts["host_leapfrog"] += (time.perf_counter() - t1) * 1e3
+            for k, v in topo.evaluate_times().items():
+                parts[k] += v
         e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / nsteps, dist, "cuda")
-        e2e = {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "ms_per_step": e2e_ms,
-               "h2d_bytes_per_step": int(hpos.nbytes), "d2h_bytes_per_step": int(hfrc.nbytes + 16 * 8),
-               "path": "pmb_evaluate (C ABI) with pinned host positions/forces + host leapfrog"}
+        return {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(hpos.nbytes), "d2h_bytes_per_step": int(hfrc.nbytes + 16 * 8),
+                "breakdown_ms": {k: v / nsteps for k, v in parts.items()},
+                "path": "pmb_evaluate (C ABI) with pinned host positions/forces + host leapfrog"}
+
+    def forces_at_start(topo, fl):
+        """Forces and energies of the nonbonded terms (LJ + PME) at the starting coordinates."""
+        frc = np.zeros((topo.n_atoms, 3))
+        en = F.ScalarStructure(1)
+        F.evaluate_all(topo, fl, box["pos"], frc, en)
+        return frc, en.table[0, :4].copy()
+
+    e2e = e2e_leg(topo, fl) if (rank == 0 or world > 1) else None
+    start = {args.precision: forces_at_start(topo, [fl[1], fl[2]])}
 
     # plain FP64 path on the same workload (the drop-in); the headline is the mixed path
     fp64 = None
@@ -315,7 +423,9 @@ def run_b200(args, rank, world, local_rank):
         ms64, _, _ = time_md(topo64, fl64, max(3, args.steps // 2), 3)
         ms64 = max_over_ranks(ms64, dist, "cuda")
         fp64 = {"value": world * ns_per_day(ms64), "ms_per_step": ms64,
-                "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64)}
+                "mixed_over_fp64": ns_per_day(ms) / ns_per_day(ms64),
+                "e2e": e2e_leg(topo64, fl64) if (rank == 0 or world > 1) else None}
+        start["fp64"] = forces_at_start(topo64, [fl64[1], fl64[2]])
         topo64.close()
 
     serving = None
@@ -328,9 +438,19 @@ def run_b200(args, rank, world, local_rank):
         batched["ms_per_step"] = max_over_ranks(batched["ms_per_step"], dist, "cuda")
         batched["value"] = world * batched["atoms"] / (batched["ms_per_step"] * 1e-3)
 
-    base = None
+    base, accuracy, cpu_ens = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        base = cpu_baseline(box, steps=args.cpu_steps)
+        base, f_ref, e_ref = cpu_baseline(box, steps=args.cpu_steps)
+        accuracy = {"against": "the reference's own FP64 force classes (%s) on the starting coordinates, "
+                               "LJ C2 + PME" % base["kind"]}
+        for prec, (f, e) in start.items():
+            accuracy[prec] = force_errors(f, e, f_ref, e_ref)
+        if not args.no_batch:
+            cpu_ens = cpu_ensemble()
+            batched["cpu_reference_nproc"] = cpu_ens
+    elif rank == 0 and "fp64" in start:
+        accuracy = {"against": "the plain FP64 GPU path on the starting coordinates (no CPU leg run)",
+                    args.precision: force_errors(*start[args.precision], *start["fp64"])}
 
     if dist:
         dist.barrier()
@@ -353,6 +473,7 @@ def run_b200(args, rank, world, local_rank):
                      "work": "%d FLOP x %d in-cutoff pairs per launch" % (FLOPS_PER_PAIR, npairs),
                      "kernel_ms": t_pair, "peak_source": "measured FP32 FMA issue rate (pmb_fp32_peak)"},
         "stages_ms": stages, "plain_fp64": fp64, "batched": batched, "serving": serving, "cpu_baseline": base,
+        "accuracy": accuracy,
     }
     print(json.dumps(line), flush=True)
 
@@ -662,7 +783,7 @@ def run_reference(args, rank, world):
     steps = max(1, min(args.steps, args.ref_steps))
     for _ in range(min(args.warmup, 1)):
         cpu_baseline(box, steps=1)
-    base = cpu_baseline(box, steps=steps)
+    base = cpu_baseline(box, steps=steps)[0]
     line = {"metric": "ns/day at 98k atoms (TIP3P, LJ C2 + PME 96^3, 1 fs leapfrog)", "impl": "reference",
             "value": base["value"], "unit": "ns/day", "n_gpus": world, "steps": steps,
             "warmup": min(args.warmup, 1), "ms_per_step": 86400.0 * DT_FS * 1e-6 / base["value"] * 1e3,

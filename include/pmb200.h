@@ -138,7 +138,9 @@ int pmb_ewald_reciprocal(pmb_system *sys, const double *positions, double alpha,
                          double *energies, int virial);
 int pmb_system_set_vacuum(pmb_system *sys, int on);
 /* Waits for the system's stream and reports whether a neighbour list overflowed since the last
- * check: PMB_ERR_CAPACITY, with the list storage enlarged so that the next evaluation fits.  The
+ * check: PMB_ERR_CAPACITY, with the list storage enlarged so that the next evaluation fits; or
+ * whether an evaluation met a non-finite position (device evaluations, MD runs that blew up):
+ * PMB_ERR_NUMERIC.  The
  * host-pointer entry points check by themselves and retry; pmb_evaluate_device does not
  * synchronise, so its callers call this after their evaluations and repeat one that overflowed. */
 int pmb_system_check(pmb_system *sys);
@@ -146,6 +148,11 @@ int pmb_system_check(pmb_system *sys);
  * moved more than half the skin).  Synchronises the system stream.  No counterpart in the
  * reference, which rebuilds its cell lists at every evaluation. */
 int pmb_system_list_builds(pmb_system *sys, long long *n);
+/* Host time of the last pmb_evaluate / pmb_force_evaluate, in ms: [0] checks and enqueueing
+ * (the position upload and every launch), [1] waiting for the device's first results (status
+ * and energies), [2] adding the forces into the caller's array while their device->host copies
+ * land piece by piece.  No counterpart in the reference (TimerStatistic times whole forces). */
+int pmb_system_evaluate_times(const pmb_system *sys, double ms[3]);
 
 /* Forces ------------------------------------------------------------------------------------- */
 pmb_force *pmb_force_create(pmb_system *sys, const pmb_force_desc *desc);
@@ -158,7 +165,9 @@ int pmb_force_alpha(const pmb_force *f, double *alpha);
  * virial slots (ScalarStructure::virial()). */
 int pmb_force_evaluate(pmb_force *f, const double *positions, double *forces, double *energies,
                        int virial);
-/* Several forces of one system in one device pass (ForceGroup::evaluateSystemForces). */
+/* Several forces of one system in one device pass (ForceGroup::evaluateSystemForces).  A
+ * non-finite position gives PMB_ERR_NUMERIC with forces and energies untouched (detected on the
+ * device by the list kernels, on the host for force sets that need no list). */
 int pmb_evaluate(pmb_system *sys, pmb_force *const *forces, int n_forces, const double *positions,
                  double *forces_out, double *energies, int virial);
 /* Same, with device pointers and no host synchronisation: d_forces and d_energies are
@@ -267,9 +276,10 @@ int pmb_fp32_peak(double *tflops);
  * the system's stream) before using it, so nothing has to start at zero.
  * d_positions [3 N], d_forces [3 N] (overwritten) and d_energies [n_boxes * PMB_E_STRIDE]
  * (overwritten; may be NULL) are device pointers; work is enqueued on the system's stream with
- * no host synchronisation.  The first call on a device (the current device) looks the scratch
- * up with cudaGetSymbolAddress, which may load the module: make that first call before any
- * stream capture.  Calls whose executions overlap on one device (other streams, systems or host
+ * no host synchronisation.  The first call on a device (the current device), and the first in
+ * a new context of that device (after cudaDeviceReset), looks the scratch up with
+ * cudaGetSymbolAddress, which may load the module: make that first call before any stream
+ * capture.  Calls whose executions overlap on one device (other streams, systems or host
  * threads) share the scratch and race on it: order them on one stream or synchronise between. */
 int pmb_cutoff_evaluate_static(pmb_force *f, const double *d_positions, double *d_forces,
                                double *d_energies, int virial);

@@ -62,7 +62,7 @@ def lib():
         build()
         _lib = C.CDLL(LIB)
         for fn in ("orc_cutoff", "orc_pme", "orc_bonded", "orc_leapfrog",
-                   "orc_leapfrog_constrained", "orc_shake", "orc_rattle"):
+                   "orc_leapfrog_constrained", "orc_shake", "orc_rattle", "orc_langevin"):
             getattr(_lib, fn).restype = C.c_int
         _lib.orc_pme_alpha.restype = C.c_double
         _lib.orc_pme_alpha.argtypes = [C.c_double, C.c_double]
@@ -173,6 +173,31 @@ def leapfrog(system, pos, vel, dt, nsteps, cutoff=None, pme=None, bonded=True):
     return pos, vel, f, e
 
 
+def langevin(system, pos, vel, dt, nsteps, temperature, gamma, seed=1234, first_step=0,
+             cutoff=None, pme=None, bonded=True):
+    """LangevinLeapfrogIntegrator::run(nsteps) as orc_langevin restates it (temperature in K,
+    gamma in 1/ps), with the device's counter-based noise stream; first_step = steps taken since
+    the state was set.  Returns pos, vel, forces, energies of the last evaluation."""
+    L = lib()
+    pos = np.ascontiguousarray(pos, np.float64).copy()
+    vel = np.ascontiguousarray(vel, np.float64).copy()
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    rc = L.orc_langevin(C.byref(system.s), C.byref(cutoff) if cutoff is not None else None,
+                        C.byref(pme) if pme is not None else None, int(bonded), C.c_double(dt),
+                        C.c_double(temperature), C.c_double(gamma), C.c_ulonglong(seed),
+                        C.c_longlong(first_step), int(nsteps), _p(pos), _p(vel), _p(f), _p(e))
+    if rc:
+        raise ValueError("orc_langevin: gamma > 0 and temperature >= 0")
+    return pos, vel, f, e
+
+
+def gauss3(seed, atom, stream):
+    g = np.zeros(3)
+    lib().orc_gauss3(C.c_ulonglong(seed), int(atom), C.c_longlong(stream), _p(g))
+    return g
+
+
 def leapfrog_constrained(system, pos, vel, dt, nsteps, constraints, shake=(1e-5, 30),
                          rattle=(1e-5, 30), cutoff=None, pme=None, bonded=False, last_pos=None):
     """LeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step) as
@@ -237,7 +262,14 @@ def ref_available():
     return os.path.exists(REF_LIB)
 
 
-def build_ref(ref_root="/root/reference"):
+def ref_root():
+    """The ProtoMol 3 source tree the checkers compile from: $PROTOMOL3_REF, else the tree's
+    location in the build container."""
+    return os.environ.get("PROTOMOL3_REF", "/root/reference")
+
+
+def build_ref(ref_root=None):
+    ref_root = ref_root or globals()["ref_root"]()
     if os.path.isdir(ref_root):
         subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", "REF=" + ref_root])
     return ref_available()
@@ -335,6 +367,40 @@ def _ref_md_lib():
         ref_lib()
         _ref_md = C.CDLL(REF_MD_LIB)
     return _ref_md
+
+
+def ref_md_run(system, pos, vel, dt, nsteps, cutoff=None, pme=None, bonded=True, langevin=None,
+               keep=("energies",), cellsize=5.0):
+    """The reference's own LeapfrogIntegrator (or, with langevin = (temperature, gamma_ps,
+    seed), its LangevinLeapfrogIntegrator) stepped by run(1) nsteps times, as ProtoMolApp steps it
+    with outputfreq 1 (oracle/ref_md.cpp).  Returns a dict with the arrays named in ``keep``:
+    energies [nsteps+1, 4] (Coulomb, LJ, bond, angle), pos / vel / forces [nsteps+1, n, 3]; row k
+    is the state after k steps (row 0: the initial forces)."""
+    L = _ref_md_lib()
+    pos = np.ascontiguousarray(pos, np.float64)
+    vel = np.ascontiguousarray(vel, np.float64)
+    r = _ref_input(system, pos, cellsize)
+    c = p = None
+    if cutoff is not None:
+        c = RefCutoff()
+        C.memmove(C.byref(c), C.byref(cutoff), C.sizeof(c))
+    if pme is not None:
+        p = RefPME()
+        p.nx, p.ny, p.nz, p.order = pme.nx, pme.ny, pme.nz, pme.order
+        p.cutoff, p.accuracy, p.alpha, p.real_switch = pme.cutoff, pme.accuracy, pme.alpha, pme.real_switch
+    out = {"energies": np.zeros((nsteps + 1, 4))}
+    for k in ("pos", "vel", "forces"):
+        if k in keep:
+            out[k] = np.zeros((nsteps + 1, system.n, 3))
+    kind, temp, gam, seed = (0, 0.0, 0.0, 0) if langevin is None else (1,) + tuple(langevin)
+    rc = L.ref_md_run(C.byref(r), C.byref(c) if c is not None else None,
+                      C.byref(p) if p is not None else None, int(bonded), int(kind), C.c_double(dt),
+                      C.c_double(temp), C.c_double(gam), int(seed), _p(vel), int(nsteps),
+                      _p(out["energies"]), *[_p(out[k]) if k in out else None
+                                             for k in ("pos", "vel", "forces")])
+    if rc:
+        raise RuntimeError("reference MD run failed")
+    return out
 
 
 def ref_write_dcd(path, frames, timestep=1.0, first_step=0):

@@ -7,6 +7,7 @@
 #include "pm_oracle.h"
 
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -781,6 +782,97 @@ int orc_leapfrog(const orc_system *s, const orc_cutoff_params *cp, const orc_pme
     }
     for (int i = 0; i < n; i++)
       for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h * 0.5 / s->mass[i];
+  }
+  memcpy(energies_out, e, sizeof(e));
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------------------------
+ * Langevin leapfrog (integrator/base/LangevinLeapfrogIntegrator.cpp:23-29 constructor units,
+ * :36-41 doDrift, :44-71 doHalfKick; integrator/StandardIntegrator.cpp:27-37 run): every step is
+ * a half kick, a drift, the forces and a half kick, where a half kick is
+ *   v = v vdt + F fdt / m + g sqrt(2 kB T gamma / m) ndt,
+ *   fdt = (1 - exp(-gamma h / 2)) / gamma, vdt = exp(-gamma h / 2),
+ *   ndt = sqrt((1 - exp(-gamma h)) / (2 gamma)),
+ * gamma in the reference's internal unit (gamma_ps / (1000 INV_TIMEFACTOR)) and h = dt
+ * INV_TIMEFACTOR.  The operations are rounded in the reference's order (Vector3D * scalar,
+ * then / mass).
+ *
+ * The Gaussian numbers g: the reference draws them from one serial generator
+ * (base/MathUtilities.cpp:206-238) in atom order, which a device thread per atom cannot replay.
+ * The device draws them from a counter-based generator keyed by the seed, with the counter (atom,
+ * half-kick index); half kick j of a run (j = 0, 1, ... from the state set) uses stream j.  The
+ * generator is restated here so that runs at T > 0 can be compared too: Philox4x32 with 10 rounds
+ * (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC 2011), 53-bit
+ * uniforms (v + 1/2) 2^-53 in (0, 1), and the Box-Muller transform.  At T = 0 the noise term is
+ * exactly zero whatever g, which is how the reference's own integrator pins this function.
+ * ------------------------------------------------------------------------------------------ */
+static const double BOLTZMANN = 0.001987191; /* base/PMConstants.cpp */
+
+static void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+  for (int r = 0; r < 10; r++) {
+    uint64_t p0 = (uint64_t)M0 * c[0], p1 = (uint64_t)M1 * c[2];
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += W0;
+    k1 += W1;
+  }
+}
+
+static double u01(uint32_t a, uint32_t b) {
+  uint64_t v = (((uint64_t)a << 21) ^ (uint64_t)b) & ((1ull << 53) - 1);
+  return ((double)v + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+void orc_gauss3(unsigned long long seed, int atom, long long stream, double g[3]) {
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  uint32_t c0[4] = {(uint32_t)atom, (uint32_t)stream, (uint32_t)((uint64_t)stream >> 32), 0u};
+  uint32_t c1[4] = {(uint32_t)atom, (uint32_t)stream, (uint32_t)((uint64_t)stream >> 32), 1u};
+  philox10(c0, k0, k1);
+  philox10(c1, k0, k1);
+  double u1 = u01(c0[0], c0[1]), u2 = u01(c0[2], c0[3]), u3 = u01(c1[0], c1[1]), u4 = u01(c1[2], c1[3]);
+  double r1 = sqrt(-2.0 * log(u1)), r2 = sqrt(-2.0 * log(u3));
+  g[0] = r1 * cos(2.0 * M_PI * u2);
+  g[1] = r1 * sin(2.0 * M_PI * u2);
+  g[2] = r2 * cos(2.0 * M_PI * u4);
+}
+
+static void langevin_half_kick(const orc_system *s, const double *f, double h, double gamma,
+                               double kT, unsigned long long seed, long long stream, double *vel) {
+  const double fdt = (1.0 - exp(-0.5 * gamma * h)) / gamma;
+  const double vdt = exp(-0.5 * gamma * h);
+  const double ndt = sqrt((1.0 - exp(-gamma * h)) / (2.0 * gamma));
+  const double fc = 2 * kT * gamma;
+  for (int i = 0; i < s->n; i++) {
+    double g[3], m = s->mass[i], sq = sqrt(fc / m);
+    orc_gauss3(seed, i, stream, g);
+    for (int q = 0; q < 3; q++)
+      vel[3 * i + q] = vel[3 * i + q] * vdt + f[3 * i + q] * fdt / m + g[q] * sq * ndt;
+  }
+}
+
+int orc_langevin(const orc_system *s, const orc_cutoff_params *cp, const orc_pme_params *pme,
+                 int do_bonded, double dt_fs, double temperature, double gamma_ps,
+                 unsigned long long seed, long long first_step, int nsteps, double *pos, double *vel,
+                 double *forces_out, double *energies_out) {
+  double *f = forces_out, e[ORC_E_COUNT];
+  const double h = dt_fs * INV_TIMEFACTOR;
+  const double gamma = gamma_ps / (1000 * INV_TIMEFACTOR);
+  const double kT = BOLTZMANN * temperature;
+  if (!(gamma > 0) || temperature < 0) return 1;
+  all_forces(s, cp, pme, do_bonded, pos, f, e);
+  for (int st = 0; st < nsteps; st++) {
+    long long j = 2 * (first_step + st);
+    langevin_half_kick(s, f, h, gamma, kT, seed, j, vel);
+    for (int i = 0; i < 3 * s->n; i++) pos[i] += vel[i] * h;
+    all_forces(s, cp, pme, do_bonded, pos, f, e);
+    langevin_half_kick(s, f, h, gamma, kT, seed, j + 1, vel);
   }
   memcpy(energies_out, e, sizeof(e));
   return 0;

@@ -81,6 +81,19 @@ int orc_leapfrog(const orc_system *s, const orc_cutoff_params *cp, const orc_pme
                  int do_bonded, double dt_fs, int nsteps, double *pos, double *vel,
                  double *forces_out, double *energies_out);
 
+/* LangevinLeapfrogIntegrator run(nsteps) (integrator/base/LangevinLeapfrogIntegrator.cpp:44-71
+ * through integrator/StandardIntegrator.cpp:27-37) with bonded + cutoff (+ optional PME) forces,
+ * temperature in K and gamma in 1/ps as the reference's parameters.  The Gaussian numbers are the
+ * device integrator's counter-based stream (orc_gauss3), first_step = steps already taken since
+ * the state was set (half kick j uses stream j).  pos/vel updated in place; forces_out and
+ * energies_out as orc_leapfrog. */
+int orc_langevin(const orc_system *s, const orc_cutoff_params *cp, const orc_pme_params *pme,
+                 int do_bonded, double dt_fs, double temperature, double gamma_ps,
+                 unsigned long long seed, long long first_step, int nsteps, double *pos, double *vel,
+                 double *forces_out, double *energies_out);
+/* Three standard normals of the device's Langevin noise for (atom, stream). */
+void orc_gauss3(unsigned long long seed, int atom, long long stream, double g[3]);
+
 /* SHAKE / RATTLE bond constraints (modifier/ModifierShake.cpp, ModifierRattle.cpp): the
  * constraint list in the reference's order (topology/TopologyUtilities.cpp:695-775).  A sweep
  * applies every constraint in list order (Gauss-Seidel); sweeps repeat while the mean error over

@@ -88,9 +88,9 @@ static SystemForce *with_coul(const ref_cutoff *c, S sa) {
   }
 }
 
-extern "C" int ref_cutoff_eval(const ref_input *in, const ref_cutoff *c, double *forces,
-                               double *energies, double *virial) {
-  Topo *t = make_topo(in);
+// The reference's cutoff force for c (NULL when c selects no potential); also used by the MD
+// harness (ref_md.cpp), which puts it in a ForceGroup.
+SystemForce *ref_new_cutoff_force(const ref_cutoff *c) {
   SystemForce *f = 0;
   if (c->do_lj && c->do_coul) {
     switch (c->lj_switch) {
@@ -115,15 +115,21 @@ extern "C" int ref_cutoff_eval(const ref_input *in, const ref_cutoff *c, double 
     else
       f = make_one<CutoffSwitchingFunction, CoulombForce>(c->coul_cutoff, CutoffSwitchingFunction(c->coul_cutoff));
   }
+  return f;
+}
+
+extern "C" int ref_cutoff_eval(const ref_input *in, const ref_cutoff *c, double *forces,
+                               double *energies, double *virial) {
+  Topo *t = make_topo(in);
+  SystemForce *f = ref_new_cutoff_force(c);
   if (f) run_force(f, t, in, forces, energies, virial);
   delete f;
   delete t;
   return 0;
 }
 
-extern "C" int ref_pme_eval(const ref_input *in, const ref_pme *p, double *forces,
-                            double *energies, double *virial) {
-  Topo *t = make_topo(in);
+// The reference's PME force for p (with the real, reciprocal and correction terms).
+SystemForce *ref_new_pme_force(const ref_pme *p) {
   SystemForce *f;
   if (p->real_switch == 1)
     f = new NonbondedPMEwaldSystemForce<PBC, CubicCellManager, true, true, true, BSpline,
@@ -133,6 +139,13 @@ extern "C" int ref_pme_eval(const ref_input *in, const ref_pme *p, double *force
     f = new NonbondedPMEwaldSystemForce<PBC, CubicCellManager, true, true, true, BSpline,
                                         CutoffSwitchingFunction>(p->nx, p->ny, p->nz, p->order,
                                                                  p->cutoff, p->accuracy, p->alpha, 3.0);
+  return f;
+}
+
+extern "C" int ref_pme_eval(const ref_input *in, const ref_pme *p, double *forces,
+                            double *energies, double *virial) {
+  Topo *t = make_topo(in);
+  SystemForce *f = ref_new_pme_force(p);
   run_force(f, t, in, forces, energies, virial);
   delete f;
   delete t;

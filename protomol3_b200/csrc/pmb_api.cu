@@ -8,6 +8,7 @@
 //     (topology/PeriodicBoundaryConditions.cpp:79-106);
 //   * grid tables exp(-pi^2 m^2/alpha^2) and the B-spline moduli (Grid.h:498-600).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -210,6 +211,12 @@ struct pmb_system {
   double *d_fout = nullptr, *d_eout = nullptr;
   double *h_fout = nullptr, *h_eout = nullptr;  // pinned
   int *h_status = nullptr;                      // pinned
+  // host-pointer evaluations: the device->host copies go in EVAL_CHUNKS pieces, each followed by
+  // an event, so that the host adds one piece while the next is in flight
+  static constexpr int EVAL_CHUNKS = 4;
+  cudaEvent_t ev_out[EVAL_CHUNKS + 1] = {};
+  double eval_ms[3] = {0.0, 0.0, 0.0};  // last pmb_evaluate: enqueue, wait, accumulate (host ms)
+  bool last_used_list = false;          // the last evaluation ran the list kernels
   // neighbour list
   bool nb_ready = false;
   double nb_cutoff = 0.0;    // radius the list storage is sized for
@@ -241,6 +248,8 @@ struct pmb_system {
     return s;
   }
   ~pmb_system() {
+    for (cudaEvent_t e : ev_out)
+      if (e) cudaEventDestroy(e);
     if (flush_buf) cudaFree(flush_buf);
     if (h_fout) cudaFreeHost(h_fout);
     if (h_eout) cudaFreeHost(h_eout);
@@ -452,6 +461,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   bool need_pme_slots = false;
   for (int i = 0; i < n; i++) need_pme_slots |= fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal;
   const bool need_list = !jobs.empty() || need_pme_slots;
+  s->last_used_list = need_list;
   // PME, exclusion corrections and bonded terms run on the side stream beside the list build and
   // the pair kernel (every sum is an integer atomic, so the interleaving does not change a bit):
   // the corrections and bonded terms from the start, the PME chain once this step's slot records
@@ -556,15 +566,23 @@ void add_const(pmb_force *const *fs, int n, int nbox, int virial, double *e) {
   }
 }
 
+// The status words as they were copied to s->h_status: capacity before non-finite positions
+// (a retry with larger lists comes first).  Clears the device words that were set.
+int status_code(pmb_system *s) {
+  if (s->h_status[0] || s->h_status[1] || s->h_status[2]) {
+    cudaMemsetAsync(s->nb.status, 0, 4 * sizeof(int), s->stream);
+    if (s->h_status[0] || s->h_status[1])
+      return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded (atoms denser than expected)");
+    return fail(PMB_ERR_NUMERIC, "non-finite position");
+  }
+  return PMB_OK;
+}
+
 int check_status(pmb_system *s) {
   if (!s->nb_ready) return PMB_OK;
   CK(cudaMemcpyAsync(s->h_status, s->nb.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  if (s->h_status[0] || s->h_status[1]) {
-    cudaMemsetAsync(s->nb.status, 0, 4 * sizeof(int), s->stream);
-    return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded (atoms denser than expected)");
-  }
-  return PMB_OK;
+  return status_code(s);
 }
 
 int grow_and_retry_needed(pmb_system *s) {
@@ -812,6 +830,12 @@ int pmb_system_list_builds(pmb_system *s, long long *n) {
   CK(cudaMemcpyAsync(&v, s->nb.ctl + 4, sizeof(v), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   *n = (long long)v;
+  return PMB_OK;
+}
+
+int pmb_system_evaluate_times(const pmb_system *s, double ms[3]) {
+  if (!s || !ms) return fail(PMB_ERR_ARG, "null argument");
+  for (int k = 0; k < 3; k++) ms[k] = s->eval_ms[k];
   return PMB_OK;
 }
 
@@ -1192,9 +1216,9 @@ int pmb_system_set_vacuum(pmb_system *s, int on) {
 
 int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, double *forces,
                  double *energies, int virial) {
+  using clk = std::chrono::steady_clock;
+  const clk::time_point t0 = clk::now();
   if (!s || !pos) return fail(PMB_ERR_ARG, "null argument");
-  for (int i = 0; i < 3 * s->natoms; i++)
-    if (!std::isfinite(pos[i])) return fail(PMB_ERR_NUMERIC, "non-finite position");
   if (s->vacuum) {
     // the periodic box stands in for vacuum only while no two atoms of a box are half an edge
     // apart: then every minimal-image difference is the plain difference
@@ -1211,21 +1235,53 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
       }
   }
   cudaStream_t st = s->stream;
+  if (!s->ev_out[0])
+    for (cudaEvent_t &e : s->ev_out) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  const long long nf = 3LL * s->natoms;
+  const long long chunk = (nf + pmb_system::EVAL_CHUNKS - 1) / pmb_system::EVAL_CHUNKS;
   for (int attempt = 0; attempt < 3; attempt++) {
-    CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
     s->have_pos = true;
     int rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(s->h_fout, s->d_fout, sizeof(double) * 3 * s->natoms, cudaMemcpyDeviceToHost, st));
+    // status and energies first, then the forces piece by piece
+    if (s->nb_ready) CK(cudaMemcpyAsync(s->h_status, s->nb.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(s->h_eout, s->d_eout, sizeof(double) * s->nbox * ACC_PER_BOX, cudaMemcpyDeviceToHost, st));
-    rc = check_status(s);
+    CK(cudaEventRecord(s->ev_out[0], st));
+    for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
+      const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
+      if (b1 > b0)
+        CK(cudaMemcpyAsync(s->h_fout + b0, s->d_fout + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost, st));
+      CK(cudaEventRecord(s->ev_out[c + 1], st));
+    }
+    const clk::time_point t1 = clk::now();
+    CK(cudaEventSynchronize(s->ev_out[0]));
+    const clk::time_point t2 = clk::now();
+    rc = s->nb_ready && s->last_used_list ? status_code(s) : PMB_OK;
+    if (rc == PMB_OK && !s->last_used_list)  // no list kernel looked at the positions
+      for (long long i = 0; i < nf; i++)
+        if (!std::isfinite(pos[i])) {
+          rc = fail(PMB_ERR_NUMERIC, "non-finite position");
+          break;
+        }
+    if (rc) CK(cudaStreamSynchronize(st));  // the copies in flight land before a retry or return
     if (rc == PMB_ERR_CAPACITY) {
       if (grow_and_retry_needed(s)) return PMB_ERR_CUDA;
       continue;
     }
     if (rc) return rc;
-    if (forces)
-      for (int i = 0; i < 3 * s->natoms; i++) forces[i] += s->h_fout[i];
+    for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
+      CK(cudaEventSynchronize(s->ev_out[c + 1]));
+      if (!forces) continue;
+      const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
+      double *__restrict__ dst = forces;
+      const double *__restrict__ src = s->h_fout;
+      for (long long i = b0; i < b1; i++) dst[i] += src[i];
+    }
+    const clk::time_point t3 = clk::now();
+    s->eval_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    s->eval_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    s->eval_ms[2] = std::chrono::duration<double, std::milli>(t3 - t2).count();
     if (energies) {
       add_const(fs, n, s->nbox, virial, s->h_eout);
       for (int b = 0; b < s->nbox; b++) {

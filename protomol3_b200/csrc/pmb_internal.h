@@ -43,7 +43,7 @@ struct NbListDev {
   int *tile_blk;               // [tile_cap] block of each tile
   int *tile_k;                 // [tile_cap] tile index within the block
   int tile_cap;
-  int *status;                 // [4] overflow flags
+  int *status;                 // [4]: list / tile overflow, non-finite position, unused
   // per slot
   int nslot;
   int *slot_orig;              // [nslot] original atom index or -1

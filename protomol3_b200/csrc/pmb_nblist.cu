@@ -140,12 +140,16 @@ __global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out, c
 // ---------------------------------------------------------------- binning and sort
 // Rebuild decision: max |x - x_ref|^2 over all atoms (last block decides, no host round trip);
 // ctl = {max displacement^2 as float bits, rebuild flag, finished blocks, forced rebuild}.
+// It reads every position of every evaluation, so it also raises status[2] for a non-finite
+// one (the host reports PMB_ERR_NUMERIC; every later kernel maps such a position to an in-range
+// cell and grid index, so nothing reads out of bounds meanwhile).
 __global__ void k_disp_check(SystemDev s, NbListDev nb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
   if (i < s.natoms) {
-    double dx = s.pos[3 * i] - nb.xref[3 * i], dy = s.pos[3 * i + 1] - nb.xref[3 * i + 1],
-           dz = s.pos[3 * i + 2] - nb.xref[3 * i + 2];
+    const double x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
+    if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicExch(&nb.status[2], 1);
+    double dx = x - nb.xref[3 * i], dy = y - nb.xref[3 * i + 1], dz = z - nb.xref[3 * i + 2];
     double r2 = dx * dx + dy * dy + dz * dz;
     d2 = r2 < 3.0e38 ? (float)r2 : 3.0e38f;
     if (!(d2 >= 0.f)) d2 = 3.0e38f;  // NaN positions force a rebuild

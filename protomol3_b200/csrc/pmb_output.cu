@@ -92,7 +92,7 @@ struct pmb_traj {
   bool stop = false, started = false;
   int err = PMB_OK;
   std::string err_msg;
-  int device = -1;
+  int device = -1;  // the device of the first frame: the staging buffers and copy stream live there
 
   template <typename T>
   void put(T v) {
@@ -288,6 +288,12 @@ int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
   int rc = md_frame_source(md, &d_pos, &n, &st, &dev);
   if (rc) return rc;
   if (n != t->n_atoms) return set_error("trajectory atom count differs from the MD run's"), PMB_ERR_ARG;
+  // the staging buffers and the copy stream belong to the device of the first frame (also when
+  // that attempt failed half way and this call retries it)
+  if (t->device >= 0 && dev != t->device)
+    return set_error("trajectory frames come from device " + std::to_string(t->device) +
+                     "; this MD run is on device " + std::to_string(dev)),
+           PMB_ERR_ARG;
   if (!t->started) {
     t->device = dev;
     const size_t bytes = sizeof(double) * 3 * (size_t)n;

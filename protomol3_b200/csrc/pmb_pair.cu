@@ -29,6 +29,8 @@
 //   * mixed: positions as 32-bit fractional fixed point per box edge, so the minimal image is the
 //     wrap-around of an int32 difference and the pair vector keeps full FP32 precision however
 //     large the box; FP32 arithmetic with MUFU rsqrt/exp2/rcp.
+#include <cuda.h>
+
 #include <mutex>
 #include <type_traits>
 
@@ -1060,20 +1062,54 @@ __global__ void __launch_bounds__(AP_THREADS)
 
 }  // namespace
 
+// Identity of the calling thread's current CUDA context (cuCtxGetId, unique over the process's
+// life even when a context is destroyed and another gets its handle), through the driver entry
+// points the runtime hands out, so the library does not link the driver library itself.  0 when
+// it cannot be had.
+static unsigned long long current_context_id() {
+  using get_current_t = CUresult (*)(CUcontext *);
+  using get_id_t = CUresult (*)(CUcontext, unsigned long long *);
+  static get_current_t get_current = nullptr;
+  static get_id_t get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void *f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<get_current_t>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<get_id_t>(f);
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
+
+// The device address of the static scratch in the current context, looked up once per device
+// and context: an address belongs to the context it was taken in, so a context made after
+// cudaDeviceReset gets its own lookup.
 cudaError_t static_eacc_address(long long **out) {
   constexpr int MAX_DEV = 64;
   static std::mutex mu;
   static long long *addr[MAX_DEV] = {};
+  static unsigned long long ctx[MAX_DEV] = {};
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+  const unsigned long long id = current_context_id();
   std::lock_guard<std::mutex> g(mu);
-  if (!addr[dev]) {
+  if (!addr[dev] || id != ctx[dev]) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_eacc);
     if (e != cudaSuccess) return e;
     addr[dev] = static_cast<long long *>(p);
+    ctx[dev] = id;
   }
   *out = addr[dev];
   return cudaSuccess;

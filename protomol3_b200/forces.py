@@ -125,6 +125,13 @@ class Topology:
         L.check(L.lib().pmb_system_list_builds(self.system(), C.byref(n)))
         return n.value
 
+    def evaluate_times(self):
+        """Host time (ms) of the last host-pointer evaluation: enqueue, wait for the device's
+        first results, accumulation into the caller's arrays."""
+        t = np.zeros(3)
+        L.check(L.lib().pmb_system_evaluate_times(self.system(), _p(t)))
+        return {"enqueue": t[0], "wait_device": t[1], "accumulate": t[2]}
+
     def set_stream(self, stream_handle):
         L.check(L.lib().pmb_system_set_stream(self.system(), C.c_void_p(stream_handle)))
 

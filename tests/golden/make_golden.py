@@ -3,7 +3,7 @@
 Run once in a container that holds the ProtoMol 3 source tree (read as text only; nothing of
 the reference is executed):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <ProtoMol 3 tree>]
 
 It writes two small ``.npz`` fixtures next to this script:
 
@@ -205,8 +205,11 @@ def read_xyzbin(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PROTOMOL3_REF"),
+                    help="ProtoMol 3 source tree (default: $PROTOMOL3_REF)")
     ref = ap.parse_args().ref
+    if not ref:
+        raise SystemExit("pass --ref <ProtoMol 3 tree> or set PROTOMOL3_REF")
 
     d = os.path.join(ref, "test/tests/data")
     e = os.path.join(ref, "test/tests/expected")

@@ -4,7 +4,7 @@ Run in a container that holds the ProtoMol 3 source tree, after ``make -C oracle
 compiled the reference's cutoff forces with VacuumBoundaryConditions in place
 (``oracle/_ref/libpmref_md.so``, harness ``oracle/ref_vacuum.cpp``):
 
-    python tests/golden/make_golden_vacuum.py [--ref /root/reference]
+    python tests/golden/make_golden_vacuum.py [--ref <ProtoMol 3 tree>]
 
 It writes ``vacuum_ref.npz`` next to this script with two inputs and the reference's forces and
 energies for each force set:
@@ -53,8 +53,11 @@ def droplet():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PROTOMOL3_REF"),
+                    help="ProtoMol 3 source tree (default: $PROTOMOL3_REF)")
     ref = ap.parse_args().ref
+    if not ref:
+        raise SystemExit("pass --ref <ProtoMol 3 tree> or set PROTOMOL3_REF")
     if not O.ref_md_available():
         raise SystemExit("oracle/_ref/libpmref_md.so is missing: run make -C oracle ref first")
     d = os.path.join(ref, "protomol-test/ConfigTests/data")

@@ -49,7 +49,13 @@ def test_pme_through_the_reference_factory(precision):
     assert made.startswith(PME)
     fr, er, vr = O.ref_evaluate(s, b["pos"], pme=O.pme_params((20, 20, 20), 8.0), virial=True)
     assert _rel(f, fr) < TOL[precision]
-    assert abs(e[0] - er[0]) < TOL[precision] * 1e3 * abs(er[0]) + 1e-6  # Coulomb: cancelling terms
+    # Coulomb is real + reciprocal + intra-molecular + self, terms that cancel (here 28 + 351 +
+    # 16,246 - 16,663 = -39): the real and reciprocal terms are computed in the tested precision
+    # and judged against their magnitudes; the correction and self terms are FP64 in both
+    # precisions (1e-12 of theirs); plus the fixed-point resolution
+    _, _, _, info = O.evaluate(s, b["pos"], pme=O.pme_params((20, 20, 20), 8.0))
+    t = np.abs(info["terms"])
+    assert abs(e[0] - er[0]) <= TOL[precision] * (t[0] + t[1]) + 1e-12 * (t[2] + t[3]) + s.n * 2.0 ** -31
     np.testing.assert_allclose(v, vr, rtol=0, atol=10 * TOL[precision] * np.abs(vr).max() + 1e-6)
 
 

@@ -200,17 +200,78 @@ def test_leapfrog_matches_oracle_pme(graph):
     assert np.abs(vel - vo).max() < 1e-8
 
 
-def test_config2_size_mixed_vs_oracle():
-    """The full 98,304-atom box (32,768 waters, 96^3 grid, rc 10, LJ C2 8->10)."""
+@pytest.fixture(scope="module")
+def config2():
+    """The full 98,304-atom box (32,768 waters, 96^3 grid, rc 10, LJ C2 8->10) and the oracle's
+    forces, energies and terms on it (computed once for both precisions)."""
     b = W.water_box(32768, seed=1234)
-    lj = F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0))
-    pme = F.NonbondedPMEwaldSystemForce((96, 96, 96), 10.0)
-    f, e, topo = gpu_eval(b, [lj, pme], "mixed")
     fo, eo, _, info = O.evaluate(O.System(b), b["pos"], cutoff=O.cutoff_params(lj=("C2", 8.0, 10.0)),
                                  pme=O.pme_params((96, 96, 96), 10.0))
-    assert rel_rms(f, fo) < 1e-5
+    return b, fo, eo, info
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config2_size_vs_oracle(config2, precision):
+    """The plain FP64 path (the drop-in) and the mixed path at full size, against the oracle."""
+    b, fo, eo, info = config2
+    lj = F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0))
+    pme = F.NonbondedPMEwaldSystemForce((96, 96, 96), 10.0)
+    f, e, topo = gpu_eval(b, [lj, pme], precision)
+    assert rel_rms(f, fo) < TOL[precision]
     assert energy_ok(e[F.ScalarStructure.COULOMB], eo[O.E_COULOMB],
-                     abs(info["terms"][0]) + abs(info["terms"][1]), "mixed", topo.n_atoms)
+                     abs(info["terms"][0]) + abs(info["terms"][1]), precision, topo.n_atoms)
+    assert energy_ok(e[F.ScalarStructure.LENNARDJONES], eo[O.E_LJ], abs(eo[O.E_LJ]), precision,
+                     topo.n_atoms)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_ensemble_subset_vs_oracle(precision):
+    """Boxes of the ensemble workload (LJ C2 7.5 -> 9 A, PME rc 9 A at ~1 A grid spacing,
+    order 4, bonded) advanced as one batched system, each compared with the oracle evaluated on
+    that box alone.  Four of the six are under twice the cutoff (100-190 waters, 14.4-17.8 A),
+    where the reference's cutoff LJ takes a single minimal image (force/OneAtomPair.h:55-57) and
+    PME's real term sums lattice images."""
+    boxes = [W.water_box(n, seed=60 + n) for n in (100, 120, 150, 190, 450, 1300)]
+    grids = [W.pme_grid_for(b["box"][0]) for b in boxes]
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", 7.5, 9.0)),
+          F.NonbondedPMEwaldSystemForce((0, 0, 0), 9.0, box_grids=[[g] * 3 for g in grids]),
+          F.BondedSystemForce()]
+    fb, eb, topo = gpu_eval(boxes, fl, precision, virial=True)
+    off = 0
+    for k, (b, g) in enumerate(zip(boxes, grids)):
+        n = len(b["charge"])
+        fo, eo, vo, info = O.evaluate(O.System(b), b["pos"], cutoff=O.cutoff_params(lj=("C2", 7.5, 9.0)),
+                                      pme=O.pme_params((g,) * 3, 9.0), bonded=True, virial=True)
+        assert rel_rms(fb[off:off + n], fo) < TOL[precision], k
+        assert energy_ok(eb.table[k, F.ScalarStructure.LENNARDJONES], eo[O.E_LJ], abs(eo[O.E_LJ]),
+                         precision, n), k
+        assert energy_ok(eb.table[k, F.ScalarStructure.COULOMB], eo[O.E_COULOMB],
+                         abs(info["terms"][0]) + abs(info["terms"][1]), precision, n), k
+        for slot, j in ((F.ScalarStructure.BOND, O.E_BOND), (F.ScalarStructure.ANGLE, O.E_ANGLE)):
+            assert abs(eb.table[k, slot] - eo[j]) <= 1e-9 * abs(eo[j]) + n * 2.0 ** -31, k
+        np.testing.assert_allclose(eb.virial(k).ravel(), vo, rtol=0,
+                                   atol=10 * TOL[precision] * np.abs(vo).max(), err_msg=str(k))
+        off += n
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pme_charged_box_vs_oracle(precision):
+    """A box with a net charge of -0.834 e: the charged-system energy
+    -pi (sum q)^2 / (2 V alpha^2) of NonbondedPMEwaldSystemForce.h:555-575 enters the Coulomb
+    energy (oracle pinned to the compiled reference in tests/test_oracle.py)."""
+    b = dict(W.water_box(216, seed=13))
+    q = b["charge"].copy()
+    q[1] = q[2] = 0.0
+    b["charge"] = q
+    pme = F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0)
+    f, e, topo = gpu_eval(b, [pme], precision, virial=True)
+    fo, eo, vo, info = O.evaluate(O.System(b), b["pos"], pme=O.pme_params((20, 20, 20), 8.0), virial=True)
+    # the charged term is present: -pi (sum q)^2 / (2 V alpha^2) = -0.36 kcal/mol here
+    assert info["terms"][4] < -0.3
+    assert rel_rms(f, fo) < TOL[precision]
+    assert energy_ok(e[F.ScalarStructure.COULOMB], eo[O.E_COULOMB],
+                     abs(info["terms"][0]) + abs(info["terms"][1]), precision, topo.n_atoms)
+    np.testing.assert_allclose(e.virial().ravel(), vo, rtol=0, atol=TOL[precision] * np.abs(vo).max() * 10)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -253,3 +314,36 @@ def test_profile_needs_positions():
     for stage in ("nblist", "pair", "pme_spread", "pme_fft", "pme_gather", "bonded"):
         assert stage in st and st[stage] >= 0.0
 
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_non_finite_position_is_an_error_and_changes_nothing(precision):
+    """A NaN or infinite position gives PMB_ERR_NUMERIC and leaves the caller's forces and
+    energies as they were, whether the list kernels saw it on the device (pair and PME forces) or
+    the host did (bonded terms alone, no list); the next finite evaluation is right again."""
+    from protomol3_b200 import _lib as L
+    b = W.water_box(216, seed=4)
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
+          F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0), F.BondedSystemForce()]
+    for forces, bad in ((fl, np.nan), (fl, np.inf), ([F.BondedSystemForce()], -np.inf)):
+        topo = F.Topology(b, precision)
+        pos = b["pos"].copy()
+        pos[5, 1] = bad
+        frc = np.full((topo.n_atoms, 3), 7.0)
+        e = F.ScalarStructure(1)
+        with pytest.raises(L.PMBError) as err:
+            F.evaluate_all(topo, forces, pos, frc, e)
+        assert err.value.code == L.PMB_ERR_NUMERIC
+        assert (frc == 7.0).all() and (e.table == 0).all()
+        frc[:] = 0.0
+        F.evaluate_all(topo, forces, b["pos"], frc, e)
+        fo = np.zeros_like(frc)
+        for fc in forces:
+            if isinstance(fc, F.BondedSystemForce):
+                fo += O.evaluate(O.System(b), b["pos"], bonded=True)[0]
+            elif isinstance(fc, F.NonbondedCutoffSystemForce):
+                fo += O.evaluate(O.System(b), b["pos"], cutoff=O.cutoff_params(lj=("C2", 7.0, 8.0)))[0]
+            else:
+                fo += O.evaluate(O.System(b), b["pos"], pme=O.pme_params((20, 20, 20), 8.0))[0]
+        assert rel_rms(frc, fo) < TOL[precision]
+        topo.close()

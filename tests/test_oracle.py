@@ -95,3 +95,60 @@ def test_oracle_matches_reference_cutoff():
     fr, er, vr = O.ref_evaluate(s, b["pos"], cutoff=cp, bonded=True, virial=True)
     assert np.abs(f - fr).max() < 1e-10
     np.testing.assert_allclose(e, er, rtol=1e-12, atol=1e-9)
+
+
+@needs_ref
+@pytest.mark.parametrize("nw", [100, 150, 190])
+def test_oracle_matches_reference_small_box_lj(nw):
+    """Boxes whose edge is under twice the cutoff (14.4-17.2 A against 2 x 9 A; about 5% of the
+    ensemble workload's boxes): the reference's cutoff LJ takes one minimal image per pair
+    (force/OneAtomPair.h:55-57) while its PME real term sums lattice images; the oracle follows
+    both."""
+    b = W.water_box(nw, seed=50 + nw)
+    assert b["box"][0] < 18.0
+    s = O.System(b)
+    cp = O.cutoff_params(lj=("C2", 7.5, 9.0))
+    grid = (W.pme_grid_for(b["box"][0]),) * 3
+    pm = O.pme_params(grid, 9.0)
+    f, e, v, _ = O.evaluate(s, b["pos"], cutoff=cp, pme=pm, bonded=True, virial=True)
+    fr, er, vr = O.ref_evaluate(s, b["pos"], cutoff=cp, pme=pm, bonded=True, virial=True)
+    assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) < 1e-12
+    np.testing.assert_allclose(e, er, rtol=1e-12, atol=1e-9)
+    assert np.abs(v - vr).max() < 1e-8 * np.abs(vr).max()
+
+
+def charged_box(nw=216, seed=13):
+    """A water box with a net charge: the first water's hydrogens lose their charge
+    (total charge -0.834 e)."""
+    b = dict(W.water_box(nw, seed=seed))
+    q = b["charge"].copy()
+    q[1] = q[2] = 0.0
+    b["charge"] = q
+    return b
+
+
+def test_charged_box_charged_term():
+    """The charged-system term of NonbondedPMEwaldSystemForce::initialize
+    (mdl/interface/force/nonbonded/NonbondedPMEwaldSystemForce.h:555-575): -pi (sum q)^2 /
+    (2 V alpha^2), present only when |sum q * 0.00268283| > 1e-5."""
+    b = charged_box()
+    s = O.System(b)
+    pm = O.pme_params((20, 20, 20), 8.0)
+    _, _, _, info = O.evaluate(s, b["pos"], pme=pm)
+    qs, a, V = b["charge"].sum(), info["alpha"], np.prod(b["box"])
+    assert abs(qs * 0.00268283) > 1e-5
+    assert info["terms"][4] == pytest.approx(-np.pi * qs * qs / (2 * V * a * a), rel=1e-14)
+    _, _, _, info0 = O.evaluate(O.System(W.water_box(216, seed=13)), b["pos"], pme=pm)
+    assert info0["terms"][4] == 0.0
+
+
+@needs_ref
+def test_oracle_matches_reference_charged_box():
+    b = charged_box()
+    s = O.System(b)
+    pm = O.pme_params((20, 20, 20), 8.0)
+    f, e, v, _ = O.evaluate(s, b["pos"], pme=pm, virial=True)
+    fr, er, vr = O.ref_evaluate(s, b["pos"], pme=pm, virial=True)
+    assert np.sqrt(((f - fr) ** 2).sum() / (fr ** 2).sum()) < 1e-12
+    assert abs(e[0] - er[0]) < 1e-12 * abs(er[0])
+    assert np.abs(v - vr).max() < 1e-8

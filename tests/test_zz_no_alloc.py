@@ -118,3 +118,42 @@ def test_static_rejects_pme():
     f = torch.zeros((topo.n_atoms, 3), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     assert L.lib().pmb_cutoff_evaluate_static(h, _ptr(pos), _ptr(f), None, 0) == L.PMB_ERR_UNSUPPORTED
+
+
+def test_static_first_on_a_fresh_system_and_allocates_nothing():
+    """The use the entry point exists for: the first evaluation of a newly made system, with no
+    neighbour list allocated yet.  It matches pmb_evaluate_device called afterwards, and once one
+    call has run, further calls leave the device's free memory exactly as it was."""
+    import torch
+    boxes, force = _case("two_boxes_lj_cutoff_coulomb_c2")
+    topo = F.Topology(boxes, "fp64")
+    h = force.handle(topo)
+    n, nb = topo.n_atoms, topo.n_boxes
+    dev = torch.device("cuda")
+    pos = torch.tensor(topo.positions(), dtype=torch.float64, device=dev)
+    f = torch.full((n, 3), float("nan"), dtype=torch.float64, device=dev)
+    e = torch.full((nb * L.E_STRIDE,), float("nan"), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    L.check(L.lib().pmb_cutoff_evaluate_static(h, _ptr(pos), _ptr(f), _ptr(e), 1))
+    torch.cuda.synchronize()
+    fa, ea = f.cpu().numpy(), e.cpu().numpy().reshape(nb, L.E_STRIDE)
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        L.check(L.lib().pmb_cutoff_evaluate_static(h, _ptr(pos), _ptr(f), _ptr(e), 1))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert np.array_equal(f.cpu().numpy(), fa)
+    f_ref = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    e_ref = torch.zeros(nb * L.E_STRIDE, dtype=torch.float64, device=dev)
+    fs = (C.c_void_p * 1)(h)
+    L.check(L.lib().pmb_evaluate_device(topo.system(), fs, 1, _ptr(pos), _ptr(f_ref), _ptr(e_ref), 1))
+    if L.lib().pmb_system_check(topo.system()) == L.PMB_ERR_CAPACITY:
+        L.check(L.lib().pmb_evaluate_device(topo.system(), fs, 1, _ptr(pos), _ptr(f_ref), _ptr(e_ref), 1))
+        L.check(L.lib().pmb_system_check(topo.system()))
+    torch.cuda.synchronize()
+    fr, er = f_ref.cpu().numpy(), e_ref.cpu().numpy().reshape(nb, L.E_STRIDE)
+    assert _rel_rms(fa, fr) < TOL["fp64"]
+    for b in range(nb):
+        nab = len(boxes[b]["charge"])
+        for slot in (L.E_COULOMB, L.E_LJ):
+            assert abs(ea[b, slot] - er[b, slot]) <= TOL["fp64"] * abs(er[b, slot]) + nab * 2.0 ** -31
