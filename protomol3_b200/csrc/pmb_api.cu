@@ -1376,6 +1376,7 @@ struct pmb_md {
   double *d_vel = nullptr, *d_kin = nullptr;
   long long *d_step = nullptr;
   bool have_state = false, use_graph = true;
+  long long steps = 0;  // steps since the state was set (a checkpoint's step count)
   cudaGraphExec_t g_first = nullptr, g_next = nullptr;
   int kernels_per_step = 0;
   std::vector<double> h_e, h_k;
@@ -1646,30 +1647,72 @@ int pmb_md_constraint_sweeps(pmb_md *m, int *shake_sweeps, int *rattle_sweeps) {
 }
 
 int pmb_md_set_state(pmb_md *m, const double *pos, const double *vel) {
+  return pmb_md_set_checkpoint(m, pos, vel, nullptr, 0);
+}
+
+int pmb_md_get_checkpoint(pmb_md *m, double *pos, double *vel, double *list_reference, long long *step) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  if (!m->have_state) return fail(PMB_ERR_STATE, "pmb_md_set_state must come first");
+  pmb_system *s = m->sys;
+  const size_t bytes = sizeof(double) * 3 * (size_t)s->natoms;
+  if (pos) CK(cudaMemcpyAsync(pos, s->d_pos, bytes, cudaMemcpyDeviceToHost, s->stream));
+  if (vel) CK(cudaMemcpyAsync(vel, m->d_vel, bytes, cudaMemcpyDeviceToHost, s->stream));
+  // the list's reference positions (those of its last build); a run without a list has none,
+  // and its positions stand in
+  if (list_reference)
+    CK(cudaMemcpyAsync(list_reference, s->nb_ready ? s->nb.xref : s->d_pos, bytes, cudaMemcpyDeviceToHost,
+                       s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (step) *step = m->steps;
+  return check_status(s);
+}
+
+int pmb_md_set_checkpoint(pmb_md *m, const double *pos, const double *vel, const double *list_reference,
+                          long long step) {
   if (!m || !pos) return fail(PMB_ERR_ARG, "null argument");
+  if (step < 0) return fail(PMB_ERR_ARG, "step count < 0");
   pmb_system *s = m->sys;
   for (int i = 0; i < 3 * s->natoms; i++)
-    if (!std::isfinite(pos[i]) || (vel && !std::isfinite(vel[i]))) return fail(PMB_ERR_NUMERIC, "non-finite state");
-  CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
-  s->have_pos = true;
-  if (vel) CK(cudaMemcpyAsync(m->d_vel, vel, sizeof(double) * 3 * s->natoms, cudaMemcpyHostToDevice, s->stream));
-  else CK(cudaMemsetAsync(m->d_vel, 0, sizeof(double) * 3 * s->natoms, s->stream));
-  CK(cudaMemsetAsync(m->d_step, 0, sizeof(long long), s->stream));
-  constraints_init(m->con, m->in, s->stream);  // the new positions are SHAKE's last ones
+    if (!std::isfinite(pos[i]) || (vel && !std::isfinite(vel[i])) ||
+        (list_reference && !std::isfinite(list_reference[i])))
+      return fail(PMB_ERR_NUMERIC, "non-finite state");
+  const size_t bytes = sizeof(double) * 3 * (size_t)s->natoms;
   SystemDev sd = s->dev();
+  m->have_state = false;
   for (int attempt = 0; attempt < 3; attempt++) {
-    zero_accumulators(sd, s->stream);
-    int rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
-    if (rc) return rc;
-    rc = check_status(s);
+    int rc = PMB_OK;
+    if (list_reference) {
+      // the list of the run the checkpoint comes from: built at its reference positions (the
+      // build is deterministic), so that every later step sums the same tiles in the same order
+      CK(cudaMemcpyAsync(s->d_pos, list_reference, bytes, cudaMemcpyHostToDevice, s->stream));
+      s->have_pos = true;
+      if (s->nb_ready) CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, s->stream));  // rebuild
+      zero_accumulators(sd, s->stream);
+      rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+      if (rc) return rc;
+      rc = check_status(s);
+    }
+    if (rc == PMB_OK) {
+      CK(cudaMemcpyAsync(s->d_pos, pos, bytes, cudaMemcpyHostToDevice, s->stream));
+      s->have_pos = true;
+      if (vel) CK(cudaMemcpyAsync(m->d_vel, vel, bytes, cudaMemcpyHostToDevice, s->stream));
+      else CK(cudaMemsetAsync(m->d_vel, 0, bytes, s->stream));
+      // the Langevin noise counter: the restored run draws the streams the original would have
+      CK(cudaMemcpyAsync(m->d_step, &step, sizeof(long long), cudaMemcpyHostToDevice, s->stream));
+      constraints_init(m->con, m->in, s->stream);  // the new positions are SHAKE's last ones
+      zero_accumulators(sd, s->stream);
+      rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+      if (rc) return rc;
+      rc = check_status(s);  // also waits for the step count's host copy
+    }
     if (rc == PMB_ERR_CAPACITY) {
       if (grow_and_retry_needed(s)) return PMB_ERR_CUDA;
-      if (m->g_first) { cudaGraphExecDestroy(m->g_first); m->g_first = nullptr; }
-      if (m->g_next) { cudaGraphExecDestroy(m->g_next); m->g_next = nullptr; }
+      m->drop_graphs();  // they hold the old list's buffers
       continue;
     }
     if (rc) return rc;
     m->have_state = true;
+    m->steps = step;
     return PMB_OK;
   }
   return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded");
@@ -1704,6 +1747,7 @@ int pmb_md_run(pmb_md *m, int n) {
   integrate_half_kick(s->dev(), m->in, s->stream);
   if (m->rattle && constraints_apply(m->con, m->in, 1, s->stream)) return fail(PMB_ERR_CUDA, "RATTLE launch");
   CK(cudaGetLastError());
+  m->steps += n;
   return PMB_OK;
 }
 

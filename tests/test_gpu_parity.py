@@ -322,7 +322,9 @@ def test_non_finite_position_is_an_error_and_changes_nothing(precision):
     energies as they were, whether the list kernels saw it on the device (pair and PME forces) or
     the host did (bonded terms alone, no list); the next finite evaluation is right again."""
     from protomol3_b200 import _lib as L
-    b = W.water_box(216, seed=4)
+    b = dict(W.water_box(216, seed=4))
+    # off the waters' rest geometry, so that the bonded forces are not zero
+    b["pos"] = b["pos"] + np.random.default_rng(4).uniform(-0.05, 0.05, b["pos"].shape)
     fl = [F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
           F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0), F.BondedSystemForce()]
     for forces, bad in ((fl, np.nan), (fl, np.inf), ([F.BondedSystemForce()], -np.inf)):
