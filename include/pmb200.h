@@ -183,6 +183,33 @@ pmb_md *pmb_md_create(pmb_system *sys, pmb_force *const *forces, int n_forces,
 int pmb_md_destroy(pmb_md *md);
 /* Host state in; computes the initial forces (StandardIntegrator::initializeForces). */
 int pmb_md_set_state(pmb_md *md, const double *positions, const double *velocities);
+/* Checkpoint of the run's resident state, exact (the checkpoint's content of OutputCheckpoint,
+ * output/OutputCheckpoint.cpp:58-70, 137-178, without its text rounding): positions and
+ * velocities [3 N], the neighbour list's reference positions [3 N] (those of its last build;
+ * NULL skips them) and the steps taken since the state was set (the Langevin noise counter).
+ * Waits for the system's stream. */
+int pmb_md_get_checkpoint(pmb_md *md, double *positions, double *velocities, double *list_reference,
+                          long long *step);
+/* Restores a checkpoint into this run, which may belong to another system made from the same
+ * boxes and forces (a segment moved to another slot or device), and computes the initial forces
+ * as pmb_md_set_state does (CheckpointModule::read / postBuild, module/CheckpointModule.cpp:30-48).
+ * With list_reference the neighbour list is first built at those positions, so that the run
+ * continues bit for bit as the run the checkpoint came from; without it (NULL) the list is built
+ * at the positions and the continuation agrees to the rounding of the arithmetic.  velocities
+ * NULL: zero.  pmb_md_set_state is this call with no list reference and step 0. */
+int pmb_md_set_checkpoint(pmb_md *md, const double *positions, const double *velocities,
+                          const double *list_reference, long long step);
+/* Writes a checkpoint in the reference's files (OutputCheckpoint::doIt, :58-70): positions to
+ * pos_base + id + ".pos" and velocities to vel_base + id + ".vel" as XYZWriter writes them
+ * (io/XYZWriter.cpp:28-53; names: one string per atom), then the checkpoint file config_path
+ * (written to config_path + ".tmp" and renamed, as WriteConfig does) in CheckpointConfigWriter's
+ * layout (io/CheckpointConfigWriter.cpp:11-25): "!Checkpoint File!", #ID, #Step (first_step +
+ * the steps taken), #Random and #Integrator.  #Random holds this library's noise state,
+ * "philox4x32-10 <seed> <half kicks drawn>", in place of the reference's serial generator;
+ * #Integrator is empty, as the leapfrog and Langevin integrators write nothing there.  The files
+ * of checkpoint id - 1 are removed, as the reference removes them. */
+int pmb_md_write_checkpoint(pmb_md *md, const char *config_path, int id, long long first_step,
+                            const char *pos_base, const char *vel_base, const char *const *names);
 int pmb_md_get_state(pmb_md *md, double *positions, double *velocities);
 int pmb_md_get_forces(pmb_md *md, double *forces);
 /* LeapfrogIntegrator::run(n) / StandardIntegrator::run(n) semantics. */
@@ -227,6 +254,22 @@ pmb_traj *pmb_traj_open_dcd(const char *path, int n_atoms, double timestep, int 
 /* An XYZ file in the format of XYZWriter::write (io/XYZWriter.cpp:28-53); every frame rewrites
  * it (final positions, as OutputFinalXYZPos).  names: one string per atom. */
 pmb_traj *pmb_traj_open_xyz(const char *path, int n_atoms, const char *const *names);
+/* An XYZ trajectory in the format of XYZTrajectoryWriter (io/XYZTrajectoryWriter.cpp:64-160): a
+ * first line holding the frame count in 19 characters, rewritten with every frame, then per frame
+ * the atom count and per atom the name and three coordinates as XYZWriter writes them.
+ * OutputXYZTrajectoryForce (output/OutputXYZTrajectoryForce.cpp:39-44) writes the integrator's
+ * forces into such a file: pmb_md_write_force_frame. */
+pmb_traj *pmb_traj_open_xyz_trajectory(const char *path, int n_atoms, const char *const *names);
+/* Minimal-image output for a DCD trajectory (OutputDCDTrajectory with minimalImage,
+ * output/OutputDCDTrajectory.cpp:67, through OutputCache::getMinimalPositions and
+ * SemiGenericTopology::minimalImage, topology/SemiGenericTopology.h:127-150): every frame is
+ * written after, per molecule, each bonded pair's second atom is moved by lattice vectors to the
+ * image nearest its first atom (pairs in ascending (first, second) order, as the topology builder
+ * sorts them), and the molecule by lattice vectors so that its centre of mass (masses [n_atoms],
+ * Kahan sum) lies in the box around origin.  molecule [n_atoms] as in pmb_box_desc, pairs
+ * [2 n_pairs] the bonds, box the orthogonal edges.  Host positions and device frames alike. */
+int pmb_traj_set_minimal_image(pmb_traj *t, const double *mass, const int *molecule, int n_pairs,
+                               const int *pairs, const double box[3], const double origin[3]);
 /* A frame from host positions [3 n_atoms]; written before the call returns. */
 int pmb_traj_write_host(pmb_traj *t, const double *positions);
 /* A frame of the MD run's current positions, taken without stopping the device: a device
@@ -235,6 +278,10 @@ int pmb_traj_write_host(pmb_traj *t, const double *positions);
  * (OutputDCDTrajectory::doRun without the synchronisation).  Waits only when all three buffers
  * are in flight; the first frame allocates the buffers.  Not during a stream capture. */
 int pmb_md_write_frame(pmb_md *md, pmb_traj *t);
+/* A frame of the MD run's forces (those of its last evaluation, as the integrator's getForces()
+ * holds them after a step), taken like pmb_md_write_frame: the conversion to FP64 on the
+ * system's stream, the host copy on the trajectory's stream. */
+int pmb_md_write_force_frame(pmb_md *md, pmb_traj *t);
 /* Waits until every frame handed over is in the file; the first write error, if any. */
 int pmb_traj_flush(pmb_traj *t);
 int pmb_traj_frames(pmb_traj *t, long long *frames);

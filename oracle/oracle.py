@@ -422,6 +422,55 @@ def ref_write_xyz(path, pos, names):
         raise RuntimeError("reference XYZ writer failed")
 
 
+def ref_write_xyz_trajectory(path, frames, names):
+    """The reference's XYZTrajectoryWriter as OutputXYZTrajectoryForce uses it, one write per frame
+    of ``frames`` [n_frames, n_atoms, 3]."""
+    fr = np.ascontiguousarray(frames, np.float64)
+    arr = (C.c_char_p * len(names))(*[str(n).encode() for n in names])
+    rc = _ref_md_lib().ref_write_xyz_trajectory(str(path).encode(), int(fr.shape[1]), int(fr.shape[0]), _p(fr), arr)
+    if rc:
+        raise RuntimeError("reference XYZ trajectory writer failed")
+
+
+def ref_write_dcd_minimal(path, system, frames, pairs, origin):
+    """The reference's minimal-image DCD output (SemiGenericTopology::minimalImage on each frame,
+    then DCDTrajectoryWriter), molecules from the system's molecule indices with ``pairs`` [m, 2]
+    as their bonded pairs, box origin ``origin``."""
+    fr = np.ascontiguousarray(frames, np.float64)
+    r = _ref_input(system, np.ascontiguousarray(fr[0]), 5.0)
+    for q in range(3):
+        r.origin[q] = float(origin[q])
+    pr = np.ascontiguousarray(pairs, np.int32)
+    rc = _ref_md_lib().ref_write_dcd_minimal(C.byref(r), int(len(pr)), _p(pr), int(fr.shape[0]), _p(fr),
+                                             str(path).encode())
+    if rc:
+        raise RuntimeError("reference minimal-image DCD writer failed")
+
+
+def ref_write_checkpoint_config(path, ident, step):
+    """The reference's CheckpointConfigWriter with its Random and a LeapfrogIntegrator."""
+    with _quiet():
+        rc = _ref_md_lib().ref_write_checkpoint_config(str(path).encode(), int(ident), int(step))
+    if rc:
+        raise RuntimeError("reference checkpoint writer failed")
+
+
+class _quiet:
+    """Keeps the reference's report stream (stdout) out of the caller's output."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.fd = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        import sys
+        sys.stdout.flush()
+        os.dup2(self.fd, 1)
+        os.close(self.fd)
+
+
 def ref_evaluate_vacuum(system, pos, cutoff, cellsize=5.0):
     """The reference's cutoff forces with VacuumBoundaryConditions (oracle/ref_vacuum.cpp):
     forces (n, 3), energies[4] (Coulomb, LJ, bond, angle), virial (9,)."""

@@ -19,6 +19,7 @@ using namespace ProtoMol::Report;
 #include <protomol/topology/SemiGenericTopology.h>
 #include <protomol/force/bonded/AngleSystemForce.h>
 #include <protomol/force/bonded/BondSystemForce.h>
+#include <protomol/io/DCDTrajectoryWriter.h>
 #include <protomol/integrator/base/LangevinLeapfrogIntegrator.h>
 #include <protomol/integrator/leapfrog/LeapfrogIntegrator.h>
 #include <protomol/topology/CubicCellManager.h>
@@ -32,6 +33,8 @@ typedef PeriodicBoundaryConditions PBC;
 typedef Topology<PBC, CubicCellManager> Topo;
 
 #include "ref_topology.h"
+
+#include <algorithm>
 
 SystemForce *ref_new_cutoff_force(const ref_cutoff *c);
 SystemForce *ref_new_pme_force(const ref_pme *p);
@@ -103,5 +106,39 @@ extern "C" int ref_md_run(const ref_input *in, const ref_cutoff *c, const ref_pm
     read_out(app, it, in->n, k, energies, pos, vel, forces);
   }
   delete it;  // deletes its force group
+  return 0;
+}
+
+// DCD frames in minimal image as OutputDCDTrajectory with minimalImage writes them
+// (output/OutputDCDTrajectory.cpp:64-70 through OutputCache::getMinimalPositions,
+// output/OutputCache.cpp:226-235): SemiGenericTopology::minimalImage on a copy of each frame.
+// The topology's molecules are the atoms of each molecule index with the given bonded pairs,
+// (first, second) with first < second, in ascending order as the topology builder leaves them
+// (topology/BuildTopology.cpp:1034-1050); the box origin is in->origin.
+extern "C" int ref_write_dcd_minimal(const ref_input *in, int n_pairs, const int *pairs, int n_frames,
+                                     const double *frames, const char *path) {
+  Topo *t = make_topo(in);
+  for (int i = 0; i < in->n; i++) {
+    t->molecules[in->molecule[i]].atoms.push_back(i);
+    t->molecules[in->molecule[i]].mass += t->atoms[i].scaledMass;
+  }
+  for (int k = 0; k < n_pairs; k++) {
+    int a = pairs[2 * k], b = pairs[2 * k + 1];
+    if (a > b) std::swap(a, b);
+    t->molecules[in->molecule[a]].pairs.push_back(PairInt(a, b));
+  }
+  for (unsigned int m = 0; m < t->molecules.size(); m++)
+    std::sort(t->molecules[m].pairs.begin(), t->molecules[m].pairs.end());
+  DCDTrajectoryWriter w(std::string(path), 1.0, 0u);
+  if (!w.open()) return 1;
+  Vector3DBlock v(in->n);
+  for (int f = 0; f < n_frames; f++) {
+    for (int i = 0; i < in->n; i++)
+      for (int c = 0; c < 3; c++) v[i][c] = frames[3 * ((size_t)f * in->n + i) + c];
+    t->minimalImage(v);
+    if (!w.write(v)) return 2;
+  }
+  w.close();
+  delete t;
   return 0;
 }

@@ -5,10 +5,19 @@
 //   27-43: timestep argument 1.0, first step from the configuration, native byte order), one
 //   write() per frame (io/DCDTrajectoryWriter.cpp)
 //   XYZWriter::write(coords, names) (io/XYZWriter.cpp), as OutputFinalXYZPos uses it
+//   XYZTrajectoryWriter opened and written as OutputXYZTrajectoryForce does
+//   (output/OutputXYZTrajectoryForce.cpp:30-44), one write() per frame
+//   CheckpointConfigWriter::write (io/CheckpointConfigWriter.cpp:11-25) with the reference's
+//   Random and a LeapfrogIntegrator, as OutputCheckpoint::WriteConfig calls it
 #include <protomol/base/Report.h>
 using namespace ProtoMol::Report;
 
+#include <protomol/base/Random.h>
+#include <protomol/force/ForceGroup.h>
+#include <protomol/integrator/leapfrog/LeapfrogIntegrator.h>
+#include <protomol/io/CheckpointConfigWriter.h>
 #include <protomol/io/DCDTrajectoryWriter.h>
+#include <protomol/io/XYZTrajectoryWriter.h>
 #include <protomol/io/XYZWriter.h>
 #include <protomol/type/Vector3DBlock.h>
 
@@ -43,4 +52,27 @@ extern "C" int ref_write_xyz(const char *path, int n_atoms, const double *pos, c
   fill(v, pos, n_atoms);
   std::vector<std::string> nm(names, names + n_atoms);
   return w.write(v, nm) ? 0 : 1;
+}
+
+extern "C" int ref_write_xyz_trajectory(const char *path, int n_atoms, int n_frames, const double *frames,
+                                        const char *const *names) {
+  XYZTrajectoryWriter w((std::string(path)));
+  if (!w.open()) return 1;
+  std::vector<std::string> nm(names, names + n_atoms);
+  Vector3DBlock v;
+  for (int f = 0; f < n_frames; f++) {
+    fill(v, frames + 3 * (size_t)n_atoms * f, n_atoms);
+    if (!w.write(v, nm)) return 2;
+  }
+  w.close();
+  return 0;
+}
+
+extern "C" int ref_write_checkpoint_config(const char *path, int id, int step) {
+  CheckpointConfigWriter w;
+  if (!w.open(std::string(path))) return 1;
+  LeapfrogIntegrator integ(1.0, new ForceGroup());
+  if (!w.write(id, step, Random::Instance(), &integ)) return 2;
+  w.close();
+  return 0;
 }

@@ -79,6 +79,10 @@ _PROTOS = [
     ("pmb_md_create", C.c_void_p, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     ("pmb_md_destroy", C.c_int, [C.c_void_p]),
     ("pmb_md_set_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pmb_md_get_checkpoint", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pmb_md_set_checkpoint", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("pmb_md_write_checkpoint", C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_longlong, C.c_char_p,
+                                          C.c_char_p, C.c_void_p]),
     ("pmb_md_get_state", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_get_forces", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_run", C.c_int, [C.c_void_p, C.c_int]),
@@ -88,8 +92,12 @@ _PROTOS = [
     ("pmb_md_constraint_sweeps", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_traj_open_dcd", C.c_void_p, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]),
     ("pmb_traj_open_xyz", C.c_void_p, [C.c_char_p, C.c_int, C.c_void_p]),
+    ("pmb_traj_open_xyz_trajectory", C.c_void_p, [C.c_char_p, C.c_int, C.c_void_p]),
+    ("pmb_traj_set_minimal_image", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]),
     ("pmb_traj_write_host", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_write_frame", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_md_write_force_frame", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_traj_flush", C.c_int, [C.c_void_p]),
     ("pmb_traj_frames", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_traj_close", C.c_int, [C.c_void_p]),

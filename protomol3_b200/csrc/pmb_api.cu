@@ -1630,6 +1630,20 @@ int md_frame_source(pmb_md *m, const double **d_pos, int *n_atoms, cudaStream_t 
   CK(cudaGetDevice(device));
   return PMB_OK;
 }
+
+int md_force_frame(pmb_md *m, double *d_out) {
+  if (!m->have_state) return fail(PMB_ERR_STATE, "pmb_md_set_state must come first");
+  pmb_system *s = m->sys;
+  forces_to_double(s->dev(), d_out, s->stream);
+  CK(cudaGetLastError());
+  return PMB_OK;
+}
+
+int md_noise(pmb_md *m, int *kind, unsigned long long *seed) {
+  *kind = m->d.kind;
+  *seed = m->d.seed;
+  return PMB_OK;
+}
 }  // namespace pmb
 
 extern "C" {

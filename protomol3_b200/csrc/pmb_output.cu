@@ -10,6 +10,12 @@
 //   XYZ as XYZWriter::write (io/XYZWriter.cpp:28-53): the atom count, then per atom the name, a
 //   tab and the three coordinates in 24-wide fields at 15 significant digits; every frame
 //   rewrites the file (final-position output).
+//   XYZ trajectory as XYZTrajectoryWriter (io/XYZTrajectoryWriter.cpp:64-160): a first line with
+//   the frame count in 19 characters (rewritten on every frame), then the frames in the XYZ form.
+//   Checkpoints as OutputCheckpoint writes them (output/OutputCheckpoint.cpp:58-178): positions
+//   and velocities in the XYZ form, then the checkpoint file of CheckpointConfigWriter.
+//   Minimal-image DCD frames as OutputCache::getMinimalPositions makes them
+//   (topology/SemiGenericTopology.h:127-150), computed by the writer thread on the host copy.
 //
 // pmb_md_write_frame takes a frame off the device without stopping it: a device-to-device
 // snapshot of the positions on the system's stream (the next step waits only for that), the
@@ -18,6 +24,8 @@
 // only when all three buffers are still in flight.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +43,10 @@
 namespace pmb {
 // defined in pmb_api.cu: the positions, atom count and stream of an MD run
 int md_frame_source(pmb_md *md, const double **d_pos, int *n_atoms, cudaStream_t *stream, int *device);
+// enqueues the MD run's forces (of its last evaluation) as FP64 into d_out on its stream
+int md_force_frame(pmb_md *md, double *d_out);
+// the MD run's integrator kind and noise seed
+int md_noise(pmb_md *md, int *kind, unsigned long long *seed);
 }  // namespace pmb
 
 using namespace pmb;
@@ -64,10 +76,84 @@ std::string right_fill(const std::string &s, size_t n) {
   return s.size() < n ? s + std::string(n - s.size(), ' ') : s.substr(0, n);
 }
 
+// One frame as XYZWriter::write / XYZTrajectoryWriter::write print it (io/XYZWriter.cpp:42-53).
+std::string xyz_text(int n, const std::vector<std::string> &names, const double *v) {
+  std::ostringstream o;
+  o << n << std::endl;
+  o.precision(15);
+  for (int i = 0; i < n; i++) {
+    o << names[i] << "\t";
+    for (int c = 0; c < 3; c++) {
+      o.width(24);
+      o << v[3 * i + c];
+    }
+    o << std::endl;
+  }
+  return o.str();
+}
+
+bool write_file(const std::string &path, const std::string &text) {
+  std::FILE *x = std::fopen(path.c_str(), "wb");
+  if (!x) return false;
+  const bool ok = std::fwrite(text.data(), 1, text.size(), x) == text.size();
+  return std::fclose(x) == 0 && ok;
+}
+
+// Minimal image of one frame (SemiGenericTopology::minimalImage with the orthogonal
+// PeriodicBoundaryConditions of topology/PeriodicBoundaryConditions.cpp:32-77, .h:150-185).
+struct MinimalImage {
+  std::vector<std::vector<int>> atoms;                  // per molecule, ascending
+  std::vector<std::vector<std::pair<int, int>>> pairs;  // per molecule, ascending (first < second)
+  std::vector<double> mass;
+  double L[3], Lr[3], origin[3], D;
+
+  // the lattice translation of d (minimalTranslationDifference / Position): none while |d|^2 is
+  // within the safe distance, else L rint(d / L) per axis
+  void translation(const double d[3], double t[3]) const {
+    if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] <= D) {
+      t[0] = t[1] = t[2] = 0.0;
+      return;
+    }
+    for (int c = 0; c < 3; c++) t[c] = L[c] * std::rint(Lr[c] * d[c]);
+  }
+  void apply(double *x) const {
+    const double EPS = 1.0e-14;  // base/PMConstants.cpp:50
+    for (size_t m = 0; m < atoms.size(); m++) {
+      for (const std::pair<int, int> &p : pairs[m]) {
+        const double d[3] = {x[3 * p.second] - x[3 * p.first], x[3 * p.second + 1] - x[3 * p.first + 1],
+                             x[3 * p.second + 2] - x[3 * p.first + 2]};
+        double t[3];
+        translation(d, t);
+        if (t[0] * t[0] + t[1] * t[1] + t[2] * t[2] > EPS)
+          for (int c = 0; c < 3; c++) x[3 * p.second + c] -= t[c];
+      }
+      // molecularCenterOfMass (topology/TopologyUtilities.cpp:646-674): Kahan summation
+      const std::vector<int> &a = atoms[m];
+      double mt = mass[a[0]], cen[3], kc[3] = {0.0, 0.0, 0.0};
+      for (int c = 0; c < 3; c++) cen[c] = x[3 * a[0] + c] * mt;
+      for (size_t i = 1; i < a.size(); i++) {
+        const double w = mass[a[i]];
+        mt += w;
+        for (int c = 0; c < 3; c++) {
+          const double tx = x[3 * a[i] + c] * w, ty = tx - kc[c], tt = cen[c] + ty;
+          kc[c] = (tt - cen[c]) - ty;
+          cen[c] = tt;
+        }
+      }
+      double d[3], t[3];
+      for (int c = 0; c < 3; c++) d[c] = cen[c] / mt - origin[c];
+      translation(d, t);
+      if (t[0] * t[0] + t[1] * t[1] + t[2] * t[2] > EPS)
+        for (int i : a)
+          for (int c = 0; c < 3; c++) x[3 * i + c] -= t[c];
+    }
+  }
+};
+
 }  // namespace
 
 struct pmb_traj {
-  int kind = 0;  // 0 DCD, 1 XYZ
+  int kind = 0;  // 0 DCD, 1 XYZ, 2 XYZ trajectory
   std::string path, comment;
   int n_atoms = 0, first_step = 0;
   double timestep = 1.0;
@@ -93,6 +179,8 @@ struct pmb_traj {
   int err = PMB_OK;
   std::string err_msg;
   int device = -1;  // the device of the first frame: the staging buffers and copy stream live there
+  MinimalImage *minimal = nullptr;  // DCD frames in minimal image
+  std::vector<double> scratch;      // a frame's minimal-image copy
 
   template <typename T>
   void put(T v) {
@@ -163,27 +251,35 @@ struct pmb_traj {
   }
 
   int write_xyz(const double *pos) {
-    std::ostringstream o;
-    o << n_atoms << std::endl;
-    o.precision(15);
-    for (int i = 0; i < n_atoms; i++) {
-      o << names[i] << "\t";
-      for (int c = 0; c < 3; c++) {
-        o.width(24);
-        o << pos[3 * i + c];
-      }
-      o << std::endl;
-    }
-    std::FILE *x = std::fopen(path.c_str(), "wb");
-    if (!x) return PMB_ERR_ARG;
-    const std::string s = o.str();
-    const bool ok = std::fwrite(s.data(), 1, s.size(), x) == s.size();
-    std::fclose(x);
+    const bool ok = write_file(path, xyz_text(n_atoms, names, pos));
     frames++;
     return ok ? PMB_OK : PMB_ERR_ARG;
   }
 
-  int write(const double *pos) { return kind == 0 ? write_dcd(pos) : write_xyz(pos); }
+  // XYZTrajectoryWriter::reopen + write: the frame count line, 19 characters and a newline,
+  // rewritten in place; the frame appended
+  int write_xyz_trajectory(const double *pos) {
+    const std::string head = right_fill(std::to_string(frames + 1), 19) + "\n";
+    std::FILE *x = std::fopen(path.c_str(), frames == 0 ? "wb" : "r+b");
+    if (!x) return PMB_ERR_ARG;
+    bool ok = std::fwrite(head.data(), 1, head.size(), x) == head.size();
+    const std::string body = xyz_text(n_atoms, names, pos);
+    ok = ok && std::fseek(x, 0, SEEK_END) == 0 && std::fwrite(body.data(), 1, body.size(), x) == body.size();
+    ok = std::fclose(x) == 0 && ok;
+    frames++;
+    return ok ? PMB_OK : PMB_ERR_ARG;
+  }
+
+  int write(const double *pos) {
+    if (kind == 1) return write_xyz(pos);
+    if (kind == 2) return write_xyz_trajectory(pos);
+    if (minimal) {
+      scratch.assign(pos, pos + 3 * (size_t)n_atoms);
+      minimal->apply(scratch.data());
+      return write_dcd(scratch.data());
+    }
+    return write_dcd(pos);
+  }
 
   void writer_loop() {
     if (device >= 0) cudaSetDevice(device);
@@ -236,6 +332,7 @@ struct pmb_traj {
     }
     if (copy) cudaStreamDestroy(copy);
     if (f) std::fclose(f);
+    delete minimal;
   }
 };
 
@@ -280,7 +377,11 @@ int pmb_traj_write_host(pmb_traj *t, const double *positions) {
   return rc;
 }
 
-int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
+}  // extern "C"
+
+namespace {
+// A frame of the MD run's positions (forces = false) or forces, taken without stopping the device.
+int md_frame(pmb_md *md, pmb_traj *t, bool forces) {
   if (!md || !t) return set_error("null argument"), PMB_ERR_ARG;
   const double *d_pos = nullptr;
   int n = 0, dev = 0;
@@ -327,8 +428,9 @@ int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
   // own stream, beside the steps that follow
   pmb_traj::Stage &sg = t->stage[k];
   const size_t bytes = sizeof(double) * 3 * (size_t)n;
-  if (cudaMemcpyAsync(sg.dev, d_pos, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-      cudaEventRecord(sg.taken, st) != cudaSuccess || cudaStreamWaitEvent(t->copy, sg.taken, 0) != cudaSuccess ||
+  const bool snap = forces ? md_force_frame(md, sg.dev) == PMB_OK
+                           : cudaMemcpyAsync(sg.dev, d_pos, bytes, cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+  if (!snap || cudaEventRecord(sg.taken, st) != cudaSuccess || cudaStreamWaitEvent(t->copy, sg.taken, 0) != cudaSuccess ||
       cudaMemcpyAsync(sg.host, sg.dev, bytes, cudaMemcpyDeviceToHost, t->copy) != cudaSuccess ||
       cudaEventRecord(sg.ev, t->copy) != cudaSuccess) {
     std::lock_guard<std::mutex> lk(t->mu);
@@ -340,6 +442,122 @@ int pmb_md_write_frame(pmb_md *md, pmb_traj *t) {
     t->queue.push_back(k);
   }
   t->cv.notify_all();
+  return PMB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int pmb_md_write_frame(pmb_md *md, pmb_traj *t) { return md_frame(md, t, false); }
+
+int pmb_md_write_force_frame(pmb_md *md, pmb_traj *t) { return md_frame(md, t, true); }
+
+pmb_traj *pmb_traj_open_xyz_trajectory(const char *path, int n_atoms, const char *const *names) {
+  pmb_traj *t = pmb_traj_open_xyz(path, n_atoms, names);
+  if (t) t->kind = 2;
+  return t;
+}
+
+int pmb_traj_set_minimal_image(pmb_traj *t, const double *mass, const int *molecule, int n_pairs,
+                               const int *pairs, const double box[3], const double origin[3]) {
+  if (!t || !mass || !molecule || n_pairs < 0 || (n_pairs > 0 && !pairs) || !box || !origin)
+    return set_error("null argument"), PMB_ERR_ARG;
+  if (t->kind != 0) return set_error("minimal image applies to DCD trajectories"), PMB_ERR_ARG;
+  if (t->started || t->frames) return set_error("minimal image must be set before the first frame"), PMB_ERR_STATE;
+  const int n = t->n_atoms;
+  for (int c = 0; c < 3; c++)
+    if (!(box[c] > 0) || !std::isfinite(origin[c])) return set_error("box edges > 0, finite origin"), PMB_ERR_ARG;
+  int nmol = 0;
+  for (int i = 0; i < n; i++) {
+    if (molecule[i] < 0 || molecule[i] >= n) return set_error("molecule index out of range"), PMB_ERR_ARG;
+    nmol = std::max(nmol, molecule[i] + 1);
+  }
+  MinimalImage *mi = new MinimalImage();
+  mi->atoms.resize(nmol);
+  mi->pairs.resize(nmol);
+  for (int i = 0; i < n; i++) mi->atoms[molecule[i]].push_back(i);
+  for (int k = 0; k < n_pairs; k++) {
+    int a = pairs[2 * k], b = pairs[2 * k + 1];
+    if (a < 0 || a >= n || b < 0 || b >= n || molecule[a] != molecule[b] || a == b) {
+      delete mi;
+      return set_error("pair " + std::to_string(k) + " does not join two atoms of one molecule"), PMB_ERR_ARG;
+    }
+    if (a > b) std::swap(a, b);
+    mi->pairs[molecule[a]].push_back(std::make_pair(a, b));
+  }
+  for (auto &p : mi->pairs) std::sort(p.begin(), p.end());
+  // molecule ids without atoms leave empty molecules, which the transform skips
+  std::vector<std::vector<int>> atoms;
+  std::vector<std::vector<std::pair<int, int>>> prs;
+  for (int m = 0; m < nmol; m++)
+    if (!mi->atoms[m].empty()) {
+      atoms.push_back(mi->atoms[m]);
+      prs.push_back(mi->pairs[m]);
+    }
+  mi->atoms.swap(atoms);
+  mi->pairs.swap(prs);
+  mi->mass.assign(mass, mass + n);
+  // PeriodicBoundaryConditions::set (topology/PeriodicBoundaryConditions.cpp:32-77) for the
+  // orthogonal box (e1, e2, e3) = diag(box): reciprocal edges and the safe distance
+  const double lx = box[0], ly = box[1], lz = box[2];
+  mi->L[0] = lx;
+  mi->L[1] = ly;
+  mi->L[2] = lz;
+  mi->Lr[0] = (ly * lz) / (lx * (ly * lz));
+  mi->Lr[1] = (lz * lx) / (ly * (lz * lx));
+  mi->Lr[2] = (lx * ly) / (lz * (lx * ly));
+  for (int c = 0; c < 3; c++) mi->origin[c] = origin[c];
+  const double dx = (lx * 0.5) * (lx * 0.5), dy = (ly * 0.5) * (ly * 0.5), dz = (lz * 0.5) * (lz * 0.5);
+  mi->D = std::min(dx, std::min(dy, dz));
+  delete t->minimal;
+  t->minimal = mi;
+  return PMB_OK;
+}
+
+int pmb_md_write_checkpoint(pmb_md *md, const char *config_path, int id, long long first_step,
+                            const char *pos_base, const char *vel_base, const char *const *names) {
+  if (!md || !config_path || !*config_path || !pos_base || !vel_base || !names)
+    return set_error("null argument"), PMB_ERR_ARG;
+  const double *d_pos = nullptr;
+  int n = 0, dev = 0, kind = 0;
+  cudaStream_t st = nullptr;
+  int rc = md_frame_source(md, &d_pos, &n, &st, &dev);
+  if (rc) return rc;
+  std::vector<std::string> nm(n);
+  for (int i = 0; i < n; i++) {
+    if (!names[i]) return set_error("null atom name"), PMB_ERR_ARG;
+    nm[i] = names[i];
+  }
+  std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n);
+  long long steps = 0;
+  rc = pmb_md_get_checkpoint(md, x.data(), v.data(), nullptr, &steps);
+  if (rc) return rc;
+  unsigned long long seed = 0;
+  md_noise(md, &kind, &seed);
+  const std::string pos_file = std::string(pos_base) + std::to_string(id) + ".pos";
+  const std::string vel_file = std::string(vel_base) + std::to_string(id) + ".vel";
+  if (!write_file(pos_file, xyz_text(n, nm, x.data())))
+    return set_error("cannot write " + pos_file), PMB_ERR_ARG;
+  if (!write_file(vel_file, xyz_text(n, nm, v.data())))
+    return set_error("cannot write " + vel_file), PMB_ERR_ARG;
+  // CheckpointConfigWriter::write (io/CheckpointConfigWriter.cpp:11-25); the leapfrog and
+  // Langevin integrators write nothing after #Integrator (Integrator::streamWrite)
+  std::ostringstream o;
+  o << "!Checkpoint File!" << std::endl
+    << "#ID" << std::endl
+    << id << std::endl
+    << "#Step" << std::endl
+    << first_step + steps << std::endl
+    << "#Random" << std::endl
+    << "philox4x32-10 " << seed << " " << (kind == PMB_LANGEVIN ? 2 * steps : 0) << std::endl
+    << "#Integrator" << std::endl
+    << std::endl;
+  const std::string tmp = std::string(config_path) + ".tmp";
+  if (!write_file(tmp, o.str()) || std::rename(tmp.c_str(), config_path) != 0)
+    return set_error(std::string("cannot write ") + config_path), PMB_ERR_ARG;
+  // the previous checkpoint's files go (OutputCheckpoint::doIt)
+  std::remove((std::string(pos_base) + std::to_string(id - 1) + ".pos").c_str());
+  std::remove((std::string(vel_base) + std::to_string(id - 1) + ".vel").c_str());
   return PMB_OK;
 }
 

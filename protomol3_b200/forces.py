@@ -401,6 +401,39 @@ class Integrator:
         asynchronous copy and a writer thread; ``traj.flush()`` waits for the file)."""
         L.check(L.lib().pmb_md_write_frame(self._h, traj.handle()))
 
+    def write_force_frame(self, traj):
+        """Appends the forces of the last evaluation to ``traj`` (OutputXYZTrajectoryForce with an
+        ``Trajectory.xyz_trajectory``), taken like ``write_frame``."""
+        L.check(L.lib().pmb_md_write_force_frame(self._h, traj.handle()))
+
+    def checkpoint(self):
+        """Exact snapshot of the resident state: dict of positions, velocities, the neighbour
+        list's reference positions and the steps taken since the state was set."""
+        n = self.topo.n_atoms
+        pos, vel, ref = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        step = C.c_longlong(0)
+        L.check(L.lib().pmb_md_get_checkpoint(self._h, _p(pos), _p(vel), _p(ref), C.byref(step)))
+        return {"positions": pos, "velocities": vel, "list_reference": ref, "step": step.value}
+
+    def restore(self, ckpt, exact=True):
+        """Restores ``checkpoint()``'s dict, in this run or another of the same boxes and forces;
+        ``exact`` rebuilds the neighbour list at the checkpoint's reference positions, so the run
+        continues bit for bit."""
+        pos = np.ascontiguousarray(ckpt["positions"], np.float64)
+        vel = ckpt.get("velocities")
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64)
+        ref = np.ascontiguousarray(ckpt["list_reference"], np.float64) if exact else None
+        L.check(L.lib().pmb_md_set_checkpoint(self._h, _p(pos), _p(vel), _p(ref) if ref is not None else None,
+                                              int(ckpt.get("step", 0))))
+
+    def write_checkpoint(self, config_path, ident, pos_base, vel_base, names, first_step=0):
+        """The reference's checkpoint files (OutputCheckpoint): pos_base<id>.pos and
+        vel_base<id>.vel in XYZ form and the checkpoint file ``config_path``."""
+        arr = (C.c_char_p * len(names))(*[str(x).encode() for x in names])
+        L.check(L.lib().pmb_md_write_checkpoint(self._h, str(config_path).encode(), int(ident), int(first_step),
+                                                str(pos_base).encode(), str(vel_base).encode(),
+                                                C.cast(arr, C.c_void_p)))
+
     def set_state(self, positions, velocities=None):
         pos = np.ascontiguousarray(positions, np.float64)
         vel = None if velocities is None else np.ascontiguousarray(velocities, np.float64)
@@ -492,6 +525,24 @@ class Trajectory:
         arr = (C.c_char_p * len(names))(*[str(n).encode() for n in names])
         return cls(L.lib().pmb_traj_open_xyz(str(path).encode(), len(names), C.cast(arr, C.c_void_p)),
                    len(names))
+
+    @classmethod
+    def xyz_trajectory(cls, path, names):
+        """An XYZ trajectory (XYZTrajectoryWriter: a frame-count line, then the frames), the
+        file OutputXYZTrajectoryForce writes forces into."""
+        arr = (C.c_char_p * len(names))(*[str(n).encode() for n in names])
+        return cls(L.lib().pmb_traj_open_xyz_trajectory(str(path).encode(), len(names), C.cast(arr, C.c_void_p)),
+                   len(names))
+
+    def set_minimal_image(self, mass, molecule, pairs, box, origin=(0.0, 0.0, 0.0)):
+        """DCD frames in minimal image (OutputDCDTrajectory's minimal-image option): molecules
+        whole and their centres of mass in the box around ``origin``; ``pairs`` [m, 2] bonds."""
+        self._mi = [np.ascontiguousarray(mass, np.float64), np.ascontiguousarray(molecule, np.int32),
+                    np.ascontiguousarray(pairs, np.int32).reshape(-1), np.ascontiguousarray(box, np.float64),
+                    np.ascontiguousarray(origin, np.float64)]
+        m, mol, pr, bx, org = self._mi
+        L.check(L.lib().pmb_traj_set_minimal_image(self._h, _p(m), _p(mol), int(pr.size // 2), _p(pr), _p(bx),
+                                                   _p(org)))
 
     def handle(self):
         return self._h

@@ -104,3 +104,53 @@ def test_live_reference_writers_on_another_case(tmp_path, monkeypatch):
     t.write(fr[0])
     t.close()
     assert open("r.xyz", "rb").read() == open("m.xyz", "rb").read()
+
+
+def test_xyz_trajectory_matches_reference_writer(tmp_path):
+    """XYZTrajectoryWriter as OutputXYZTrajectoryForce writes it: a frame-count line rewritten
+    with every frame, the frames appended (golden water27_ref_traj.xyz)."""
+    fr = _frames()
+    t = F.Trajectory.xyz_trajectory(tmp_path / "t.xyz", _names())
+    for f in fr:
+        t.write(f)
+    assert t.frames() == 3
+    t.close()
+    assert (tmp_path / "t.xyz").read_bytes() == open(os.path.join(GOLD, "water27_ref_traj.xyz"), "rb").read()
+
+
+def test_dcd_minimal_image_matches_reference(tmp_path):
+    """OutputDCDTrajectory's minimal-image option: frames whose atoms were scattered over
+    periodic images come out as the reference's SemiGenericTopology::minimalImage writes them
+    (golden water27_ref_min.dcd), byte for byte but the first title line."""
+    from protomol3_b200 import waterbox as W
+    d = np.load(os.path.join(GOLD, "water27_frames.npz"))
+    box = W.water_box(27, seed=3)
+    t = F.Trajectory.dcd(tmp_path / "m.dcd", 81)
+    t.set_minimal_image(box["mass"], box["molecule"], box["bonds"], box["box"], d["origin"])
+    for f in d["scrambled"]:
+        t.write(f)
+    t.close()
+    mine = (tmp_path / "m.dcd").read_bytes()
+    gold = open(os.path.join(GOLD, "water27_ref_min.dcd"), "rb").read()
+    assert _same_but_title(mine, gold)
+    # and the scrambling was undone: every water whole, its centre of mass inside the box
+    plain = F.Trajectory.dcd(tmp_path / "p.dcd", 81)
+    for f in d["scrambled"]:
+        plain.write(f)
+    plain.close()
+    assert (tmp_path / "p.dcd").read_bytes()[200:] != mine[200:]
+
+
+def test_minimal_image_refuses_bad_input(tmp_path):
+    from protomol3_b200 import waterbox as W
+    box = W.water_box(27, seed=3)
+    t = F.Trajectory.dcd(tmp_path / "m.dcd", 81)
+    bad = box["bonds"].copy()
+    bad[0] = (0, 5)  # atoms of two waters
+    with pytest.raises(RuntimeError):
+        t.set_minimal_image(box["mass"], box["molecule"], bad, box["box"])
+    x = F.Trajectory.xyz(tmp_path / "x.xyz", _names())
+    with pytest.raises(RuntimeError):
+        x.set_minimal_image(box["mass"], box["molecule"], box["bonds"], box["box"])
+    t.close()
+    x.close()
