@@ -118,6 +118,21 @@ int pmb_system_n_boxes(const pmb_system *sys);
  * every evaluation like Topology::updateCellLists.  The pair set evaluated is the same either
  * way (every pair within the cutoff). */
 int pmb_system_set_skin(pmb_system *sys, double skin);
+/* Knobs that change the speed of a system's evaluations but not which pairs are evaluated, set
+ * by the autotuner (protomol3_b200/autotune.py) per workload; no counterpart in the reference.
+ *   skin: as pmb_system_set_skin;
+ *   sort_cell: smallest edge (A) of the sort cells that order atoms along a Hilbert curve before
+ *     they are grouped into 8-atom clusters (default 2.4; cells per axis are powers of two);
+ *   pair_ctas_per_sm: resident CTAs per SM of the persistent pair kernel (0: as many as fit).
+ * A change of skin or sort_cell re-sizes the neighbour list; MD runs capture their step again.
+ * Results differ only in the rounding order of the FP32 / FP64 partial sums. */
+typedef struct {
+  double skin;
+  double sort_cell;
+  int pair_ctas_per_sm;
+} pmb_tuning;
+int pmb_system_set_tuning(pmb_system *sys, const pmb_tuning *tuning);
+int pmb_system_get_tuning(const pmb_system *sys, pmb_tuning *tuning);
 /* Vacuum (VacuumBoundaryConditions, topology/VacuumBoundaryConditions.h: the plain difference,
  * no images; cell pairs of CellListEnumerator_standard) for the cutoff forces: a box whose edges
  * are more than twice the extent of its atoms stands in for vacuum, because every minimal-image
@@ -217,6 +232,9 @@ int pmb_md_run(pmb_md *md, int n_steps);
 /* Energies of the last force evaluation [n_boxes * PMB_E_STRIDE] and kinetic energy per box. */
 int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
 int pmb_md_use_graph(pmb_md *md, int enable);
+/* Runs n_steps (pmb_md_run) between two CUDA events on the system's stream and returns the mean
+ * device time per step in ms (the autotuner's clock). */
+int pmb_md_time(pmb_md *md, int n_steps, double *ms_per_step);
 /* Bond constraints of a leapfrog run (replaces ModifierShake / ModifierRattle as
  * module/ModifierModule.cpp:106-128 installs them): SHAKE after every drift, RATTLE after every
  * step, on a constraint list in the reference's order (topology/TopologyUtilities.cpp:695-775,

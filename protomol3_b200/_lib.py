@@ -44,6 +44,10 @@ class IntegratorDesc(C.Structure):
                 ("gamma_ps", C.c_double), ("seed", C.c_ulonglong)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("skin", C.c_double), ("sort_cell", C.c_double), ("pair_ctas_per_sm", C.c_int)]
+
+
 class ConstraintDesc(C.Structure):
     _fields_ = [("n_constraints", C.c_int), ("atom1", C.c_void_p), ("atom2", C.c_void_p),
                 ("rest_length", C.c_void_p), ("shake", C.c_int), ("shake_epsilon", C.c_double),
@@ -61,6 +65,8 @@ _PROTOS = [
     ("pmb_system_n_atoms", C.c_int, [C.c_void_p]),
     ("pmb_system_n_boxes", C.c_int, [C.c_void_p]),
     ("pmb_system_set_skin", C.c_int, [C.c_void_p, C.c_double]),
+    ("pmb_system_set_tuning", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_system_get_tuning", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_vacuum_box", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     ("pmb_system_set_vacuum", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_ewald_reciprocal", C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p,
@@ -88,6 +94,7 @@ _PROTOS = [
     ("pmb_md_run", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_energies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_use_graph", C.c_int, [C.c_void_p, C.c_int]),
+    ("pmb_md_time", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("pmb_md_set_constraints", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_constraint_sweeps", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_traj_open_dcd", C.c_void_p, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]),

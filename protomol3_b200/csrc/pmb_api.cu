@@ -223,8 +223,12 @@ struct pmb_system {
   double nb_build_rl = -1.0; // radius the current list was built with
   double skin = 0.8;         // list radius = pair cutoff + skin
   bool vacuum = false;       // boxes stand in for vacuum: evaluations check the extent
+  double sort_cell = 2.4;    // smallest edge of a sort cell (A)
+  int pair_ctas = 0;         // resident CTAs per SM of the pair kernel (0: as many as fit)
   NbListDev nb{};
   Allocs nba;
+  long long nb_gen = 0;      // list storage generation: MD graphs captured before a reallocation
+                             // hold its old buffers and are captured again
   int n_bonded = 0;
   // stage profiler: events recorded between launches when non-null
   std::vector<std::pair<std::string, cudaEvent_t>> *prof = nullptr;
@@ -278,8 +282,19 @@ struct pmb_force {
 
 namespace {
 
+// Sort cells per axis of a box edge: the largest power of two (at most 512) whose cells are at
+// least min_edge long.
+int sort_cells(double edge, double min_edge) {
+  int nc = 1;
+  while (nc < 512 && edge / (2 * nc) >= min_edge) nc *= 2;
+  return nc;
+}
+
 // Neighbour-list storage sized for list cutoff rl.
 int nblist_alloc(pmb_system *s, double rl) {
+  cudaStreamSynchronize(s->stream);  // no kernel of the system may still read the old storage
+  if (s->side) cudaStreamSynchronize(s->side);
+  s->nb_gen++;
   s->nba.~Allocs();
   new (&s->nba) Allocs();
   NbListDev &nb = s->nb;
@@ -452,11 +467,21 @@ void mark(void *ctx, const char *name) {
 }
 
 // Enqueues every force of the set on the system stream; accumulators must be zero.
+// The neighbour-list radius a force set needs (pair cutoff + skin + a margin for the fixed-point
+// culling), or 0 when no force of the set uses the list (no pair term, no PME reciprocal term).
+double list_radius(pmb_system *s, pmb_force *const *fs, int n) {
+  double rl = 0.0;
+  bool need = false;
+  for (int i = 0; i < n; i++) {
+    rl = std::max(rl, force_pair_cutoff(fs[i]));
+    need |= pair_jobs(s, fs + i, 1, 0).size() > 0 || (fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal);
+  }
+  return need ? std::max(rl, 1.0) + s->skin + 1e-3 : 0.0;
+}
+
 int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   SystemDev sd = s->dev();
   cudaStream_t st = s->stream;
-  double rl = 0.0;
-  for (int i = 0; i < n; i++) rl = std::max(rl, force_pair_cutoff(fs[i]));
   std::vector<PairJob> jobs = pair_jobs(s, fs, n, virial);
   bool need_pme_slots = false;
   for (int i = 0; i < n; i++) need_pme_slots |= fs[i]->kind == PMB_FORCE_PME && fs[i]->d.reciprocal;
@@ -509,8 +534,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   if (split)
     for (int i = 0; i < n; i++) launch_atom_terms(fs[i]);
   if (need_list) {
-    // list radius: pair cutoff + skin (+ a margin for the fixed-point culling)
-    const double rlist = std::max(rl, 1.0) + s->skin + 1e-3;
+    const double rlist = list_radius(s, fs, n);
     int rc = ensure_nblist(s, rlist);
     if (rc) return rc;
     if (rlist != s->nb_build_rl) {  // a list built for another radius cannot be reused
@@ -540,6 +564,7 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     pl.lj = s->d_lj;
     pl.lattice = j.lattice;
     pl.multi = 0;
+    pl.ctas_per_sm = s->pair_ctas;
     if (j.p.coul_mode == 2 && j.lattice)
       for (const BoxDev &b : s->hbox) pl.multi |= b.multi_image;
     if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
@@ -644,9 +669,7 @@ pmb_system *pmb_system_create(const pmb_box_desc *boxes, int n_boxes, int precis
       double lo = -d.box[k] * 0.5, hi = d.box[k] * 0.5;
       b.H[k] = hi - lo;
       b.H2[k] = b.H[k] * 0.5;
-      int nc = 1;
-      while (nc < 512 && d.box[k] / (2 * nc) >= 2.4) nc *= 2;
-      b.nc[k] = nc;
+      b.nc[k] = sort_cells(d.box[k], s->sort_cell);
     }
     b.D = std::min((d.box[0] * 0.5) * (d.box[0] * 0.5),
                    std::min((d.box[1] * 0.5) * (d.box[1] * 0.5), (d.box[2] * 0.5) * (d.box[2] * 0.5)));
@@ -807,6 +830,39 @@ int pmb_system_set_skin(pmb_system *s, double skin) {
   cudaStreamSynchronize(s->stream);
   s->skin = skin;
   s->nb_ready = false;  // storage is sized for cutoff + skin
+  return PMB_OK;
+}
+
+int pmb_system_set_tuning(pmb_system *s, const pmb_tuning *t) {
+  if (!s || !t) return fail(PMB_ERR_ARG, "null argument");
+  if (!(t->skin >= 0.0) || t->skin > 5.0) return fail(PMB_ERR_ARG, "skin must be in [0, 5] A");
+  if (!(t->sort_cell >= 0.5) || t->sort_cell > 50.0) return fail(PMB_ERR_ARG, "sort_cell must be in [0.5, 50] A");
+  if (t->pair_ctas_per_sm < 0 || t->pair_ctas_per_sm > 32) return fail(PMB_ERR_ARG, "pair_ctas_per_sm in [0, 32]");
+  CK(cudaStreamSynchronize(s->stream));
+  s->pair_ctas = t->pair_ctas_per_sm;
+  if (t->skin != s->skin || t->sort_cell != s->sort_cell) {
+    s->skin = t->skin;
+    s->sort_cell = t->sort_cell;
+    // sort cells and their key ranges per box, then the lists are sized again at next use
+    int key0 = 0;
+    for (BoxDev &b : s->hbox) {
+      int ncm = 1;
+      for (int k = 0; k < 3; k++) ncm = std::max(ncm, sort_cells(b.L[k], s->sort_cell));
+      b.nc[0] = b.nc[1] = b.nc[2] = ncm;
+      b.key0 = key0;
+      key0 += ncm * ncm * ncm;
+    }
+    CK(cudaMemcpy(s->d_box, s->hbox.data(), sizeof(BoxDev) * s->hbox.size(), cudaMemcpyHostToDevice));
+    s->nb_ready = false;
+  }
+  return PMB_OK;
+}
+
+int pmb_system_get_tuning(const pmb_system *s, pmb_tuning *t) {
+  if (!s || !t) return fail(PMB_ERR_ARG, "null argument");
+  t->skin = s->skin;
+  t->sort_cell = s->sort_cell;
+  t->pair_ctas_per_sm = s->pair_ctas;
   return PMB_OK;
 }
 
@@ -1378,6 +1434,7 @@ struct pmb_md {
   bool have_state = false, use_graph = true;
   long long steps = 0;  // steps since the state was set (a checkpoint's step count)
   cudaGraphExec_t g_first = nullptr, g_next = nullptr;
+  long long graph_gen = -1;  // list generation the graphs were captured with
   int kernels_per_step = 0;
   std::vector<double> h_e, h_k;
   // SHAKE after every drift, RATTLE after every step (absent: ngroup == 0)
@@ -1413,6 +1470,22 @@ int md_step_enqueue(pmb_md *m, double kick) {
   }
   if (m->shake && constraints_apply(m->con, m->in, 0, s->stream)) return fail(PMB_ERR_CUDA, "SHAKE launch");
   return enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+}
+
+// Before a capture: the list storage the run's forces need exists, and a change of list radius
+// has been marked (a rebuild) outside the graph, so that the captured step neither allocates nor
+// forces a rebuild on every replay.
+int md_prepare_list(pmb_md *m) {
+  pmb_system *s = m->sys;
+  const double rlist = list_radius(s, m->forces.data(), (int)m->forces.size());
+  if (rlist <= 0.0) return PMB_OK;
+  int rc = ensure_nblist(s, rlist);
+  if (rc) return rc;
+  if (rlist != s->nb_build_rl) {
+    CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, s->stream));
+    s->nb_build_rl = rlist;
+  }
+  return PMB_OK;
 }
 
 int md_capture(pmb_md *m, double kick, cudaGraphExec_t *out) {
@@ -1740,6 +1813,10 @@ int pmb_md_run(pmb_md *m, int n) {
   // the legacy default stream cannot be captured: replay eagerly there
   const bool graph_ok = s->stream != nullptr && s->stream != cudaStreamLegacy;
   if (m->use_graph && graph_ok) {
+    int prc = md_prepare_list(m);
+    if (prc) return prc;
+    if (m->graph_gen != s->nb_gen) m->drop_graphs();
+    m->graph_gen = s->nb_gen;
     if (!m->g_first) {
       int rc = md_capture(m, 0.5, &m->g_first);
       if (rc) return rc;
@@ -1763,6 +1840,30 @@ int pmb_md_run(pmb_md *m, int n) {
   CK(cudaGetLastError());
   m->steps += n;
   return PMB_OK;
+}
+
+int pmb_md_time(pmb_md *m, int n, double *ms) {
+  if (!m || !ms || n < 1) return fail(PMB_ERR_ARG, "md, n_steps >= 1 and an output");
+  if (!m->have_state) return fail(PMB_ERR_STATE, "pmb_md_set_state must come first");
+  pmb_system *s = m->sys;
+  cudaEvent_t a = nullptr, b = nullptr;
+  CK(cudaEventCreate(&a));
+  if (cudaEventCreate(&b) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return fail(PMB_ERR_CUDA, "cudaEventCreate");
+  }
+  int rc = PMB_OK;
+  float t = 0.f;
+  if (cudaEventRecord(a, s->stream) != cudaSuccess) rc = fail(PMB_ERR_CUDA, "cudaEventRecord");
+  if (!rc) rc = pmb_md_run(m, n);
+  if (!rc && (cudaEventRecord(b, s->stream) != cudaSuccess || cudaEventSynchronize(b) != cudaSuccess ||
+              cudaEventElapsedTime(&t, a, b) != cudaSuccess))
+    rc = fail(PMB_ERR_CUDA, "timing events");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (!rc) rc = check_status(s);
+  *ms = (double)t / n;
+  return rc;
 }
 
 int pmb_md_device_bytes(const pmb_md *m, unsigned long long *bytes) {

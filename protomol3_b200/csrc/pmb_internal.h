@@ -94,6 +94,7 @@ struct PairLaunch {
   const float *ljf;               // float copy
   const double *lattice;          // [nlat_total*3]
   int multi;                      // some box needs Ewald lattice images
+  int ctas_per_sm;                // resident CTAs per SM of the persistent kernel (0: all that fit)
   PairParams p;
 };
 int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st);

@@ -910,9 +910,9 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
   size_t smem = ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx) +
                                         (VIR ? 8 : 2) * 32 * sizeof(long long) + warp_pref_bytes<MIXED>());
-  static int resident = 0;
+  static int n_sm = 0, occupancy = 0;
   static size_t conf_smem = 0;
-  if (!resident || conf_smem != smem) {
+  if (!n_sm || conf_smem != smem) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, nsm = 0, occ = 0;
@@ -920,10 +920,14 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, PAIR_THREADS, smem);
     if (occ < 1) occ = 1;
-    resident = nsm * occ;
+    n_sm = nsm;
+    occupancy = occ;
     conf_smem = smem;
   }
-  const int grid = resident;  // persistent: every resident CTA walks its share of the tiles
+  // persistent: every resident CTA walks its share of the tiles (chunks claimed from a counter,
+  // so any grid size gives the same result)
+  const int per_sm = pl.ctas_per_sm > 0 && pl.ctas_per_sm < occupancy ? pl.ctas_per_sm : occupancy;
+  const int grid = n_sm * per_sm;
   using T = typename std::conditional<MIXED, float, double>::type;
   kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, params_t<T>(pl.p), pl.lj, pl.lattice);
   return 0;

@@ -113,6 +113,20 @@ class Topology:
     def set_skin(self, skin):
         L.check(L.lib().pmb_system_set_skin(self.system(), float(skin)))
 
+    def tuning(self):
+        """The speed knobs of this system: dict of skin, sort_cell, pair_ctas_per_sm."""
+        t = L.Tuning()
+        L.check(L.lib().pmb_system_get_tuning(self.system(), C.byref(t)))
+        return {"skin": t.skin, "sort_cell": t.sort_cell, "pair_ctas_per_sm": t.pair_ctas_per_sm}
+
+    def set_tuning(self, skin=None, sort_cell=None, pair_ctas_per_sm=None):
+        cur = self.tuning()
+        t = L.Tuning()
+        t.skin = cur["skin"] if skin is None else float(skin)
+        t.sort_cell = cur["sort_cell"] if sort_cell is None else float(sort_cell)
+        t.pair_ctas_per_sm = cur["pair_ctas_per_sm"] if pair_ctas_per_sm is None else int(pair_ctas_per_sm)
+        L.check(L.lib().pmb_system_set_tuning(self.system(), C.byref(t)))
+
     def set_vacuum(self, on=True):
         """Vacuum boundary conditions for the cutoff forces: the box (edges from
         ``vacuum_box``) stands in for vacuum, and evaluations refuse positions spread over half
@@ -447,6 +461,12 @@ class Integrator:
         pos, vel = np.zeros((n, 3)), np.zeros((n, 3))
         L.check(L.lib().pmb_md_get_state(self._h, _p(pos), _p(vel)))
         return pos, vel
+
+    def time_steps(self, n):
+        """Mean device time (ms) of a step over n steps (CUDA events on the system's stream)."""
+        ms = C.c_double(0.0)
+        L.check(L.lib().pmb_md_time(self._h, int(n), C.byref(ms)))
+        return ms.value
 
     def kernels_per_step(self):
         """Kernel launches of one MD step (the list-rebuild kernels exit at once when no rebuild
