@@ -8,7 +8,11 @@
 //     (topology/PeriodicBoundaryConditions.cpp:79-106);
 //   * grid tables exp(-pi^2 m^2/alpha^2) and the B-spline moduli (Grid.h:498-600).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -186,6 +190,97 @@ int valid_switch(int k) { return k == SW_CUTOFF || k == SW_C1 || k == SW_C2; }
 }  // namespace
 
 // ================================================================================== system
+// Threads that add the forces of a host-pointer evaluation into the caller's array while the
+// device->host copies land piece by piece: worker k (the calling thread is worker 0) waits for
+// each piece's event and adds its share of the piece.  Workers spin for a while between
+// evaluations (back-to-back MD steps) and then block.
+struct AddPool {
+  int nthreads = 1, device = 0;
+  std::vector<std::thread> th;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::atomic<long long> gen{0};
+  std::atomic<int> pending{0};
+  std::atomic<bool> stop{false};
+  // the job
+  double *dst = nullptr;
+  const double *src = nullptr;
+  long long n = 0, chunk = 0;
+  int nchunks = 0;
+  const cudaEvent_t *ev = nullptr;  // ev[c]: piece c has landed
+
+  void part(int k) {
+    for (int c = 0; c < nchunks; c++) {
+      cudaEventSynchronize(ev[c]);
+      const long long b0 = c * chunk, b1 = std::min(n, b0 + chunk), len = b1 - b0;
+      const long long q0 = b0 + len * k / nthreads, q1 = b0 + len * (k + 1) / nthreads;
+      double *__restrict__ d = dst;
+      const double *__restrict__ s = src;
+      for (long long i = q0; i < q1; i++) d[i] += s[i];
+    }
+  }
+  void worker(int k) {
+    cudaSetDevice(device);
+    long long seen = 0;
+    for (;;) {
+      // spin up to ~2 ms for the next job, then block
+      auto t0 = std::chrono::steady_clock::now();
+      while (gen.load(std::memory_order_acquire) == seen && !stop &&
+             std::chrono::steady_clock::now() - t0 < std::chrono::milliseconds(2))
+        std::this_thread::yield();
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop.load() || gen.load(std::memory_order_acquire) != seen; });
+        if (stop) return;
+        seen = gen.load(std::memory_order_acquire);
+      }
+      part(k);
+      pending.fetch_sub(1, std::memory_order_acq_rel);
+    }
+  }
+  void start(int threads, int dev) {
+    nthreads = threads;
+    device = dev;
+    for (int k = 1; k < nthreads; k++) th.emplace_back([this, k] { worker(k); });
+  }
+  // dst[0..n) += src[0..n), piece c of `chunk` elements once ev[c] has completed
+  void run(double *d, const double *s, long long n_, long long chunk_, int nchunks_, const cudaEvent_t *ev_) {
+    dst = d;
+    src = s;
+    n = n_;
+    chunk = chunk_;
+    nchunks = nchunks_;
+    ev = ev_;
+    pending.store(nthreads - 1, std::memory_order_release);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      gen.fetch_add(1, std::memory_order_acq_rel);
+    }
+    cv.notify_all();
+    part(0);
+    while (pending.load(std::memory_order_acquire) > 0) std::this_thread::yield();
+  }
+  ~AddPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv.notify_all();
+    for (std::thread &t : th) t.join();
+  }
+};
+
+// A host-pointer evaluation captured as a CUDA graph: the force passes, the conversions and the
+// device->host copies with their events, for one force set and virial flag.
+struct EvalGraph {
+  std::vector<unsigned long long> ids;
+  int virial = 0;
+  long long gen = -1;  // list storage generation it was captured with
+  double rlist = 0.0;
+  bool used_list = false;
+  cudaGraphExec_t exec = nullptr;
+};
+
 struct pmb_system {
   int precision = 0, nbox = 0, natoms = 0, ntypes = 0;
   cudaStream_t stream = nullptr;
@@ -217,6 +312,10 @@ struct pmb_system {
   cudaEvent_t ev_out[EVAL_CHUNKS + 1] = {};
   double eval_ms[3] = {0.0, 0.0, 0.0};  // last pmb_evaluate: enqueue, wait, accumulate (host ms)
   bool last_used_list = false;          // the last evaluation ran the list kernels
+  bool eval_graph = true;               // host-pointer evaluations replay captured graphs
+  AddPool *add_pool = nullptr;          // made at the first large host-pointer evaluation
+  std::vector<EvalGraph> eval_graphs;   // at most EVAL_GRAPHS, most recent last
+  static constexpr int EVAL_GRAPHS = 4;
   // neighbour list
   bool nb_ready = false;
   double nb_cutoff = 0.0;    // radius the list storage is sized for
@@ -252,6 +351,9 @@ struct pmb_system {
     return s;
   }
   ~pmb_system() {
+    delete add_pool;
+    for (EvalGraph &g : eval_graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : ev_out)
       if (e) cudaEventDestroy(e);
     if (flush_buf) cudaFree(flush_buf);
@@ -267,6 +369,7 @@ struct pmb_system {
 };
 
 struct pmb_force {
+  unsigned long long id = 0;  // unique over the process (keys the captured evaluations)
   pmb_system *sys = nullptr;
   pmb_force_desc d{};
   int kind = 0;
@@ -367,10 +470,12 @@ int nblist_alloc(pmb_system *s, double rl) {
   int maxn = std::max(nb.nkeys, nblk) + 1;
   nb.scan_tmp = s->nba.get<int>(maxn / 4096 + 2);
   nb.xref = s->nba.get<double>(3 * (size_t)s->natoms);
-  nb.ctl = s->nba.get<unsigned>(8);
+  nb.ctl = s->nba.get<unsigned>(12);
   nb.half_skin2 = (float)(0.25 * s->skin * s->skin);
   if (!nb.xref || !nb.ctl) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
-  const unsigned ctl0[8] = {0u, 0u, 0u, 1u, 0u, 0u, 0u, 0u};  // first use builds the list
+  // {max displacement, rebuild, finished blocks, forced rebuild, builds (64-bit), pair chunk
+  // counter and finished warps of the two pair launches}; first use builds the list
+  const unsigned ctl0[12] = {0u, 0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   CK(cudaMemcpy(nb.ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice));
   s->nb_build_rl = -1.0;
   if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.blk_c || !nb.blk_h || !nb.sblk_c || !nb.sblk_h || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.fslot ||
@@ -467,6 +572,18 @@ void mark(void *ctx, const char *name) {
 }
 
 // Enqueues every force of the set on the system stream; accumulators must be zero.
+// The second (higher-priority) stream of the system and its fork / join events.
+int ensure_side_stream(pmb_system *s) {
+  if (s->side) return PMB_OK;
+  int lo = 0, hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  CK(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi));
+  CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s->ev_slots, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  return PMB_OK;
+}
+
 // The neighbour-list radius a force set needs (pair cutoff + skin + a margin for the fixed-point
 // culling), or 0 when no force of the set uses the list (no pair term, no PME reciprocal term).
 double list_radius(pmb_system *s, pmb_force *const *fs, int n) {
@@ -497,16 +614,8 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   if (split && !s->side) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) {
-      split = false;  // created outside a capture only
-    } else {
-      int lo = 0, hi = 0;
-      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-      CK(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, hi));
-      CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&s->ev_slots, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
-    }
+    if (cs != cudaStreamCaptureStatusNone) split = false;  // created outside a capture only
+    else if (int rc = ensure_side_stream(s)) return rc;
   }
   cudaStream_t so = st;
   if (split) {
@@ -565,9 +674,33 @@ int enqueue_forces(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     pl.lattice = j.lattice;
     pl.multi = 0;
     pl.ctas_per_sm = s->pair_ctas;
-    if (j.p.coul_mode == 2 && j.lattice)
-      for (const BoxDev &b : s->hbox) pl.multi |= b.multi_image;
-    if (pair_launch(sd, s->nb, pl, st)) return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+    pl.blk_lo = 0;
+    pl.blk_hi = s->nb.nblk_total;
+    pl.wslot = 0;
+    int split_blk = -1;  // first block of the lattice-image suffix
+    if (j.p.coul_mode == 2 && j.lattice) {
+      int first = s->nb.nblk_total, nmulti = 0;
+      for (const BoxDev &b : s->hbox)
+        if (b.multi_image) {
+          pl.multi = 1;
+          first = std::min(first, b.blk0);
+          nmulti += b.nblk;
+        }
+      if (pl.multi && first > 0 && first + nmulti == s->nb.nblk_total) split_blk = first;
+    }
+    if (split_blk > 0) {
+      // the boxes that need no lattice image on the faster instance, the rest (a suffix of the
+      // tile map) on the lattice-image one, each with its own chunk counter
+      PairLaunch pa = pl, pb = pl;
+      pa.multi = 0;
+      pa.blk_hi = split_blk;
+      pb.blk_lo = split_blk;
+      pb.wslot = 1;
+      if (pair_launch(sd, s->nb, pa, st) || pair_launch(sd, s->nb, pb, st))
+        return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+    } else if (pair_launch(sd, s->nb, pl, st)) {
+      return fail(PMB_ERR_UNSUPPORTED, "too many LJ types");
+    }
     mark(s, "pair");
   }
   if (split) {
@@ -589,6 +722,90 @@ void add_const(pmb_force *const *fs, int n, int nbox, int virial, double *e) {
         for (int k = 0; k < 9; k++) e[b * ACC_PER_BOX + E_VIR + k] += fs[i]->const_vir[b * 9 + k];
     }
   }
+}
+
+// Device->host copies of a host-pointer evaluation on the system stream (inside or outside a
+// capture): status and energies, then the forces in EVAL_CHUNKS pieces, each followed by its
+// event (external events, so that the host can wait on them when they come from a graph).
+int enqueue_eval_copies(pmb_system *s) {
+  cudaStream_t st = s->stream;
+  const long long nf = 3LL * s->natoms;
+  const long long chunk = (nf + pmb_system::EVAL_CHUNKS - 1) / pmb_system::EVAL_CHUNKS;
+  if (s->nb_ready) CK(cudaMemcpyAsync(s->h_status, s->nb.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(s->h_eout, s->d_eout, sizeof(double) * s->nbox * ACC_PER_BOX, cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecordWithFlags(s->ev_out[0], st, cudaEventRecordExternal));
+  for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
+    const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
+    if (b1 > b0)
+      CK(cudaMemcpyAsync(s->h_fout + b0, s->d_fout + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecordWithFlags(s->ev_out[c + 1], st, cudaEventRecordExternal));
+  }
+  return PMB_OK;
+}
+
+// One host-pointer evaluation's device work (the positions are already on the device): from a
+// CUDA graph of the force set, captured at its first use.  A graph is kept while the list
+// storage it captured stays (generation) and the list radius is unchanged; the list storage and
+// radius are settled before any capture, so a captured step neither allocates nor forces a
+// rebuild on every replay.
+int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
+  cudaStream_t st = s->stream;
+  const double rlist = list_radius(s, fs, n);
+  if (rlist > 0.0) {
+    int rc = ensure_nblist(s, rlist);
+    if (rc) return rc;
+    if (rlist != s->nb_build_rl) {
+      CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, st));
+      s->nb_build_rl = rlist;
+    }
+  }
+  if (int rc = ensure_side_stream(s)) return rc;
+  std::vector<unsigned long long> ids(n);
+  for (int i = 0; i < n; i++) ids[i] = fs[i]->id;
+  EvalGraph *g = nullptr;
+  for (size_t k = 0; k < s->eval_graphs.size(); k++) {
+    EvalGraph &e = s->eval_graphs[k];
+    if (e.ids == ids && e.virial == virial && e.gen == s->nb_gen && e.rlist == rlist) {
+      std::rotate(s->eval_graphs.begin() + k, s->eval_graphs.begin() + k + 1, s->eval_graphs.end());
+      g = &s->eval_graphs.back();
+      break;
+    }
+  }
+  if (!g) {
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    SystemDev sd = s->dev();
+    zero_accumulators(sd, st);
+    int rc = enqueue_forces(s, fs, n, virial);
+    if (!rc) {
+      forces_to_double(sd, s->d_fout, st);
+      energies_to_double(sd, nullptr, s->d_eout, st);
+      rc = enqueue_eval_copies(s);
+    }
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc ? rc : fail(PMB_ERR_CUDA, std::string("evaluation capture: ") + cudaGetErrorString(e));
+    }
+    EvalGraph ng;
+    ng.ids = ids;
+    ng.virial = virial;
+    ng.gen = s->nb_gen;
+    ng.rlist = rlist;
+    ng.used_list = s->last_used_list;
+    e = cudaGraphInstantiate(&ng.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(PMB_ERR_CUDA, std::string("evaluation graph: ") + cudaGetErrorString(e));
+    if ((int)s->eval_graphs.size() >= pmb_system::EVAL_GRAPHS) {
+      cudaGraphExecDestroy(s->eval_graphs.front().exec);
+      s->eval_graphs.erase(s->eval_graphs.begin());
+    }
+    s->eval_graphs.push_back(ng);
+    g = &s->eval_graphs.back();
+  }
+  s->last_used_list = g->used_list;
+  CK(cudaGraphLaunch(g->exec, st));
+  return PMB_OK;
 }
 
 // The status words as they were copied to s->h_status: capacity before non-finite positions
@@ -754,6 +971,20 @@ pmb_system *pmb_system_create(const pmb_box_desc *boxes, int n_boxes, int precis
     epart[estart[b] + fill[b]] = a;
     ekind[estart[b] + fill[b]++] = s->h_excl_kind[k];
   }
+  // Slot blocks of the boxes in order of decreasing smallest edge (stable): boxes small enough to
+  // need Ewald lattice images come last in the tile map, so the pair kernel's lattice-image
+  // instance runs over that suffix alone.  Atoms keep the caller's order.
+  {
+    std::vector<int> order(s->nbox);
+    for (int bi = 0; bi < s->nbox; bi++) order[bi] = bi;
+    auto min_edge = [&](int bi) { return std::min(s->hbox[bi].L[0], std::min(s->hbox[bi].L[1], s->hbox[bi].L[2])); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return min_edge(a) > min_edge(b); });
+    int b0 = 0;
+    for (int bi : order) {
+      s->hbox[bi].blk0 = b0;
+      b0 += s->hbox[bi].nblk;
+    }
+  }
   int rc = 0;
   rc |= upload(s->a, s->d_box, s->hbox);
   rc |= upload(s->a, s->d_atom_box, s->h_atom_box);
@@ -898,6 +1129,8 @@ int pmb_system_evaluate_times(const pmb_system *s, double ms[3]) {
 pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
   if (!s || !d) return fail(PMB_ERR_ARG, "null argument"), nullptr;
   pmb_force *f = new pmb_force();
+  static std::atomic<unsigned long long> next_id{1};
+  f->id = next_id++;
   f->sys = s;
   f->d = *d;
   f->kind = d->kind;
@@ -1295,21 +1528,19 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
     for (cudaEvent_t &e : s->ev_out) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   const long long nf = 3LL * s->natoms;
   const long long chunk = (nf + pmb_system::EVAL_CHUNKS - 1) / pmb_system::EVAL_CHUNKS;
+  // a captured graph per force set, except under the stage profiler or on the legacy stream
+  const bool graphed = s->eval_graph && !s->prof && st != nullptr && st != cudaStreamLegacy;
   for (int attempt = 0; attempt < 3; attempt++) {
     CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
     s->have_pos = true;
-    int rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
-    if (rc) return rc;
-    // status and energies first, then the forces piece by piece
-    if (s->nb_ready) CK(cudaMemcpyAsync(s->h_status, s->nb.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(s->h_eout, s->d_eout, sizeof(double) * s->nbox * ACC_PER_BOX, cudaMemcpyDeviceToHost, st));
-    CK(cudaEventRecord(s->ev_out[0], st));
-    for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
-      const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
-      if (b1 > b0)
-        CK(cudaMemcpyAsync(s->h_fout + b0, s->d_fout + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost, st));
-      CK(cudaEventRecord(s->ev_out[c + 1], st));
+    int rc;
+    if (graphed) {
+      rc = eval_graph_launch(s, fs, n, virial);
+    } else {
+      rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
+      if (!rc) rc = enqueue_eval_copies(s);
     }
+    if (rc) return rc;
     const clk::time_point t1 = clk::now();
     CK(cudaEventSynchronize(s->ev_out[0]));
     const clk::time_point t2 = clk::now();
@@ -1326,13 +1557,25 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
       continue;
     }
     if (rc) return rc;
-    for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
-      CK(cudaEventSynchronize(s->ev_out[c + 1]));
-      if (!forces) continue;
-      const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
-      double *__restrict__ dst = forces;
-      const double *__restrict__ src = s->h_fout;
-      for (long long i = b0; i < b1; i++) dst[i] += src[i];
+    if (forces && nf >= (1 << 16)) {
+      // large systems: the pool's threads share every piece as it lands
+      if (!s->add_pool) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        s->add_pool = new AddPool();
+        s->add_pool->start((int)std::max(1u, std::min(4u, hw / 4)), dev);
+      }
+      s->add_pool->run(forces, s->h_fout, nf, chunk, pmb_system::EVAL_CHUNKS, s->ev_out + 1);
+    } else {
+      for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
+        CK(cudaEventSynchronize(s->ev_out[c + 1]));
+        if (!forces) continue;
+        const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
+        double *__restrict__ dst = forces;
+        const double *__restrict__ src = s->h_fout;
+        for (long long i = b0; i < b1; i++) dst[i] += src[i];
+      }
     }
     const clk::time_point t3 = clk::now();
     s->eval_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();

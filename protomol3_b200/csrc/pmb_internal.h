@@ -95,6 +95,8 @@ struct PairLaunch {
   const double *lattice;          // [nlat_total*3]
   int multi;                      // some box needs Ewald lattice images
   int ctas_per_sm;                // resident CTAs per SM of the persistent kernel (0: all that fit)
+  int blk_lo, blk_hi;             // the blocks whose tiles this launch evaluates
+  int wslot;                      // which chunk counter of the list's ctl words it uses (0 or 1)
   PairParams p;
 };
 int pair_launch(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cudaStream_t st);

@@ -436,7 +436,7 @@ template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI>
 __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR_MINB : 2)
     k_pair(SystemDev s, NbListDev nb, PairParams p,
            ParamsT<typename std::conditional<MIXED, float, double>::type> pt, const double *ljd,
-           const double *lat) {
+           const double *lat, int blk_lo, int blk_hi, int wslot) {
   using T = typename std::conditional<MIXED, float, double>::type;
   using T2 = typename std::conditional<MIXED, float2, double2>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -462,8 +462,10 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
   float4 *qb = qa + FAST_ENTRIES;
   int2 *qt = reinterpret_cast<int2 *>(reinterpret_cast<float4 *>(wstage) + 2 * FAST_ENTRIES) + qe;
   const int gwarp = blockIdx.x * PAIR_WARPS + wib, nwarps = gridDim.x * PAIR_WARPS;
-  int total = nb.tile_off[nb.nblk_total];
-  if (total > nb.tile_cap) total = nb.tile_cap;
+  // this launch's tiles: those of blocks [blk_lo, blk_hi)
+  int t_lo = nb.tile_off[blk_lo], t_hi = nb.tile_off[blk_hi];
+  if (t_hi > nb.tile_cap) t_hi = nb.tile_cap;
+  if (t_lo > t_hi) t_lo = t_hi;
 
   int curI = -1, curBox = -1;
   // energies (and virials) per lane: summed in the arithmetic type over a chunk of tiles, then
@@ -624,19 +626,19 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
   };
 
   // Tiles go to warps in chunks of CHUNK consecutive tiles: chunk gwarp first, then the next
-  // unclaimed chunk from a counter (ctl[6]), so warps that start late (SMs busy with the PME
+  // unclaimed chunk from the launch's counter (ctl[6 + 2 wslot]), so warps that start late (SMs busy with the PME
   // kernels beside this one) take fewer chunks.  The floating-point partial sums (i-forces,
   // energies, virial) are closed at every chunk end, so the result does not depend on which warp
   // took which chunk.  Per chunk the tile records and their j-list words are fetched once (one
   // round trip each); each tile's slot records are copied one tile ahead into the other buffer,
   // so only the first tile of a chunk waits for them.
-  unsigned *wq = nb.ctl + 6;
-  const int nchunk = (total + CHUNK - 1) / CHUNK;
+  unsigned *wq = nb.ctl + 6 + 2 * wslot;
+  const int nchunk = (t_hi - t_lo + CHUNK - 1) / CHUNK;
   for (int ci = gwarp; ci < nchunk;) {
     int tnext = 0;
     if (lane == 0) tnext = nwarps + (int)atomicAdd(wq, 1u);  // claimed now, read at chunk end
-    const int c0 = ci * CHUNK;
-    const int nc = min(CHUNK, total - c0);
+    const int c0 = t_lo + ci * CHUNK;
+    const int nc = min(CHUNK, t_hi - c0);
     tI = -1;
     tk = -1;
     tjb = 0;
@@ -929,7 +931,8 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   const int per_sm = pl.ctas_per_sm > 0 && pl.ctas_per_sm < occupancy ? pl.ctas_per_sm : occupancy;
   const int grid = n_sm * per_sm;
   using T = typename std::conditional<MIXED, float, double>::type;
-  kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, params_t<T>(pl.p), pl.lj, pl.lattice);
+  kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, params_t<T>(pl.p), pl.lj, pl.lattice, pl.blk_lo, pl.blk_hi,
+                                         pl.wslot);
   return 0;
 }
 

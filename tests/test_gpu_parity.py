@@ -156,9 +156,10 @@ def test_batched_boxes_match_single(precision):
     for k, (b, g) in enumerate(zip(boxes, grids)):
         fs, es, _ = gpu_eval(b, forces([[g] * 3]), precision)
         n = len(b["charge"])
-        # the same box alone and inside the batch: equal within the precision's tolerance (a
-        # batch that contains a box smaller than twice the cutoff runs the lattice-image kernel
-        # instance for all its boxes, whose compiled arithmetic may round differently)
+        # the same box alone and inside the batch: equal within the precision's tolerance (the
+        # partial sums of a batch close at other tile boundaries, and a box smaller than twice the
+        # cutoff runs on the lattice-image kernel instance, whose compiled arithmetic may round
+        # differently)
         assert rel_rms(fb[off:off + n], fs) < TOL[precision] * 0.1
         np.testing.assert_allclose(eb.table[k, :4], es.table[0, :4], rtol=TOL[precision],
                                    atol=n * 2.0 ** -30)
