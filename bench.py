@@ -320,9 +320,21 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    # the speed knobs (skin, sort cells, pair CTAs per SM) of each precision's system, picked by
+    # the autotuner from whole MD steps before anything is timed; they change no evaluated pair
+    tuned = {}
+    if not args.no_tune:
+        from protomol3_b200 import autotune as AT
+        tuner = AT.Autotuner(steps=30, warmup=10)
+        for prec in ([args.precision] + (["fp64"] if args.precision == "mixed" and not args.no_fp64 else [])):
+            tuned[prec] = tuner.tune_knobs([box], [GRID], RC, SWITCHON, order=4, precision=prec,
+                                           stream=stream.cuda_stream)
+
     def make(precision):
         topo = F.Topology(box, precision)
         topo.set_stream(stream.cuda_stream)
+        if precision in tuned:
+            topo.set_tuning(**tuned[precision]["knobs"])
         fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", SWITCHON, RC)),
               F.NonbondedPMEwaldSystemForce((GRID,) * 3, RC)]
         return topo, fl
@@ -465,7 +477,9 @@ def run_b200(args, rank, world, local_rank):
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": dict(config_dict(), precision=args.precision,
-                       parallelism="replicas" if world > 1 else "single"),
+                       parallelism="replicas" if world > 1 else "single",
+                       tuning={k: {"knobs": v["knobs"], "untuned_ms_per_step": v["default_ms_per_step"],
+                                   "search_s": v["search_s"]} for k, v in tuned.items()}),
         "clocks": clk, "gpu_launches": kps, "list_rebuilds": rebuilds, "e2e": e2e,
         "roofline": {"bound": "fp32", "kernel": "k_pair (LJ C2 + Ewald real space)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -826,6 +840,7 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=5)
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-box ensemble leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-tune", action="store_true", help="default knobs instead of the autotuner's")
     ap.add_argument("--chunk", type=int, default=500, help="nve: steps between energy reads")
     ap.add_argument("--serve-requests", type=int, default=24, help="serve: requests per load level")
     ap.add_argument("--mode", choices=["bench", "profile", "batch", "nve", "serve", "rigid", "frames"], default="bench",

@@ -235,7 +235,7 @@ int pmb_md_use_graph(pmb_md *md, int enable);
 /* Runs n_steps (pmb_md_run) between two CUDA events on the system's stream and returns the mean
  * device time per step in ms (the autotuner's clock). */
 int pmb_md_time(pmb_md *md, int n_steps, double *ms_per_step);
-/* Bond constraints of a leapfrog run (replaces ModifierShake / ModifierRattle as
+/* Bond constraints of a leapfrog or Langevin run (replaces ModifierShake / ModifierRattle as
  * module/ModifierModule.cpp:106-128 installs them): SHAKE after every drift, RATTLE after every
  * step, on a constraint list in the reference's order (topology/TopologyUtilities.cpp:695-775,
  * buildRattleShakeBondConstraintList).  A modifier is on when its flag is set, epsilon > 0 and
@@ -243,8 +243,10 @@ int pmb_md_time(pmb_md *md, int n_steps, double *ms_per_step);
  * reference does until the mean error is at most epsilon, at most max_iter + 1 sweeps; the
  * constraint virial is not accumulated.  Constrained groups (atoms linked by constraints) hold at
  * most 8 atoms and 16 constraints; max_iter below 256.  The SHAKE reference positions are the
- * positions at pmb_md_set_state, or the current ones when this is called after it.
- * PMB_ERR_UNSUPPORTED for the Langevin integrator. */
+ * positions at pmb_md_set_state, or the current ones when this is called after it.  With the
+ * Langevin integrator the modifiers sit where StandardIntegrator::run calls them
+ * (integrator/StandardIntegrator.cpp:27-37; STSIntegrator::doDriftOrNextIntegrator): SHAKE after
+ * the drift, RATTLE after the step's closing half kick. */
 typedef struct {
   int n_constraints;
   const int *atom1, *atom2;   /* [n_constraints] */

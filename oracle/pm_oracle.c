@@ -1015,3 +1015,34 @@ int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
   memcpy(energies_out, e, sizeof(e));
   return 0;
 }
+
+/* LangevinLeapfrogIntegrator run(nsteps) with SHAKE as a post-drift modifier and RATTLE as a
+ * post-step modifier (integrator/StandardIntegrator.cpp:27-37: half kick, doDriftOrNextIntegrator
+ * = drift then the post-drift modifiers, forces, half kick, the post-step modifiers;
+ * integrator/STSIntegrator.cpp:28-32), the half kicks as orc_langevin. */
+int orc_langevin_constrained(const orc_system *s, const orc_cutoff_params *cp, const orc_pme_params *pme,
+                             int do_bonded, const orc_constraints *c, double dt_fs, double temperature,
+                             double gamma_ps, unsigned long long seed, long long first_step, int nsteps,
+                             double *pos, double *vel, double *last_pos, double *forces_out,
+                             double *energies_out) {
+  const int n = s->n;
+  const int shake = c && c->n > 0 && c->shake_eps > 0 && c->shake_maxiter > 0;
+  const int rattle = c && c->n > 0 && c->rattle_eps > 0 && c->rattle_maxiter > 0;
+  double *f = forces_out, e[ORC_E_COUNT];
+  const double h = dt_fs * INV_TIMEFACTOR;
+  const double gamma = gamma_ps / (1000 * INV_TIMEFACTOR);
+  const double kT = BOLTZMANN * temperature;
+  if (!(gamma > 0) || temperature < 0) return 1;
+  all_forces(s, cp, pme, do_bonded, pos, f, e);
+  for (int st = 0; st < nsteps; st++) {
+    long long j = 2 * (first_step + st);
+    langevin_half_kick(s, f, h, gamma, kT, seed, j, vel);
+    for (int i = 0; i < 3 * n; i++) pos[i] += vel[i] * h;
+    if (shake) orc_shake(c, s->mass, n, dt_fs, pos, vel, last_pos);
+    all_forces(s, cp, pme, do_bonded, pos, f, e);
+    langevin_half_kick(s, f, h, gamma, kT, seed, j + 1, vel);
+    if (rattle) orc_rattle(c, s->mass, dt_fs, pos, vel);
+  }
+  memcpy(energies_out, e, sizeof(e));
+  return 0;
+}

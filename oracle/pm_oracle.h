@@ -126,6 +126,14 @@ int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
                              double dt_fs, int nsteps, double *pos, double *vel, double *last_pos,
                              double *forces_out, double *energies_out);
 
+/* LangevinLeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step), the half kicks
+ * and noise as orc_langevin, the modifiers as orc_leapfrog_constrained. */
+int orc_langevin_constrained(const orc_system *s, const orc_cutoff_params *cp, const orc_pme_params *pme,
+                             int do_bonded, const orc_constraints *c, double dt_fs, double temperature,
+                             double gamma_ps, unsigned long long seed, long long first_step, int nsteps,
+                             double *pos, double *vel, double *last_pos, double *forces_out,
+                             double *energies_out);
+
 #ifdef __cplusplus
 }
 #endif

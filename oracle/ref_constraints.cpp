@@ -15,6 +15,7 @@ using namespace ProtoMol::Report;
 
 #include <protomol/ProtoMolApp.h>
 #include <protomol/force/ForceGroup.h>
+#include <protomol/integrator/base/LangevinLeapfrogIntegrator.h>
 #include <protomol/integrator/leapfrog/LeapfrogIntegrator.h>
 #include <protomol/modifier/ModifierRattle.h>
 #include <protomol/modifier/ModifierShake.h>
@@ -43,11 +44,13 @@ defineInputValue(InputOutputfreq, "outputfreq")
 // elem[i]: first letter of atom i's name ('O', 'H', ...), which is all the constraint builder
 // reads of a name.  On return: pos/vel after run(nsteps); cons[3k..3k+2] = atom1, atom2 and
 // rest_len[k] of the first max_cons constraints of the reference's list; *n_cons its length.
-extern "C" int ref_leapfrog_constrained(const ref_input *in, const char *elem, int shake,
-                                        double shake_eps, int shake_maxiter, int rattle,
-                                        double rattle_eps, int rattle_maxiter, int all,
-                                        double dt_fs, int nsteps, double *pos, double *vel,
-                                        int *n_cons, int *cons, double *rest_len, int max_cons) {
+// kind 0: LeapfrogIntegrator(dt); kind 1: LangevinLeapfrogIntegrator(dt, temperature, gamma_ps,
+// seed), its half kicks and drift with the modifiers where StandardIntegrator::run places them.
+static int run_constrained(const ref_input *in, const char *elem, int shake, double shake_eps,
+                           int shake_maxiter, int rattle, double rattle_eps, int rattle_maxiter, int all,
+                           int kind, double dt_fs, double temperature, double gamma_ps, int seed,
+                           int nsteps, double *pos, double *vel, int *n_cons, int *cons, double *rest_len,
+                           int max_cons) {
   Topo *t = make_topo(in);
   for (int i = 0; i < in->n; i++) t->atoms[i].name = std::string(1, elem[i]);
   // what the topology builder sets besides: each atom's bond list and each molecule's atoms
@@ -70,7 +73,11 @@ extern "C" int ref_leapfrog_constrained(const ref_input *in, const char *elem, i
       app->positions[i][c] = pos[3 * i + c];
       app->velocities[i][c] = vel[3 * i + c];
     }
-  LeapfrogIntegrator *li = new LeapfrogIntegrator(dt_fs, new ForceGroup());
+  STSIntegrator *li;
+  if (kind == 1)
+    li = new LangevinLeapfrogIntegrator(dt_fs, temperature, gamma_ps, seed, new ForceGroup());
+  else
+    li = new LeapfrogIntegrator(dt_fs, new ForceGroup());
   li->initialize(app);
   if (shake) li->adoptPostDriftOrNextModifier(new ModifierShake(shake_eps, shake_maxiter, all != 0));
   if (rattle) li->adoptPostStepModifier(new ModifierRattle(rattle_eps, rattle_maxiter, all != 0));
@@ -89,4 +96,25 @@ extern "C" int ref_leapfrog_constrained(const ref_input *in, const char *elem, i
     rest_len[k] = cl[k].restLength;
   }
   return 0;
+}
+
+extern "C" int ref_leapfrog_constrained(const ref_input *in, const char *elem, int shake,
+                                        double shake_eps, int shake_maxiter, int rattle,
+                                        double rattle_eps, int rattle_maxiter, int all,
+                                        double dt_fs, int nsteps, double *pos, double *vel,
+                                        int *n_cons, int *cons, double *rest_len, int max_cons) {
+  return run_constrained(in, elem, shake, shake_eps, shake_maxiter, rattle, rattle_eps, rattle_maxiter, all, 0,
+                         dt_fs, 0.0, 0.0, 0, nsteps, pos, vel, n_cons, cons, rest_len, max_cons);
+}
+
+// The same with the LangevinLeapfrogIntegrator (temperature 0 makes its noise term vanish).
+extern "C" int ref_langevin_constrained(const ref_input *in, const char *elem, int shake,
+                                        double shake_eps, int shake_maxiter, int rattle,
+                                        double rattle_eps, int rattle_maxiter, int all, double dt_fs,
+                                        double temperature, double gamma_ps, int seed, int nsteps,
+                                        double *pos, double *vel, int *n_cons, int *cons,
+                                        double *rest_len, int max_cons) {
+  return run_constrained(in, elem, shake, shake_eps, shake_maxiter, rattle, rattle_eps, rattle_maxiter, all, 1,
+                         dt_fs, temperature, gamma_ps, seed, nsteps, pos, vel, n_cons, cons, rest_len,
+                         max_cons);
 }

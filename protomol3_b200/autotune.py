@@ -34,7 +34,7 @@ from . import waterbox as W
 
 SKINS = (0.5, 0.8, 1.1)
 SORT_CELLS = (1.8, 2.4, 3.2)
-PAIR_CTAS = (0, 2)
+PAIR_CTAS = (0, 2, 1)
 
 
 def grid_candidates(edge, spacing=1.0, headroom=0.15, minimum=8):
@@ -84,8 +84,10 @@ class Autotuner:
         return h.hexdigest()
 
     # ------------------------------------------------------------------ measurements
-    def _md_ms(self, boxes, grids, rc, switchon, order, precision, knobs):
+    def _md_ms(self, boxes, grids, rc, switchon, order, precision, knobs, stream=None):
         topo = F.Topology(boxes, precision)
+        if stream is not None:
+            topo.set_stream(stream)
         topo.set_tuning(**knobs)
         md = F.Integrator(topo, self.force_list(grids, rc, switchon, order), timestep=1.0)
         pos = np.concatenate([b["pos"] for b in boxes])
@@ -96,6 +98,48 @@ class Autotuner:
         md.close()
         topo.close()
         return ms
+
+    def _descend(self, measure):
+        """Coordinate descent over the system knobs from the defaults; a change is kept only
+        when it is clearly (0.5%) faster."""
+        knobs = {"skin": 0.8, "sort_cell": 2.4, "pair_ctas_per_sm": 0}
+        trials = []
+
+        def timed(kn):
+            ms = measure(kn)
+            trials.append(dict(kn, ms_per_step=ms))
+            if self.verbose:
+                print("autotune", kn, "%.4f ms" % ms, flush=True)
+            return ms
+        best = timed(knobs)
+        for name, values in (("skin", SKINS), ("sort_cell", SORT_CELLS), ("pair_ctas_per_sm", PAIR_CTAS)):
+            for v in values:
+                if v == knobs[name]:
+                    continue
+                kn = dict(knobs, **{name: v})
+                ms = timed(kn)
+                if ms < best * 0.995:
+                    best, knobs = ms, kn
+        return knobs, best, trials
+
+    def tune_knobs(self, boxes, grids, rc, switchon, order=4, precision="mixed", stream=None):
+        """The system knobs alone, for fixed PME grids (e.g. one large box), by whole MD steps."""
+        key = "knobs:" + self.signature(boxes, rc, switchon, order, precision) + ":" + ",".join(map(str, grids))
+        if key in self._cache:
+            return dict(self._cache[key], cached=True)
+        t0 = time.perf_counter()
+        knobs, best, trials = self._descend(
+            lambda kn: self._md_ms(boxes, grids, rc, switchon, order, precision, kn, stream))
+        out = {"knobs": knobs, "ms_per_step": best, "default_ms_per_step": trials[0]["ms_per_step"],
+               "trials": trials, "search_s": time.perf_counter() - t0}
+        self._cache[key] = out
+        self._save()
+        return dict(out, cached=False)
+
+    def _save(self):
+        if self.cache_path:
+            with open(self.cache_path, "w") as fh:
+                json.dump(self._cache, fh)
 
     def _pme_ms(self, box, grid, rc, order, precision):
         """PME (spread + transforms + gather) of ``class_copies`` copies of one box in one
@@ -133,24 +177,8 @@ class Autotuner:
             for k in c["boxes"]:
                 grids[k] = class_choice[n0]
         # system knobs, coordinate descent from the defaults
-        knobs = {"skin": 0.8, "sort_cell": 2.4, "pair_ctas_per_sm": 0}
-        trials = []
-
-        def measure(kn):
-            ms = self._md_ms(boxes, grids, rc, switchon, order, precision, kn)
-            trials.append(dict(kn, ms_per_step=ms))
-            if self.verbose:
-                print("autotune", kn, "%.4f ms" % ms, flush=True)
-            return ms
-        best = measure(knobs)
-        for name, values in (("skin", SKINS), ("sort_cell", SORT_CELLS), ("pair_ctas_per_sm", PAIR_CTAS)):
-            for v in values:
-                if v == knobs[name]:
-                    continue
-                kn = dict(knobs, **{name: v})
-                ms = measure(kn)
-                if ms < best * 0.995:  # keep a change only when it is clearly faster
-                    best, knobs = ms, kn
+        knobs, best, trials = self._descend(
+            lambda kn: self._md_ms(boxes, grids, rc, switchon, order, precision, kn))
         out = {"grids": grids, "knobs": knobs, "ms_per_step": best,
                "default_ms_per_step": trials[0]["ms_per_step"],
                "classes": {str(n0): {"boxes": len(c["boxes"]), "candidates": c["candidates"],
@@ -159,9 +187,7 @@ class Autotuner:
                            for n0, c in sorted(classes.items())},
                "trials": trials, "search_s": time.perf_counter() - t0}
         self._cache[key] = out
-        if self.cache_path:
-            with open(self.cache_path, "w") as fh:
-                json.dump(self._cache, fh)
+        self._save()
         return dict(out, cached=False)
 
     def apply(self, boxes, result, rc, switchon, order=4, precision="mixed"):

@@ -192,8 +192,8 @@ int valid_switch(int k) { return k == SW_CUTOFF || k == SW_C1 || k == SW_C2; }
 // ================================================================================== system
 // Threads that add the forces of a host-pointer evaluation into the caller's array while the
 // device->host copies land piece by piece: worker k (the calling thread is worker 0) waits for
-// each piece's event and adds its share of the piece.  Workers spin for a while between
-// evaluations (back-to-back MD steps) and then block.
+// each piece's event and adds its share of the piece.  Between evaluations the workers sleep on
+// a condition variable (spinning would take cores from the caller's own threads).
 struct AddPool {
   int nthreads = 1, device = 0;
   std::vector<std::thread> th;
@@ -223,11 +223,6 @@ struct AddPool {
     cudaSetDevice(device);
     long long seen = 0;
     for (;;) {
-      // spin up to ~2 ms for the next job, then block
-      auto t0 = std::chrono::steady_clock::now();
-      while (gen.load(std::memory_order_acquire) == seen && !stop &&
-             std::chrono::steady_clock::now() - t0 < std::chrono::milliseconds(2))
-        std::this_thread::yield();
       {
         std::unique_lock<std::mutex> lk(mu);
         cv.wait(lk, [&] { return stop.load() || gen.load(std::memory_order_acquire) != seen; });
@@ -301,6 +296,8 @@ struct pmb_system {
   bool have_pos = false;  // positions were uploaded at least once (evaluate, profile, set_state)
   int *d_excl_start = nullptr, *d_excl_partner = nullptr, *d_excl_kindc = nullptr;
   int *d_excl_pairs = nullptr, *d_excl_kind = nullptr;
+  int4 *d_swork = nullptr;   // PME spread work items (box, slot range), fixed by the block layout
+  int nswork = 0;
   BondedDev bonded{};
   long long *d_facc = nullptr, *d_eacc = nullptr;
   double *d_fout = nullptr, *d_eout = nullptr;
@@ -402,6 +399,8 @@ int nblist_alloc(pmb_system *s, double rl) {
   new (&s->nba) Allocs();
   NbListDev &nb = s->nb;
   std::memset(&nb, 0, sizeof(nb));
+  nb.swork = s->d_swork;
+  nb.nswork = s->nswork;
   int nblk = 0;
   for (auto &b : s->hbox) nblk += b.nblk;
   nb.nblk_total = nblk;
@@ -985,7 +984,17 @@ pmb_system *pmb_system_create(const pmb_box_desc *boxes, int n_boxes, int precis
       b0 += s->hbox[bi].nblk;
     }
   }
+  // PME spread work items: runs of PME_SPREAD_SLOTS slots of one box (Hilbert-contiguous, so a
+  // run's stencils cover a compact part of the box's grid)
+  std::vector<int4> swork;
+  for (int bi = 0; bi < s->nbox; bi++) {
+    const BoxDev &b = s->hbox[bi];
+    const int s0 = b.blk0 * BLOCK, s1 = (b.blk0 + b.nblk) * BLOCK;
+    for (int q = s0; q < s1; q += PME_SPREAD_SLOTS) swork.push_back(make_int4(bi, q, std::min(s1, q + PME_SPREAD_SLOTS), 0));
+  }
+  s->nswork = (int)swork.size();
   int rc = 0;
+  rc |= upload(s->a, s->d_swork, swork);
   rc |= upload(s->a, s->d_box, s->hbox);
   rc |= upload(s->a, s->d_atom_box, s->h_atom_box);
   rc |= upload(s->a, s->d_charge, s->h_charge);
@@ -1833,8 +1842,6 @@ int pmb_md_set_constraints(pmb_md *m, const pmb_constraint_desc *d) {
   const bool rattle = d->rattle && d->rattle_epsilon > 0 && d->rattle_max_iter > 0 && nc > 0;
   if ((shake && d->shake_max_iter >= CON_MAX_SWEEPS) || (rattle && d->rattle_max_iter >= CON_MAX_SWEEPS))
     return fail(PMB_ERR_ARG, "max_iter must be below 256");
-  if ((shake || rattle) && m->d.kind != PMB_LEAPFROG)
-    return fail(PMB_ERR_UNSUPPORTED, "constraints are supported with the leapfrog integrator");
   for (int k = 0; k < nc; k++) {
     const int a = d->atom1[k], b = d->atom2[k];
     if (a < 0 || b < 0 || a >= s->natoms || b >= s->natoms || a == b)
