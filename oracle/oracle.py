@@ -62,7 +62,8 @@ def lib():
         build()
         _lib = C.CDLL(LIB)
         for fn in ("orc_cutoff", "orc_pme", "orc_bonded", "orc_leapfrog",
-                   "orc_leapfrog_constrained", "orc_shake", "orc_rattle", "orc_langevin"):
+                   "orc_leapfrog_constrained", "orc_shake", "orc_rattle", "orc_langevin",
+                   "orc_langevin_constrained"):
             getattr(_lib, fn).restype = C.c_int
         _lib.orc_pme_alpha.restype = C.c_double
         _lib.orc_pme_alpha.argtypes = [C.c_double, C.c_double]
@@ -222,6 +223,34 @@ def leapfrog_constrained(system, pos, vel, dt, nsteps, constraints, shake=(1e-5,
     return pos, vel, f, e
 
 
+def langevin_constrained(system, pos, vel, dt, nsteps, constraints, temperature, gamma, seed=1234,
+                         first_step=0, shake=(1e-5, 30), rattle=(1e-5, 30), cutoff=None, pme=None,
+                         bonded=False, last_pos=None):
+    """LangevinLeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step) as
+    orc_langevin_constrained restates them.  Returns pos, vel, forces, energies."""
+    L = lib()
+    pos = np.ascontiguousarray(pos, np.float64).copy()
+    vel = np.ascontiguousarray(vel, np.float64).copy()
+    last = pos.copy() if last_pos is None else np.ascontiguousarray(last_pos, np.float64).copy()
+    keep = [np.ascontiguousarray(constraints[0], np.int32), np.ascontiguousarray(constraints[1], np.int32),
+            np.ascontiguousarray(constraints[2], np.float64)]
+    c = OrcConstraints()
+    c.n = len(keep[0])
+    c.a1, c.a2, c.len = _p(keep[0]), _p(keep[1]), _p(keep[2])
+    c.shake_eps, c.shake_maxiter = shake if shake is not None else (0.0, 0)
+    c.rattle_eps, c.rattle_maxiter = rattle if rattle is not None else (0.0, 0)
+    f = np.zeros((system.n, 3))
+    e = np.zeros(4)
+    rc = L.orc_langevin_constrained(C.byref(system.s), C.byref(cutoff) if cutoff is not None else None,
+                                    C.byref(pme) if pme is not None else None, int(bonded), C.byref(c),
+                                    C.c_double(dt), C.c_double(temperature), C.c_double(gamma),
+                                    C.c_ulonglong(seed), C.c_longlong(first_step), int(nsteps), _p(pos),
+                                    _p(vel), _p(last), _p(f), _p(e))
+    if rc:
+        raise ValueError("orc_langevin_constrained: gamma > 0 and temperature >= 0")
+    return pos, vel, f, e
+
+
 def pme_alpha(cutoff, accuracy):
     return lib().orc_pme_alpha(cutoff, accuracy)
 
@@ -333,9 +362,10 @@ def ref_md_available():
 
 
 def ref_leapfrog_constrained(system, elem, pos, vel, dt, nsteps, shake=(1e-5, 30),
-                             rattle=(1e-5, 30), all_bonds=True):
+                             rattle=(1e-5, 30), all_bonds=True, langevin=None):
     """The reference run with no force terms: returns pos, vel and the reference's constraint
-    list (atom1, atom2, rest_length)."""
+    list (atom1, atom2, rest_length).  langevin = (temperature, gamma_ps, seed) runs its
+    LangevinLeapfrogIntegrator instead of the LeapfrogIntegrator."""
     global _ref_md
     if _ref_md is None:
         ref_lib()  # its force path library first (the md library links against it)
@@ -350,10 +380,17 @@ def ref_leapfrog_constrained(system, elem, pos, vel, dt, nsteps, shake=(1e-5, 30
     ncon = C.c_int(0)
     se, sm = shake if shake is not None else (0.0, 0)
     re_, rm = rattle if rattle is not None else (0.0, 0)
-    rc = _ref_md.ref_leapfrog_constrained(
-        C.byref(r), el, int(shake is not None), C.c_double(se), int(sm), int(rattle is not None),
-        C.c_double(re_), int(rm), int(all_bonds), C.c_double(dt), int(nsteps), _p(pos), _p(vel),
-        C.byref(ncon), _p(cons), _p(lens), cap)
+    if langevin is None:
+        rc = _ref_md.ref_leapfrog_constrained(
+            C.byref(r), el, int(shake is not None), C.c_double(se), int(sm), int(rattle is not None),
+            C.c_double(re_), int(rm), int(all_bonds), C.c_double(dt), int(nsteps), _p(pos), _p(vel),
+            C.byref(ncon), _p(cons), _p(lens), cap)
+    else:
+        temp, gam, seed = langevin
+        rc = _ref_md.ref_langevin_constrained(
+            C.byref(r), el, int(shake is not None), C.c_double(se), int(sm), int(rattle is not None),
+            C.c_double(re_), int(rm), int(all_bonds), C.c_double(dt), C.c_double(temp), C.c_double(gam),
+            int(seed), int(nsteps), _p(pos), _p(vel), C.byref(ncon), _p(cons), _p(lens), cap)
     if rc:
         raise RuntimeError("reference run failed")
     n = min(ncon.value, cap)

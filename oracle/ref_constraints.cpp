@@ -1,11 +1,14 @@
-// Test-infrastructure harness: ProtoMol 3's own leapfrog integrator with its SHAKE and RATTLE
-// modifiers, compiled from the reference sources by oracle/Makefile, run on a topology built in
+// Test-infrastructure harness: ProtoMol 3's own leapfrog and Langevin leapfrog integrators with
+// its SHAKE and RATTLE modifiers, compiled from the reference sources by oracle/Makefile, run on a
+// topology built in
 // memory with no force terms (the forces are exactly zero), so that the constrained drift, the
 // constraint list and every SHAKE/RATTLE sweep are the reference's own.  Tests compare the CPU
 // restatement (orc_leapfrog_constrained in pm_oracle.c) and the CUDA path against it.
 //
 // What is run (all reference code):
-//   LeapfrogIntegrator::run (integrator/leapfrog/LeapfrogIntegrator.cpp:89-102)
+//   LeapfrogIntegrator::run (integrator/leapfrog/LeapfrogIntegrator.cpp:89-102), or
+//   LangevinLeapfrogIntegrator through StandardIntegrator::run (integrator/StandardIntegrator.cpp:
+//   27-37) at temperature 0 (its noise term vanishes)
 //   ModifierShake as a post-drift modifier, ModifierRattle as a post-step modifier, with the
 //   placement ModifierModule::addModifiers gives them (module/ModifierModule.cpp:106-128)
 //   buildRattleShakeBondConstraintList (topology/TopologyUtilities.cpp:695-775), reached through

@@ -296,8 +296,6 @@ struct pmb_system {
   bool have_pos = false;  // positions were uploaded at least once (evaluate, profile, set_state)
   int *d_excl_start = nullptr, *d_excl_partner = nullptr, *d_excl_kindc = nullptr;
   int *d_excl_pairs = nullptr, *d_excl_kind = nullptr;
-  int4 *d_swork = nullptr;   // PME spread work items (box, slot range), fixed by the block layout
-  int nswork = 0;
   BondedDev bonded{};
   long long *d_facc = nullptr, *d_eacc = nullptr;
   double *d_fout = nullptr, *d_eout = nullptr;
@@ -399,8 +397,6 @@ int nblist_alloc(pmb_system *s, double rl) {
   new (&s->nba) Allocs();
   NbListDev &nb = s->nb;
   std::memset(&nb, 0, sizeof(nb));
-  nb.swork = s->d_swork;
-  nb.nswork = s->nswork;
   int nblk = 0;
   for (auto &b : s->hbox) nblk += b.nblk;
   nb.nblk_total = nblk;
@@ -984,17 +980,7 @@ pmb_system *pmb_system_create(const pmb_box_desc *boxes, int n_boxes, int precis
       b0 += s->hbox[bi].nblk;
     }
   }
-  // PME spread work items: runs of PME_SPREAD_SLOTS slots of one box (Hilbert-contiguous, so a
-  // run's stencils cover a compact part of the box's grid)
-  std::vector<int4> swork;
-  for (int bi = 0; bi < s->nbox; bi++) {
-    const BoxDev &b = s->hbox[bi];
-    const int s0 = b.blk0 * BLOCK, s1 = (b.blk0 + b.nblk) * BLOCK;
-    for (int q = s0; q < s1; q += PME_SPREAD_SLOTS) swork.push_back(make_int4(bi, q, std::min(s1, q + PME_SPREAD_SLOTS), 0));
-  }
-  s->nswork = (int)swork.size();
   int rc = 0;
-  rc |= upload(s->a, s->d_swork, swork);
   rc |= upload(s->a, s->d_box, s->hbox);
   rc |= upload(s->a, s->d_atom_box, s->h_atom_box);
   rc |= upload(s->a, s->d_charge, s->h_charge);

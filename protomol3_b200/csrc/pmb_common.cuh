@@ -31,7 +31,6 @@ static_assert(BLOCK == 8 || BLOCK == 16, "i-cluster of 8 or 16 atoms");
 constexpr int JCHUNK = 32;         // j-atoms per tile
 constexpr int JSAME = 1 << 30;     // j-list flag: the j-atom shares a molecule with the i-cluster
 constexpr int MAX_LJ_TYPES = 32;   // LJ table kept in shared memory up to this many types
-constexpr int PME_SPREAD_SLOTS = 256;  // slots per work item (CTA) of the tiled order-4 spread
 
 struct BoxDev {
   double L[3], Lr[3];    // edges and reciprocals

@@ -44,8 +44,6 @@ struct NbListDev {
   int *tile_k;                 // [tile_cap] tile index within the block
   int tile_cap;
   int *status;                 // [4]: list / tile overflow, non-finite position, unused
-  const int4 *swork;           // [nswork] PME spread work items: box, first slot, end slot (runs of
-  int nswork;                  // at most 256 slots of one box)
   // per slot
   int nslot;
   int *slot_orig;              // [nslot] original atom index or -1

@@ -5,9 +5,8 @@
 // NonbondedPMEwaldSystemForce.h (reciprocalTerm :812-864, correctionTerm :874-911).
 //
 // Pipeline per step (every kernel batched over the boxes of a system):
-//   k_spread      B-spline weights, 64 int64 fixed-point atomics per atom slot (order 4, tiled:
-//                 a run of 256 Hilbert-ordered slots per CTA sums its stencils in a shared-memory
-//                 part of the grid and adds each non-zero point of it to the grid once)
+//   k_spread      B-spline weights, 64 int64 fixed-point atomics per atom slot (order 4: four
+//                 threads per slot, one x-plane of the stencil each)
 //   k_fft_z_fwd   z-lines of the fixed-point grid (cleared as it is read), two real lines packed
 //                 per complex FFT, half spectrum written as [kz][x][y]
 //   k_fft_y       y-lines of the half spectrum (groups of up to 16 rows of one kz plane)
@@ -15,8 +14,7 @@
 //                 with energy and virial partials added to the box accumulators, inverse FFT
 //   k_fft_y       inverse y-lines
 //   k_fft_z_inv   inverse z transform back to the real potential grid [x][y][z]
-//   k_gather      one thread per atom slot, 64-point stencil, fixed-point force atomics (order 4,
-//                 tiled: the run's part of the potential grid read once into shared memory)
+//   k_gather      one thread per atom slot, 64-point stencil, fixed-point force atomics
 // The transforms are unnormalised, as the reference's ZFFT/FFTW calls; r2c/c2r replace the
 // reference's full complex transform of a real grid (identical result: the spectrum is Hermitian
 // and the influence function even in m).
@@ -305,142 +303,6 @@ __device__ __forceinline__ void weights4(const PmeBoxPlan &pl, uint4 f, double4 
   }
 }
 
-// Order 4, tiled: one CTA per run of up to PME_SPREAD_SLOTS slots of one box, one thread per
-// slot.  The run's slots follow the Hilbert order, so their stencils cover a compact part of the
-// grid: the CTA adds its 64 values per atom into that part kept in shared memory (int64 fixed
-// point, the same products as k_spread4, so the grid is the same bit for bit), then adds each
-// non-zero point of it to the grid once.  The part's origin is taken relative to the run's first
-// atom with the periodic wrap undone (atoms on both sides of a periodic face stay neighbours); a
-// run whose part exceeds SPREAD_CAP points adds its values to the grid directly.
-constexpr int SPREAD_CAP = 12288;  // int64 points of the shared sub-grid (96 KiB)
-
-// The part of a box's grid that the stencils of a run's valid slots cover: the first valid
-// slot's base as reference, offsets rel[] of this thread's base from it with the periodic wrap
-// undone, and the smallest / largest offset over the run (in s_min / s_max).  Returns false when
-// the run holds no atom.  Every thread of the CTA calls it.
-__device__ bool run_part(bool valid, const int base[3], const int n3[3], int rel[3], int *s_first, int *s_ref,
-                         int *s_min, int *s_max) {
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    *s_first = 0x7fffffff;
-    for (int d = 0; d < 3; d++) {
-      s_min[d] = 0x7fffffff;
-      s_max[d] = -0x7fffffff;
-    }
-  }
-  __syncthreads();
-  if (valid) atomicMin(s_first, tid);
-  __syncthreads();
-  if (*s_first == 0x7fffffff) return false;
-  if (tid == *s_first)
-    for (int d = 0; d < 3; d++) s_ref[d] = base[d];
-  __syncthreads();
-  for (int d = 0; d < 3; d++) {
-    int r = base[d] - s_ref[d];  // bases lie in [n - 1, 2n - 1): |r| < n
-    if (2 * r > n3[d]) r -= n3[d];
-    else if (2 * r < -n3[d]) r += n3[d];
-    rel[d] = r;
-  }
-  if (valid)
-    for (int d = 0; d < 3; d++) {
-      atomicMin(&s_min[d], rel[d]);
-      atomicMax(&s_max[d], rel[d]);
-    }
-  __syncthreads();
-  return true;
-}
-
-template <bool MIXED>
-__global__ void __launch_bounds__(PME_SPREAD_SLOTS) k_spread4_tiled(NbListDev nb, PmeDev pm) {
-  using T = typename std::conditional<MIXED, float, double>::type;
-  extern __shared__ long long sg[];  // [SPREAD_CAP]
-  __shared__ int s_first, s_ref[3], s_min[3], s_max[3];
-  const int4 w = nb.swork[blockIdx.x];
-  const int tid = threadIdx.x, sl = w.y + tid;
-  const PmeBoxPlan &pl = pm.plan[w.x];
-  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
-  const int n3[3] = {nx, ny, nz};
-  bool valid = false;
-  T th[3][4];
-  int base[3] = {0, 0, 0};
-  T q = T(0);
-  if (sl < w.z) {
-    const int4 m = nb.slot_meta[sl];
-    uint4 f4 = make_uint4(0, 0, 0, 0);
-    double4 p4 = make_double4(0, 0, 0, 0);
-    if constexpr (MIXED) f4 = nb.slot_fx[sl];
-    else p4 = nb.slot_pq[sl];
-    if (m.x >= 0) {
-      valid = true;
-      weights4<MIXED, false>(pl, f4, p4, th, th, base, q);
-    }
-  }
-  int rel[3];
-  if (!run_part(valid, base, n3, rel, &s_first, s_ref, s_min, s_max)) return;  // padding only
-  const int e0 = s_max[0] - s_min[0] + 4, e1 = s_max[1] - s_min[1] + 4, e2 = s_max[2] - s_min[2] + 4;
-  const long long vol = (long long)e0 * e1 * e2;
-  long long *g = pm.qgrid + pl.grid0;
-  if (vol > SPREAD_CAP) {  // not compact enough: straight to the grid (the values of k_spread4)
-    if (!valid) return;
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-      const T qa = q * th[0][a];
-      const int i1 = wrap3(a + base[0], nx);
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const T ab = qa * th[1][j];
-        long long *row = g + ((long long)i1 * ny + wrap3(j + base[1], ny)) * nz;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
-          if (v) red_add(row + wrap3(k + base[2], nz), v);
-        }
-      }
-    }
-    return;
-  }
-  for (long long i = tid; i < vol; i += blockDim.x) sg[i] = 0;
-  __syncthreads();
-  if (valid) {
-    const int l0 = rel[0] - s_min[0], l1 = rel[1] - s_min[1], l2 = rel[2] - s_min[2];
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-      const T qa = q * th[0][a];
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const T ab = qa * th[1][j];
-        unsigned long long *row =
-            reinterpret_cast<unsigned long long *>(sg + ((long long)(l0 + a) * e1 + (l1 + j)) * e2 + l2);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
-          if (v) atomicAdd(row + k, (unsigned long long)v);
-        }
-      }
-    }
-  }
-  __syncthreads();
-  // the sub-grid's origin on the grid: the reference atom's base plus the smallest offset,
-  // in [0, n) (bases lie in [n - 1, 2n - 1), offsets in [-n/2, 0])
-  int o[3];
-  for (int d = 0; d < 3; d++) {
-    int x = s_ref[d] + s_min[d];
-    o[d] = x >= n3[d] ? x - n3[d] : x;
-  }
-  // one warp per (x, y) row of the sub-grid, lanes along z (consecutive grid addresses)
-  const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  for (int row = warp; row < e0 * e1; row += nw) {
-    const int lx = row / e1, ly = row - lx * e1;
-    const int gx = wrap3(o[0] + lx, nx), gy = wrap3(o[1] + ly, ny);
-    long long *grow = g + ((long long)gx * ny + gy) * nz;
-    const long long *srow = sg + (long long)row * e2;
-    for (int lz = lane; lz < e2; lz += 32) {
-      const long long v = srow[lz];
-      if (v) red_add(grow + wrap3(o[2] + lz, nz), v);
-    }
-  }
-}
-
 // v[p] for a run-time p in [0, 4) without indexing a register array (which would go to local
 // memory).
 template <typename T>
@@ -543,84 +405,6 @@ __global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
     }
   }
   long long *f = s.facc + 3 * (long long)m.x;
-  red_add(f, f2fix((double)(fx * T(pl.hr[0]) * q), FORCE_SCALE));
-  red_add(f + 1, f2fix((double)(fy * T(pl.hr[1]) * q), FORCE_SCALE));
-  red_add(f + 2, f2fix((double)(fz * T(pl.hr[2]) * q), FORCE_SCALE));
-}
-
-// Order 4, tiled like k_spread4_tiled: the run's part of the real potential grid is copied into
-// shared memory once (rows along z, coalesced), and every stencil read comes from there.  The
-// arithmetic is k_gather's, term for term, so the forces are the same bit for bit; a run whose
-// part exceeds SPREAD_CAP points reads the grid directly.
-template <bool MIXED>
-__global__ void __launch_bounds__(PME_SPREAD_SLOTS) k_gather4_tiled(const SystemDev s, NbListDev nb, PmeDev pm) {
-  using T = typename std::conditional<MIXED, float, double>::type;
-  extern __shared__ __align__(16) unsigned char gather_raw[];
-  T *sg = reinterpret_cast<T *>(gather_raw);  // [SPREAD_CAP]
-  __shared__ int s_first, s_ref[3], s_min[3], s_max[3];
-  const int4 w = nb.swork[blockIdx.x];
-  const int tid = threadIdx.x, sl = w.y + tid;
-  const PmeBoxPlan &pl = pm.plan[w.x];
-  const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
-  const int n3[3] = {nx, ny, nz};
-  bool valid = false;
-  T th[3][4], dth[3][4];
-  int base[3] = {0, 0, 0};
-  T q = T(0);
-  int orig = -1;
-  if (sl < w.z) {
-    const int4 m = nb.slot_meta[sl];
-    uint4 f4 = make_uint4(0, 0, 0, 0);
-    double4 p4 = make_double4(0, 0, 0, 0);
-    if constexpr (MIXED) f4 = nb.slot_fx[sl];
-    else p4 = nb.slot_pq[sl];
-    if (m.x >= 0) {
-      valid = true;
-      orig = m.x;
-      weights4<MIXED, true>(pl, f4, p4, th, dth, base, q);
-    }
-  }
-  int rel[3];
-  if (!run_part(valid, base, n3, rel, &s_first, s_ref, s_min, s_max)) return;
-  const int e0 = s_max[0] - s_min[0] + 4, e1 = s_max[1] - s_min[1] + 4, e2 = s_max[2] - s_min[2] + 4;
-  const long long vol = (long long)e0 * e1 * e2;
-  const T *g = reinterpret_cast<const T *>(pm.rgrid) + pl.grid0;
-  const bool tiled = vol <= SPREAD_CAP;
-  if (tiled) {
-    int o[3];
-    for (int d = 0; d < 3; d++) {
-      const int x = s_ref[d] + s_min[d];
-      o[d] = x >= n3[d] ? x - n3[d] : x;
-    }
-    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    for (int row = warp; row < e0 * e1; row += nw) {
-      const int lx = row / e1, ly = row - lx * e1;
-      const T *grow = g + ((long long)wrap3(o[0] + lx, nx) * ny + wrap3(o[1] + ly, ny)) * nz;
-      T *srow = sg + (long long)row * e2;
-      for (int lz = lane; lz < e2; lz += 32) srow[lz] = grow[wrap3(o[2] + lz, nz)];
-    }
-  }
-  __syncthreads();
-  if (!valid) return;
-  const int l0 = rel[0] - s_min[0], l1 = rel[1] - s_min[1], l2 = rel[2] - s_min[2];
-  T fx = 0, fy = 0, fz = 0;
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const T xij = dth[0][i] * th[1][j], yij = th[0][i] * dth[1][j], zij = th[0][i] * th[1][j];
-      const T *row = tiled ? sg + ((long long)(l0 + i) * e1 + (l1 + j)) * e2 + l2
-                           : g + ((long long)wrap3(i + base[0], nx) * ny + wrap3(j + base[1], ny)) * nz;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const T term = tiled ? row[k] : row[wrap3(k + base[2], nz)];
-        fx -= term * xij * th[2][k];
-        fy -= term * yij * th[2][k];
-        fz -= term * zij * dth[2][k];
-      }
-    }
-  }
-  long long *f = s.facc + 3 * (long long)orig;
   red_add(f, f2fix((double)(fx * T(pl.hr[0]) * q), FORCE_SCALE));
   red_add(f + 1, f2fix((double)(fy * T(pl.hr[1]) * q), FORCE_SCALE));
   red_add(f + 2, f2fix((double)(fz * T(pl.hr[2]) * q), FORCE_SCALE));
@@ -863,19 +647,8 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   const int TB = 256;
   constexpr bool MIXED = sizeof(T) == 4;
   const long long n4 = 4ll * nb.nslot;
-  if (pm.order == 4 && nb.nswork > 0) {
-    static bool sconf = false;
-    if (!sconf) {
-      cudaFuncSetAttribute(k_spread4_tiled<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(SPREAD_CAP * sizeof(long long)));
-      sconf = true;
-    }
-    k_spread4_tiled<MIXED><<<nb.nswork, PME_SPREAD_SLOTS, SPREAD_CAP * sizeof(long long), st>>>(nb, pm);
-  } else if (pm.order == 4) {
-    k_spread4<MIXED><<<(unsigned)((n4 + TB - 1) / TB), TB, 0, st>>>(nb, pm);
-  } else {
-    k_spread<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
-  }
+  if (pm.order == 4) k_spread4<MIXED><<<(unsigned)((n4 + TB - 1) / TB), TB, 0, st>>>(nb, pm);
+  else k_spread<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(nb, pm);
   if (mark) mark(mctx, "pme_spread");
   // shared memory sized to the largest work item of the plan (caps ZMAXE / LMAXE)
   const size_t zsmem = sizeof(T2) * (256 + 2 * (size_t)pm.zbuf);
@@ -900,19 +673,8 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, +1);
   k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   if (mark) mark(mctx, "pme_fft");
-  if (pm.order == 4 && nb.nswork > 0) {
-    static bool gconf = false;
-    if (!gconf) {
-      cudaFuncSetAttribute(k_gather4_tiled<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(SPREAD_CAP * sizeof(T)));
-      gconf = true;
-    }
-    k_gather4_tiled<MIXED><<<nb.nswork, PME_SPREAD_SLOTS, SPREAD_CAP * sizeof(T), st>>>(s, nb, pm);
-  } else if (pm.order == 4) {
-    k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
-  } else {
-    k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
-  }
+  if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
+  else k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   if (mark) mark(mctx, "pme_gather");
   return 0;
 }

@@ -15,7 +15,9 @@ step, for four modifier settings (``shake``/``rattle`` with their epsilon and ma
 * ``s``: SHAKE alone, 20 steps;
 * ``r``: RATTLE alone, 20 steps;
 * ``tight``: SHAKE (1e-8, 5) and RATTLE (1e-9, 3), 15 steps, where max_iter ends every
-  application before convergence.
+  application before convergence;
+* ``lv``: the LangevinLeapfrogIntegrator at temperature 0 (noise term exactly zero) with
+  gamma 50/ps, SHAKE and RATTLE at the defaults, 20 steps.
 """
 import os
 import sys
@@ -47,6 +49,9 @@ def main():
         out[name + "_shake"] = np.array(shake if shake else (0.0, 0))
         out[name + "_rattle"] = np.array(rattle if rattle else (0.0, 0))
         out["con_a1"], out["con_a2"], out["con_len"] = cons
+    pos, vel, cons = O.ref_leapfrog_constrained(system, box["elem"], box["pos"], box["vel"], 2.0, 20,
+                                                shake=(1e-5, 30), rattle=(1e-5, 30), langevin=(0.0, 50.0, 1234))
+    out["lv_pos"], out["lv_vel"], out["lv_steps"], out["lv_gamma"] = pos, vel, 20, 50.0
     np.savez_compressed(os.path.join(HERE, "water64_rigid_ref.npz"), **out)
 
 

@@ -51,6 +51,17 @@ def test_oracle_equals_reference_run(gold, case):
     assert np.array_equal(vel, gold[case + "_vel"])
 
 
+def test_oracle_langevin_equals_reference_run(gold):
+    """LangevinLeapfrogIntegrator with SHAKE and RATTLE at temperature 0 (gamma 50/ps): the
+    oracle's restatement equals the reference's run bit for bit."""
+    box = W.water_box(64, seed=7)
+    cons = CS.rattle_shake_constraints(box)
+    pos, vel, _, _ = O.langevin_constrained(O.System(box), gold["pos0"], gold["vel0"], float(gold["dt"]),
+                                            int(gold["lv_steps"]), cons, 0.0, float(gold["lv_gamma"]))
+    assert np.array_equal(pos, gold["lv_pos"])
+    assert np.array_equal(vel, gold["lv_vel"])
+
+
 def test_planted_mistake_is_caught(gold):
     """A rest length off by one part in 10^12 in the oracle's input must break exact equality."""
     box = W.water_box(64, seed=7)

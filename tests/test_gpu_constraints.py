@@ -24,9 +24,9 @@ def _opt(a):
 
 
 def _device_run(box, cons, dt, steps, shake, rattle, precision="fp64", forces=(), chunks=None,
-                use_graph=True):
+                use_graph=True, **integ):
     topo = F.Topology(box, precision)
-    md = F.Integrator(topo, list(forces), timestep=dt, use_graph=use_graph)
+    md = F.Integrator(topo, list(forces), timestep=dt, use_graph=use_graph, **integ)
     md.set_constraints(cons, shake=shake is not None, shake_epsilon=(shake or (0, 0))[0],
                        shake_max_iter=(shake or (0, 0))[1], rattle=rattle is not None,
                        rattle_epsilon=(rattle or (0, 0))[0], rattle_max_iter=(rattle or (0, 0))[1])
@@ -124,12 +124,45 @@ def test_device_with_forces_close_to_oracle():
     assert np.abs(vel - ref_vel).max() < 1e-9
 
 
-def test_langevin_with_constraints_is_refused():
-    box = W.water_box(27, seed=1)
-    topo = F.Topology(box, "fp64")
-    md = F.Integrator(topo, [], kind="langevin")
-    with pytest.raises(RuntimeError):
-        md.set_constraints(CS.rattle_shake_constraints(box))
+def test_langevin_with_constraints_equals_reference_golden():
+    """SHAKE after the drift and RATTLE after the closing half kick of the LangevinLeapfrogIntegrator
+    (temperature 0, gamma 50/ps): the reference's own run (golden case lv).  The friction factor
+    exp(-gamma h / 2) comes from the device's exp, which may differ from the host's in the last
+    bit, so equality is to 1e-13 rather than bit for bit."""
+    g = np.load(GOLD)
+    box = W.water_box(64, seed=7)
+    cons = CS.rattle_shake_constraints(box)
+    pos, vel, _ = _device_run(box, cons, float(g["dt"]), int(g["lv_steps"]), (1e-5, 30), (1e-5, 30),
+                              kind="langevin", temperature=0.0, gamma=float(g["lv_gamma"]), seed=3)
+    assert np.abs(pos - g["lv_pos"]).max() < 1e-13
+    assert np.abs(vel - g["lv_vel"]).max() < 1e-13 * max(1.0, np.abs(g["lv_vel"]).max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_langevin_with_constraints_and_noise_equals_oracle(precision):
+    """Rigid water under Langevin at 300 K (gamma 1/ps, 2 fs) with forces, runs split over
+    calls: against the oracle with the same counter-based noise, step for step."""
+    box = W.water_box(216, seed=8)
+    cons = CS.rattle_shake_constraints(box)
+    forces = [F.BondedSystemForce(),
+              F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0), coulomb=("C2", 7.0, 8.0))]
+    s = O.System(box)
+    cp = O.cutoff_params(lj=("C2", 7.0, 8.0), coul=("C2", 7.0, 8.0))
+    topo = F.Topology(box, precision)
+    md = F.Integrator(topo, forces, timestep=2.0, kind="langevin", temperature=300.0, gamma=1.0, seed=21)
+    md.set_constraints(cons)
+    md.set_state(box["pos"], box["vel"])
+    pos, vel = box["pos"].copy(), box["vel"].copy()
+    tol = 1e-11 if precision == "fp64" else 1e-5
+    for k in range(10):
+        md.run(1)
+        p, v = md.state()
+        po, vo, _, _ = O.langevin_constrained(s, pos, vel, 2.0, 1, cons, 300.0, 1.0, seed=21, first_step=k,
+                                              cutoff=cp, bonded=True, last_pos=pos)
+        assert np.abs(p - po).max() < tol and np.abs(v - vo).max() < tol * 100, k
+        pos, vel = p, v
+    a1, a2, ln = cons
+    d2 = ((pos[a2] - pos[a1]) ** 2).sum(1)
+    assert np.mean(np.abs(d2 - ln ** 2) / (2 * ln ** 2)) <= 1e-5
     md.close()
     topo.close()
-    assert L.lib() is not None
