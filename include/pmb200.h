@@ -232,6 +232,13 @@ int pmb_md_run(pmb_md *md, int n_steps);
 /* Energies of the last force evaluation [n_boxes * PMB_E_STRIDE] and kinetic energy per box. */
 int pmb_md_energies(pmb_md *md, double *energies, double *kinetic);
 int pmb_md_use_graph(pmb_md *md, int enable);
+/* The virial in the MD run's energies (ScalarStructure::virial() on): every step evaluates the
+ * force virial, and RATTLE adds its constraint terms (2 dp) x rab (modifier/ModifierRattle.cpp:58).
+ * pmb_md_energies then fills the virial slots: after run(n), those of the last evaluation plus the
+ * last RATTLE application, what the reference's energies hold then (the SHAKE terms of
+ * modifier/ModifierShake.cpp:65-68 are cleared by the force evaluation after each drift,
+ * integrator/STSIntegrator.cpp:34-46, so they never reach an output).  Off by default. */
+int pmb_md_set_virial(pmb_md *md, int on);
 /* Runs n_steps (pmb_md_run) between two CUDA events on the system's stream and returns the mean
  * device time per step in ms (the autotuner's clock). */
 int pmb_md_time(pmb_md *md, int n_steps, double *ms_per_step);
@@ -241,7 +248,7 @@ int pmb_md_time(pmb_md *md, int n_steps, double *ms_per_step);
  * buildRattleShakeBondConstraintList).  A modifier is on when its flag is set, epsilon > 0 and
  * max_iter > 0 (the reference's defaults: 1e-5 and 30).  Each application sweeps the list as the
  * reference does until the mean error is at most epsilon, at most max_iter + 1 sweeps; the
- * constraint virial is not accumulated.  Constrained groups (atoms linked by constraints) hold at
+ * constraint virial enters the energies with pmb_md_set_virial.  Constrained groups (atoms linked by constraints) hold at
  * most 8 atoms and 16 constraints; max_iter below 256.  The SHAKE reference positions are the
  * positions at pmb_md_set_state, or the current ones when this is called after it.  With the
  * Langevin integrator the modifiers sit where StandardIntegrator::run calls them

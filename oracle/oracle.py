@@ -200,10 +200,12 @@ def gauss3(seed, atom, stream):
 
 
 def leapfrog_constrained(system, pos, vel, dt, nsteps, constraints, shake=(1e-5, 30),
-                         rattle=(1e-5, 30), cutoff=None, pme=None, bonded=False, last_pos=None):
+                         rattle=(1e-5, 30), cutoff=None, pme=None, bonded=False, last_pos=None,
+                         rattle_virial=None):
     """LeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step) as
     orc_leapfrog_constrained restates them.  constraints = (atom1, atom2, rest_length);
-    shake / rattle = (epsilon, max_iter) or None.  Returns pos, vel, forces, energies."""
+    shake / rattle = (epsilon, max_iter) or None.  Returns pos, vel, forces, energies;
+    rattle_virial (numpy array of 9) receives the last RATTLE application's virial."""
     L = lib()
     pos = np.ascontiguousarray(pos, np.float64).copy()
     vel = np.ascontiguousarray(vel, np.float64).copy()
@@ -219,13 +221,14 @@ def leapfrog_constrained(system, pos, vel, dt, nsteps, constraints, shake=(1e-5,
     e = np.zeros(4)
     L.orc_leapfrog_constrained(C.byref(system.s), C.byref(cutoff) if cutoff is not None else None,
                                C.byref(pme) if pme is not None else None, int(bonded), C.byref(c),
-                               C.c_double(dt), int(nsteps), _p(pos), _p(vel), _p(last), _p(f), _p(e))
+                               C.c_double(dt), int(nsteps), _p(pos), _p(vel), _p(last), _p(f), _p(e),
+                               _p(rattle_virial) if rattle_virial is not None else None)
     return pos, vel, f, e
 
 
 def langevin_constrained(system, pos, vel, dt, nsteps, constraints, temperature, gamma, seed=1234,
                          first_step=0, shake=(1e-5, 30), rattle=(1e-5, 30), cutoff=None, pme=None,
-                         bonded=False, last_pos=None):
+                         bonded=False, last_pos=None, rattle_virial=None):
     """LangevinLeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step) as
     orc_langevin_constrained restates them.  Returns pos, vel, forces, energies."""
     L = lib()
@@ -245,7 +248,8 @@ def langevin_constrained(system, pos, vel, dt, nsteps, constraints, temperature,
                                     C.byref(pme) if pme is not None else None, int(bonded), C.byref(c),
                                     C.c_double(dt), C.c_double(temperature), C.c_double(gamma),
                                     C.c_ulonglong(seed), C.c_longlong(first_step), int(nsteps), _p(pos),
-                                    _p(vel), _p(last), _p(f), _p(e))
+                                    _p(vel), _p(last), _p(f), _p(e),
+                                    _p(rattle_virial) if rattle_virial is not None else None)
     if rc:
         raise ValueError("orc_langevin_constrained: gamma > 0 and temperature >= 0")
     return pos, vel, f, e
@@ -362,10 +366,11 @@ def ref_md_available():
 
 
 def ref_leapfrog_constrained(system, elem, pos, vel, dt, nsteps, shake=(1e-5, 30),
-                             rattle=(1e-5, 30), all_bonds=True, langevin=None):
+                             rattle=(1e-5, 30), all_bonds=True, langevin=None, virial=None):
     """The reference run with no force terms: returns pos, vel and the reference's constraint
     list (atom1, atom2, rest_length).  langevin = (temperature, gamma_ps, seed) runs its
-    LangevinLeapfrogIntegrator instead of the LeapfrogIntegrator."""
+    LangevinLeapfrogIntegrator instead of the LeapfrogIntegrator; virial (numpy array of 9)
+    receives the virial its energies hold after the run (the last RATTLE's)."""
     global _ref_md
     if _ref_md is None:
         ref_lib()  # its force path library first (the md library links against it)
@@ -384,13 +389,14 @@ def ref_leapfrog_constrained(system, elem, pos, vel, dt, nsteps, shake=(1e-5, 30
         rc = _ref_md.ref_leapfrog_constrained(
             C.byref(r), el, int(shake is not None), C.c_double(se), int(sm), int(rattle is not None),
             C.c_double(re_), int(rm), int(all_bonds), C.c_double(dt), int(nsteps), _p(pos), _p(vel),
-            C.byref(ncon), _p(cons), _p(lens), cap)
+            C.byref(ncon), _p(cons), _p(lens), cap, _p(virial) if virial is not None else None)
     else:
         temp, gam, seed = langevin
         rc = _ref_md.ref_langevin_constrained(
             C.byref(r), el, int(shake is not None), C.c_double(se), int(sm), int(rattle is not None),
             C.c_double(re_), int(rm), int(all_bonds), C.c_double(dt), C.c_double(temp), C.c_double(gam),
-            int(seed), int(nsteps), _p(pos), _p(vel), C.byref(ncon), _p(cons), _p(lens), cap)
+            int(seed), int(nsteps), _p(pos), _p(vel), C.byref(ncon), _p(cons), _p(lens), cap,
+            _p(virial) if virial is not None else None)
     if rc:
         raise RuntimeError("reference run failed")
     n = min(ncon.value, cap)

@@ -945,9 +945,11 @@ static double rattle_error(const orc_constraints *c, const double *x, const doub
   return error / c->n;
 }
 
-int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const double *pos,
-               double *vel) {
-  /* ModifierRattle::doExecute (ModifierRattle.cpp:17-64); the virial term is not accumulated */
+/* ModifierRattle::doExecute (ModifierRattle.cpp:17-64), with its virial term when virial is
+ * not NULL: every constraint of every sweep adds (2 dp) x rab as ScalarStructure::addVirial does
+ * (type/ScalarStructure.cpp:36-54), dp = rab gab. */
+static int rattle_v(const orc_constraints *c, const double *mass, double dt_fs, const double *pos,
+                    double *vel, double *virial) {
   double error = rattle_error(c, pos, vel);
   const double dt = dt_fs / TIMEFACTOR;
   int iter = 0;
@@ -962,10 +964,24 @@ int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const
       const double vab[3] = {v1[0] - v2[0], v1[1] - v2[1], v1[2] - v2[2]};
       const double rvab = rab[0] * vab[0] + rab[1] * vab[1] + rab[2] * vab[2];
       const double gab = -rvab / (dt * (rM1 + rM2) * rabsq);
+      double dp[3];
       for (int q = 0; q < 3; q++) {
-        const double dp = rab[q] * gab;
-        v1[q] += dp * dt * rM1;
-        v2[q] -= dp * dt * rM2;
+        dp[q] = rab[q] * gab;
+        v1[q] += dp[q] * dt * rM1;
+        v2[q] -= dp[q] * dt * rM2;
+      }
+      if (virial) {
+        const double f[3] = {dp[0] * 2, dp[1] * 2, dp[2] * 2};
+        const double xy = f[0] * rab[1], xz = f[0] * rab[2], yz = f[1] * rab[2];
+        virial[0] += f[0] * rab[0];
+        virial[1] += xy;
+        virial[2] += xz;
+        virial[3] += xy;
+        virial[4] += f[1] * rab[1];
+        virial[5] += yz;
+        virial[6] += xz;
+        virial[7] += yz;
+        virial[8] += f[2] * rab[2];
       }
     }
     error = rattle_error(c, pos, vel);
@@ -975,10 +991,15 @@ int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const
   return iter;
 }
 
+int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const double *pos,
+               double *vel) {
+  return rattle_v(c, mass, dt_fs, pos, vel, NULL);
+}
+
 int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
                              const orc_pme_params *pme, int do_bonded, const orc_constraints *c,
                              double dt_fs, int nsteps, double *pos, double *vel, double *last_pos,
-                             double *forces_out, double *energies_out) {
+                             double *forces_out, double *energies_out, double *rattle_virial) {
   const int n = s->n;
   const int shake = c && c->n > 0 && c->shake_eps > 0 && c->shake_maxiter > 0;
   const int rattle = c && c->n > 0 && c->rattle_eps > 0 && c->rattle_maxiter > 0;
@@ -1010,7 +1031,10 @@ int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
     }
     for (int i = 0; i < n; i++)
       for (int q = 0; q < 3; q++) vel[3 * i + q] += f[3 * i + q] * h * 0.5 / s->mass[i];
-    if (rattle) orc_rattle(c, s->mass, dt_fs, pos, vel);
+    if (rattle) {
+      if (rattle_virial) memset(rattle_virial, 0, 9 * sizeof(double));
+      rattle_v(c, s->mass, dt_fs, pos, vel, rattle_virial);
+    }
   }
   memcpy(energies_out, e, sizeof(e));
   return 0;
@@ -1024,7 +1048,7 @@ int orc_langevin_constrained(const orc_system *s, const orc_cutoff_params *cp, c
                              int do_bonded, const orc_constraints *c, double dt_fs, double temperature,
                              double gamma_ps, unsigned long long seed, long long first_step, int nsteps,
                              double *pos, double *vel, double *last_pos, double *forces_out,
-                             double *energies_out) {
+                             double *energies_out, double *rattle_virial) {
   const int n = s->n;
   const int shake = c && c->n > 0 && c->shake_eps > 0 && c->shake_maxiter > 0;
   const int rattle = c && c->n > 0 && c->rattle_eps > 0 && c->rattle_maxiter > 0;
@@ -1041,7 +1065,10 @@ int orc_langevin_constrained(const orc_system *s, const orc_cutoff_params *cp, c
     if (shake) orc_shake(c, s->mass, n, dt_fs, pos, vel, last_pos);
     all_forces(s, cp, pme, do_bonded, pos, f, e);
     langevin_half_kick(s, f, h, gamma, kT, seed, j + 1, vel);
-    if (rattle) orc_rattle(c, s->mass, dt_fs, pos, vel);
+    if (rattle) {
+      if (rattle_virial) memset(rattle_virial, 0, 9 * sizeof(double));
+      rattle_v(c, s->mass, dt_fs, pos, vel, rattle_virial);
+    }
   }
   memcpy(energies_out, e, sizeof(e));
   return 0;

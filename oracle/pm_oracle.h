@@ -120,11 +120,13 @@ int orc_rattle(const orc_constraints *c, const double *mass, double dt_fs, const
 /* LeapfrogIntegrator::run(nsteps) with SHAKE as a post-drift modifier and RATTLE as a post-step
  * modifier (LeapfrogIntegrator.cpp:56-87,89-102; ModifierModule.cpp:106-128).  last_pos holds
  * the SHAKE reference positions (the initial positions before the first run).  cp/pme may be
- * NULL; with no force terms the forces are zero. */
+ * NULL; with no force terms the forces are zero.  rattle_virial (9 doubles, may be NULL): the
+ * virial the last RATTLE application adds, what the reference's energies hold of the modifiers
+ * after run(n) (the SHAKE terms are cleared by the next force evaluation). */
 int orc_leapfrog_constrained(const orc_system *s, const orc_cutoff_params *cp,
                              const orc_pme_params *pme, int do_bonded, const orc_constraints *c,
                              double dt_fs, int nsteps, double *pos, double *vel, double *last_pos,
-                             double *forces_out, double *energies_out);
+                             double *forces_out, double *energies_out, double *rattle_virial);
 
 /* LangevinLeapfrogIntegrator::run with SHAKE (post-drift) and RATTLE (post-step), the half kicks
  * and noise as orc_langevin, the modifiers as orc_leapfrog_constrained. */
@@ -132,7 +134,7 @@ int orc_langevin_constrained(const orc_system *s, const orc_cutoff_params *cp, c
                              int do_bonded, const orc_constraints *c, double dt_fs, double temperature,
                              double gamma_ps, unsigned long long seed, long long first_step, int nsteps,
                              double *pos, double *vel, double *last_pos, double *forces_out,
-                             double *energies_out);
+                             double *energies_out, double *rattle_virial);
 
 #ifdef __cplusplus
 }

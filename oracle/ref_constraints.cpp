@@ -26,6 +26,7 @@ using namespace ProtoMol::Report;
 #include <protomol/topology/CubicCellManager.h>
 #include <protomol/topology/PeriodicBoundaryConditions.h>
 #include <protomol/topology/Topology.h>
+#include <protomol/type/ScalarStructure.h>
 
 #include <cstring>
 
@@ -53,7 +54,7 @@ static int run_constrained(const ref_input *in, const char *elem, int shake, dou
                            int shake_maxiter, int rattle, double rattle_eps, int rattle_maxiter, int all,
                            int kind, double dt_fs, double temperature, double gamma_ps, int seed,
                            int nsteps, double *pos, double *vel, int *n_cons, int *cons, double *rest_len,
-                           int max_cons) {
+                           int max_cons, double *virial) {
   Topo *t = make_topo(in);
   for (int i = 0; i < in->n; i++) t->atoms[i].name = std::string(1, elem[i]);
   // what the topology builder sets besides: each atom's bond list and each molecule's atoms
@@ -81,10 +82,16 @@ static int run_constrained(const ref_input *in, const char *elem, int shake, dou
     li = new LangevinLeapfrogIntegrator(dt_fs, temperature, gamma_ps, seed, new ForceGroup());
   else
     li = new LeapfrogIntegrator(dt_fs, new ForceGroup());
+  app->energies.virial(virial != 0);
+  app->energies.molecularVirial(false);
   li->initialize(app);
   if (shake) li->adoptPostDriftOrNextModifier(new ModifierShake(shake_eps, shake_maxiter, all != 0));
   if (rattle) li->adoptPostStepModifier(new ModifierRattle(rattle_eps, rattle_maxiter, all != 0));
   li->run(nsteps);
+  // with no force terms what the energies hold after run(n) is the last RATTLE's virial (SHAKE's
+  // terms are cleared by the force evaluation that follows each drift)
+  if (virial)
+    for (int k = 0; k < 9; k++) virial[k] = app->energies[(ScalarStructure::Index)(ScalarStructure::VIRIALXX + k)];
   for (int i = 0; i < in->n; i++)
     for (int c = 0; c < 3; c++) {
       pos[3 * i + c] = app->positions[i][c];
@@ -105,9 +112,10 @@ extern "C" int ref_leapfrog_constrained(const ref_input *in, const char *elem, i
                                         double shake_eps, int shake_maxiter, int rattle,
                                         double rattle_eps, int rattle_maxiter, int all,
                                         double dt_fs, int nsteps, double *pos, double *vel,
-                                        int *n_cons, int *cons, double *rest_len, int max_cons) {
+                                        int *n_cons, int *cons, double *rest_len, int max_cons,
+                                        double *virial) {
   return run_constrained(in, elem, shake, shake_eps, shake_maxiter, rattle, rattle_eps, rattle_maxiter, all, 0,
-                         dt_fs, 0.0, 0.0, 0, nsteps, pos, vel, n_cons, cons, rest_len, max_cons);
+                         dt_fs, 0.0, 0.0, 0, nsteps, pos, vel, n_cons, cons, rest_len, max_cons, virial);
 }
 
 // The same with the LangevinLeapfrogIntegrator (temperature 0 makes its noise term vanish).
@@ -116,8 +124,8 @@ extern "C" int ref_langevin_constrained(const ref_input *in, const char *elem, i
                                         double rattle_eps, int rattle_maxiter, int all, double dt_fs,
                                         double temperature, double gamma_ps, int seed, int nsteps,
                                         double *pos, double *vel, int *n_cons, int *cons,
-                                        double *rest_len, int max_cons) {
+                                        double *rest_len, int max_cons, double *virial) {
   return run_constrained(in, elem, shake, shake_eps, shake_maxiter, rattle, rattle_eps, rattle_maxiter, all, 1,
                          dt_fs, temperature, gamma_ps, seed, nsteps, pos, vel, n_cons, cons, rest_len,
-                         max_cons);
+                         max_cons, virial);
 }

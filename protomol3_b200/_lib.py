@@ -95,6 +95,7 @@ _PROTOS = [
     ("pmb_md_energies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_use_graph", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_time", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("pmb_md_set_virial", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_set_constraints", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_constraint_sweeps", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_traj_open_dcd", C.c_void_p, [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_char_p]),

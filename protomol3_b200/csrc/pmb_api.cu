@@ -1670,6 +1670,7 @@ struct pmb_md {
   double *d_vel = nullptr, *d_kin = nullptr;
   long long *d_step = nullptr;
   bool have_state = false, use_graph = true;
+  bool virial = false;  // the steps evaluate the virial (forces and RATTLE's constraint terms)
   long long steps = 0;  // steps since the state was set (a checkpoint's step count)
   cudaGraphExec_t g_first = nullptr, g_next = nullptr;
   long long graph_gen = -1;  // list generation the graphs were captured with
@@ -1707,7 +1708,7 @@ int md_step_enqueue(pmb_md *m, double kick) {
     integrate_kick_drift(sd, m->in, kick, s->stream);
   }
   if (m->shake && constraints_apply(m->con, m->in, 0, s->stream)) return fail(PMB_ERR_CUDA, "SHAKE launch");
-  return enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+  return enqueue_forces(s, m->forces.data(), (int)m->forces.size(), m->virial ? 1 : 0);
 }
 
 // Before a capture: the list storage the run's forces need exists, and a change of list radius
@@ -1919,6 +1920,9 @@ int pmb_md_set_constraints(pmb_md *m, const pmb_constraint_desc *d) {
   c.clamp = std::min(1e6, 4611686018427387904.0 / (CON_ERR_SCALE * std::max(ng, 1)));
   const double TIMEFACTOR = 48.88821290839616;  // base/PMConstants.cpp:53
   c.dt = m->d.timestep_fs / TIMEFACTOR;  // ModifierShake.cpp:22, ModifierRattle.cpp:22
+  c.virial = m->virial ? 1 : 0;
+  c.eacc = s->d_eacc;
+  c.atom_box = s->d_atom_box;
   c.shake_eps = d->shake_epsilon;
   c.shake_max = shake ? d->shake_max_iter : 0;
   c.rattle_eps = d->rattle_epsilon;
@@ -2011,7 +2015,7 @@ int pmb_md_set_checkpoint(pmb_md *m, const double *pos, const double *vel, const
       s->have_pos = true;
       if (s->nb_ready) CK(cudaMemsetAsync(s->nb.ctl + 3, 1, 1, s->stream));  // rebuild
       zero_accumulators(sd, s->stream);
-      rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+      rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), m->virial ? 1 : 0);
       if (rc) return rc;
       rc = check_status(s);
     }
@@ -2024,7 +2028,7 @@ int pmb_md_set_checkpoint(pmb_md *m, const double *pos, const double *vel, const
       CK(cudaMemcpyAsync(m->d_step, &step, sizeof(long long), cudaMemcpyHostToDevice, s->stream));
       constraints_init(m->con, m->in, s->stream);  // the new positions are SHAKE's last ones
       zero_accumulators(sd, s->stream);
-      rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), 0);
+      rc = enqueue_forces(s, m->forces.data(), (int)m->forces.size(), m->virial ? 1 : 0);
       if (rc) return rc;
       rc = check_status(s);  // also waits for the step count's host copy
     }
@@ -2075,6 +2079,18 @@ int pmb_md_run(pmb_md *m, int n) {
   if (m->rattle && constraints_apply(m->con, m->in, 1, s->stream)) return fail(PMB_ERR_CUDA, "RATTLE launch");
   CK(cudaGetLastError());
   m->steps += n;
+  return PMB_OK;
+}
+
+int pmb_md_set_virial(pmb_md *m, int on) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  pmb_system *s = m->sys;
+  CK(cudaStreamSynchronize(s->stream));
+  m->virial = on != 0;
+  m->con.virial = m->virial ? 1 : 0;
+  m->con.eacc = s->d_eacc;
+  m->con.atom_box = s->d_atom_box;
+  m->drop_graphs();  // the step's kernels differ
   return PMB_OK;
 }
 
@@ -2139,10 +2155,11 @@ int pmb_md_energies(pmb_md *m, double *energies, double *kinetic) {
   CK(cudaMemcpyAsync(m->h_e.data(), s->d_eout, sizeof(double) * m->h_e.size(), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaMemcpyAsync(m->h_k.data(), m->d_kin, sizeof(double) * m->h_k.size(), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  add_const(m->forces.data(), (int)m->forces.size(), s->nbox, 0, m->h_e.data());
+  add_const(m->forces.data(), (int)m->forces.size(), s->nbox, m->virial ? 1 : 0, m->h_e.data());
   for (int b = 0; b < s->nbox; b++) {
     if (energies)
-      for (int k = 0; k < PMB_E_STRIDE; k++) energies[b * PMB_E_STRIDE + k] = k < E_VIR ? m->h_e[b * ACC_PER_BOX + k] : 0.0;
+      for (int k = 0; k < PMB_E_STRIDE; k++)
+        energies[b * PMB_E_STRIDE + k] = k < E_VIR || (m->virial && k < E_VIR + 9) ? m->h_e[b * ACC_PER_BOX + k] : 0.0;
     if (kinetic) kinetic[b] = m->h_k[b];
   }
   return check_status(s);

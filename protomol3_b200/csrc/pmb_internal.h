@@ -204,6 +204,10 @@ struct ConstraintDev {
   double dt;               // timestep / TIMEFACTOR, as the modifiers use it
   double shake_eps, rattle_eps;
   int shake_max, rattle_max;
+  // RATTLE's constraint virial (ModifierRattle.cpp:58), added to the box accumulators when set
+  int virial;
+  long long *eacc;
+  const int *atom_box;
 };
 constexpr int CON_MAX_SWEEPS = 256;  // max_iter + 1 bound
 constexpr int CON_ERR_BLOCK = 2 * (CON_MAX_SWEEPS + 1) + 2;

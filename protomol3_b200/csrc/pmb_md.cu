@@ -406,8 +406,10 @@ __device__ void shake_sweep(ConGroup<MA, MC> &g, double dt) {
   }
 }
 
+// vir6 (not null): adds the sweep's virial terms (2 dp) x rab of ModifierRattle.cpp:58, as
+// ScalarStructure::addVirial forms them (xx, xy, xz, yy, yz, zz)
 template <int MA, int MC>
-__device__ void rattle_sweep(ConGroup<MA, MC> &g, double dt) {
+__device__ void rattle_sweep(ConGroup<MA, MC> &g, double dt, double *vir6 = nullptr) {
 #pragma unroll
   for (int k = 0; k < MC; k++) {
     if (k < g.nc) {
@@ -426,14 +428,24 @@ __device__ void rattle_sweep(ConGroup<MA, MC> &g, double dt) {
       const double rabsq = dot3_rn(rab, rab);
       const double rvab = dot3_rn(rab, vab);
       const double gab = __ddiv_rn(-rvab, __dmul_rn(__dmul_rn(dt, __dadd_rn(rM1, rM2)), rabsq));
+      double f2[3];
 #pragma unroll
       for (int q = 0; q < 3; q++) {
         const double dp = __dmul_rn(rab[q], gab);
+        f2[q] = __dmul_rn(dp, 2.0);
         v1[q] = __dadd_rn(v1[q], __dmul_rn(__dmul_rn(dp, dt), rM1));
         v2[q] = __dsub_rn(v2[q], __dmul_rn(__dmul_rn(dp, dt), rM2));
       }
       put3(g.v, a1, v1);
       put3(g.v, a2, v2);
+      if (vir6) {
+        vir6[0] = __dadd_rn(vir6[0], __dmul_rn(f2[0], rab[0]));
+        vir6[1] = __dadd_rn(vir6[1], __dmul_rn(f2[0], rab[1]));
+        vir6[2] = __dadd_rn(vir6[2], __dmul_rn(f2[0], rab[2]));
+        vir6[3] = __dadd_rn(vir6[3], __dmul_rn(f2[1], rab[1]));
+        vir6[4] = __dadd_rn(vir6[4], __dmul_rn(f2[1], rab[2]));
+        vir6[5] = __dadd_rn(vir6[5], __dmul_rn(f2[2], rab[2]));
+      }
     }
   }
 }
@@ -590,6 +602,10 @@ __global__ void __launch_bounds__(CON_THREADS) k_con_apply(ConstraintDev c, Inte
   ConGroup<MA, MC> g;
   con_load<MA, MC>(c, in, gi, !RATTLE, g);
   const int a0 = c.group_atom[gi], na = c.group_atom[gi + 1] - a0;
+  // the constraint virial needs every sweep's multipliers: replay rather than copy
+  const bool vir = RATTLE && c.virial;
+  if (vir) from_window = false;
+  double v6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   if (from_window) {
 #pragma unroll
     for (int i = 0; i < MA; i++) {
@@ -601,8 +617,22 @@ __global__ void __launch_bounds__(CON_THREADS) k_con_apply(ConstraintDev c, Inte
         }
       }
     }
+  } else if (vir) {
+    for (int k = 0; k < K; k++) rattle_sweep(g, c.dt, v6);
   } else {
     for (int k = 0; k < K; k++) con_sweep<MA, MC, RATTLE>(g, c.dt);
+  }
+  if (vir) {
+    // the group's terms in fixed point (ENERGY_SCALE) into its box's virial slots, row-major
+    long long *acc = c.eacc + (long long)c.atom_box[c.atoms[a0]] * ACC_PER_BOX + E_VIR;
+    const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const long long v = f2fix(v6[k], ENERGY_SCALE);
+      if (!v) continue;
+      red_add(acc + slot[k][0], v);
+      if (slot[k][1] != slot[k][0]) red_add(acc + slot[k][1], v);
+    }
   }
 #pragma unroll
   for (int i = 0; i < MA; i++) {

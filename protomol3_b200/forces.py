@@ -462,6 +462,11 @@ class Integrator:
         L.check(L.lib().pmb_md_get_state(self._h, _p(pos), _p(vel)))
         return pos, vel
 
+    def set_virial(self, on=True):
+        """Energies with the virial (forces and RATTLE's constraint terms), ScalarStructure's
+        virial() switch."""
+        L.check(L.lib().pmb_md_set_virial(self._h, int(on)))
+
     def time_steps(self, n):
         """Mean device time (ms) of a step over n steps (CUDA events on the system's stream)."""
         ms = C.c_double(0.0)

@@ -18,6 +18,9 @@ step, for four modifier settings (``shake``/``rattle`` with their epsilon and ma
   application before convergence;
 * ``lv``: the LangevinLeapfrogIntegrator at temperature 0 (noise term exactly zero) with
   gamma 50/ps, SHAKE and RATTLE at the defaults, 20 steps.
+
+Every case also keeps ``<case>_virial``: the virial the reference's energies hold after the run
+(ScalarStructure with virial on; with no force terms, the last RATTLE application's terms).
 """
 import os
 import sys
@@ -42,16 +45,19 @@ def main():
     system = O.System(box)
     out = {"pos0": box["pos"], "vel0": box["vel"], "dt": 2.0}
     for name, (shake, rattle, steps) in CASES.items():
+        vir = np.zeros(9)
         pos, vel, cons = O.ref_leapfrog_constrained(system, box["elem"], box["pos"], box["vel"],
-                                                    2.0, steps, shake=shake, rattle=rattle)
-        out[name + "_pos"], out[name + "_vel"] = pos, vel
+                                                    2.0, steps, shake=shake, rattle=rattle, virial=vir)
+        out[name + "_pos"], out[name + "_vel"], out[name + "_virial"] = pos, vel, vir
         out[name + "_steps"] = steps
         out[name + "_shake"] = np.array(shake if shake else (0.0, 0))
         out[name + "_rattle"] = np.array(rattle if rattle else (0.0, 0))
         out["con_a1"], out["con_a2"], out["con_len"] = cons
+    vir = np.zeros(9)
     pos, vel, cons = O.ref_leapfrog_constrained(system, box["elem"], box["pos"], box["vel"], 2.0, 20,
-                                                shake=(1e-5, 30), rattle=(1e-5, 30), langevin=(0.0, 50.0, 1234))
-    out["lv_pos"], out["lv_vel"], out["lv_steps"], out["lv_gamma"] = pos, vel, 20, 50.0
+                                                shake=(1e-5, 30), rattle=(1e-5, 30), langevin=(0.0, 50.0, 1234),
+                                                virial=vir)
+    out["lv_pos"], out["lv_vel"], out["lv_steps"], out["lv_gamma"], out["lv_virial"] = pos, vel, 20, 50.0, vir
     np.savez_compressed(os.path.join(HERE, "water64_rigid_ref.npz"), **out)
 
 

@@ -43,12 +43,17 @@ def test_constraint_list_matches_reference_builder(gold):
 def test_oracle_equals_reference_run(gold, case):
     box = W.water_box(64, seed=7)
     cons = CS.rattle_shake_constraints(box)
+    vir = np.zeros(9)
     pos, vel, _, _ = O.leapfrog_constrained(O.System(box), gold["pos0"], gold["vel0"], float(gold["dt"]),
                                             int(gold[case + "_steps"]), cons,
                                             shake=_opt(gold[case + "_shake"]),
-                                            rattle=_opt(gold[case + "_rattle"]))
+                                            rattle=_opt(gold[case + "_rattle"]), rattle_virial=vir)
     assert np.array_equal(pos, gold[case + "_pos"])
     assert np.array_equal(vel, gold[case + "_vel"])
+    # the constraint virial the reference's energies hold after the run: the last RATTLE's
+    # (ModifierRattle.cpp:58; SHAKE's terms, ModifierShake.cpp:65-68, are cleared by the force
+    # evaluation after each drift, so a SHAKE-only run reports none)
+    assert np.array_equal(vir, gold[case + "_virial"])
 
 
 def test_oracle_langevin_equals_reference_run(gold):
@@ -56,10 +61,13 @@ def test_oracle_langevin_equals_reference_run(gold):
     oracle's restatement equals the reference's run bit for bit."""
     box = W.water_box(64, seed=7)
     cons = CS.rattle_shake_constraints(box)
+    vir = np.zeros(9)
     pos, vel, _, _ = O.langevin_constrained(O.System(box), gold["pos0"], gold["vel0"], float(gold["dt"]),
-                                            int(gold["lv_steps"]), cons, 0.0, float(gold["lv_gamma"]))
+                                            int(gold["lv_steps"]), cons, 0.0, float(gold["lv_gamma"]),
+                                            rattle_virial=vir)
     assert np.array_equal(pos, gold["lv_pos"])
     assert np.array_equal(vel, gold["lv_vel"])
+    assert np.array_equal(vir, gold["lv_virial"])
 
 
 def test_planted_mistake_is_caught(gold):

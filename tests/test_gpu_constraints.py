@@ -166,3 +166,62 @@ def test_langevin_with_constraints_and_noise_equals_oracle(precision):
     assert np.mean(np.abs(d2 - ln ** 2) / (2 * ln ** 2)) <= 1e-5
     md.close()
     topo.close()
+
+
+@pytest.mark.parametrize("case", ["sr", "r", "tight", "s", "lv"])
+def test_rattle_constraint_virial_equals_reference(case):
+    """With the virial on, the run's energies hold after run(n) what the reference's do: the
+    virial of the last RATTLE application (ModifierRattle.cpp:58; no force terms here), and none
+    for SHAKE alone (its terms are cleared by the force evaluation after each drift)."""
+    g = np.load(GOLD)
+    box = W.water_box(64, seed=7)
+    cons = CS.rattle_shake_constraints(box)
+    topo = F.Topology(box, "fp64")
+    if case == "lv":
+        md = F.Integrator(topo, [], timestep=float(g["dt"]), kind="langevin", temperature=0.0,
+                          gamma=float(g["lv_gamma"]), seed=3)
+        shake, rattle, steps = (1e-5, 30), (1e-5, 30), int(g["lv_steps"])
+    else:
+        md = F.Integrator(topo, [], timestep=float(g["dt"]))
+        shake, rattle, steps = _opt(g[case + "_shake"]), _opt(g[case + "_rattle"]), int(g[case + "_steps"])
+    md.set_virial(True)
+    md.set_constraints(cons, shake=shake is not None, shake_epsilon=(shake or (0, 0))[0],
+                       shake_max_iter=(shake or (0, 0))[1], rattle=rattle is not None,
+                       rattle_epsilon=(rattle or (0, 0))[0], rattle_max_iter=(rattle or (0, 0))[1])
+    md.set_state(box["pos"], box["vel"])
+    md.run(steps)
+    e, _ = md.energies()
+    vir = e[0, L.E_VIRIAL:L.E_VIRIAL + 9]
+    ref = g[case + "_virial"]
+    assert np.abs(vir - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()) + 64 * 2.0 ** -31
+    md.close()
+    topo.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_md_force_virial_equals_evaluation(precision):
+    """Without constraints the run's virial after a step is the force virial of the step's
+    evaluation: the same as pmb_evaluate's at the run's positions."""
+    box = W.water_box(216, seed=12)
+    fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
+          F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0)]
+    topo = F.Topology(box, precision)
+    md = F.Integrator(topo, fl, timestep=1.0)
+    md.set_virial(True)
+    md.set_state(box["pos"], box["vel"])
+    md.run(3)
+    e, _ = md.energies()
+    pos, _ = md.state()
+    t2 = F.Topology(box, precision)
+    f = np.zeros((t2.n_atoms, 3))
+    ss = F.ScalarStructure(1, virial=True)
+    F.evaluate_all(t2, [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
+                        F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0)], pos, f, ss)
+    tol = 1e-9 if precision == "fp64" else 1e-5
+    v, vr = e[0, L.E_VIRIAL:L.E_VIRIAL + 9], ss.virial().ravel()
+    assert np.abs(v - vr).max() <= tol * np.abs(vr).max() * 10
+    np.testing.assert_allclose(e[0, :4], ss.table[0, :4], rtol=tol, atol=216 * 3 * 2.0 ** -31)
+    for m, t in ((md, topo),):
+        m.close()
+        t.close()
+    t2.close()
