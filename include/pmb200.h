@@ -139,8 +139,10 @@ int pmb_system_get_tuning(const pmb_system *sys, pmb_tuning *tuning);
  * difference is then the plain difference.  pmb_vacuum_box gives such edges for positions
  * [3 n_atoms]: 2 (extent + margin) + 1 per axis (margin: room for the atoms to move, e.g. the
  * list radius).  With pmb_system_set_vacuum on, pmb_evaluate and pmb_force_evaluate check the
- * extent of every box's atoms and return PMB_ERR_STATE once it reaches half an edge (device
- * positions and MD runs are not checked). */
+ * extent of every box's atoms and return PMB_ERR_STATE once it reaches half an edge; evaluations
+ * of device positions and MD runs check it on the device (the list's displacement check, for
+ * force sets with a pair term), reported by pmb_system_check and the MD calls that wait for the
+ * stream (pmb_md_get_state, pmb_md_energies, ...). */
 int pmb_vacuum_box(const double *positions, int n_atoms, double margin, double edges[3]);
 /* Exact Ewald reciprocal sum, the check path for the PME reciprocal term: what
  * NonbondedFullEwaldSystemForce with only -reciprocal adds (reciprocalTerm,

@@ -466,11 +466,18 @@ int nblist_alloc(pmb_system *s, double rl) {
   nb.scan_tmp = s->nba.get<int>(maxn / 4096 + 2);
   nb.xref = s->nba.get<double>(3 * (size_t)s->natoms);
   nb.ctl = s->nba.get<unsigned>(12);
+  nb.vext = s->nba.get<int>(6 * (size_t)s->nbox);
+  if (nb.vext) {
+    std::vector<int> ext(6 * (size_t)s->nbox);
+    for (size_t k = 0; k < ext.size(); k++) ext[k] = (k % 6) < 3 ? 0x7fffffff : (int)0x80000000;
+    CK(cudaMemcpy(nb.vext, ext.data(), sizeof(int) * ext.size(), cudaMemcpyHostToDevice));
+  }
   nb.half_skin2 = (float)(0.25 * s->skin * s->skin);
-  if (!nb.xref || !nb.ctl) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
+  if (!nb.xref || !nb.ctl || !nb.vext) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
   // {max displacement, rebuild, finished blocks, forced rebuild, builds (64-bit), pair chunk
-  // counter and finished warps of the two pair launches}; first use builds the list
-  const unsigned ctl0[12] = {0u, 0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  // counter and finished warps of the two pair launches, vacuum extent check}; first use builds
+  // the list
+  const unsigned ctl0[12] = {0u, 0u, 0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, s->vacuum ? 1u : 0u, 0u};
   CK(cudaMemcpy(nb.ctl, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice));
   s->nb_build_rl = -1.0;
   if (!nb.blk_lo || !nb.sblk_lo || !nb.sblk_hi || !nb.blk_c || !nb.blk_h || !nb.sblk_c || !nb.sblk_h || !nb.jlist || !nb.tile_blk || !nb.slot_meta || !nb.fslot ||
@@ -806,11 +813,13 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
 // The status words as they were copied to s->h_status: capacity before non-finite positions
 // (a retry with larger lists comes first).  Clears the device words that were set.
 int status_code(pmb_system *s) {
-  if (s->h_status[0] || s->h_status[1] || s->h_status[2]) {
+  if (s->h_status[0] || s->h_status[1] || s->h_status[2] || s->h_status[3]) {
     cudaMemsetAsync(s->nb.status, 0, 4 * sizeof(int), s->stream);
     if (s->h_status[0] || s->h_status[1])
       return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded (atoms denser than expected)");
-    return fail(PMB_ERR_NUMERIC, "non-finite position");
+    if (s->h_status[2]) return fail(PMB_ERR_NUMERIC, "non-finite position");
+    return fail(PMB_ERR_STATE, "vacuum: the atoms spread over half a box edge; make the system again with "
+                               "edges from pmb_vacuum_box");
   }
   return PMB_OK;
 }
@@ -1495,6 +1504,11 @@ int pmb_vacuum_box(const double *pos, int n_atoms, double margin, double edges[3
 int pmb_system_set_vacuum(pmb_system *s, int on) {
   if (!s) return fail(PMB_ERR_ARG, "null system");
   s->vacuum = on != 0;
+  if (s->nb_ready) {
+    const unsigned v = s->vacuum ? 1u : 0u;
+    CK(cudaMemcpyAsync(s->nb.ctl + 10, &v, sizeof(v), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
   return PMB_OK;
 }
 

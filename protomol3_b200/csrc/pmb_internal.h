@@ -43,7 +43,7 @@ struct NbListDev {
   int *tile_blk;               // [tile_cap] block of each tile
   int *tile_k;                 // [tile_cap] tile index within the block
   int tile_cap;
-  int *status;                 // [4]: list / tile overflow, non-finite position, unused
+  int *status;                 // [4]: list / tile overflow, non-finite position, vacuum extent
   // per slot
   int nslot;
   int *slot_orig;              // [nslot] original atom index or -1
@@ -68,6 +68,8 @@ struct NbListDev {
                                // force flag, list builds (64-bit counter in [4..5]), the pair
                                // kernel's next chunk and finished warps ([6], [7]; zero between launches)
   float half_skin2;
+  int *vext;                   // [6 nbox] vacuum extent per box: smallest and largest x, y, z as
+                               // order-preserving int images of their float values (ctl[10] on)
 };
 
 struct SystemDev {

@@ -142,13 +142,33 @@ __global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out, c
 // ctl = {max displacement^2 as float bits, rebuild flag, finished blocks, forced rebuild}.
 // It reads every position of every evaluation, so it also raises status[2] for a non-finite
 // one (the host reports PMB_ERR_NUMERIC; every later kernel maps such a position to an in-range
-// cell and grid index, so nothing reads out of bounds meanwhile).
+// cell and grid index, so nothing reads out of bounds meanwhile), and, for a system whose boxes
+// stand in for vacuum (ctl[10]), status[3] once the atoms of a box spread over half an edge
+// (the minimal image would no longer be the plain difference).
+__device__ __forceinline__ int ford(float f) {  // order-preserving int image of a float
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float fuord(int o) { return __int_as_float(o >= 0 ? o : o ^ 0x7fffffff); }
+
 __global__ void k_disp_check(SystemDev s, NbListDev nb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
+  const bool vacuum = nb.ctl[10] != 0u;
   if (i < s.natoms) {
     const double x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicExch(&nb.status[2], 1);
+    if (vacuum) {
+      int *e = nb.vext + 6 * s.atom_box[i];
+      const double p[3] = {x, y, z};
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const int o = ford((float)p[d]);
+        atomicMin(e + d, o);
+        atomicMax(e + 3 + d, o);
+      }
+      __threadfence();
+    }
     double dx = x - nb.xref[3 * i], dy = y - nb.xref[3 * i + 1], dz = z - nb.xref[3 * i + 2];
     double r2 = dx * dx + dy * dy + dz * dz;
     d2 = r2 < 3.0e38 ? (float)r2 : 3.0e38f;
@@ -167,6 +187,14 @@ __global__ void k_disp_check(SystemDev s, NbListDev nb) {
     unsigned done = atomicAdd(&nb.ctl[2], 1u);
     if (done == gridDim.x - 1) {
       __threadfence();
+      if (vacuum)
+        for (int b = 0; b < s.nbox; b++)
+          for (int d = 0; d < 3; d++) {
+            // read and reset for the next evaluation
+            const float lo = fuord(atomicExch(nb.vext + 6 * b + d, 0x7fffffff));
+            const float hi = fuord(atomicExch(nb.vext + 6 * b + 3 + d, (int)0x80000000));
+            if (!((double)hi - (double)lo < 0.5 * s.box[b].L[d])) atomicExch(&nb.status[3], 1);
+          }
       float mx = __uint_as_float(atomicAdd(&nb.ctl[0], 0u));
       const unsigned rebuild = (nb.ctl[3] != 0u || mx > nb.half_skin2) ? 1u : 0u;
       nb.ctl[1] = rebuild;

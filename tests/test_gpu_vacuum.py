@@ -51,3 +51,33 @@ def test_spread_beyond_half_an_edge_is_refused():
     with pytest.raises(RuntimeError):
         force.evaluate(tp, pos, np.zeros_like(pos), F.ScalarStructure(1))
     tp.close()
+
+
+def test_md_in_vacuum_refuses_atoms_spread_over_half_an_edge():
+    """Device-resident MD in a vacuum box: a run whose atoms stay together goes on; once an
+    atom flies off beyond half an edge from the others, the device's extent check stops the
+    run's results with PMB_ERR_STATE (the minimal image would no longer be the plain
+    difference)."""
+    from protomol3_b200 import _lib as L
+    g = np.load(GOLD)
+    t = topo(g, "ala", margin=2.0)
+    force = F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0), coulomb=("C2", 8.0, 10.0))
+    for fly in (False, True):
+        tp = F.Topology(t, "fp64")
+        tp.set_vacuum()
+        md = F.Integrator(tp, [F.BondedSystemForce(), force], timestep=1.0)
+        vel = np.zeros_like(t["pos"])
+        if fly:
+            vel[0, 0] = 5.0  # A per internal time unit: ~0.1 A per fs, far past the margin in 100 fs
+        md.set_state(t["pos"], vel)
+        if fly:
+            with pytest.raises(L.PMBError) as err:
+                md.run(200)
+                md.state()
+            assert err.value.code == L.PMB_ERR_STATE and "vacuum" in str(err.value)
+        else:
+            md.run(50)
+            pos, _ = md.state()
+            assert np.isfinite(pos).all()
+        md.close()
+        tp.close()
