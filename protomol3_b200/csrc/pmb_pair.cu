@@ -330,8 +330,9 @@ struct Acc2 {
 
 // HALF steps of one lane over its lane group's j-pairs; fi collects +f (the i-force is -fi).
 // sa: this lane's first entry of the packed staging positions (z, charges at + FAST_ENTRIES);
-// sty: its first entry of the packed types.
-template <int LSW, int CM, int CSW, bool VIR>
+// sty: its first entry of the packed types.  ALL: the LJ and Coulomb cutoffs both cover the pair
+// cutoff (the common case), so the pair mask is the only one (chosen per tile, not per step).
+template <int LSW, int CM, int CSW, bool VIR, bool ALL>
 __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float2 *__restrict__ ljab,
                                             int tio, const float4 *sa, const int2 *sty, int nxt,
                                             float xi, float yi, float zi, float qi, Acc2 &a) {
@@ -350,7 +351,7 @@ __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float
     if constexpr (LSW != NONE) {
       if (LSW != SWR || p.do_lj) {
         float2 ml = m;
-        if (!p.lj_all) ml = mul2(m, make_float2(le_mask(r2.x, p.lj_cut2), le_mask(r2.y, p.lj_cut2)));
+        if (!ALL && !p.lj_all) ml = mul2(m, make_float2(le_mask(r2.x, p.lj_cut2), le_mask(r2.y, p.lj_cut2)));
         const float2 pa = ljab[tio + ty.x], pb = ljab[tio + ty.y];
         const float2 A = mul2(make_float2(pa.x, pb.x), ml), B = mul2(make_float2(pa.y, pb.y), ml);
         const float2 r6 = mul2(mul2(rd2, rd2), rd2);
@@ -364,7 +365,7 @@ __device__ __forceinline__ void tile_pairs2(const ParamsT<float> &p, const float
     }
     if constexpr (CM != 0) {
       float2 mc = m;
-      if (!p.coul_all) mc = mul2(m, make_float2(le_mask(r2.x, p.coul_cut2), le_mask(r2.y, p.coul_cut2)));
+      if (!ALL && !p.coul_all) mc = mul2(m, make_float2(le_mask(r2.x, p.coul_cut2), le_mask(r2.y, p.coul_cut2)));
       const float2 q = mul2(make_float2(v.z, v.w), mul2(mc, qi2));
       float2 e, f;
       if constexpr (CM == 1) {
@@ -757,8 +758,12 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
           __syncwarp();
 #pragma unroll
           for (int c = 0; c < 3; c++) a2p.fj[c] = sp2(0.f);
-          tile_pairs2<LSW, CM, CSW, VIR>(pt, reinterpret_cast<const float2 *>(ljab), tio, qa, qt, nxt, xi,
-                                         yi, zi, qi, a2p);
+          if (pt.lj_all && pt.coul_all)
+            tile_pairs2<LSW, CM, CSW, VIR, true>(pt, reinterpret_cast<const float2 *>(ljab), tio, qa, qt, nxt, xi,
+                                                 yi, zi, qi, a2p);
+          else
+            tile_pairs2<LSW, CM, CSW, VIR, false>(pt, reinterpret_cast<const float2 *>(ljab), tio, qa, qt, nxt,
+                                                  xi, yi, zi, qi, a2p);
           // after HALF rotations: .y holds this lane's j-atom, .x that of the lane HALF away
 #pragma unroll
           for (int c = 0; c < 3; c++) tfj[c] = a2p.fj[c].y + __shfl_xor_sync(0xffffffffu, a2p.fj[c].x, HALF);
