@@ -394,7 +394,7 @@ def run_b200(args, rank, world, local_rank):
         hpos[:] = box["pos"]
         h = DT_FS * 0.02045482828087295
         tvel = torch.from_numpy(box["vel"].copy())
-        thinv = torch.from_numpy(h / box["mass"])[:, None]
+        thinv = torch.from_numpy(np.repeat(h / box["mass"], 3).reshape(n, 3))
         en = F.ScalarStructure(1)
         nsteps = max(3, args.steps // 2)
         parts = {"enqueue": 0.0, "wait_device": 0.0, "accumulate": 0.0, "host_leapfrog": 0.0}

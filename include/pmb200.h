@@ -168,7 +168,8 @@ int pmb_system_list_builds(pmb_system *sys, long long *n);
 /* Host time of the last pmb_evaluate / pmb_force_evaluate, in ms: [0] checks and enqueueing
  * (the position upload and every launch), [1] waiting for the device's first results (status
  * and energies), [2] adding the forces into the caller's array while their device->host copies
- * land piece by piece.  No counterpart in the reference (TimerStatistic times whole forces). */
+ * land piece by piece (a page-locked force array: waiting for the sum to land in it).  No
+ * counterpart in the reference (TimerStatistic times whole forces). */
 int pmb_system_evaluate_times(const pmb_system *sys, double ms[3]);
 
 /* Forces ------------------------------------------------------------------------------------- */
@@ -184,7 +185,10 @@ int pmb_force_evaluate(pmb_force *f, const double *positions, double *forces, do
                        int virial);
 /* Several forces of one system in one device pass (ForceGroup::evaluateSystemForces).  A
  * non-finite position gives PMB_ERR_NUMERIC with forces and energies untouched (detected on the
- * device by the list kernels, on the host for force sets that need no list). */
+ * device by the list kernels, on the host for force sets that need no list).  A page-locked
+ * forces_out (cudaMallocHost, cudaHostAlloc, cudaHostRegister) is uploaded beside the force
+ * kernels, added to on the device and copied back into directly, with no host pass over it; a
+ * pageable one is added to on the host.  Both give the same doubles. */
 int pmb_evaluate(pmb_system *sys, pmb_force *const *forces, int n_forces, const double *positions,
                  double *forces_out, double *energies, int virial);
 /* Same, with device pointers and no host synchronisation: d_forces and d_energies are

@@ -270,6 +270,7 @@ struct AddPool {
 struct EvalGraph {
   std::vector<unsigned long long> ids;
   int virial = 0;
+  bool direct = false;  // forces added on the device to the caller's uploaded array (no host add)
   long long gen = -1;  // list storage generation it was captured with
   double rlist = 0.0;
   bool used_list = false;
@@ -309,6 +310,12 @@ struct pmb_system {
   bool last_used_list = false;          // the last evaluation ran the list kernels
   bool eval_graph = true;               // host-pointer evaluations replay captured graphs
   AddPool *add_pool = nullptr;          // made at the first large host-pointer evaluation
+  // host-pointer evaluations whose force array is page-locked: the array goes up on its own copy
+  // stream once the positions have landed (the copy overlaps the force kernels), the device adds
+  // the new forces to it and the sum comes back straight into the caller's array
+  double *d_fin = nullptr;
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_pos = nullptr, ev_fin = nullptr;
   std::vector<EvalGraph> eval_graphs;   // at most EVAL_GRAPHS, most recent last
   static constexpr int EVAL_GRAPHS = 4;
   // neighbour list
@@ -347,6 +354,9 @@ struct pmb_system {
   }
   ~pmb_system() {
     delete add_pool;
+    if (copy) cudaStreamDestroy(copy);
+    if (ev_pos) cudaEventDestroy(ev_pos);
+    if (ev_fin) cudaEventDestroy(ev_fin);
     for (EvalGraph &g : eval_graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : ev_out)
@@ -729,14 +739,14 @@ void add_const(pmb_force *const *fs, int n, int nbox, int virial, double *e) {
 // Device->host copies of a host-pointer evaluation on the system stream (inside or outside a
 // capture): status and energies, then the forces in EVAL_CHUNKS pieces, each followed by its
 // event (external events, so that the host can wait on them when they come from a graph).
-int enqueue_eval_copies(pmb_system *s) {
+int enqueue_eval_copies(pmb_system *s, bool with_forces = true) {
   cudaStream_t st = s->stream;
   const long long nf = 3LL * s->natoms;
   const long long chunk = (nf + pmb_system::EVAL_CHUNKS - 1) / pmb_system::EVAL_CHUNKS;
   if (s->nb_ready) CK(cudaMemcpyAsync(s->h_status, s->nb.status, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(s->h_eout, s->d_eout, sizeof(double) * s->nbox * ACC_PER_BOX, cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecordWithFlags(s->ev_out[0], st, cudaEventRecordExternal));
-  for (int c = 0; c < pmb_system::EVAL_CHUNKS; c++) {
+  for (int c = 0; c < pmb_system::EVAL_CHUNKS && with_forces; c++) {
     const long long b0 = c * chunk, b1 = std::min(nf, b0 + chunk);
     if (b1 > b0)
       CK(cudaMemcpyAsync(s->h_fout + b0, s->d_fout + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost, st));
@@ -750,7 +760,7 @@ int enqueue_eval_copies(pmb_system *s) {
 // storage it captured stays (generation) and the list radius is unchanged; the list storage and
 // radius are settled before any capture, so a captured step neither allocates nor forces a
 // rebuild on every replay.
-int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
+int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bool direct) {
   cudaStream_t st = s->stream;
   const double rlist = list_radius(s, fs, n);
   if (rlist > 0.0) {
@@ -767,7 +777,7 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   EvalGraph *g = nullptr;
   for (size_t k = 0; k < s->eval_graphs.size(); k++) {
     EvalGraph &e = s->eval_graphs[k];
-    if (e.ids == ids && e.virial == virial && e.gen == s->nb_gen && e.rlist == rlist) {
+    if (e.ids == ids && e.virial == virial && e.direct == direct && e.gen == s->nb_gen && e.rlist == rlist) {
       std::rotate(s->eval_graphs.begin() + k, s->eval_graphs.begin() + k + 1, s->eval_graphs.end());
       g = &s->eval_graphs.back();
       break;
@@ -780,9 +790,14 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     zero_accumulators(sd, st);
     int rc = enqueue_forces(s, fs, n, virial);
     if (!rc) {
-      forces_to_double(sd, s->d_fout, st);
+      if (direct) {  // the caller's forces, uploaded beside the force kernels, are the base
+        CK(cudaStreamWaitEvent(st, s->ev_fin, cudaEventWaitExternal));
+        forces_to_double(sd, s->d_fout, st, s->d_fin);
+      } else {
+        forces_to_double(sd, s->d_fout, st);
+      }
       energies_to_double(sd, nullptr, s->d_eout, st);
-      rc = enqueue_eval_copies(s);
+      rc = enqueue_eval_copies(s, !direct);
     }
     cudaError_t e = cudaStreamEndCapture(st, &graph);
     if (rc || e != cudaSuccess) {
@@ -792,6 +807,7 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
     EvalGraph ng;
     ng.ids = ids;
     ng.virial = virial;
+    ng.direct = direct;
     ng.gen = s->nb_gen;
     ng.rlist = rlist;
     ng.used_list = s->last_used_list;
@@ -808,6 +824,20 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial) {
   s->last_used_list = g->used_list;
   CK(cudaGraphLaunch(g->exec, st));
   return PMB_OK;
+}
+
+// True when both ends of the n doubles at p are page-locked host memory (cudaMallocHost,
+// cudaHostAlloc or cudaHostRegister), which the copy engines read and write directly.
+bool host_pinned(const double *p, long long n) {
+  for (const double *q : {p, p + n - 1}) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (at.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
 }
 
 // The status words as they were copied to s->h_status: capacity before non-finite positions
@@ -1539,12 +1569,35 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
   const long long chunk = (nf + pmb_system::EVAL_CHUNKS - 1) / pmb_system::EVAL_CHUNKS;
   // a captured graph per force set, except under the stage profiler or on the legacy stream
   const bool graphed = s->eval_graph && !s->prof && st != nullptr && st != cudaStreamLegacy;
+  // page-locked force array: added to on the device and copied back into directly
+  const bool direct = graphed && forces && nf > 0 && host_pinned(forces, nf);
+  if (direct && !s->d_fin) {
+    if (cudaMalloc(&s->d_fin, sizeof(double) * nf) != cudaSuccess) {
+      s->d_fin = nullptr;
+      return fail(PMB_ERR_CUDA, "cudaMalloc failed for the force upload");
+    }
+    CK(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&s->ev_pos, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s->ev_fin, cudaEventDisableTiming));
+  }
   for (int attempt = 0; attempt < 3; attempt++) {
     CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
     s->have_pos = true;
+    if (direct && attempt == 0) {
+      // after the positions (the two uploads would share the link), beside the force kernels;
+      // a retry keeps this copy of the caller's forces
+      CK(cudaEventRecord(s->ev_pos, st));
+      CK(cudaStreamWaitEvent(s->copy, s->ev_pos, 0));
+      CK(cudaMemcpyAsync(s->d_fin, forces, sizeof(double) * nf, cudaMemcpyHostToDevice, s->copy));
+      CK(cudaEventRecord(s->ev_fin, s->copy));
+    }
     int rc;
     if (graphed) {
-      rc = eval_graph_launch(s, fs, n, virial);
+      rc = eval_graph_launch(s, fs, n, virial, direct);
+      if (!rc && direct) {
+        CK(cudaMemcpyAsync(forces, s->d_fout, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(s->ev_out[1], st));
+      }
     } else {
       rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
       if (!rc) rc = enqueue_eval_copies(s);
@@ -1560,13 +1613,21 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
           rc = fail(PMB_ERR_NUMERIC, "non-finite position");
           break;
         }
-    if (rc) CK(cudaStreamSynchronize(st));  // the copies in flight land before a retry or return
+    if (rc) {
+      CK(cudaStreamSynchronize(st));  // the copies in flight land before a retry or return
+      if (direct) {  // the caller's array gets its own values back
+        CK(cudaMemcpyAsync(forces, s->d_fin, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+      }
+    }
     if (rc == PMB_ERR_CAPACITY) {
       if (grow_and_retry_needed(s)) return PMB_ERR_CUDA;
       continue;
     }
     if (rc) return rc;
-    if (forces && nf >= (1 << 16)) {
+    if (direct) {
+      CK(cudaEventSynchronize(s->ev_out[1]));
+    } else if (forces && nf >= (1 << 16)) {
       // large systems: the pool's threads share every piece as it lands
       if (!s->add_pool) {
         const unsigned hw = std::thread::hardware_concurrency();

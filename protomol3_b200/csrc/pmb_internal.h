@@ -169,7 +169,8 @@ struct BondedDev {
   int virial;
 };
 int bonded_launch(const SystemDev &s, const BondedDev &b, cudaStream_t st);
-int forces_to_double(const SystemDev &s, double *out, cudaStream_t st);
+// out = base + the accumulated forces (base may be null)
+int forces_to_double(const SystemDev &s, double *out, cudaStream_t st, const double *base = nullptr);
 int energies_to_double(const SystemDev &s, const double *const_e, double *out, cudaStream_t st);
 int zero_accumulators(const SystemDev &s, cudaStream_t st);
 

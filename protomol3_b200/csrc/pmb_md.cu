@@ -83,10 +83,11 @@ __global__ void k_angles(const SystemDev s, BondedDev b) {
   box_accumulate(s.eacc, box, valid, E_ANGLE, en, b.virial ? vir : nullptr);
 }
 
-__global__ void k_forces_to_double(const SystemDev s, double *out) {
+__global__ void k_forces_to_double(const SystemDev s, double *out, const double *base) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 3 * s.natoms) return;
-  out[i] = (double)s.facc[i] * (1.0 / FORCE_SCALE);
+  const double f = (double)s.facc[i] * (1.0 / FORCE_SCALE);
+  out[i] = base ? base[i] + f : f;
 }
 
 __global__ void k_energies_to_double(const SystemDev s, const double *cst, double *out) {
@@ -699,9 +700,9 @@ int bonded_launch(const SystemDev &s, const BondedDev &b, cudaStream_t st) {
   return 0;
 }
 
-int forces_to_double(const SystemDev &s, double *out, cudaStream_t st) {
+int forces_to_double(const SystemDev &s, double *out, cudaStream_t st, const double *base) {
   const int T = 256, n = 3 * s.natoms;
-  if (n > 0) k_forces_to_double<<<(n + T - 1) / T, T, 0, st>>>(s, out);
+  if (n > 0) k_forces_to_double<<<(n + T - 1) / T, T, 0, st>>>(s, out, base);
   return 0;
 }
 

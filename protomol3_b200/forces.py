@@ -141,7 +141,8 @@ class Topology:
 
     def evaluate_times(self):
         """Host time (ms) of the last host-pointer evaluation: enqueue, wait for the device's
-        first results, accumulation into the caller's arrays."""
+        first results, accumulation into the caller's arrays (a page-locked force array: the
+        wait for the device's sum to land in it)."""
         t = np.zeros(3)
         L.check(L.lib().pmb_system_evaluate_times(self.system(), _p(t)))
         return {"enqueue": t[0], "wait_device": t[1], "accumulate": t[2]}

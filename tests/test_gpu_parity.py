@@ -317,11 +317,49 @@ def test_profile_needs_positions():
 
 
 
+def pinned_array(shape, fill):
+    """A numpy view of page-locked host memory (what a caller gets from cudaMallocHost)."""
+    import torch
+    a = torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    a[...] = fill
+    return a
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_non_finite_position_is_an_error_and_changes_nothing(precision):
+@pytest.mark.parametrize("n_waters", [216, 27000])
+def test_page_locked_force_array_gets_the_same_sum(precision, n_waters):
+    """A page-locked force array is added to on the device and copied back into directly; a
+    pageable one receives the forces in a host staging buffer and is added to on the host.  Both
+    add the same two doubles per component, so the results are equal bit for bit, evaluation
+    after evaluation (the graphed evaluation is replayed), and the energies too."""
+    b = W.water_box(n_waters, seed=11)
+    edge = b["box"][0]
+    grid = W.pme_grid_for(edge)
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0)),
+          F.NonbondedPMEwaldSystemForce((grid,) * 3, 8.0), F.BondedSystemForce()]
+    topo = F.Topology(b, precision)
+    rng = np.random.default_rng(3)
+    pos = b["pos"].copy()
+    for it in range(3):
+        start = rng.normal(size=(topo.n_atoms, 3))
+        fa, fb = start.copy(), pinned_array((topo.n_atoms, 3), start)
+        ea, eb = F.ScalarStructure(1, virial=True), F.ScalarStructure(1, virial=True)
+        F.evaluate_all(topo, fl, pos, fa, ea)
+        F.evaluate_all(topo, fl, pos, fb, eb)
+        assert np.array_equal(fa, fb)
+        assert np.array_equal(ea.table, eb.table)
+        assert not np.array_equal(fa, start)
+        pos = pos + rng.uniform(-0.02, 0.02, pos.shape)
+    topo.close()
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_non_finite_position_is_an_error_and_changes_nothing(precision, pinned):
     """A NaN or infinite position gives PMB_ERR_NUMERIC and leaves the caller's forces and
     energies as they were, whether the list kernels saw it on the device (pair and PME forces) or
-    the host did (bonded terms alone, no list); the next finite evaluation is right again."""
+    the host did (bonded terms alone, no list), and whether the force array is pageable or
+    page-locked (added to on the device); the next finite evaluation is right again."""
     from protomol3_b200 import _lib as L
     b = dict(W.water_box(216, seed=4))
     # off the waters' rest geometry, so that the bonded forces are not zero
@@ -332,7 +370,7 @@ def test_non_finite_position_is_an_error_and_changes_nothing(precision):
         topo = F.Topology(b, precision)
         pos = b["pos"].copy()
         pos[5, 1] = bad
-        frc = np.full((topo.n_atoms, 3), 7.0)
+        frc = pinned_array((topo.n_atoms, 3), 7.0) if pinned else np.full((topo.n_atoms, 3), 7.0)
         e = F.ScalarStructure(1)
         with pytest.raises(L.PMBError) as err:
             F.evaluate_all(topo, forces, pos, frc, e)
