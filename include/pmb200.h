@@ -220,6 +220,14 @@ int pmb_md_get_checkpoint(pmb_md *md, double *positions, double *velocities, dou
  * NULL: zero.  pmb_md_set_state is this call with no list reference and step 0. */
 int pmb_md_set_checkpoint(pmb_md *md, const double *positions, const double *velocities,
                           const double *list_reference, long long step);
+/* Per-box Langevin noise streams.  An atom's noise is keyed by its box's seed, its index within
+ * the box and its box's step count, so a box draws the same numbers alone and beside other boxes.
+ * seeds[n_boxes] (NULL keeps them; a run made with seed s starts box b at s + b) and steps[n_boxes],
+ * each box's own step count at the run's current step (NULL keeps them; by default the run's):
+ * a box restored from another run continues that run's noise.  No counterpart in the reference
+ * (one serial generator per run, base/MathUtilities.cpp:206-238). */
+int pmb_md_set_box_noise(pmb_md *md, const unsigned long long *seeds, const long long *steps);
+int pmb_md_get_box_noise(const pmb_md *md, unsigned long long *seeds, long long *steps);
 /* Writes a checkpoint in the reference's files (OutputCheckpoint::doIt, :58-70): positions to
  * pos_base + id + ".pos" and velocities to vel_base + id + ".vel" as XYZWriter writes them
  * (io/XYZWriter.cpp:28-53; names: one string per atom), then the checkpoint file config_path

@@ -95,6 +95,8 @@ _PROTOS = [
     ("pmb_md_energies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_use_graph", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_time", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("pmb_md_set_box_noise", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pmb_md_get_box_noise", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pmb_md_set_virial", C.c_int, [C.c_void_p, C.c_int]),
     ("pmb_md_set_constraints", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_md_constraint_sweeps", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

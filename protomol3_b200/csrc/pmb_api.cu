@@ -429,6 +429,7 @@ int nblist_alloc(pmb_system *s, double rl) {
     }
   }
   for (int k = 0; k < nblk; k++) jcap_off[k + 1] += jcap_off[k];
+  tiles += (long long)s->nbox * (TILE_CHUNK - 1);  // each box's tiles start at a multiple of TILE_CHUNK
   if (tiles > 0x7fffffffLL || jcap_off[nblk] < 0) return fail(PMB_ERR_CAPACITY, "neighbour list too large");
   nb.tile_cap = (int)tiles;
   int *d_blk_box, *d_jcap;
@@ -447,6 +448,7 @@ int nblist_alloc(pmb_system *s, double rl) {
   nb.jcount = s->nba.get<int>(nblk + 1);
   nb.jlist = s->nba.get<int>((size_t)jcap_off[nblk], false);
   nb.tile_off = s->nba.get<int>(nblk + 1);
+  nb.tile_start = s->nba.get<int>(nblk + 1);
   nb.tile_blk = s->nba.get<int>(nb.tile_cap);
   nb.tile_k = s->nba.get<int>(nb.tile_cap);
   nb.status = s->nba.get<int>(4);
@@ -483,7 +485,20 @@ int nblist_alloc(pmb_system *s, double rl) {
     CK(cudaMemcpy(nb.vext, ext.data(), sizeof(int) * ext.size(), cudaMemcpyHostToDevice));
   }
   nb.half_skin2 = (float)(0.25 * s->skin * s->skin);
-  if (!nb.xref || !nb.ctl || !nb.vext) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
+  nb.nbox = s->nbox;
+  nb.box_d2 = s->nba.get<unsigned>(s->nbox);
+  nb.box_rb = s->nba.get<unsigned>(s->nbox);
+  nb.box_shift = s->nba.get<int>(s->nbox);
+  {
+    std::vector<int> order(s->nbox);
+    for (int b = 0; b < s->nbox; b++) order[b] = b;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return s->hbox[a].blk0 < s->hbox[b].blk0; });
+    int *d_order;
+    if (upload(s->nba, d_order, order)) return PMB_ERR_CUDA;
+    nb.box_order = d_order;
+  }
+  if (!nb.xref || !nb.ctl || !nb.vext || !nb.box_d2 || !nb.box_rb || !nb.box_shift || !nb.tile_start)
+    return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
   // {max displacement, rebuild, finished blocks, forced rebuild, builds (64-bit), pair chunk
   // counter and finished warps of the two pair launches, vacuum extent check}; first use builds
   // the list
@@ -1744,6 +1759,10 @@ struct pmb_md {
   Allocs a;
   double *d_vel = nullptr, *d_kin = nullptr;
   long long *d_step = nullptr;
+  unsigned long long *d_box_seed = nullptr;  // per box noise seed and step offset
+  long long *d_box_step0 = nullptr;
+  std::vector<unsigned long long> h_box_seed;
+  std::vector<long long> h_box_step0;
   bool have_state = false, use_graph = true;
   bool virial = false;  // the steps evaluate the virial (forces and RATTLE's constraint terms)
   long long steps = 0;  // steps since the state was set (a checkpoint's step count)
@@ -1854,7 +1873,11 @@ pmb_md *pmb_md_create(pmb_system *s, pmb_force *const *fs, int n, const pmb_inte
   m->d_vel = m->a.get<double>(3 * (size_t)s->natoms);
   m->d_kin = m->a.get<double>(s->nbox);
   m->d_step = m->a.get<long long>(1);
-  if (!m->d_vel || !m->d_kin || !m->d_step) {
+  m->h_box_seed.resize(s->nbox);
+  m->h_box_step0.assign(s->nbox, 0);
+  for (int b = 0; b < s->nbox; b++) m->h_box_seed[b] = d->seed + (unsigned long long)b;
+  if (!m->d_vel || !m->d_kin || !m->d_step || upload(m->a, m->d_box_seed, m->h_box_seed) ||
+      upload(m->a, m->d_box_step0, m->h_box_step0)) {
     delete m;
     return fail(PMB_ERR_CUDA, "allocation failed"), nullptr;
   }
@@ -1863,6 +1886,8 @@ pmb_md *pmb_md_create(pmb_system *s, pmb_force *const *fs, int n, const pmb_inte
   m->in.gamma = d->gamma_ps / (1000 * INV_TIMEFACTOR);  // LangevinLeapfrogIntegrator.cpp:28
   m->in.kT = BOLTZMANN * d->temperature;
   m->in.seed = d->seed;
+  m->in.box_seed = m->d_box_seed;
+  m->in.box_step0 = m->d_box_step0;
   m->in.mass = s->d_mass;
   m->in.pos = s->d_pos;
   m->in.vel = m->d_vel;
@@ -2118,6 +2143,33 @@ int pmb_md_set_checkpoint(pmb_md *m, const double *pos, const double *vel, const
     return PMB_OK;
   }
   return fail(PMB_ERR_CAPACITY, "neighbour list capacity exceeded");
+}
+
+int pmb_md_set_box_noise(pmb_md *m, const unsigned long long *seeds, const long long *steps) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  pmb_system *s = m->sys;
+  if (steps)
+    for (int b = 0; b < s->nbox; b++)
+      if (steps[b] < 0) return fail(PMB_ERR_ARG, "step count < 0");
+  for (int b = 0; b < s->nbox; b++) {
+    if (seeds) m->h_box_seed[b] = seeds[b];
+    if (steps) m->h_box_step0[b] = steps[b] - m->steps;
+  }
+  CK(cudaMemcpyAsync(m->d_box_seed, m->h_box_seed.data(), sizeof(unsigned long long) * s->nbox,
+                     cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(m->d_box_step0, m->h_box_step0.data(), sizeof(long long) * s->nbox,
+                     cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return PMB_OK;
+}
+
+int pmb_md_get_box_noise(const pmb_md *m, unsigned long long *seeds, long long *steps) {
+  if (!m) return fail(PMB_ERR_ARG, "null md");
+  for (int b = 0; b < m->sys->nbox; b++) {
+    if (seeds) seeds[b] = m->h_box_seed[b];
+    if (steps) steps[b] = m->h_box_step0[b] + m->steps;
+  }
+  return PMB_OK;
 }
 
 int pmb_md_run(pmb_md *m, int n) {

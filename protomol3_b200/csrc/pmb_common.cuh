@@ -29,6 +29,8 @@ constexpr int BLOCK = 8;           // atoms per i-cluster (a lane group; the j-c
 constexpr int GROUPS = 32 / BLOCK; // lane groups per warp
 static_assert(BLOCK == 8 || BLOCK == 16, "i-cluster of 8 or 16 atoms");
 constexpr int JCHUNK = 32;         // j-atoms per tile
+constexpr int TILE_CHUNK = 8;      // consecutive tiles per warp assignment of the pair kernel; each
+                                   // box's tiles start at a multiple of it
 constexpr int JSAME = 1 << 30;     // j-list flag: the j-atom shares a molecule with the i-cluster
 constexpr int MAX_LJ_TYPES = 32;   // LJ table kept in shared memory up to this many types
 
@@ -94,9 +96,10 @@ __device__ inline long long warp_sum_ll(long long v) {
 }
 
 // Adds one energy (slot) and optionally a symmetric virial (xx xy xz yy yz zz) per lane to the
-// per-box accumulators.  When every valid lane of the warp belongs to the same box the warp sums
-// first (one atomic per warp instead of 32 on the same address); the lane-to-term mapping of the
-// callers is fixed, so the grouping and therefore the rounding are reproducible.
+// per-box accumulators.  Every term is rounded to fixed point on its own, so a box's sum does not
+// depend on which terms of other boxes share its warps; when every valid lane of the warp belongs
+// to the same box the warp adds the integers first (one atomic per warp instead of 32 on the
+// same address).
 __device__ inline void box_accumulate(long long *eacc, int box, bool valid, int slot, double e,
                                       const double *vir6) {
   const int lane = threadIdx.x & 31;
@@ -105,29 +108,31 @@ __device__ inline void box_accumulate(long long *eacc, int box, bool valid, int 
   const int b0 = __shfl_sync(0xffffffffu, box, __ffs(act) - 1);
   const bool same = __all_sync(0xffffffffu, !valid || box == b0);
   const int map[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};
+  const long long ev = valid ? f2fix(e, ENERGY_SCALE) : 0;
+  long long vv[6] = {0, 0, 0, 0, 0, 0};
+  if (vir6 && valid)
+    for (int c = 0; c < 6; c++) vv[c] = f2fix(vir6[c], ENERGY_SCALE);
   if (same) {
-    double es = warp_sum(valid ? e : 0.0);
-    double vs[6];
+    const long long es = warp_sum_ll(ev);
+    long long vs[6];
     if (vir6)
-      for (int c = 0; c < 6; c++) vs[c] = warp_sum(valid ? vir6[c] : 0.0);
+      for (int c = 0; c < 6; c++) vs[c] = warp_sum_ll(vv[c]);
     if (lane == 0) {
       long long *acc = eacc + (long long)b0 * ACC_PER_BOX;
-      red_add(acc + slot, f2fix(es, ENERGY_SCALE));
+      red_add(acc + slot, es);
       if (vir6)
         for (int c = 0; c < 6; c++) {
-          long long v = f2fix(vs[c], ENERGY_SCALE);
-          red_add(acc + E_VIR + map[c][0], v);
-          if (map[c][1] != map[c][0]) red_add(acc + E_VIR + map[c][1], v);
+          red_add(acc + E_VIR + map[c][0], vs[c]);
+          if (map[c][1] != map[c][0]) red_add(acc + E_VIR + map[c][1], vs[c]);
         }
     }
   } else if (valid) {
     long long *acc = eacc + (long long)box * ACC_PER_BOX;
-    red_add(acc + slot, f2fix(e, ENERGY_SCALE));
+    red_add(acc + slot, ev);
     if (vir6)
       for (int c = 0; c < 6; c++) {
-        long long v = f2fix(vir6[c], ENERGY_SCALE);
-        red_add(acc + E_VIR + map[c][0], v);
-        if (map[c][1] != map[c][0]) red_add(acc + E_VIR + map[c][1], v);
+        red_add(acc + E_VIR + map[c][0], vv[c]);
+        if (map[c][1] != map[c][0]) red_add(acc + E_VIR + map[c][1], vv[c]);
       }
   }
 }

@@ -40,7 +40,10 @@ struct NbListDev {
   int *jcount;                 // [nblk] tiles per block (its j-list, own slots first, in 32s)
   int *jlist;                  // [jcap_off[nblk]] j slots (-1 padding), JSAME flag bit
   int *tile_off;               // [nblk+1] exclusive scan of jcount
-  int *tile_blk;               // [tile_cap] block of each tile
+  int *tile_start;             // [nblk+1] first tile of each block: tile_off moved on so that
+                               // each box's tiles start at a multiple of TILE_CHUNK (a box's
+                               // last block is followed by up to TILE_CHUNK - 1 empty tiles)
+  int *tile_blk;               // [tile_cap] block of each tile (-1: empty)
   int *tile_k;                 // [tile_cap] tile index within the block
   int tile_cap;
   int *status;                 // [4]: list / tile overflow, non-finite position, vacuum extent
@@ -68,6 +71,13 @@ struct NbListDev {
                                // force flag, list builds (64-bit counter in [4..5]), the pair
                                // kernel's next chunk and finished warps ([6], [7]; zero between launches)
   float half_skin2;
+  // per box: rebuilds are decided box by box (a box's list, slot order and therefore its
+  // rounding do not depend on the other boxes of the system); ctl[1] says whether any box rebuilds
+  int nbox;
+  unsigned *box_d2;            // [nbox] max displacement^2 since the box's last build (float bits)
+  unsigned *box_rb;            // [nbox] 1: the box rebuilds this step
+  const int *box_order;        // [nbox] the boxes in ascending order of their first block
+  int *box_shift;              // [nbox] tiles of padding before the box's first tile
   int *vext;                   // [6 nbox] vacuum extent per box: smallest and largest x, y, z as
                                // order-preserving int images of their float values (ctl[10] on)
 };
@@ -179,6 +189,11 @@ struct IntegratorDev {
   double h;            // dt * INV_TIMEFACTOR
   double gamma, kT;    // Langevin (internal units)
   unsigned long long seed;
+  // per box: the noise seed and the offset of the box's step count from the run's (a box that
+  // joined the run part-way); an atom's noise is keyed by its box's seed, its index within the
+  // box and its box's step, so a box draws the same numbers alone and beside other boxes
+  const unsigned long long *box_seed;  // [nbox]
+  const long long *box_step0;          // [nbox]
   const double *mass;  // [natoms]
   double *pos, *vel;
   long long *step;     // device step counter

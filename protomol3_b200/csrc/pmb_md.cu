@@ -6,8 +6,9 @@
 //   (integrator/leapfrog/LeapfrogIntegrator.cpp:33-104) with h = dt * INV_TIMEFACTOR.
 // Langevin: LangevinLeapfrogIntegrator::doHalfKick (integrator/base/LangevinLeapfrogIntegrator.cpp:44-71);
 //   the reference's serial Park-Miller generator cannot be reproduced on a GPU, so the Gaussian
-//   noise comes from a counter-based generator keyed by (seed, atom, step, component): every
-//   trajectory is reproducible bit for bit and independent of how systems are batched.
+//   noise comes from a counter-based generator keyed by (the box's seed, the atom's index within
+//   its box, the box's step, component): every trajectory is reproducible bit for bit and
+//   independent of how boxes are batched.
 #include "pmb_internal.h"
 
 namespace pmb {
@@ -159,14 +160,15 @@ __global__ void k_kick_drift(const SystemDev s, IntegratorDev in, double kick) {
     // kick, drift, forces, noisy half kick.  The half kick closing step s-1 (noise stream 2s-1)
     // is applied here together with the opening half kick of step s (stream 2s); run() ends
     // with k_half_kick closing the last step.
-    const long long step = *in.step;
+    const int b = s.atom_box[i], ia = i - s.box[b].atom0;
+    const long long step = *in.step + in.box_step0[b];
     const double g = in.gamma;
     const double fdt = (1.0 - exp(-0.5 * g * h)) / g, vdt = exp(-0.5 * g * h);
     const double ndt = sqrt((1.0 - exp(-g * h)) / (2.0 * g));
     const double sq = sqrt(2.0 * in.kT * g / m);
     double ra[3], rb[3];
-    gauss3(in.seed, i, 2 * step, ra);
-    if (kick == 1.0) gauss3(in.seed, i, 2 * step - 1, rb);
+    gauss3(in.box_seed[b], ia, 2 * step, ra);
+    if (kick == 1.0) gauss3(in.box_seed[b], ia, 2 * step - 1, rb);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       double f = (double)fa[c] * (1.0 / FORCE_SCALE);
@@ -187,13 +189,14 @@ __global__ void k_half_kick(const SystemDev s, IntegratorDev in) {
   if (in.kind == 0) {
     for (int c = 0; c < 3; c++) v[c] += ((double)fa[c] * (1.0 / FORCE_SCALE)) * h * 0.5 / m;
   } else {
-    const long long step = *in.step;
+    const int b = s.atom_box[i], ia = i - s.box[b].atom0;
+    const long long step = *in.step + in.box_step0[b];
     const double g = in.gamma;
     const double fdt = (1.0 - exp(-0.5 * g * h)) / g, vdt = exp(-0.5 * g * h);
     const double ndt = sqrt((1.0 - exp(-g * h)) / (2.0 * g));
     const double sq = sqrt(2.0 * in.kT * g / m);
     double rp[3];
-    gauss3(in.seed, i, 2 * step - 1, rp);  // closes the last completed step
+    gauss3(in.box_seed[b], ia, 2 * step - 1, rp);  // closes the last completed step
     for (int c = 0; c < 3; c++)
       v[c] = v[c] * vdt + ((double)fa[c] * (1.0 / FORCE_SCALE)) * fdt / m + rp[c] * sq * ndt;
   }

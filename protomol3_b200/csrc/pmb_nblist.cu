@@ -138,8 +138,9 @@ __global__ void k_scan_apply(const int *in, int n, const int *chunk, int *out, c
 }
 
 // ---------------------------------------------------------------- binning and sort
-// Rebuild decision: max |x - x_ref|^2 over all atoms (last block decides, no host round trip);
-// ctl = {max displacement^2 as float bits, rebuild flag, finished blocks, forced rebuild}.
+// Rebuild decision, box by box: max |x - x_ref|^2 over each box's atoms (box_d2), then the last
+// block sets box_rb[b] for every box that moved more than half the skin and ctl[1] when any did
+// (no host round trip); ctl = {-, any box rebuilds, finished blocks, forced rebuild of all}.
 // It reads every position of every evaluation, so it also raises status[2] for a non-finite
 // one (the host reports PMB_ERR_NUMERIC; every later kernel maps such a position to an in-range
 // cell and grid index, so nothing reads out of bounds meanwhile), and, for a system whose boxes
@@ -154,8 +155,10 @@ __device__ __forceinline__ float fuord(int o) { return __int_as_float(o >= 0 ? o
 __global__ void k_disp_check(SystemDev s, NbListDev nb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   float d2 = 0.f;
+  int box = -1;
   const bool vacuum = nb.ctl[10] != 0u;
   if (i < s.natoms) {
+    box = s.atom_box[i];
     const double x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
     if (!(isfinite(x) && isfinite(y) && isfinite(z))) atomicExch(&nb.status[2], 1);
     if (vacuum) {
@@ -174,35 +177,70 @@ __global__ void k_disp_check(SystemDev s, NbListDev nb) {
     d2 = r2 < 3.0e38 ? (float)r2 : 3.0e38f;
     if (!(d2 >= 0.f)) d2 = 3.0e38f;  // NaN positions force a rebuild
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+  // per-box maxima (float bits of non-negative values order as unsigned): a warp whose atoms
+  // belong to one box takes its maximum first, and the block adds one atomic per run of such
+  // warps of the same box
+  __shared__ int wbox[32];
   __shared__ float wmax[32];
-  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned act = __ballot_sync(0xffffffffu, box >= 0);
+  int wb = -1;  // the warp's box when all its atoms share one, else -1 (atomics already added)
+  float m = 0.f;
+  if (act) {
+    const int b0 = __shfl_sync(0xffffffffu, box, __ffs(act) - 1);
+    if (__all_sync(0xffffffffu, box < 0 || box == b0)) {
+      m = d2;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      wb = b0;
+    } else if (box >= 0) {
+      atomicMax(&nb.box_d2[box], __float_as_uint(d2));
+    }
+  }
+  if (lane == 0) {
+    wbox[w] = wb;
+    wmax[w] = m;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    float m = 0.f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wmax[w]);
-    atomicMax(&nb.ctl[0], __float_as_uint(m));
-    __threadfence();
-    unsigned done = atomicAdd(&nb.ctl[2], 1u);
-    if (done == gridDim.x - 1) {
-      __threadfence();
-      if (vacuum)
-        for (int b = 0; b < s.nbox; b++)
-          for (int d = 0; d < 3; d++) {
-            // read and reset for the next evaluation
-            const float lo = fuord(atomicExch(nb.vext + 6 * b + d, 0x7fffffff));
-            const float hi = fuord(atomicExch(nb.vext + 6 * b + 3 + d, (int)0x80000000));
-            if (!((double)hi - (double)lo < 0.5 * s.box[b].L[d])) atomicExch(&nb.status[3], 1);
-          }
-      float mx = __uint_as_float(atomicAdd(&nb.ctl[0], 0u));
-      const unsigned rebuild = (nb.ctl[3] != 0u || mx > nb.half_skin2) ? 1u : 0u;
-      nb.ctl[1] = rebuild;
-      if (rebuild) ++*reinterpret_cast<unsigned long long *>(nb.ctl + 4);
-      nb.ctl[0] = 0u;
-      nb.ctl[2] = 0u;
-      nb.ctl[3] = 0u;
+    const int nw = (int)(blockDim.x >> 5);
+    for (int k = 0; k < nw;) {
+      const int b = wbox[k];
+      float mm = wmax[k];
+      int k2 = k + 1;
+      for (; k2 < nw && wbox[k2] == b; k2++) mm = fmaxf(mm, wmax[k2]);
+      if (b >= 0) atomicMax(&nb.box_d2[b], __float_as_uint(mm));
+      k = k2;
     }
+  }
+  __threadfence();
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x == 0) last = atomicAdd(&nb.ctl[2], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const bool forced = nb.ctl[3] != 0u;
+  int any = 0;
+  for (int b = threadIdx.x; b < s.nbox; b += blockDim.x) {
+    const float mx = __uint_as_float(atomicExch(&nb.box_d2[b], 0u));  // read and reset
+    const unsigned rb = (forced || mx > nb.half_skin2) ? 1u : 0u;
+    nb.box_rb[b] = rb;
+    any |= (int)rb;
+    if (vacuum)
+      for (int d = 0; d < 3; d++) {
+        // read and reset for the next evaluation
+        const float lo = fuord(atomicExch(nb.vext + 6 * b + d, 0x7fffffff));
+        const float hi = fuord(atomicExch(nb.vext + 6 * b + 3 + d, (int)0x80000000));
+        if (!((double)hi - (double)lo < 0.5 * s.box[b].L[d])) atomicExch(&nb.status[3], 1);
+      }
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    nb.ctl[1] = any ? 1u : 0u;
+    if (any) ++*reinterpret_cast<unsigned long long *>(nb.ctl + 4);
+    nb.ctl[2] = 0u;
+    nb.ctl[3] = 0u;
   }
 }
 
@@ -212,11 +250,13 @@ __global__ void k_zero_bins(int *bin_count, int n, const unsigned *go) {
   if (i <= n) bin_count[i] = 0;
 }
 
-__global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count, const unsigned *go) {
+__global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count, const unsigned *go, const unsigned *rb) {
   if (!go[1]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.natoms) return;
-  const BoxDev &b = s.box[s.atom_box[i]];
+  const int bi = s.atom_box[i];
+  if (!rb[bi]) return;  // the box keeps its slots
+  const BoxDev &b = s.box[bi];
   unsigned c[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -229,11 +269,13 @@ __global__ void k_bin(SystemDev s, int *key, int *rank, int *bin_count, const un
 }
 
 __global__ void k_scatter(SystemDev s, const int *key, const int *rank, const int *bin_start,
-                          int *slot_orig, const unsigned *go) {
+                          int *slot_orig, const unsigned *go, const unsigned *rb) {
   if (!go[1]) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.natoms) return;
-  const BoxDev &b = s.box[s.atom_box[i]];
+  const int bi = s.atom_box[i];
+  if (!rb[bi]) return;
+  const BoxDev &b = s.box[bi];
   int base = b.blk0 * BLOCK - bin_start[b.key0];
   slot_orig[base + bin_start[key[i]] + rank[i]] = i;
 }
@@ -271,7 +313,7 @@ __global__ void k_pack(SystemDev s, NbListDev nb, int want_fp64) {
   int bi = s.atom_box[o];
   const BoxDev &b = s.box[bi];
   double x = s.pos[3 * o], y = s.pos[3 * o + 1], z = s.pos[3 * o + 2], q = s.charge[o];
-  if (nb.ctl[1]) {  // list rebuilt this step: new reference positions
+  if (nb.ctl[1] && nb.box_rb[bi]) {  // the box's list is rebuilt this step: new reference positions
     nb.xref[3 * o] = x;
     nb.xref[3 * o + 1] = y;
     nb.xref[3 * o + 2] = z;
@@ -302,7 +344,7 @@ __global__ void k_block_bbox(NbListDev nb) {
     }
   unsigned bal = __ballot_sync(0xffffffffu, valid);
   int cnt = __popc(bal & (((1u << BLOCK) - 1u) << (lane & ~(BLOCK - 1))));
-  if (inr && (lane & (BLOCK - 1)) == 0) {
+  if (inr && (lane & (BLOCK - 1)) == 0 && nb.box_rb[nb.blk_box[blk]]) {
     if (cnt == 0) lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
     nb.blk_lo[blk] = make_uint4(lo[0], lo[1], lo[2], (unsigned)cnt);
     nb.blk_hi[blk] = make_uint4(hi[0], hi[1], hi[2], 0u);
@@ -377,6 +419,7 @@ __global__ void __launch_bounds__(BL_THREADS, 4) k_build_lists(SystemDev s, NbLi
   if (I >= nb.nblk_total) return;
   int *cl = cand_all[threadIdx.x >> 5];
   const int bi = nb.blk_box[I];
+  if (!nb.box_rb[bi]) return;  // the box keeps its list
   const BoxDev &b = s.box[bi];
   const uint4 cIv = nb.blk_c[I], hIv = nb.blk_h[I];
   if (cIv.w == 0) {
@@ -546,18 +589,52 @@ __global__ void __launch_bounds__(BL_THREADS, 4) k_build_lists(SystemDev s, NbLi
   }
 }
 
-// One warp per block: its tiles' (block, index) entries, written by consecutive lanes.
-__global__ void k_tile_map(NbListDev nb) {
+// Padding that starts every box's tiles at a multiple of TILE_CHUNK (one block of threads, the
+// boxes in the order of their blocks): the pair kernel's warp assignments then never mix boxes,
+// and a box's partial sums are grouped as when it is alone.
+__global__ void k_box_pad(SystemDev s, NbListDev nb) {
+  if (!nb.ctl[1]) return;
+  const int per = (nb.nbox + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int k0 = min(nb.nbox, (int)threadIdx.x * per), k1 = min(nb.nbox, k0 + per);
+  auto pad = [&](int b) {
+    const BoxDev &bx = s.box[b];
+    const int tot = nb.tile_off[bx.blk0 + bx.nblk] - nb.tile_off[bx.blk0];
+    return (TILE_CHUNK - tot % TILE_CHUNK) % TILE_CHUNK;
+  };
+  int acc = 0;
+  for (int k = k0; k < k1; k++) acc += pad(nb.box_order[k]);
+  int tot;
+  int ex = block_exclusive_scan(acc, &tot);
+  for (int k = k0; k < k1; k++) {
+    const int b = nb.box_order[k];
+    nb.box_shift[b] = ex;
+    ex += pad(b);
+  }
+  if (threadIdx.x == 0) nb.tile_start[nb.nblk_total] = nb.tile_off[nb.nblk_total] + tot;
+}
+
+// One warp per block: its first tile and its tiles' (block, index) entries, written by
+// consecutive lanes; a box's last block also writes the box's empty padding tiles.
+__global__ void k_tile_map(SystemDev s, NbListDev nb) {
   if (!nb.ctl[1]) return;
   const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (I >= nb.nblk_total) return;
-  const int off = nb.tile_off[I], cnt = nb.jcount[I];
-  if (off + cnt > nb.tile_cap) {
+  const int b = nb.blk_box[I];
+  const BoxDev &bx = s.box[b];
+  const int shift = nb.box_shift[b];
+  const int off = nb.tile_off[I] + shift, cnt = nb.jcount[I];
+  int end = off + cnt;
+  if (I == bx.blk0 + bx.nblk - 1) {
+    const int start = nb.tile_off[bx.blk0] + shift;
+    end = start + (end - start + TILE_CHUNK - 1) / TILE_CHUNK * TILE_CHUNK;
+  }
+  if (lane == 0) nb.tile_start[I] = off;
+  if (end > nb.tile_cap) {
     if (lane == 0) atomicExch(&nb.status[1], 1);
     return;
   }
-  for (int k = lane; k < cnt; k += 32) {
-    nb.tile_blk[off + k] = I;
+  for (int k = lane; k < end - off; k += 32) {
+    nb.tile_blk[off + k] = k < cnt ? I : -1;
     nb.tile_k[off + k] = k;
   }
 }
@@ -583,9 +660,9 @@ int nblist_sort(const SystemDev &s, NbListDev &nb, cudaStream_t st) {
   // (inside a CUDA graph such a launch costs about a microsecond)
   k_disp_check<<<(na + T - 1) / T, T, 0, st>>>(s, nb);
   k_zero_bins<<<(nb.nkeys + T) / T, T, 0, st>>>(nb.bin_count, nb.nkeys, nb.ctl);
-  k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count, nb.ctl);
+  k_bin<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_count, nb.ctl, nb.box_rb);
   scan_exclusive(nb.bin_count, nb.bin_start, nb.nkeys, nb.scan_tmp, st, nb.ctl);
-  k_scatter<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_start, nb.slot_orig, nb.ctl);
+  k_scatter<<<(na + T - 1) / T, T, 0, st>>>(s, nb.key, nb.rank, nb.bin_start, nb.slot_orig, nb.ctl, nb.box_rb);
   k_sort_bins<<<(nb.nkeys + T - 1) / T, T, 0, st>>>(s, nb.bin_box, nb.bin_start, nb.bin_count,
                                                    nb.nkeys, nb.slot_orig, nb.ctl);
   k_pack<<<(nb.nslot + T - 1) / T, T, 0, st>>>(s, nb, nb.want_fp64);
@@ -601,7 +678,8 @@ int nblist_lists(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   k_superblock_bbox<<<(nb.nsblk * 32 + T - 1) / T, T, 0, st>>>(nb);
   k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
   scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st, nb.ctl);
-  k_tile_map<<<(wthreads + T - 1) / T, T, 0, st>>>(nb);
+  k_box_pad<<<1, 1024, 0, st>>>(s, nb);
+  k_tile_map<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb);
   return 0;
 }
 

@@ -42,7 +42,7 @@ namespace {
 
 constexpr int PAIR_THREADS = 256;
 constexpr int PAIR_WARPS = PAIR_THREADS / 32;
-constexpr int CHUNK = 8;  // consecutive tiles per warp assignment
+constexpr int CHUNK = TILE_CHUNK;  // consecutive tiles per warp assignment
 
 // switch / potential selectors (template parameters)
 constexpr int SWR = -1;   // read the switching function kind at run time
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR
   int2 *qt = reinterpret_cast<int2 *>(reinterpret_cast<float4 *>(wstage) + 2 * FAST_ENTRIES) + qe;
   const int gwarp = blockIdx.x * PAIR_WARPS + wib, nwarps = gridDim.x * PAIR_WARPS;
   // this launch's tiles: those of blocks [blk_lo, blk_hi)
-  int t_lo = nb.tile_off[blk_lo], t_hi = nb.tile_off[blk_hi];
+  int t_lo = nb.tile_start[blk_lo], t_hi = nb.tile_start[blk_hi];
   if (t_hi > nb.tile_cap) t_hi = nb.tile_cap;
   if (t_lo > t_hi) t_lo = t_hi;
 

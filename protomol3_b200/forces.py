@@ -441,6 +441,23 @@ class Integrator:
         L.check(L.lib().pmb_md_set_checkpoint(self._h, _p(pos), _p(vel), _p(ref) if ref is not None else None,
                                               int(ckpt.get("step", 0))))
 
+    def set_box_noise(self, seeds=None, steps=None):
+        """Per-box Langevin noise streams: ``seeds[b]`` and ``steps[b]``, box b's own step count
+        at this moment (None keeps them).  A box's noise depends only on its seed, the atom's
+        index within the box and its step count, so a box moved into this run from another
+        continues that run's noise."""
+        nb = self.topo.n_boxes
+        sd = None if seeds is None else np.ascontiguousarray(seeds, np.uint64).reshape(nb)
+        st = None if steps is None else np.ascontiguousarray(steps, np.int64).reshape(nb)
+        L.check(L.lib().pmb_md_set_box_noise(self._h, _p(sd), _p(st)))
+
+    def box_noise(self):
+        """(seeds, steps) of every box's noise stream."""
+        nb = self.topo.n_boxes
+        sd, st = np.zeros(nb, np.uint64), np.zeros(nb, np.int64)
+        L.check(L.lib().pmb_md_get_box_noise(self._h, _p(sd), _p(st)))
+        return sd, st
+
     def write_checkpoint(self, config_path, ident, pos_base, vel_base, names, first_step=0):
         """The reference's checkpoint files (OutputCheckpoint): pos_base<id>.pos and
         vel_base<id>.vel in XYZ form and the checkpoint file ``config_path``."""

@@ -143,29 +143,6 @@ def test_mixed_bit_reproducible():
         assert np.array_equal(et, outs[0][1])
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batched_boxes_match_single(precision):
-    boxes = [W.water_box(n, seed=30 + n) for n in (100, 257, 640)]
-    grids = [W.pme_grid_for(b["box"][0]) for b in boxes]
-
-    def forces(bg):
-        return [F.NonbondedCutoffSystemForce(lj=("C2", 7.5, 9.0)),
-                F.NonbondedPMEwaldSystemForce((0, 0, 0), 9.0, box_grids=bg), F.BondedSystemForce()]
-    fb, eb, _ = gpu_eval(boxes, forces([[g] * 3 for g in grids]), precision)
-    off = 0
-    for k, (b, g) in enumerate(zip(boxes, grids)):
-        fs, es, _ = gpu_eval(b, forces([[g] * 3]), precision)
-        n = len(b["charge"])
-        # the same box alone and inside the batch: equal within the precision's tolerance (the
-        # partial sums of a batch close at other tile boundaries, and a box smaller than twice the
-        # cutoff runs on the lattice-image kernel instance, whose compiled arithmetic may round
-        # differently)
-        assert rel_rms(fb[off:off + n], fs) < TOL[precision] * 0.1
-        np.testing.assert_allclose(eb.table[k, :4], es.table[0, :4], rtol=TOL[precision],
-                                   atol=n * 2.0 ** -30)
-        off += n
-
-
 def test_leapfrog_golden_trajectory_fp64():
     """200 leapfrog steps of water_CHARMM_PERIODIC_L on the device vs the reference's output."""
     d = dict(np.load(os.path.join(GOLD, "water423_periodic.npz")))
