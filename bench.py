@@ -756,7 +756,9 @@ def serve_leg(n_requests=24, loads=(0.5, 0.8, 0.95), budget_gb=32.0, max_active=
     atoms, 1,000-20,000 steps, 300 K, gamma 1/ps, 1 fs, LJ C2 7.5 -> 9 A, PME at ~1 A spacing,
     mixed precision).  Capacity is measured first with every request of the trace present at
     t = 0; then the same request mix is offered at each fraction of that capacity.  Latency is
-    arrival to completion (wall clock, includes admission wait); p50/p99 per load."""
+    arrival to completion (wall clock, includes admission wait); p50/p99 per load.  The server
+    folds resident segments of one size class into batched systems (FoldingServer); the capacity
+    of one system per segment (MDServer) is reported beside it."""
     from protomol3_b200 import serving as S
     from protomol3_b200 import waterbox as W
 
@@ -765,19 +767,24 @@ def serve_leg(n_requests=24, loads=(0.5, 0.8, 0.95), budget_gb=32.0, max_active=
         return [S.SegmentRequest(k, W.water_box(w, seed=seed + k), st, seed=sd, arrival=a)
                 for k, (a, w, st, sd) in enumerate(tr)]
 
-    def serve(reqs, precision="mixed"):
-        srv = S.MDServer(hbm_budget_bytes=int(budget_gb * (1 << 30)), max_active=max_active, chunk=chunk,
-                         precision=precision)
+    def serve(reqs, precision="mixed", fold=True):
+        kind = S.FoldingServer if fold else S.MDServer
+        srv = kind(hbm_budget_bytes=int(budget_gb * (1 << 30)), max_active=max_active, chunk=chunk,
+                   precision=precision)
         res = srv.run_trace(reqs)
         out = S.latency_summary(res)
-        out.update(peak_active=srv.peak_active, peak_device_gb=srv.peak_used / (1 << 30))
+        out.update(peak_active=srv.peak_active, peak_booked_gb=srv.peak_used / (1 << 30))
+        if fold:
+            out.update(cohorts_made=srv.cohorts_made, peak_cohorts=srv.peak_cohorts,
+                       peak_device_gb=srv.peak_device / (1 << 30))
         return out
 
     # warm-up: module load, first graph captures
     S.MDServer(max_active=2, chunk=chunk).run_trace(requests(0.0)[:2])
+    S.FoldingServer(max_active=2, chunk=chunk).run_trace(requests(0.0)[:2])
     cap = serve(requests(0.0))
     capacity = cap["throughput_req_s"]
-    legs = {"capacity": cap}
+    legs = {"capacity": cap, "capacity_one_system_per_segment": serve(requests(0.0), fold=False)}
     for f in loads:
         legs["load_%02d" % round(100 * f)] = dict(serve(requests(f * capacity)), offered_req_s=f * capacity)
     # the plain FP64 path serving the same request mix, all present at t = 0
@@ -787,7 +794,7 @@ def serve_leg(n_requests=24, loads=(0.5, 0.8, 0.95), budget_gb=32.0, max_active=
             "requests_per_load": n_requests, "capacity_req_s": capacity, "loads": legs,
             "plain_fp64_capacity": cap64, "capacity_over_fp64": capacity / cap64["throughput_req_s"],
             "hbm_budget_gb": budget_gb, "max_active": max_active, "chunk_steps": chunk,
-            "precision": "mixed"}
+            "precision": "mixed", "server": "FoldingServer (size classes < 2,000 / 8,000 / 20,000 atoms)"}
 
 
 def run_profile(args):

@@ -138,6 +138,14 @@ __device__ __forceinline__ void gauss3(unsigned long long seed, int atom, long l
   g[2] = r2 * cc2;
 }
 
+// One noisy half kick of LangevinLeapfrogIntegrator::doHalfKick (LangevinLeapfrogIntegrator.cpp:
+// 66-68): v vdt + (F fdt) / m + (r sq) ndt, every operation rounded on its own (no contraction),
+// so that the kick closing a step gives the same bits wherever a run is split into calls.
+__device__ __forceinline__ double langevin_half_kick(double v, double f, double r, double vdt, double fdt,
+                                                     double m, double sq, double ndt) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(v, vdt), __ddiv_rn(__dmul_rn(f, fdt), m)), __dmul_rn(__dmul_rn(r, sq), ndt));
+}
+
 // Leapfrog kick (coefficient 1 or 1/2) + drift; the force accumulator is consumed and cleared.
 __global__ void k_kick_drift(const SystemDev s, IntegratorDev in, double kick) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -173,8 +181,8 @@ __global__ void k_kick_drift(const SystemDev s, IntegratorDev in, double kick) {
     for (int c = 0; c < 3; c++) {
       double f = (double)fa[c] * (1.0 / FORCE_SCALE);
       fa[c] = 0;
-      if (kick == 1.0) v[c] = v[c] * vdt + f * fdt / m + rb[c] * sq * ndt;
-      v[c] = v[c] * vdt + f * fdt / m + ra[c] * sq * ndt;
+      if (kick == 1.0) v[c] = langevin_half_kick(v[c], f, rb[c], vdt, fdt, m, sq, ndt);
+      v[c] = langevin_half_kick(v[c], f, ra[c], vdt, fdt, m, sq, ndt);
       x[c] = __dadd_rn(x[c], __dmul_rn(v[c], h));
     }
   }
@@ -198,7 +206,7 @@ __global__ void k_half_kick(const SystemDev s, IntegratorDev in) {
     double rp[3];
     gauss3(in.box_seed[b], ia, 2 * step - 1, rp);  // closes the last completed step
     for (int c = 0; c < 3; c++)
-      v[c] = v[c] * vdt + ((double)fa[c] * (1.0 / FORCE_SCALE)) * fdt / m + rp[c] * sq * ndt;
+      v[c] = langevin_half_kick(v[c], (double)fa[c] * (1.0 / FORCE_SCALE), rp[c], vdt, fdt, m, sq, ndt);
   }
 }
 

@@ -16,6 +16,15 @@ of (seed, atom, step), so a segment run alone and in the mix gives bit-identical
 
 The GPU work goes through ``GpuSegment`` (the C ABI of libpmb200 via forces.py, PyTorch streams
 and events); the scheduler only needs its small interface, which the CPU tests replace by a fake.
+
+``FoldingServer`` folds resident segments of similar size into one batched system (a cohort: one
+box per segment, one launch per force stage and one CUDA graph per step for all of them).  A
+batched system gives every box the bits it gets alone (list rebuilds are decided per box, pair
+tiles never mix boxes, energies are summed in fixed point term by term, the Langevin noise is
+keyed by the box's seed, its atom index within the box and its own step count), and a box moves
+between batched systems exactly (checkpoint with the list's reference positions, restored with
+its noise stream), so a cohort is re-formed whenever one of its segments completes, together with
+the segments admitted since, and every result is still the one the segment gets alone.
 """
 import collections
 import time
@@ -155,13 +164,16 @@ class MDServer:
             progressed = True
         return progressed
 
+    def _busy(self):
+        return bool(self.pending or self.active)
+
     def run_trace(self, requests, idle_sleep=2e-4):
         """Serves requests whose ``arrival`` times are offsets from now; returns the results in
         completion order."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         self.t0 = self.clock()
         i = 0
-        while i < len(reqs) or self.pending or self.active:
+        while i < len(reqs) or self._busy():
             t = self.now()
             while i < len(reqs) and reqs[i].arrival <= t:
                 self.submit(reqs[i])
@@ -170,6 +182,187 @@ class MDServer:
             if not self._advance():
                 time.sleep(idle_sleep)
         return self.results
+
+
+class Member:
+    """A segment inside a folding server: its request, the steps done, the admission time, the
+    bytes booked for it and, between two cohorts, its exact state (positions, velocities and the
+    neighbour list's reference positions)."""
+
+    def __init__(self, req, booked, t_admit):
+        self.req = req
+        self.booked = booked
+        self.t_admit = t_admit
+        self.done_steps = 0
+        self.state = None
+
+    def left(self):
+        return self.req.steps - self.done_steps
+
+
+class GpuCohort:
+    """Segments advanced together as one batched system (one box each) on one CUDA stream."""
+
+    def __init__(self, members, precision="mixed", rc=9.0, switchon=7.5, temperature=300.0,
+                 gamma=1.0, timestep=1.0):
+        import torch
+        from . import forces as F
+        self.torch = torch
+        self.members = list(members)
+        boxes = [m.req.box for m in self.members]
+        self.stream = torch.cuda.Stream()
+        self.topo = F.Topology(boxes, precision)
+        self.topo.set_stream(self.stream.cuda_stream)
+        self.fl = [F.BondedSystemForce(), F.NonbondedCutoffSystemForce(lj=("C2", switchon, rc)),
+                   F.NonbondedPMEwaldSystemForce((0, 0, 0), rc,
+                                                 box_grids=[[m.req.grid] * 3 for m in self.members])]
+        self.md = F.Integrator(self.topo, self.fl, timestep=timestep, kind="langevin",
+                               temperature=temperature, gamma=gamma, seed=self.members[0].req.seed)
+        pos = np.concatenate([m.state[0] if m.state else m.req.box["pos"] for m in self.members])
+        vel = np.concatenate([m.state[1] if m.state else m.req.box["vel"] for m in self.members])
+        if any(m.state for m in self.members):
+            ref = np.concatenate([m.state[2] if m.state else m.req.box["pos"] for m in self.members])
+            self.md.restore({"positions": pos, "velocities": vel, "list_reference": ref, "step": 0})
+        else:
+            self.md.set_state(pos, vel)
+        self.md.set_box_noise(seeds=[m.req.seed for m in self.members],
+                              steps=[m.done_steps for m in self.members])
+        self.bytes = self.md.device_bytes()
+        self.event = None
+
+    def idle(self):
+        return self.event is None or self.event.query()
+
+    def left(self):
+        return min(m.left() for m in self.members)
+
+    def enqueue(self, n):
+        self.md.run(n)
+        for m in self.members:
+            m.done_steps += n
+        self.event = self.torch.cuda.Event()
+        self.event.record(self.stream)
+
+    def split(self):
+        """Ends the cohort: [(member, pos, vel, energies, kinetic)] of the completed segments and
+        the others, each holding its exact state."""
+        ck = self.md.checkpoint()
+        e, k = self.md.energies()
+        self.md.close()
+        self.topo.close()
+        done, cont = [], []
+        off = 0
+        for b, m in enumerate(self.members):
+            n = m.req.n_atoms
+            sl = slice(off, off + n)
+            off += n
+            if m.left() == 0:
+                done.append((m, ck["positions"][sl].copy(), ck["velocities"][sl].copy(), e[b].copy(), float(k[b])))
+            else:
+                m.state = (ck["positions"][sl].copy(), ck["velocities"][sl].copy(), ck["list_reference"][sl].copy())
+                cont.append(m)
+        return done, cont
+
+
+def size_class(n_atoms, bounds=(2000, 8000, 20000)):
+    """Index of the first bound above n_atoms (len(bounds) for the largest segments)."""
+    for k, b in enumerate(bounds):
+        if n_atoms < b:
+            return k
+    return len(bounds)
+
+
+class FoldingServer(MDServer):
+    """MDServer whose resident segments of one size class run as one batched system.
+
+    Admission is FIFO by HBM budget (each request books its estimate) and slot count, as in
+    MDServer.  Admitted segments, and the unfinished segments of a cohort whose shortest segment
+    has completed, are grouped by size class (``class_bounds`` atoms; segments at or above the
+    last bound run one per system) into new cohorts of at most ``max_cohort_atoms`` atoms.  Each
+    idle cohort advances by min(chunk, its shortest segment's remaining steps)."""
+
+    def __init__(self, hbm_budget_bytes=16 << 30, max_active=32, chunk=200, cohort_factory=None,
+                 class_bounds=(2000, 8000, 20000), max_cohort_atoms=200000, clock=time.perf_counter,
+                 **segment_kw):
+        super().__init__(hbm_budget_bytes, max_active, chunk, clock=clock, **segment_kw)
+        self.factory = cohort_factory or (lambda members: GpuCohort(members, **segment_kw))
+        self.class_bounds = tuple(class_bounds)
+        self.max_cohort_atoms = int(max_cohort_atoms)
+        self.cohorts = []
+        self.loose = []
+        self.n_members = 0
+        self.cohorts_made = 0
+        self.peak_cohorts = 0
+        self.device_used = 0
+        self.peak_device = 0
+
+    def _admit(self):
+        while self.pending and self.n_members < self.max_active:
+            req = self.pending[0]
+            need = estimate_bytes(req.n_atoms, req.grid)
+            if self.n_members and self.used + need > self.budget:
+                break
+            self.pending.popleft()
+            self.loose.append(Member(req, need, self.now()))
+            self.n_members += 1
+            self.used += need
+            self.peak_used = max(self.peak_used, self.used)
+            self.peak_active = max(self.peak_active, self.n_members)
+
+    def _form(self):
+        groups = collections.defaultdict(list)
+        for m in self.loose:
+            groups[size_class(m.req.n_atoms, self.class_bounds)].append(m)
+        self.loose = []
+        for cls in sorted(groups):
+            ms = groups[cls]
+            if cls == len(self.class_bounds):
+                parts = [[m] for m in ms]
+            else:
+                parts, cur, atoms = [], [], 0
+                for m in ms:
+                    if cur and atoms + m.req.n_atoms > self.max_cohort_atoms:
+                        parts.append(cur)
+                        cur, atoms = [], 0
+                    cur.append(m)
+                    atoms += m.req.n_atoms
+                if cur:
+                    parts.append(cur)
+            for part in parts:
+                c = self.factory(part)
+                self.cohorts.append(c)
+                self.cohorts_made += 1
+                self.device_used += c.bytes
+        self.peak_cohorts = max(self.peak_cohorts, len(self.cohorts))
+        self.peak_device = max(self.peak_device, self.device_used)
+
+    def _advance(self):
+        progressed = False
+        for c in list(self.cohorts):
+            if not c.idle() or c.left() > 0:
+                continue
+            done, cont = c.split()
+            self.cohorts.remove(c)
+            self.device_used -= c.bytes
+            t = self.now()
+            for m, pos, vel, e, k in done:
+                self.results.append(SegmentResult(m.req, pos, vel, e, k, m.t_admit, t, m.booked))
+                self.used -= m.booked
+                self.n_members -= 1
+            self.loose.extend(cont)
+            progressed = True
+        self._admit()  # what the completed segments freed, before the survivors are re-formed
+        if self.loose:
+            self._form()
+            progressed = True
+        for c in self.cohorts:
+            if c.idle():
+                c.enqueue(min(self.chunk, c.left()))
+                progressed = True
+        return progressed
+
+    def _busy(self):
+        return bool(self.pending or self.cohorts or self.loose)
 
 
 def poisson_trace(n, rate, seed=2024, atoms_lo=500, atoms_hi=50000, steps_lo=1000,

@@ -138,3 +138,24 @@ def test_box_moved_between_batches_continues_bit_for_bit(precision):
     assert np.array_equal(p2[:n_b], pb[sl[1]])
     assert np.array_equal(v2[:n_b], vb[sl[1]])
     assert p2.shape[0] == n_b + n_d
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_langevin_run_split_anywhere_gives_the_same_bits(precision):
+    """run(300) and run(120) + run(97) + run(83): a Langevin run's closing and opening half
+    kicks are the same operations whether they meet in one step or across two calls, so a
+    segment served in chunks of any length ends in the same state."""
+    boxes, grids = boxes_and_grids()
+    pa, va, ea, ka, _ = run_batch(boxes, grids, precision, 300, "langevin", [7, 8, 9])
+    topo = F.Topology(boxes, precision)
+    md = F.Integrator(topo, force_list(grids), timestep=1.0, kind="langevin", temperature=300.0, gamma=5.0)
+    md.set_box_noise(seeds=[7, 8, 9])
+    md.set_state(np.concatenate([b["pos"] for b in boxes]), np.concatenate([b["vel"] for b in boxes]))
+    for n in (120, 97, 83):
+        md.run(n)
+    pb, vb = md.state()
+    eb, kb = md.energies()
+    md.close()
+    topo.close()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert np.array_equal(ea, eb) and np.array_equal(ka, kb)

@@ -47,3 +47,21 @@ def test_staggered_arrivals_and_budget():
     free = _by_id(S.MDServer(max_active=8, chunk=100).run_trace(_reqs(arrivals=(0.0, 0.05, 0.1))))
     for r in res:
         assert np.array_equal(r.pos, free[r.req.rid].pos)
+
+
+def test_folded_cohorts_give_each_segment_its_result_alone():
+    """Segments of one size class folded into a batched system, re-formed as each completes
+    (with the later segment folded in), and one of another class: every final state, energy and
+    kinetic energy equals the segment's alone, bit for bit."""
+    spec = [(200, 300, 5, 0.0), (230, 500, 6, 0.0), (180, 400, 8, 0.0), (1000, 350, 7, 0.0)]
+    reqs = lambda: [S.SegmentRequest(k, W.water_box(w, seed=40 + k), st, seed=sd, arrival=a)
+                    for k, (w, st, sd, a) in enumerate(spec)]
+    srv = S.FoldingServer(max_active=8, chunk=100, class_bounds=(2000, 8000))
+    folded = _by_id(srv.run_trace(reqs()))
+    assert srv.cohorts_made >= 4  # the three small ones re-formed as each completes
+    for k, req in enumerate(reqs()):
+        alone = S.MDServer(max_active=1, chunk=100).run_trace([req])[0]
+        t = folded[k]
+        assert np.array_equal(alone.pos, t.pos), k
+        assert np.array_equal(alone.vel, t.vel), k
+        assert np.array_equal(alone.energies, t.energies) and alone.kinetic == t.kinetic, k

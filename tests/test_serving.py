@@ -97,3 +97,90 @@ def test_poisson_trace_shape():
     assert 1000 <= steps.min() and steps.max() <= 20000
     # log-uniform: the median size is near the geometric mean of the range
     assert 3000 < np.median(atoms) < 8000
+
+
+class FakeCohort:
+    """Several members advancing together; busy for ``cost`` seconds per step and member."""
+    made = []
+
+    def __init__(self, members, clock, cost=1e-5):
+        self.members, self.clock, self.cost = list(members), clock, cost
+        self.bytes = sum(m.booked for m in self.members)
+        self.busy_until = 0.0
+        self.started = [m.done_steps for m in self.members]
+        FakeCohort.made.append(self)
+
+    def idle(self):
+        return self.clock.t >= self.busy_until
+
+    def left(self):
+        return min(m.left() for m in self.members)
+
+    def enqueue(self, n):
+        assert 0 < n <= self.left()
+        for m in self.members:
+            m.done_steps += n
+        self.busy_until = self.clock.t + n * self.cost * len(self.members)
+
+    def split(self):
+        done, cont = [], []
+        for m in self.members:
+            n = m.req.n_atoms
+            if m.left() == 0:
+                done.append((m, np.full((n, 3), float(m.done_steps)), np.zeros((n, 3)), np.zeros(16), 0.0))
+            else:
+                m.state = (np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3)))
+                cont.append(m)
+        return done, cont
+
+
+def _folding(budget, max_active, clock, **kw):
+    FakeCohort.made = []
+    return S.FoldingServer(hbm_budget_bytes=budget, max_active=max_active, chunk=100, clock=clock,
+                           cohort_factory=lambda ms: FakeCohort(ms, clock), **kw)
+
+
+def test_folding_groups_by_size_class_and_reforms_when_a_segment_completes():
+    """Three small segments (steps 150, 300, 500) share one cohort, re-formed without each one
+    that completes; a large one runs in its own system; every segment runs exactly its steps."""
+    clock = FakeClock()
+    reqs = _requests([150, 160, 170, 8000], [150, 300, 500, 250], [0.0] * 4)
+    srv = _folding(1 << 40, 8, clock)
+    res = srv.run_trace(reqs)
+    assert sorted(r.req.rid for r in res) == [0, 1, 2, 3]
+    for r in res:
+        assert r.pos[0, 0] == r.req.steps  # the fake's final state records the steps run
+    small = [c for c in FakeCohort.made if c.members[0].req.n_atoms < 2000]
+    big = [c for c in FakeCohort.made if c.members[0].req.n_atoms >= 20000]
+    assert [len(c.members) for c in small] == [3, 2, 1]
+    assert [c.started for c in small] == [[0, 0, 0], [150, 150], [300]]
+    assert len(big) == 1 and len(big[0].members) == 1
+    assert srv.used == 0 and srv.n_members == 0 and not srv.cohorts
+
+
+def test_folding_admits_fifo_by_budget_and_folds_later_arrivals_in():
+    """A budget for two small segments: the third waits, then joins the survivor of the first
+    cohort when that cohort is re-formed."""
+    clock = FakeClock()
+    reqs = _requests([150, 150, 150], [100, 400, 200], [0.0, 0.0, 0.0])
+    one = S.estimate_bytes(reqs[0].n_atoms, reqs[0].grid)
+    srv = _folding(int(2.5 * one), 8, clock)
+    res = srv.run_trace(reqs)
+    assert len(res) == 3 and srv.peak_active == 2
+    first = FakeCohort.made[0]
+    assert [m.req.rid for m in first.members] == [0, 1]
+    second = FakeCohort.made[1]
+    assert sorted(m.req.rid for m in second.members) == [1, 2]
+    assert sorted(second.started) == [0, 100]
+
+
+def test_folding_caps_cohort_atoms():
+    clock = FakeClock()
+    reqs = _requests([600] * 5, [200] * 5, [0.0] * 5)  # 1,800 atoms each
+    srv = _folding(1 << 40, 8, clock, max_cohort_atoms=4000)
+    srv.run_trace(reqs)
+    assert [len(c.members) for c in FakeCohort.made] == [2, 2, 1]
+
+
+def test_size_class():
+    assert [S.size_class(n) for n in (500, 1999, 2000, 7999, 8000, 19999, 20000, 50000)] == [0, 0, 1, 1, 2, 2, 3, 3]
