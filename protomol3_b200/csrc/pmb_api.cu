@@ -510,7 +510,9 @@ int nblist_alloc(pmb_system *s, double rl) {
     return fail(PMB_ERR_CUDA, "cudaMalloc failed for the neighbour list");
   s->nb_cutoff = rl;
   s->nb_ready = true;
-  CK(cudaDeviceSynchronize());
+  // the zero fills above run on the legacy default stream; the system's streams are
+  // non-blocking, so wait for that stream alone (other streams' work keeps running)
+  CK(cudaStreamSynchronize(cudaStreamLegacy));
   return PMB_OK;
 }
 

@@ -101,9 +101,11 @@ class GpuSegment:
     def finish(self):
         pos, vel = self.md.state()
         e, k = self.md.energies()
+        return pos, vel, e[0].copy(), float(k[0])
+
+    def release(self):
         self.md.close()
         self.topo.close()
-        return pos, vel, e[0].copy(), float(k[0])
 
 
 class MDServer:
@@ -111,8 +113,12 @@ class MDServer:
     execution of the resident segments."""
 
     def __init__(self, hbm_budget_bytes=16 << 30, max_active=32, chunk=200, segment_factory=None,
-                 clock=time.perf_counter, **segment_kw):
+                 clock=time.perf_counter, release_batch=4, **segment_kw):
         self.budget = int(hbm_budget_bytes)
+        # finished systems are released in batches: freeing device memory synchronises the whole
+        # device, which would stall the other segments' queued chunks once per completion
+        self.release_batch = int(release_batch)
+        self.graveyard = []
         self.max_active = int(max_active)
         self.chunk = int(chunk)
         self.factory = segment_factory or (lambda req: GpuSegment(req, **segment_kw))
@@ -130,6 +136,18 @@ class MDServer:
 
     def submit(self, req):
         self.pending.append(req)
+
+    def _retire(self, obj):
+        rel = getattr(obj, "release", None)
+        if rel is not None:
+            self.graveyard.append(rel)
+        if len(self.graveyard) >= self.release_batch:
+            self._release_all()
+
+    def _release_all(self):
+        for rel in self.graveyard:
+            rel()
+        self.graveyard = []
 
     def _admit(self):
         while self.pending and len(self.active) < self.max_active:
@@ -159,6 +177,7 @@ class MDServer:
                 continue
             pos, vel, e, k = seg.finish()
             self.results.append(SegmentResult(seg.req, pos, vel, e, k, seg.t_admit, self.now(), seg.bytes))
+            self._retire(seg)
             self.active.remove(seg)
             self.used -= seg.bytes
             progressed = True
@@ -181,6 +200,7 @@ class MDServer:
             self._admit()
             if not self._advance():
                 time.sleep(idle_sleep)
+        self._release_all()
         return self.results
 
 
@@ -230,6 +250,10 @@ class GpuCohort:
         self.bytes = self.md.device_bytes()
         self.event = None
 
+    def release(self):
+        self.md.close()
+        self.topo.close()
+
     def idle(self):
         return self.event is None or self.event.query()
 
@@ -248,8 +272,6 @@ class GpuCohort:
         the others, each holding its exact state."""
         ck = self.md.checkpoint()
         e, k = self.md.energies()
-        self.md.close()
-        self.topo.close()
         done, cont = [], []
         off = 0
         for b, m in enumerate(self.members):
@@ -283,8 +305,9 @@ class FoldingServer(MDServer):
 
     def __init__(self, hbm_budget_bytes=16 << 30, max_active=32, chunk=200, cohort_factory=None,
                  class_bounds=(2000, 8000, 20000), max_cohort_atoms=200000, clock=time.perf_counter,
-                 **segment_kw):
-        super().__init__(hbm_budget_bytes, max_active, chunk, clock=clock, **segment_kw)
+                 release_batch=4, **segment_kw):
+        super().__init__(hbm_budget_bytes, max_active, chunk, clock=clock, release_batch=release_batch,
+                         **segment_kw)
         self.factory = cohort_factory or (lambda members: GpuCohort(members, **segment_kw))
         self.class_bounds = tuple(class_bounds)
         self.max_cohort_atoms = int(max_cohort_atoms)
@@ -342,6 +365,7 @@ class FoldingServer(MDServer):
             if not c.idle() or c.left() > 0:
                 continue
             done, cont = c.split()
+            self._retire(c)
             self.cohorts.remove(c)
             self.device_used -= c.bytes
             t = self.now()
