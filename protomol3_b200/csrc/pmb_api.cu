@@ -1396,6 +1396,19 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     pm.nxwork = (int)xwork.size();
     pm.zbuf = zbuf;
     pm.lbuf = lbuf;
+    // the warp-shuffle transforms take lines of 32 R points (R <= 5), the same R in every box
+    auto warp_r = [&](int d) {
+      int r = 0;
+      for (size_t bi = 0; bi < f->plans.size(); bi++) {
+        const int n = f->plans[bi].n[d];
+        if (n % 32 != 0 || n / 32 > 5 || (r && n / 32 != r)) return 0;
+        r = n / 32;
+      }
+      return r;
+    };
+    // (one row per warp of a 4-warp block, one column per warp of an 8-warp block)
+    pm.wy = PME_YROWS <= 4 ? warp_r(1) : 0;
+    pm.wx = PME_XCOLS <= 8 ? warp_r(0) : 0;
     pm.qgrid = f->a.get<long long>(g0);
     pm.rgrid = s->precision ? (void *)f->a.get<float>(g0) : (void *)f->a.get<double>(g0);
     pm.cgrid = s->precision ? (void *)f->a.get<float2>(c0) : (void *)f->a.get<double2>(c0);

@@ -89,6 +89,12 @@ __device__ __forceinline__ void dft_small(T2 *v, int sign) {
   }
 }
 
+// dft_small for R = 1 .. 5 (R = 1: nothing to do).
+template <int R, typename T2>
+__device__ __forceinline__ void dft_small_any(T2 *v, int sign) {
+  if constexpr (R > 1) dft_small<R>(v, sign);
+}
+
 // floor(a / d) for 0 <= a < 2^21 from r ~ 1/d (a few ulp suffice: (a + 1/2) / d stays at least
 // 1/(2d) away from an integer), without an integer division.
 __device__ __forceinline__ int divf(int a, float r) { return __float2int_rz(((float)a + 0.5f) * r); }
@@ -609,6 +615,210 @@ __global__ void __launch_bounds__(LT, 8) k_fft_x_infl(const SystemDev s, PmeDev 
   }
 }
 
+// ------------------------------------------------------------ warp-shuffle transforms (n = 32 R)
+// One line of n = 32 R points per warp, no shared-memory stages and no block barrier: lane l
+// holds points l, l + 32, ..., l + 32 (R - 1) in registers.  Forward: an R-point DFT over the
+// registers, the factors W_n^(l k1), then a 32-point decimation-in-frequency transform across
+// the lanes (five xor-shuffle butterfly stages); register k1 of lane l then holds X[k1 + R b(l)],
+// b = 5-bit reversal.  Inverse: consumes exactly that layout, decimation-in-time across the
+// lanes, the conjugate factors, the R-point DFT over the registers, and leaves point
+// l + 32 r in register r.  The factors come from the plan's table W_n^k = exp(-2 pi i k / n).
+__device__ __forceinline__ int brev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+
+template <typename T2>
+__device__ __forceinline__ T2 shfl_xor2(T2 v, int d) {
+  return cmk(__shfl_xor_sync(0xffffffffu, v.x, d), __shfl_xor_sync(0xffffffffu, v.y, d));
+}
+template <typename T2>
+__device__ __forceinline__ T2 cmulc(T2 a, T2 w) {  // a * conj(w)
+  return cmk(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+
+// Per-lane factors: st[s] = w_(2d)^(l mod d) for d = 16 >> s (w_m = exp(-2 pi i / m)), and
+// rk[k1] = W_n^(l k1).
+template <int R, typename T2>
+struct WarpTw {
+  T2 st[5], rk[R];
+};
+template <int R, typename T2, typename TW>
+__device__ __forceinline__ WarpTw<R, T2> warp_twiddles(const TW *tw) {
+  const int lane = threadIdx.x & 31;
+  WarpTw<R, T2> w;
+#pragma unroll
+  for (int s = 0; s < 5; s++) {
+    const int d = 16 >> s, j = lane & (d - 1);
+    const TW t = tw[j * (16 / d) * R];
+    w.st[s] = cmk(t.x, t.y);
+  }
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    const TW t = tw[lane * k];
+    w.rk[k] = cmk(t.x, t.y);
+  }
+  return w;
+}
+
+template <int R, typename T2>
+__device__ __forceinline__ void warp_fft_fwd(T2 v[R], const WarpTw<R, T2> &w) {
+  const int lane = threadIdx.x & 31;
+  dft_small_any<R>(v, -1);
+#pragma unroll
+  for (int k = 1; k < R; k++) v[k] = cmul(v[k], w.rk[k]);
+#pragma unroll
+  for (int s = 0; s < 5; s++) {
+    const int d = 16 >> s;
+    const bool up = (lane & d) != 0;
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const T2 p = shfl_xor2(v[k], d);
+      v[k] = up ? cmul(csub(p, v[k]), w.st[s]) : cadd(v[k], p);
+    }
+  }
+}
+
+template <int R, typename T2>
+__device__ __forceinline__ void warp_fft_inv(T2 v[R], const WarpTw<R, T2> &w) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 4; s >= 0; s--) {
+    const int d = 16 >> s;
+    const bool up = (lane & d) != 0;
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const T2 t = up ? cmulc(v[k], w.st[s]) : v[k];
+      const T2 p = shfl_xor2(t, d);
+      v[k] = up ? csub(p, t) : cadd(v[k], p);
+    }
+  }
+#pragma unroll
+  for (int k = 1; k < R; k++) v[k] = cmulc(v[k], w.rk[k]);
+  dft_small_any<R>(v, +1);
+}
+
+constexpr int WT = 128;  // threads of the warp-transform y kernel (one row per warp)
+constexpr int WX = 256;  // threads of the warp-transform x kernel (one column per warp)
+
+// y-lines with n_y = 32 R: row C[kz][x][0..ny) per warp, up to WT / 32 rows per work item.
+// The forward result is put back into natural order through a per-warp shared-memory line; the
+// inverse reads its input in the forward's lane order through it.
+template <typename T, int R>
+__global__ void __launch_bounds__(WT) k_fft_y_warp(PmeDev pm, int sign) {
+  using T2 = typename C2<T>::t;
+  __shared__ T2 sline[WT / 32][32 * R];
+  const int4 wk = pm.ywork[blockIdx.x];  // box, kz, x0, rows
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w >= wk.w) return;  // warp-uniform; no block barrier below
+  constexpr int ny = 32 * R;
+  T2 *row = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + ((long long)wk.y * nx + wk.z + w) * ny;
+  WarpTw<R, T2> tw;
+  if constexpr (sizeof(T) == 4) tw = warp_twiddles<R, T2>(pm.twiddlef + pl.tw0[1]);
+  else tw = warp_twiddles<R, T2>(pm.twiddle + pl.tw0[1]);
+  T2 *sl = sline[w];
+  T2 v[R];
+  const int b = brev5(lane);
+  if (sign < 0) {
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = row[r * 32 + lane];
+    warp_fft_fwd<R>(v, tw);
+#pragma unroll
+    for (int k = 0; k < R; k++) sl[k + R * b] = v[k];
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; r++) row[r * 32 + lane] = sl[r * 32 + lane];
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; r++) sl[r * 32 + lane] = row[r * 32 + lane];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < R; k++) v[k] = sl[k + R * b];
+    warp_fft_inv<R>(v, tw);
+#pragma unroll
+    for (int r = 0; r < R; r++) row[r * 32 + lane] = v[r];
+  }
+}
+
+// x-lines with n_x = 32 R (columns y0..y0+cols of one kz plane, one per warp): forward
+// transform, influence function with energy and virial (as k_fft_x_infl), inverse transform.
+// The block is staged through shared memory (coalesced rows in and out); between the two
+// transforms each point stays in its lane's registers.
+template <typename T, int R>
+__global__ void __launch_bounds__(WX) k_fft_x_warp(const SystemDev s, PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  constexpr int nx = 32 * R, NW = WX / 32, SP = nx + 1;  // padded column stride
+  __shared__ T2 sb[NW * SP];
+  __shared__ double red[32];
+  const int4 wk = pm.xwork[blockIdx.x];  // box, kz, y0, cols
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int ny = pl.n[1], nz = pl.n[2], kz = wk.y, y0 = wk.z, cols = wk.w;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + (long long)kz * nx * ny + y0;
+  for (int e = threadIdx.x; e < nx * cols; e += WX) {
+    const int x = e / cols, c = e - x * cols;
+    sb[c * SP + x] = C[(long long)x * ny + c];
+  }
+  __syncthreads();
+  double en = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
+  T2 v[R];
+  if (w < cols) {
+    WarpTw<R, T2> tw;
+    if constexpr (sizeof(T) == 4) tw = warp_twiddles<R, T2>(pm.twiddlef + pl.tw0[0]);
+    else tw = warp_twiddles<R, T2>(pm.twiddle + pl.tw0[0]);
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = sb[w * SP + r * 32 + lane];
+    warp_fft_fwd<R>(v, tw);
+    const T *th = reinterpret_cast<const T *>(pm.theta) + pl.cgrid0 + (long long)kz * nx * ny + y0 + w;
+    const double mk = kz * pl.mr[2];
+    const double wz = (kz > 0 && ((2 * kz != nz) || (nz & 1))) ? 2.0 : 1.0;
+    const int j = y0 + w, j0 = j <= ny / 2 ? j : j - ny;
+    const double mj = j0 * pl.mr[1];
+    const int b = brev5(lane);
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int i = k + R * b;
+      const T theta = th[(long long)i * ny];
+      const T2 c = v[k];
+      const double qq = (double)c.x * (double)c.x + (double)c.y * (double)c.y;
+      const double ee = wz * qq * (double)theta;
+      en += ee;
+      if (pm.virial && theta != T(0)) {
+        const int i0 = i <= nx / 2 ? i : i - nx;
+        const double mi = i0 * pl.mr[0];
+        const double m2 = mi * mi + mj * mj + mk * mk;
+        const double vv = 2.0 * (1.0 / m2 + pl.fac);
+        vxx += ee * (1.0 - vv * mi * mi); vxy -= ee * (vv * mi * mj); vxz -= ee * (vv * mi * mk);
+        vyy += ee * (1.0 - vv * mj * mj); vyz -= ee * (vv * mj * mk); vzz += ee * (1.0 - vv * mk * mk);
+      }
+      v[k] = cmk(c.x * theta, c.y * theta);
+    }
+    warp_fft_inv<R>(v, tw);
+#pragma unroll
+    for (int r = 0; r < R; r++) sb[w * SP + r * 32 + lane] = v[r];
+  }
+  // the CTA's energy (x 0.5, Grid.h:319-337) and virial partials in fixed point, as k_fft_x_infl
+  const double part[7] = {en, vxx, vxy, vxz, vyy, vyz, vzz};
+  const int np = pm.virial ? 7 : 1;
+  long long *eb = s.eacc + (long long)wk.x * ACC_PER_BOX;
+  const int slot[6][2] = {{0, 0}, {1, 3}, {2, 6}, {4, 4}, {5, 7}, {8, 8}};  // xx xy xz yy yz zz
+  for (int c = 0; c < np; c++) {
+    const double r = block_sum<WX, T>(part[c], red);
+    if (threadIdx.x == 0) {
+      const long long q = f2fix(r * 0.5, ENERGY_SCALE);
+      if (c == 0) {
+        red_add(eb + E_COUL, q);
+      } else {
+        red_add(eb + E_VIR + slot[c - 1][0], q);
+        if (slot[c - 1][1] != slot[c - 1][0]) red_add(eb + E_VIR + slot[c - 1][1], q);
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nx * cols; e += WX) {
+    const int x = e / cols, c = e - x * cols;
+    C[(long long)x * ny + c] = sb[c * SP + x];
+  }
+}
+
 // Exclusion correction in FP64 with the exact erf (NonbondedPMEwaldSystemForce.h:874-911).
 __global__ void k_correction(const SystemDev s, const int *pairs, const int *kind, int n,
                              double alpha, double a2pi, double csf, int virial) {
@@ -668,9 +878,26 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     cudaFuncSetAttribute(k_fft_x_infl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lcap);
     lconf = true;
   }
-  k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, -1);
-  k_fft_x_infl<T><<<pm.nxwork, LT, lsmem, st>>>(s, pm);
-  k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, +1);
+  auto fft_y = [&](int sign) {
+    switch (pm.wy) {
+      case 1: k_fft_y_warp<T, 1><<<pm.nywork, WT, 0, st>>>(pm, sign); break;
+      case 2: k_fft_y_warp<T, 2><<<pm.nywork, WT, 0, st>>>(pm, sign); break;
+      case 3: k_fft_y_warp<T, 3><<<pm.nywork, WT, 0, st>>>(pm, sign); break;
+      case 4: k_fft_y_warp<T, 4><<<pm.nywork, WT, 0, st>>>(pm, sign); break;
+      case 5: k_fft_y_warp<T, 5><<<pm.nywork, WT, 0, st>>>(pm, sign); break;
+      default: k_fft_y<T><<<pm.nywork, LT, lsmem, st>>>(pm, sign);
+    }
+  };
+  fft_y(-1);
+  switch (pm.wx) {
+    case 1: k_fft_x_warp<T, 1><<<pm.nxwork, WX, 0, st>>>(s, pm); break;
+    case 2: k_fft_x_warp<T, 2><<<pm.nxwork, WX, 0, st>>>(s, pm); break;
+    case 3: k_fft_x_warp<T, 3><<<pm.nxwork, WX, 0, st>>>(s, pm); break;
+    case 4: k_fft_x_warp<T, 4><<<pm.nxwork, WX, 0, st>>>(s, pm); break;
+    case 5: k_fft_x_warp<T, 5><<<pm.nxwork, WX, 0, st>>>(s, pm); break;
+    default: k_fft_x_infl<T><<<pm.nxwork, LT, lsmem, st>>>(s, pm);
+  }
+  fft_y(+1);
   k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   if (mark) mark(mctx, "pme_fft");
   if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);

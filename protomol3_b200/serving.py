@@ -359,26 +359,45 @@ class FoldingServer(MDServer):
         self.peak_cohorts = max(self.peak_cohorts, len(self.cohorts))
         self.peak_device = max(self.peak_device, self.device_used)
 
+    def _cls(self, c):
+        return size_class(c.members[0].req.n_atoms, self.class_bounds)
+
+    def _dissolve(self, c):
+        done, cont = c.split()
+        self._retire(c)
+        self.cohorts.remove(c)
+        self.device_used -= c.bytes
+        t = self.now()
+        for m, pos, vel, e, k in done:
+            self.results.append(SegmentResult(m.req, pos, vel, e, k, m.t_admit, t, m.booked))
+            self.used -= m.booked
+            self.n_members -= 1
+        self.loose.extend(cont)
+
     def _advance(self):
         progressed = False
         for c in list(self.cohorts):
-            if not c.idle() or c.left() > 0:
-                continue
-            done, cont = c.split()
-            self._retire(c)
-            self.cohorts.remove(c)
-            self.device_used -= c.bytes
-            t = self.now()
-            for m, pos, vel, e, k in done:
-                self.results.append(SegmentResult(m.req, pos, vel, e, k, m.t_admit, t, m.booked))
-                self.used -= m.booked
-                self.n_members -= 1
-            self.loose.extend(cont)
-            progressed = True
+            if c.idle() and c.left() == 0:
+                self._dissolve(c)
+                progressed = True
         self._admit()  # what the completed segments freed, before the survivors are re-formed
         if self.loose:
-            self._form()
-            progressed = True
+            # loose segments join their class's cohort: an idle one is dissolved and re-formed
+            # with them; while every cohort of the class is busy they wait for its chunk to end
+            # (one chunk at most), so that a class keeps one cohort instead of fragmenting
+            big = len(self.class_bounds)
+            want = {size_class(m.req.n_atoms, self.class_bounds) for m in self.loose} - {big}
+            for c in list(self.cohorts):
+                if c.idle() and self._cls(c) in want:
+                    self._dissolve(c)
+            busy = {self._cls(c) for c in self.cohorts if self._cls(c) != big}
+            ready = [m for m in self.loose if size_class(m.req.n_atoms, self.class_bounds) not in busy]
+            if ready:
+                wait = [m for m in self.loose if size_class(m.req.n_atoms, self.class_bounds) in busy]
+                self.loose = ready
+                self._form()
+                self.loose = wait
+                progressed = True
         for c in self.cohorts:
             if c.idle():
                 c.enqueue(min(self.chunk, c.left()))

@@ -184,3 +184,19 @@ def test_folding_caps_cohort_atoms():
 
 def test_size_class():
     assert [S.size_class(n) for n in (500, 1999, 2000, 7999, 8000, 19999, 20000, 50000)] == [0, 0, 1, 1, 2, 2, 3, 3]
+
+
+def test_folding_later_arrivals_join_the_running_cohort_of_their_class():
+    """A segment that arrives while its class's cohort runs a chunk waits for the chunk's end
+    and is folded in (the class keeps one cohort); one of another class gets its own."""
+    clock = FakeClock()
+    reqs = _requests([150, 160, 3000], [20000, 300, 300], [0.0, 0.05, 0.06])
+    srv = _folding(1 << 40, 8, clock)
+    res = srv.run_trace(reqs)
+    assert sorted(r.req.rid for r in res) == [0, 1, 2]
+    for r in res:
+        assert r.pos[0, 0] == r.req.steps
+    small = [c for c in FakeCohort.made if c.members[0].req.n_atoms < 2000]
+    assert [sorted(m.req.rid for m in c.members) for c in small][:2] == [[0], [0, 1]]
+    assert small[1].started[[m.req.rid for m in small[1].members].index(0)] > 0
+    assert srv.peak_cohorts == 2
