@@ -155,7 +155,7 @@ struct PmeDev {
   const int4 *xwork;          // x-line work items: box, kz, y0, columns
   int nxwork;
   int zbuf, lbuf;             // complex elements per ping-pong buffer of the z / line kernels
-  int wy, wx;                 // R > 0: every box's y (x) lines have 32 R points and the y (x)
+  int wz, wy, wx;             // R > 0: every box's z (y, x) lines have 32 R points and the z (y, x)
                               // passes run the warp-shuffle transforms; 0: the shared-memory ones
   double alpha, a2pi;
   int virial;

@@ -743,19 +743,23 @@ __global__ void __launch_bounds__(WT) k_fft_y_warp(PmeDev pm, int sign) {
 // The block is staged through shared memory (coalesced rows in and out); between the two
 // transforms each point stays in its lane's registers.
 template <typename T, int R>
-__global__ void __launch_bounds__(WX) k_fft_x_warp(const SystemDev s, PmeDev pm) {
+__global__ void __launch_bounds__(WX, 3) k_fft_x_warp(const SystemDev s, PmeDev pm) {
   using T2 = typename C2<T>::t;
   constexpr int nx = 32 * R, NW = WX / 32, SP = nx + 1;  // padded column stride
   __shared__ T2 sb[NW * SP];
+  __shared__ T sth[NW * SP];  // the block's influence function, staged like the spectrum
   __shared__ double red[32];
   const int4 wk = pm.xwork[blockIdx.x];  // box, kz, y0, cols
   const PmeBoxPlan &pl = pm.plan[wk.x];
   const int ny = pl.n[1], nz = pl.n[2], kz = wk.y, y0 = wk.z, cols = wk.w;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0 + (long long)kz * nx * ny + y0;
+  const T *thg = reinterpret_cast<const T *>(pm.theta) + pl.cgrid0 + (long long)kz * nx * ny + y0;
+  const float rcols = rcpf(cols);
   for (int e = threadIdx.x; e < nx * cols; e += WX) {
-    const int x = e / cols, c = e - x * cols;
+    const int x = divf(e, rcols), c = e - x * cols;
     sb[c * SP + x] = C[(long long)x * ny + c];
+    sth[c * SP + x] = thg[(long long)x * ny + c];
   }
   __syncthreads();
   double en = 0, vxx = 0, vxy = 0, vxz = 0, vyy = 0, vyz = 0, vzz = 0;
@@ -767,7 +771,7 @@ __global__ void __launch_bounds__(WX) k_fft_x_warp(const SystemDev s, PmeDev pm)
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = sb[w * SP + r * 32 + lane];
     warp_fft_fwd<R>(v, tw);
-    const T *th = reinterpret_cast<const T *>(pm.theta) + pl.cgrid0 + (long long)kz * nx * ny + y0 + w;
+    const T *th = sth + w * SP;
     const double mk = kz * pl.mr[2];
     const double wz = (kz > 0 && ((2 * kz != nz) || (nz & 1))) ? 2.0 : 1.0;
     const int j = y0 + w, j0 = j <= ny / 2 ? j : j - ny;
@@ -776,7 +780,7 @@ __global__ void __launch_bounds__(WX) k_fft_x_warp(const SystemDev s, PmeDev pm)
 #pragma unroll
     for (int k = 0; k < R; k++) {
       const int i = k + R * b;
-      const T theta = th[(long long)i * ny];
+      const T theta = th[i];
       const T2 c = v[k];
       const double qq = (double)c.x * (double)c.x + (double)c.y * (double)c.y;
       const double ee = wz * qq * (double)theta;
@@ -814,8 +818,111 @@ __global__ void __launch_bounds__(WX) k_fft_x_warp(const SystemDev s, PmeDev pm)
   }
   __syncthreads();
   for (int e = threadIdx.x; e < nx * cols; e += WX) {
-    const int x = e / cols, c = e - x * cols;
+    const int x = divf(e, rcols), c = e - x * cols;
     C[(long long)x * ny + c] = sb[c * SP + x];
+  }
+}
+
+// z-lines with n_z = 32 R, r2c: the z_fwd work item's lines (x, y0 .. y0 + cnt) as cnt / 2
+// packed pairs, one per warp (real part line y, imaginary part line y + 1), read from the
+// fixed-point grid and cleared; the half spectrum goes out through shared memory in rows of
+// cnt consecutive y, as k_fft_z_fwd writes it.
+constexpr int WZ = 128;  // threads of the warp z kernels: up to 8 lines (4 pairs) per work item
+template <typename T, int R>
+__global__ void __launch_bounds__(WZ) k_fft_z_fwd_warp(PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  constexpr int nz = 32 * R, nh = nz / 2 + 1, NP = WZ / 32;
+  __shared__ T2 zl[NP][nz];       // per warp: its spectrum in natural order
+  __shared__ T2 out[nh * 2 * NP];  // [k][line]
+  const int4 wk = pm.zwork[blockIdx.x];
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], ny = pl.n[1], x = wk.y, y0 = wk.z, cnt = wk.w;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (2 * w < cnt) {
+    long long *g = pm.qgrid + pl.grid0 + ((long long)x * ny + y0 + 2 * w) * nz;
+    const bool two = 2 * w + 1 < cnt;
+    // every load issued before any store (the clearing stores would order the loads behind them)
+    long long qa[R], qb[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      qa[r] = __ldcs(g + r * 32 + lane);
+      qb[r] = two ? __ldcs(g + nz + r * 32 + lane) : 0ll;
+    }
+    T2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      v[r] = cmk(T((double)qa[r] * (1.0 / GRID_SCALE)), T((double)qb[r] * (1.0 / GRID_SCALE)));
+      g[r * 32 + lane] = 0;  // the charge grid starts the next step cleared
+      if (two) g[nz + r * 32 + lane] = 0;
+    }
+    WarpTw<R, T2> tw;
+    if constexpr (sizeof(T) == 4) tw = warp_twiddles<R, T2>(pm.twiddlef + pl.tw0[2]);
+    else tw = warp_twiddles<R, T2>(pm.twiddle + pl.tw0[2]);
+    warp_fft_fwd<R>(v, tw);
+    const int b = brev5(lane);
+#pragma unroll
+    for (int k = 0; k < R; k++) zl[w][k + R * b] = v[k];
+    __syncwarp();
+    for (int k = lane; k < nh; k += 32) {
+      const T2 zk = zl[w][k], zn = zl[w][k == 0 ? 0 : nz - k];
+      // X = (Z_k + conj(Z_{n-k})) / 2, Y = -i/2 (Z_k - conj(Z_{n-k}))
+      out[k * 2 * NP + 2 * w] = cmk(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
+      out[k * 2 * NP + 2 * w + 1] = cmk(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
+    }
+  }
+  __syncthreads();
+  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0;
+  for (int e = threadIdx.x; e < nh * cnt; e += WZ) {
+    const int k = e / cnt, c = e - k * cnt;
+    C[((long long)k * nx + x) * ny + y0 + c] = out[k * 2 * NP + c];
+  }
+}
+
+// z-lines with n_z = 32 R, c2r: the inverse of k_fft_z_fwd_warp (as k_fft_z_inv), writing the
+// real potential grid [x][y][z].
+template <typename T, int R>
+__global__ void __launch_bounds__(WZ) k_fft_z_inv_warp(PmeDev pm) {
+  using T2 = typename C2<T>::t;
+  constexpr int nz = 32 * R, nh = nz / 2 + 1, NP = WZ / 32;
+  __shared__ T2 zl[NP][nz];
+  __shared__ T2 in[nh * 2 * NP];  // [k][line]
+  const int4 wk = pm.zwork[blockIdx.x];
+  const PmeBoxPlan &pl = pm.plan[wk.x];
+  const int nx = pl.n[0], ny = pl.n[1], x = wk.y, y0 = wk.z, cnt = wk.w;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const T2 *C = reinterpret_cast<const T2 *>(pm.cgrid) + pl.cgrid0;
+  for (int e = threadIdx.x; e < nh * cnt; e += WZ) {
+    const int k = e / cnt, c = e - k * cnt;
+    in[k * 2 * NP + c] = C[((long long)k * nx + x) * ny + y0 + c];
+  }
+  __syncthreads();
+  if (2 * w >= cnt) return;  // warp-uniform; no block barrier below
+  const bool two = 2 * w + 1 < cnt;
+  for (int k = lane; k < nh; k += 32) {
+    T2 X = in[k * 2 * NP + 2 * w];
+    T2 Y = two ? in[k * 2 * NP + 2 * w + 1] : cmk(T(0), T(0));
+    if (k == 0 || 2 * k == nz) {
+      X.y = T(0);
+      Y.y = T(0);
+    }
+    // Z_k = X_k + i Y_k and Z_{n-k} = conj(X_k) + i conj(Y_k)
+    zl[w][k] = cmk(X.x - Y.y, X.y + Y.x);
+    if (k > 0 && 2 * k != nz) zl[w][nz - k] = cmk(X.x + Y.y, Y.x - X.y);
+  }
+  __syncwarp();
+  WarpTw<R, T2> tw;
+  if constexpr (sizeof(T) == 4) tw = warp_twiddles<R, T2>(pm.twiddlef + pl.tw0[2]);
+  else tw = warp_twiddles<R, T2>(pm.twiddle + pl.tw0[2]);
+  const int b = brev5(lane);
+  T2 v[R];
+#pragma unroll
+  for (int k = 0; k < R; k++) v[k] = zl[w][k + R * b];
+  warp_fft_inv<R>(v, tw);
+  T *Rg = reinterpret_cast<T *>(pm.rgrid) + pl.grid0 + ((long long)x * ny + y0 + 2 * w) * nz;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    Rg[r * 32 + lane] = v[r].x;
+    if (two) Rg[nz + r * 32 + lane] = v[r].y;
   }
 }
 
@@ -869,7 +976,14 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     cudaFuncSetAttribute(k_fft_z_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, zcap);
     zconf = true;
   }
-  k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  switch (pm.wz) {
+    case 1: k_fft_z_fwd_warp<T, 1><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 2: k_fft_z_fwd_warp<T, 2><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 3: k_fft_z_fwd_warp<T, 3><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 4: k_fft_z_fwd_warp<T, 4><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 5: k_fft_z_fwd_warp<T, 5><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    default: k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  }
   const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)pm.lbuf);
   static bool lconf = false;
   if (!lconf) {
@@ -898,7 +1012,14 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     default: k_fft_x_infl<T><<<pm.nxwork, LT, lsmem, st>>>(s, pm);
   }
   fft_y(+1);
-  k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  switch (pm.wz) {
+    case 1: k_fft_z_inv_warp<T, 1><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 2: k_fft_z_inv_warp<T, 2><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 3: k_fft_z_inv_warp<T, 3><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 4: k_fft_z_inv_warp<T, 4><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    case 5: k_fft_z_inv_warp<T, 5><<<pm.nzwork, WZ, 0, st>>>(pm); break;
+    default: k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
+  }
   if (mark) mark(mctx, "pme_fft");
   if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   else k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);

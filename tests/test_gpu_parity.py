@@ -90,11 +90,12 @@ def test_pme_vs_oracle(precision, nw, grid, rc):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("grid,order", [((25, 18, 32), 6), ((27, 16, 30), 8), ((64, 96, 40), 4),
-                                        ((32, 160, 30), 4), ((128, 32, 24), 4)])
+                                        ((32, 160, 96), 4), ((128, 32, 32), 4), ((40, 64, 160), 4),
+                                        ((96, 128, 128), 4)])
 def test_pme_anisotropic_grid_and_order(precision, grid, order):
     """Grid lengths of pure radix 5, 3 and 2 in different dimensions and interpolation orders
-    other than 4 (the generic spread/gather instance); x and y lengths of 32 R points (R = 1 to 5)
-    take the warp-shuffle transforms."""
+    other than 4 (the generic spread/gather instance); lengths of 32 R points (R = 1 to 5) take
+    the warp-shuffle transforms in that dimension, the others the shared-memory ones."""
     b = W.water_box(216, seed=11)
     pme = F.NonbondedPMEwaldSystemForce(grid, 8.0, order=order)
     f, e, topo = gpu_eval(b, [pme], precision, virial=True)
