@@ -180,7 +180,7 @@ def force_errors(f, e, f_ref, e_ref):
 
 def read_profile_traffic():
     """DRAM bytes per launch of the pair kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "pair_kernel_config2.md")
+    p = os.path.join(ROOT, "profiles", "pair_kernel_water98k.md")
     if not os.path.exists(p):
         return None
     for ln in open(p):

@@ -45,7 +45,7 @@ def cutoff():
     return O.cutoff_params(lj=("C2", 7.0, 8.0), coul=("C2", 7.0, 8.0))
 
 
-def test_config1_leapfrog_1000_steps_per_step_fp64():
+def test_water216_leapfrog_1000_steps_per_step_fp64():
     d = dict(np.load(os.path.join(GOLD, "water216_md_ref.npz")))
     box, s, topo, md = setup()
     keep = list(d["lf_keep"])

@@ -182,7 +182,7 @@ def test_leapfrog_matches_oracle_pme(graph):
 
 
 @pytest.fixture(scope="module")
-def config2():
+def water98k():
     """The full 98,304-atom box (32,768 waters, 96^3 grid, rc 10, LJ C2 8->10) and the oracle's
     forces, energies and terms on it (computed once for both precisions)."""
     b = W.water_box(32768, seed=1234)
@@ -192,9 +192,9 @@ def config2():
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_config2_size_vs_oracle(config2, precision):
+def test_water98k_size_vs_oracle(water98k, precision):
     """The plain FP64 path (the drop-in) and the mixed path at full size, against the oracle."""
-    b, fo, eo, info = config2
+    b, fo, eo, info = water98k
     lj = F.NonbondedCutoffSystemForce(lj=("C2", 8.0, 10.0))
     pme = F.NonbondedPMEwaldSystemForce((96, 96, 96), 10.0)
     f, e, topo = gpu_eval(b, [lj, pme], precision)
