@@ -155,8 +155,9 @@ struct PmeDev {
   const int4 *xwork;          // x-line work items: box, kz, y0, columns
   int nxwork;
   int zbuf, lbuf;             // complex elements per ping-pong buffer of the z / line kernels
-  int wz, wy, wx;             // R > 0: every box's z (y, x) lines have 32 R points and the z (y, x)
-                              // passes run the warp-shuffle transforms; 0: the shared-memory ones
+  int wz, wy, wx;             // R > 0: every box's z (y, x) lines have 32 R points and the inverse
+                              // z pass (the y passes, the x pass) run the warp-shuffle transforms;
+                              // 0: the shared-memory ones
   double alpha, a2pi;
   int virial;
 };

@@ -823,63 +823,12 @@ __global__ void __launch_bounds__(WX, 3) k_fft_x_warp(const SystemDev s, PmeDev 
   }
 }
 
-// z-lines with n_z = 32 R, r2c: the z_fwd work item's lines (x, y0 .. y0 + cnt) as cnt / 2
-// packed pairs, one per warp (real part line y, imaginary part line y + 1), read from the
-// fixed-point grid and cleared; the half spectrum goes out through shared memory in rows of
-// cnt consecutive y, as k_fft_z_fwd writes it.
-constexpr int WZ = 128;  // threads of the warp z kernels: up to 8 lines (4 pairs) per work item
-template <typename T, int R>
-__global__ void __launch_bounds__(WZ) k_fft_z_fwd_warp(PmeDev pm) {
-  using T2 = typename C2<T>::t;
-  constexpr int nz = 32 * R, nh = nz / 2 + 1, NP = WZ / 32;
-  __shared__ T2 zl[NP][nz];       // per warp: its spectrum in natural order
-  __shared__ T2 out[nh * 2 * NP];  // [k][line]
-  const int4 wk = pm.zwork[blockIdx.x];
-  const PmeBoxPlan &pl = pm.plan[wk.x];
-  const int nx = pl.n[0], ny = pl.n[1], x = wk.y, y0 = wk.z, cnt = wk.w;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (2 * w < cnt) {
-    long long *g = pm.qgrid + pl.grid0 + ((long long)x * ny + y0 + 2 * w) * nz;
-    const bool two = 2 * w + 1 < cnt;
-    // every load issued before any store (the clearing stores would order the loads behind them)
-    long long qa[R], qb[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      qa[r] = __ldcs(g + r * 32 + lane);
-      qb[r] = two ? __ldcs(g + nz + r * 32 + lane) : 0ll;
-    }
-    T2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      v[r] = cmk(T((double)qa[r] * (1.0 / GRID_SCALE)), T((double)qb[r] * (1.0 / GRID_SCALE)));
-      g[r * 32 + lane] = 0;  // the charge grid starts the next step cleared
-      if (two) g[nz + r * 32 + lane] = 0;
-    }
-    WarpTw<R, T2> tw;
-    if constexpr (sizeof(T) == 4) tw = warp_twiddles<R, T2>(pm.twiddlef + pl.tw0[2]);
-    else tw = warp_twiddles<R, T2>(pm.twiddle + pl.tw0[2]);
-    warp_fft_fwd<R>(v, tw);
-    const int b = brev5(lane);
-#pragma unroll
-    for (int k = 0; k < R; k++) zl[w][k + R * b] = v[k];
-    __syncwarp();
-    for (int k = lane; k < nh; k += 32) {
-      const T2 zk = zl[w][k], zn = zl[w][k == 0 ? 0 : nz - k];
-      // X = (Z_k + conj(Z_{n-k})) / 2, Y = -i/2 (Z_k - conj(Z_{n-k}))
-      out[k * 2 * NP + 2 * w] = cmk(T(0.5) * (zk.x + zn.x), T(0.5) * (zk.y - zn.y));
-      out[k * 2 * NP + 2 * w + 1] = cmk(T(0.5) * (zk.y + zn.y), T(-0.5) * (zk.x - zn.x));
-    }
-  }
-  __syncthreads();
-  T2 *C = reinterpret_cast<T2 *>(pm.cgrid) + pl.cgrid0;
-  for (int e = threadIdx.x; e < nh * cnt; e += WZ) {
-    const int k = e / cnt, c = e - k * cnt;
-    C[((long long)k * nx + x) * ny + y0 + c] = out[k * 2 * NP + c];
-  }
-}
+constexpr int WZ = 128;  // threads of the warp z kernel: up to 8 lines (4 pairs) per work item
 
-// z-lines with n_z = 32 R, c2r: the inverse of k_fft_z_fwd_warp (as k_fft_z_inv), writing the
-// real potential grid [x][y][z].
+// z-lines with n_z = 32 R, c2r (as k_fft_z_inv): the z_inv work item's lines (x, y0 .. y0 + cnt)
+// as cnt / 2 packed pairs, one per warp, rebuilt from the half spectrum (read in rows of cnt
+// consecutive y through shared memory), written to the real potential grid [x][y][z].  (The r2c
+// forward pass keeps the shared-memory kernel: its warp form was no faster.)
 template <typename T, int R>
 __global__ void __launch_bounds__(WZ) k_fft_z_inv_warp(PmeDev pm) {
   using T2 = typename C2<T>::t;
@@ -976,14 +925,7 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     cudaFuncSetAttribute(k_fft_z_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, zcap);
     zconf = true;
   }
-  switch (pm.wz) {
-    case 1: k_fft_z_fwd_warp<T, 1><<<pm.nzwork, WZ, 0, st>>>(pm); break;
-    case 2: k_fft_z_fwd_warp<T, 2><<<pm.nzwork, WZ, 0, st>>>(pm); break;
-    case 3: k_fft_z_fwd_warp<T, 3><<<pm.nzwork, WZ, 0, st>>>(pm); break;
-    case 4: k_fft_z_fwd_warp<T, 4><<<pm.nzwork, WZ, 0, st>>>(pm); break;
-    case 5: k_fft_z_fwd_warp<T, 5><<<pm.nzwork, WZ, 0, st>>>(pm); break;
-    default: k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
-  }
+  k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)pm.lbuf);
   static bool lconf = false;
   if (!lconf) {
