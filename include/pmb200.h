@@ -188,7 +188,9 @@ int pmb_force_evaluate(pmb_force *f, const double *positions, double *forces, do
  * device by the list kernels, on the host for force sets that need no list).  A page-locked
  * forces_out (cudaMallocHost, cudaHostAlloc, cudaHostRegister) is uploaded beside the force
  * kernels, added to on the device and copied back into directly, with no host pass over it; a
- * pageable one is added to on the host.  Both give the same doubles. */
+ * pageable one is added to on the host.  Both give the same doubles.  With page-locked positions
+ * as well, the copies are part of the evaluation's CUDA graph (kept per pair of host arrays), so
+ * a call enqueues one graph launch. */
 int pmb_evaluate(pmb_system *sys, pmb_force *const *forces, int n_forces, const double *positions,
                  double *forces_out, double *energies, int virial);
 /* Same, with device pointers and no host synchronisation: d_forces and d_energies are

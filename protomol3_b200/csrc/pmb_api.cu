@@ -271,6 +271,9 @@ struct EvalGraph {
   std::vector<unsigned long long> ids;
   int virial = 0;
   bool direct = false;  // forces added on the device to the caller's uploaded array (no host add)
+  // page-locked caller arrays whose copies are nodes of the graph (null: copies outside it)
+  const double *hpos = nullptr;
+  double *hf = nullptr;
   long long gen = -1;  // list storage generation it was captured with
   double rlist = 0.0;
   bool used_list = false;
@@ -316,6 +319,13 @@ struct pmb_system {
   double *d_fin = nullptr;
   cudaStream_t copy = nullptr;
   cudaEvent_t ev_pos = nullptr, ev_fin = nullptr;
+  // the last host arrays checked for page-locking (address, doubles, result)
+  struct PinSeen {
+    const void *p = nullptr;
+    long long n = 0;
+    bool ok = false;
+  } pin_seen[2];
+  int pin_next = 0;
   std::vector<EvalGraph> eval_graphs;   // at most EVAL_GRAPHS, most recent last
   static constexpr int EVAL_GRAPHS = 4;
   // neighbour list
@@ -777,7 +787,8 @@ int enqueue_eval_copies(pmb_system *s, bool with_forces = true) {
 // storage it captured stays (generation) and the list radius is unchanged; the list storage and
 // radius are settled before any capture, so a captured step neither allocates nor forces a
 // rebuild on every replay.
-int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bool direct) {
+int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bool direct,
+                      const double *hpos = nullptr, double *hf = nullptr) {
   cudaStream_t st = s->stream;
   const double rlist = list_radius(s, fs, n);
   if (rlist > 0.0) {
@@ -794,7 +805,8 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bo
   EvalGraph *g = nullptr;
   for (size_t k = 0; k < s->eval_graphs.size(); k++) {
     EvalGraph &e = s->eval_graphs[k];
-    if (e.ids == ids && e.virial == virial && e.direct == direct && e.gen == s->nb_gen && e.rlist == rlist) {
+    if (e.ids == ids && e.virial == virial && e.direct == direct && e.hpos == hpos && e.hf == hf &&
+        e.gen == s->nb_gen && e.rlist == rlist) {
       std::rotate(s->eval_graphs.begin() + k, s->eval_graphs.begin() + k + 1, s->eval_graphs.end());
       g = &s->eval_graphs.back();
       break;
@@ -802,19 +814,33 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bo
   }
   if (!g) {
     cudaGraph_t graph = nullptr;
+    const long long nf = 3LL * s->natoms;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    if (hpos) CK(cudaMemcpyAsync(s->d_pos, hpos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    if (hf) {
+      // the caller's forces go up after the positions (the two uploads would share the link),
+      // beside the force kernels
+      CK(cudaEventRecord(s->ev_pos, st));
+      CK(cudaStreamWaitEvent(s->copy, s->ev_pos, 0));
+      CK(cudaMemcpyAsync(s->d_fin, hf, sizeof(double) * nf, cudaMemcpyHostToDevice, s->copy));
+      CK(cudaEventRecord(s->ev_fin, s->copy));
+    }
     SystemDev sd = s->dev();
     zero_accumulators(sd, st);
     int rc = enqueue_forces(s, fs, n, virial);
     if (!rc) {
       if (direct) {  // the caller's forces, uploaded beside the force kernels, are the base
-        CK(cudaStreamWaitEvent(st, s->ev_fin, cudaEventWaitExternal));
+        CK(cudaStreamWaitEvent(st, s->ev_fin, hf ? 0 : cudaEventWaitExternal));
         forces_to_double(sd, s->d_fout, st, s->d_fin);
       } else {
         forces_to_double(sd, s->d_fout, st);
       }
       energies_to_double(sd, nullptr, s->d_eout, st);
       rc = enqueue_eval_copies(s, !direct);
+      if (!rc && hf) {
+        CK(cudaMemcpyAsync(hf, s->d_fout, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecordWithFlags(s->ev_out[1], st, cudaEventRecordExternal));
+      }
     }
     cudaError_t e = cudaStreamEndCapture(st, &graph);
     if (rc || e != cudaSuccess) {
@@ -825,6 +851,8 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bo
     ng.ids = ids;
     ng.virial = virial;
     ng.direct = direct;
+    ng.hpos = hpos;
+    ng.hf = hf;
     ng.gen = s->nb_gen;
     ng.rlist = rlist;
     ng.used_list = s->last_used_list;
@@ -855,6 +883,19 @@ bool host_pinned(const double *p, long long n) {
     if (at.type != cudaMemoryTypeHost) return false;
   }
   return true;
+}
+
+// host_pinned for the arrays of the last calls, without asking the driver again (a stale answer
+// costs speed only: the copies are correct for page-locked and pageable memory alike).
+bool host_pinned_seen(pmb_system *s, const double *p, long long n) {
+  for (const pmb_system::PinSeen &e : s->pin_seen)
+    if (e.p == p && e.n == n) return e.ok;
+  pmb_system::PinSeen &e = s->pin_seen[s->pin_next];
+  s->pin_next = (s->pin_next + 1) % 2;
+  e.p = p;
+  e.n = n;
+  e.ok = host_pinned(p, n);
+  return e.ok;
 }
 
 // The status words as they were copied to s->h_status: capacity before non-finite positions
@@ -1601,7 +1642,9 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
   // a captured graph per force set, except under the stage profiler or on the legacy stream
   const bool graphed = s->eval_graph && !s->prof && st != nullptr && st != cudaStreamLegacy;
   // page-locked force array: added to on the device and copied back into directly
-  const bool direct = graphed && forces && nf > 0 && host_pinned(forces, nf);
+  const bool direct = graphed && forces && nf > 0 && host_pinned_seen(s, forces, nf);
+  // page-locked positions as well: every copy is a node of the evaluation's graph (one launch)
+  const bool embed = direct && host_pinned_seen(s, pos, nf);
   if (direct && !s->d_fin) {
     if (cudaMalloc(&s->d_fin, sizeof(double) * nf) != cudaSuccess) {
       s->d_fin = nullptr;
@@ -1612,9 +1655,9 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
     CK(cudaEventCreateWithFlags(&s->ev_fin, cudaEventDisableTiming));
   }
   for (int attempt = 0; attempt < 3; attempt++) {
-    CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+    if (!embed) CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
     s->have_pos = true;
-    if (direct && attempt == 0) {
+    if (direct && !embed && attempt == 0) {
       // after the positions (the two uploads would share the link), beside the force kernels;
       // a retry keeps this copy of the caller's forces
       CK(cudaEventRecord(s->ev_pos, st));
@@ -1624,8 +1667,8 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
     }
     int rc;
     if (graphed) {
-      rc = eval_graph_launch(s, fs, n, virial, direct);
-      if (!rc && direct) {
+      rc = eval_graph_launch(s, fs, n, virial, direct, embed ? pos : nullptr, embed ? forces : nullptr);
+      if (!rc && direct && !embed) {
         CK(cudaMemcpyAsync(forces, s->d_fout, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
         CK(cudaEventRecord(s->ev_out[1], st));
       }

@@ -260,13 +260,24 @@ class BondedSystemForce(SystemForce):
         super().__init__(d)
 
 
+_HANDLE_ARRAYS = {}
+
+
 def evaluate_all(topo, force_list, positions, forces, energies):
-    """ForceGroup::evaluateSystemForces (force/ForceGroup.cpp:54-70) in one device pass."""
-    hs = (C.c_void_p * len(force_list))(*[f.handle(topo) for f in force_list])
-    pos = np.ascontiguousarray(positions, np.float64)
-    f = np.ascontiguousarray(forces)
-    L.check(L.lib().pmb_evaluate(topo.system(), C.cast(hs, C.c_void_p), len(force_list), _p(pos),
-                                 _p(f), _p(energies.table), int(energies.do_virial)))
+    """ForceGroup::evaluateSystemForces (force/ForceGroup.cpp:54-70) in one device pass.  The
+    per-call Python work is kept small (a cached handle array, no copies of contiguous float64
+    arrays): it is part of every step of a host-driven integration."""
+    hk = tuple(f.handle(topo) for f in force_list)
+    hs = _HANDLE_ARRAYS.get(hk)
+    if hs is None:
+        if len(_HANDLE_ARRAYS) > 64:
+            _HANDLE_ARRAYS.clear()
+        hs = _HANDLE_ARRAYS[hk] = (C.c_void_p * len(hk))(*hk)
+    pos = positions if (isinstance(positions, np.ndarray) and positions.dtype == np.float64
+                        and positions.flags.c_contiguous) else np.ascontiguousarray(positions, np.float64)
+    f = forces if forces.flags.c_contiguous else np.ascontiguousarray(forces)
+    L.check(L.lib().pmb_evaluate(topo.system(), C.addressof(hs), len(hk), pos.ctypes.data, f.ctypes.data,
+                                 energies.table.ctypes.data, int(energies.do_virial)))
     if f is not forces:
         forces[:] = f
 

@@ -305,13 +305,15 @@ def pinned_array(shape, fill):
     return a
 
 
+@pytest.mark.parametrize("pinned_positions", [False, True])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("n_waters", [216, 27000])
-def test_page_locked_force_array_gets_the_same_sum(precision, n_waters):
-    """A page-locked force array is added to on the device and copied back into directly; a
-    pageable one receives the forces in a host staging buffer and is added to on the host.  Both
-    add the same two doubles per component, so the results are equal bit for bit, evaluation
-    after evaluation (the graphed evaluation is replayed), and the energies too."""
+def test_page_locked_force_array_gets_the_same_sum(precision, n_waters, pinned_positions):
+    """A page-locked force array is added to on the device and copied back into directly (with
+    page-locked positions too, every copy is a node of the evaluation's graph); a pageable one
+    receives the forces in a host staging buffer and is added to on the host.  Both add the same
+    two doubles per component, so the results are equal bit for bit, evaluation after evaluation
+    (the graphed evaluation is replayed), and the energies too."""
     b = W.water_box(n_waters, seed=11)
     edge = b["box"][0]
     grid = W.pme_grid_for(edge)
@@ -320,12 +322,15 @@ def test_page_locked_force_array_gets_the_same_sum(precision, n_waters):
     topo = F.Topology(b, precision)
     rng = np.random.default_rng(3)
     pos = b["pos"].copy()
+    pb = pinned_array(pos.shape, pos) if pinned_positions else None
     for it in range(3):
         start = rng.normal(size=(topo.n_atoms, 3))
         fa, fb = start.copy(), pinned_array((topo.n_atoms, 3), start)
         ea, eb = F.ScalarStructure(1, virial=True), F.ScalarStructure(1, virial=True)
         F.evaluate_all(topo, fl, pos, fa, ea)
-        F.evaluate_all(topo, fl, pos, fb, eb)
+        if pb is not None:
+            pb[...] = pos
+        F.evaluate_all(topo, fl, pos if pb is None else pb, fb, eb)
         assert np.array_equal(fa, fb)
         assert np.array_equal(ea.table, eb.table)
         assert not np.array_equal(fa, start)
@@ -333,13 +338,14 @@ def test_page_locked_force_array_gets_the_same_sum(precision, n_waters):
     topo.close()
 
 
-@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("pinned", [False, True, "both"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_non_finite_position_is_an_error_and_changes_nothing(precision, pinned):
     """A NaN or infinite position gives PMB_ERR_NUMERIC and leaves the caller's forces and
     energies as they were, whether the list kernels saw it on the device (pair and PME forces) or
     the host did (bonded terms alone, no list), and whether the force array is pageable or
-    page-locked (added to on the device); the next finite evaluation is right again."""
+    page-locked (added to on the device), with the positions page-locked as well ("both": every
+    copy inside the evaluation's graph); the next finite evaluation is right again."""
     from protomol3_b200 import _lib as L
     b = dict(W.water_box(216, seed=4))
     # off the waters' rest geometry, so that the bonded forces are not zero
@@ -348,7 +354,7 @@ def test_non_finite_position_is_an_error_and_changes_nothing(precision, pinned):
           F.NonbondedPMEwaldSystemForce((20, 20, 20), 8.0), F.BondedSystemForce()]
     for forces, bad in ((fl, np.nan), (fl, np.inf), ([F.BondedSystemForce()], -np.inf)):
         topo = F.Topology(b, precision)
-        pos = b["pos"].copy()
+        pos = pinned_array(b["pos"].shape, b["pos"]) if pinned == "both" else b["pos"].copy()
         pos[5, 1] = bad
         frc = pinned_array((topo.n_atoms, 3), 7.0) if pinned else np.full((topo.n_atoms, 3), 7.0)
         e = F.ScalarStructure(1)
