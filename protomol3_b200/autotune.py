@@ -34,7 +34,9 @@ from . import waterbox as W
 
 SKINS = (0.5, 0.8, 1.1)
 SORT_CELLS = (1.8, 2.4, 3.2)
-PAIR_CTAS = (0, 2, 1)
+# pair-kernel blocks per SM: all that fit (0; 5 of 128 threads for the mixed kernel), or fewer to
+# leave room for the PME kernels that run beside it
+PAIR_CTAS = (0, 4, 3)
 
 
 def grid_candidates(edge, spacing=1.0, headroom=0.15, minimum=8):

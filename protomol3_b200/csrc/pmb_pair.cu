@@ -40,7 +40,12 @@ namespace pmb {
 
 namespace {
 
-constexpr int PAIR_THREADS = 256;
+// 128-thread blocks, 5 per SM for the mixed kernels (up to 102 registers: no spills, 20 warps per
+// SM) measured faster than 256-thread blocks at 3 per SM (80 registers, spills): 167 against 170 us
+#ifndef PAIR_BLOCK_THREADS
+#define PAIR_BLOCK_THREADS 128
+#endif
+constexpr int PAIR_THREADS = PAIR_BLOCK_THREADS;
 constexpr int PAIR_WARPS = PAIR_THREADS / 32;
 constexpr int CHUNK = TILE_CHUNK;  // consecutive tiles per warp assignment
 
@@ -239,7 +244,7 @@ constexpr int FAST_ENTRIES = GROUPS * GSTRIDE;
 #endif
 constexpr int PAIR2_STEPS_UNROLLED = PAIR2_UNROLL;
 #ifndef PAIR_MINB
-#define PAIR_MINB 3  // resident blocks per SM of the mixed kernels
+#define PAIR_MINB 5  // resident blocks per SM of the mixed kernels
 #endif
 
 // Operations whose operands are all per-pair values use the two-wide instructions; those with a
