@@ -246,6 +246,9 @@ constexpr int PAIR2_STEPS_UNROLLED = PAIR2_UNROLL;
 #ifndef PAIR_MINB
 #define PAIR_MINB 5  // resident blocks per SM of the mixed kernels
 #endif
+#ifndef PAIR_MINB_FP64
+#define PAIR_MINB_FP64 5  // resident blocks per SM of the FP64 kernels (no virial, one image): 96 registers
+#endif
 
 // Operations whose operands are all per-pair values use the two-wide instructions; those with a
 // constant operand (kernel parameters, polynomial coefficients) are issued as two scalar
@@ -439,7 +442,7 @@ constexpr size_t warp_pref_bytes() {
 }
 
 template <bool MIXED, int LSW, int CM, int CSW, bool VIR, bool MULTI>
-__global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR_MINB : 2)
+__global__ void __launch_bounds__(PAIR_THREADS, (MIXED && !VIR && !MULTI) ? PAIR_MINB : (!MIXED && !VIR && !MULTI) ? PAIR_MINB_FP64 : 2)
     k_pair(SystemDev s, NbListDev nb, PairParams p,
            ParamsT<typename std::conditional<MIXED, float, double>::type> pt, const double *ljd,
            const double *lat, int blk_lo, int blk_hi, int wslot) {
