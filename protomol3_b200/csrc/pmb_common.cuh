@@ -29,8 +29,11 @@ constexpr int BLOCK = 8;           // atoms per i-cluster (a lane group; the j-c
 constexpr int GROUPS = 32 / BLOCK; // lane groups per warp
 static_assert(BLOCK == 8 || BLOCK == 16, "i-cluster of 8 or 16 atoms");
 constexpr int JCHUNK = 32;         // j-atoms per tile
-constexpr int TILE_CHUNK = 8;      // consecutive tiles per warp assignment of the pair kernel; each
-                                   // box's tiles start at a multiple of it
+#ifndef PAIR_TILE_CHUNK
+#define PAIR_TILE_CHUNK 16
+#endif
+constexpr int TILE_CHUNK = PAIR_TILE_CHUNK;  // consecutive tiles per warp assignment of the pair
+                                             // kernel; each box's tiles start at a multiple of it
 constexpr int JSAME = 1 << 30;     // j-list flag: the j-atom shares a molecule with the i-cluster
 constexpr int MAX_LJ_TYPES = 32;   // LJ table kept in shared memory up to this many types
 

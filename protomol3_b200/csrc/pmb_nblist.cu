@@ -404,7 +404,13 @@ __device__ __forceinline__ float gap2f(const float sL[3], const unsigned c1[3], 
   return g2;
 }
 
-constexpr int BL_THREADS = 256;
+#ifndef BL_BLOCK_THREADS
+#define BL_BLOCK_THREADS 256
+#endif
+#ifndef BL_MINB
+#define BL_MINB 4
+#endif
+constexpr int BL_THREADS = BL_BLOCK_THREADS;
 constexpr int BL_CAP = 128;  // candidate blocks buffered per warp before their atoms are tested
 
 // One warp per block I: its own slots, then the candidate blocks J > I of the same box by
@@ -412,7 +418,7 @@ constexpr int BL_CAP = 128;  // candidate blocks buffered per warp before their 
 // the atoms of GROUPS listed blocks per pass within the list cutoff of I's box, compacted into
 // I's j-list (tiles of 32 entries).  The loads of the next pass are issued before the current
 // pass is tested.
-__global__ void __launch_bounds__(BL_THREADS, 4) k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
+__global__ void __launch_bounds__(BL_THREADS, BL_MINB) k_build_lists(SystemDev s, NbListDev nb, double rlist2) {
   __shared__ int cand_all[BL_THREADS / 32][BL_CAP];
   if (!nb.ctl[1]) return;
   const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -676,7 +682,7 @@ int nblist_lists(const SystemDev &s, NbListDev &nb, double list_cutoff, cudaStre
   const int wthreads = nb.nblk_total * 32;
   k_block_bbox<<<(nb.nslot + T - 1) / T, T, 0, st>>>(nb);
   k_superblock_bbox<<<(nb.nsblk * 32 + T - 1) / T, T, 0, st>>>(nb);
-  k_build_lists<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb, list_cutoff * list_cutoff);
+  k_build_lists<<<(wthreads + BL_THREADS - 1) / BL_THREADS, BL_THREADS, 0, st>>>(s, nb, list_cutoff * list_cutoff);
   scan_exclusive(nb.jcount, nb.tile_off, nb.nblk_total, nb.scan_tmp, st, nb.ctl);
   k_box_pad<<<1, 1024, 0, st>>>(s, nb);
   k_tile_map<<<(wthreads + T - 1) / T, T, 0, st>>>(s, nb);

@@ -353,8 +353,13 @@ __global__ void k_spread4(NbListDev nb, PmeDev pm) {
   }
 }
 
+#if defined(GATHER_MINB) && GATHER_MINB > 0
+#define GATHER_BOUNDS __launch_bounds__(256, GATHER_MINB)
+#else
+#define GATHER_BOUNDS
+#endif
 template <bool MIXED, int PC>
-__global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
+__global__ void GATHER_BOUNDS k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   using T = typename std::conditional<MIXED, float, double>::type;
   int sl = blockIdx.x * blockDim.x + threadIdx.x;
   if (sl >= nb.nslot) return;
