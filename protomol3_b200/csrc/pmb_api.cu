@@ -1449,7 +1449,7 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
     };
     // (one row per warp of a 4-warp block, one column per warp of an 8-warp block)
     pm.wy = PME_YROWS <= 4 ? warp_r(1) : 0;
-    pm.wx = PME_XCOLS <= 8 ? warp_r(0) : 0;
+    pm.wx = PME_XCOLS * 32 <= PME_WX_THREADS ? warp_r(0) : 0;
     pm.wz = PME_ZLINES <= 8 ? warp_r(2) : 0;  // (two lines per warp of a 4-warp block)
     pm.qgrid = f->a.get<long long>(g0);
     pm.rgrid = s->precision ? (void *)f->a.get<float>(g0) : (void *)f->a.get<double>(g0);

@@ -161,6 +161,13 @@ struct PmeDev {
   double alpha, a2pi;
   int virial;
 };
+// Block sizes of the warp-transform x kernel (one column per warp) and of the gather.
+#ifndef PME_WX_THREADS
+#define PME_WX_THREADS 256
+#endif
+#ifndef PME_GATHER_THREADS
+#define PME_GATHER_THREADS 256
+#endif
 // Optional stage marker (profiling): called on the host between kernel launches.
 typedef void (*StageMark)(void *ctx, const char *stage);
 int pme_recip_launch(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStream_t st,

@@ -354,7 +354,7 @@ __global__ void k_spread4(NbListDev nb, PmeDev pm) {
 }
 
 #if defined(GATHER_MINB) && GATHER_MINB > 0
-#define GATHER_BOUNDS __launch_bounds__(256, GATHER_MINB)
+#define GATHER_BOUNDS __launch_bounds__(PME_GATHER_THREADS, GATHER_MINB)
 #else
 #define GATHER_BOUNDS
 #endif
@@ -701,7 +701,7 @@ __device__ __forceinline__ void warp_fft_inv(T2 v[R], const WarpTw<R, T2> &w) {
 }
 
 constexpr int WT = 128;  // threads of the warp-transform y kernel (one row per warp)
-constexpr int WX = 256;  // threads of the warp-transform x kernel (one column per warp)
+constexpr int WX = PME_WX_THREADS;  // threads of the warp-transform x kernel (one column per warp)
 
 // y-lines with n_y = 32 R: row C[kz][x][0..ny) per warp, up to WT / 32 rows per work item.
 // The forward result is put back into natural order through a per-warp shared-memory line; the
@@ -968,7 +968,8 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     default: k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   }
   if (mark) mark(mctx, "pme_fft");
-  if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
+  constexpr int TG = PME_GATHER_THREADS;
+  if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TG - 1) / TG, TG, 0, st>>>(s, nb, pm);
   else k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   if (mark) mark(mctx, "pme_gather");
   return 0;
