@@ -54,7 +54,7 @@ def test_pentane_lj_c2_energy():
 
 
 def test_alpha_bisection():
-    # erfc(alpha rc)/rc = 1e-6 at rc = 10 A gives alpha ~ 0.312 (survey of config 2)
+    # erfc(alpha rc)/rc = 1e-6 at rc = 10 A gives alpha ~ 0.312 (the 98,304-atom workload)
     a = O.pme_alpha(10.0, 1e-6)
     assert 0.31 < a < 0.315
 
