@@ -30,7 +30,7 @@ constexpr int GROUPS = 32 / BLOCK; // lane groups per warp
 static_assert(BLOCK == 8 || BLOCK == 16, "i-cluster of 8 or 16 atoms");
 constexpr int JCHUNK = 32;         // j-atoms per tile
 #ifndef PAIR_TILE_CHUNK
-#define PAIR_TILE_CHUNK 16
+#define PAIR_TILE_CHUNK 8
 #endif
 constexpr int TILE_CHUNK = PAIR_TILE_CHUNK;  // consecutive tiles per warp assignment of the pair
                                              // kernel; each box's tiles start at a multiple of it
