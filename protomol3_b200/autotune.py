@@ -32,7 +32,7 @@ import numpy as np
 from . import forces as F
 from . import waterbox as W
 
-SKINS = (0.5, 0.8, 1.1)
+SKINS = (0.4, 0.5, 0.8, 1.1)  # the FP64 path prefers the smaller skins, the mixed one 0.7-1.0
 SORT_CELLS = (1.8, 2.4, 3.2)
 # pair-kernel blocks per SM: all that fit (0; 5 of 128 threads for the mixed kernel), or fewer to
 # leave room for the PME kernels that run beside it
