@@ -319,13 +319,6 @@ struct pmb_system {
   double *d_fin = nullptr;
   cudaStream_t copy = nullptr;
   cudaEvent_t ev_pos = nullptr, ev_fin = nullptr;
-  // the last host arrays checked for page-locking (address, doubles, result)
-  struct PinSeen {
-    const void *p = nullptr;
-    long long n = 0;
-    bool ok = false;
-  } pin_seen[2];
-  int pin_next = 0;
   std::vector<EvalGraph> eval_graphs;   // at most EVAL_GRAPHS, most recent last
   static constexpr int EVAL_GRAPHS = 4;
   // neighbour list
@@ -883,19 +876,6 @@ bool host_pinned(const double *p, long long n) {
     if (at.type != cudaMemoryTypeHost) return false;
   }
   return true;
-}
-
-// host_pinned for the arrays of the last calls, without asking the driver again (a stale answer
-// costs speed only: the copies are correct for page-locked and pageable memory alike).
-bool host_pinned_seen(pmb_system *s, const double *p, long long n) {
-  for (const pmb_system::PinSeen &e : s->pin_seen)
-    if (e.p == p && e.n == n) return e.ok;
-  pmb_system::PinSeen &e = s->pin_seen[s->pin_next];
-  s->pin_next = (s->pin_next + 1) % 2;
-  e.p = p;
-  e.n = n;
-  e.ok = host_pinned(p, n);
-  return e.ok;
 }
 
 // The status words as they were copied to s->h_status: capacity before non-finite positions
@@ -1642,9 +1622,11 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
   // a captured graph per force set, except under the stage profiler or on the legacy stream
   const bool graphed = s->eval_graph && !s->prof && st != nullptr && st != cudaStreamLegacy;
   // page-locked force array: added to on the device and copied back into directly
-  const bool direct = graphed && forces && nf > 0 && host_pinned_seen(s, forces, nf);
+  // (asked of the driver at every call: an array freed and another allocated at its address may
+  // differ, and a graph's copies must only ever run on page-locked memory)
+  const bool direct = graphed && forces && nf > 0 && host_pinned(forces, nf);
   // page-locked positions as well: every copy is a node of the evaluation's graph (one launch)
-  const bool embed = direct && host_pinned_seen(s, pos, nf);
+  const bool embed = direct && host_pinned(pos, nf);
   if (direct && !s->d_fin) {
     if (cudaMalloc(&s->d_fin, sizeof(double) * nf) != cudaSuccess) {
       s->d_fin = nullptr;
