@@ -809,19 +809,21 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bo
     cudaGraph_t graph = nullptr;
     const long long nf = 3LL * s->natoms;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    if (hpos) CK(cudaMemcpyAsync(s->d_pos, hpos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
-    if (hf) {
-      // the caller's forces go up after the positions (the two uploads would share the link),
-      // beside the force kernels
-      CK(cudaEventRecord(s->ev_pos, st));
-      CK(cudaStreamWaitEvent(s->copy, s->ev_pos, 0));
-      CK(cudaMemcpyAsync(s->d_fin, hf, sizeof(double) * nf, cudaMemcpyHostToDevice, s->copy));
-      CK(cudaEventRecord(s->ev_fin, s->copy));
-    }
-    SystemDev sd = s->dev();
-    zero_accumulators(sd, st);
-    int rc = enqueue_forces(s, fs, n, virial);
-    if (!rc) {
+    // the captured work; a failing call returns from here, and the capture is ended below either way
+    auto body = [&]() -> int {
+      if (hpos) CK(cudaMemcpyAsync(s->d_pos, hpos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
+      if (hf) {
+        // the caller's forces go up after the positions (the two uploads would share the link),
+        // beside the force kernels
+        CK(cudaEventRecord(s->ev_pos, st));
+        CK(cudaStreamWaitEvent(s->copy, s->ev_pos, 0));
+        CK(cudaMemcpyAsync(s->d_fin, hf, sizeof(double) * nf, cudaMemcpyHostToDevice, s->copy));
+        CK(cudaEventRecord(s->ev_fin, s->copy));
+      }
+      SystemDev sd = s->dev();
+      zero_accumulators(sd, st);
+      int rc = enqueue_forces(s, fs, n, virial);
+      if (rc) return rc;
       if (direct) {  // the caller's forces, uploaded beside the force kernels, are the base
         CK(cudaStreamWaitEvent(st, s->ev_fin, hf ? 0 : cudaEventWaitExternal));
         forces_to_double(sd, s->d_fout, st, s->d_fin);
@@ -830,11 +832,14 @@ int eval_graph_launch(pmb_system *s, pmb_force *const *fs, int n, int virial, bo
       }
       energies_to_double(sd, nullptr, s->d_eout, st);
       rc = enqueue_eval_copies(s, !direct);
-      if (!rc && hf) {
+      if (rc) return rc;
+      if (hf) {
         CK(cudaMemcpyAsync(hf, s->d_fout, sizeof(double) * nf, cudaMemcpyDeviceToHost, st));
         CK(cudaEventRecordWithFlags(s->ev_out[1], st, cudaEventRecordExternal));
       }
-    }
+      return PMB_OK;
+    };
+    const int rc = body();
     cudaError_t e = cudaStreamEndCapture(st, &graph);
     if (rc || e != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
