@@ -380,6 +380,7 @@ def run_b200(args, rank, world, local_rank):
     # stage profile of one force evaluation (cold L2) -> pair-kernel roofline
     stages = F.profile(topo, [fl[1], fl[2], fl[0]], nrep=5, flush_l2=True)
     t_pair = stages.get("pair")
+    pair_slots = 256 * topo.list_tiles()  # what the timed pair launches evaluated
     peak = F.fp32_peak()
     npairs = pair_count(box, RC) if rank == 0 else None
 
@@ -486,6 +487,8 @@ def run_b200(args, rank, world, local_rank):
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved and peak else None, "traffic": traffic,
                      "work": "%d FLOP x %d in-cutoff pairs per launch" % (FLOPS_PER_PAIR, npairs),
+                     "pair_slots_per_launch": pair_slots,
+                     "in_cutoff_fraction": npairs / pair_slots if npairs and pair_slots else None,
                      "kernel_ms": t_pair, "peak_source": "measured FP32 FMA issue rate (pmb_fp32_peak)"},
         "stages_ms": stages, "plain_fp64": fp64, "batched": batched, "serving": serving, "cpu_baseline": base,
         "accuracy": accuracy,

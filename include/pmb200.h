@@ -165,6 +165,11 @@ int pmb_system_check(pmb_system *sys);
  * moved more than half the skin).  Synchronises the system stream.  No counterpart in the
  * reference, which rebuilds its cell lists at every evaluation. */
 int pmb_system_list_builds(pmb_system *sys, long long *n);
+/* Size of the current neighbour list in pair-kernel tiles: each tile is 8 i-atoms against 32
+ * listed j-atoms (256 pair slots), padding included, so 256 tiles over the pairs within the
+ * cutoff is the share of the evaluated pairs that count.  Synchronises the system stream.  No
+ * counterpart in the reference (its cell lists have no tiles). */
+int pmb_system_list_tiles(pmb_system *sys, long long *tiles);
 /* Host time of the last pmb_evaluate / pmb_force_evaluate, in ms: [0] checks and enqueueing
  * (the position upload and every launch), [1] waiting for the device's first results (status
  * and energies), [2] adding the forces into the caller's array while their device->host copies

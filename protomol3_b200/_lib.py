@@ -73,6 +73,7 @@ _PROTOS = [
                                        C.c_void_p, C.c_int]),
     ("pmb_system_check", C.c_int, [C.c_void_p]),
     ("pmb_system_list_builds", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pmb_system_list_tiles", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_system_evaluate_times", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pmb_force_create", C.c_void_p, [C.c_void_p, C.c_void_p]),
     ("pmb_force_destroy", C.c_int, [C.c_void_p]),

@@ -1197,6 +1197,17 @@ int pmb_system_list_builds(pmb_system *s, long long *n) {
   return PMB_OK;
 }
 
+int pmb_system_list_tiles(pmb_system *s, long long *tiles) {
+  if (!s || !tiles) return fail(PMB_ERR_ARG, "null argument");
+  *tiles = 0;
+  if (!s->nb_ready) return PMB_OK;
+  int v = 0;
+  CK(cudaMemcpyAsync(&v, s->nb.tile_start + s->nb.nblk_total, sizeof(v), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *tiles = v;
+  return PMB_OK;
+}
+
 int pmb_system_evaluate_times(const pmb_system *s, double ms[3]) {
   if (!s || !ms) return fail(PMB_ERR_ARG, "null argument");
   for (int k = 0; k < 3; k++) ms[k] = s->eval_ms[k];

@@ -139,6 +139,13 @@ class Topology:
         L.check(L.lib().pmb_system_list_builds(self.system(), C.byref(n)))
         return n.value
 
+    def list_tiles(self):
+        """Pair-kernel tiles of the current neighbour list (8 x 32 pair slots each, padding
+        included); waits for the system's stream."""
+        n = C.c_longlong(0)
+        L.check(L.lib().pmb_system_list_tiles(self.system(), C.byref(n)))
+        return n.value
+
     def evaluate_times(self):
         """Host time (ms) of the last host-pointer evaluation: enqueue, wait for the device's
         first results, accumulation into the caller's arrays (a page-locked force array: the

@@ -374,3 +374,23 @@ def test_non_finite_position_is_an_error_and_changes_nothing(precision, pinned):
                 fo += O.evaluate(O.System(b), b["pos"], pme=O.pme_params((20, 20, 20), 8.0))[0]
         assert rel_rms(frc, fo) < TOL[precision]
         topo.close()
+
+
+def test_list_tiles_cover_every_pair_within_the_cutoff():
+    """pmb_system_list_tiles: the list's pair slots (256 per tile) hold every pair within the
+    cutoff (the pairs are listed once each) and no more than a few times their number."""
+    b = W.water_box(500, seed=21)
+    rc = 9.0
+    topo = F.Topology(b, "mixed")
+    assert topo.list_tiles() == 0  # no list yet
+    f = np.zeros((topo.n_atoms, 3))
+    F.evaluate_all(topo, [F.NonbondedCutoffSystemForce(lj=("C2", 7.5, rc))], b["pos"], f, F.ScalarStructure(1))
+    slots = 256 * topo.list_tiles()
+    L = b["box"][0]
+    x = b["pos"]
+    d = x[:, None, :] - x[None, :, :]
+    d -= L * np.rint(d / L)
+    r2 = (d ** 2).sum(-1)
+    pairs = int(((r2 <= rc * rc).sum() - len(x)) // 2)
+    assert pairs <= slots <= 4 * pairs, (pairs, slots)
+    topo.close()
