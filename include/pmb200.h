@@ -124,7 +124,8 @@ int pmb_system_set_skin(pmb_system *sys, double skin);
  *   sort_cell: smallest edge (A) of the sort cells that order atoms along a Hilbert curve before
  *     they are grouped into 8-atom clusters (default 2.4; cells per axis are powers of two);
  *   pair_ctas_per_sm: resident CTAs per SM of the persistent pair kernel (0: as many as fit).
- * A change of skin or sort_cell re-sizes the neighbour list; MD runs capture their step again.
+ * A change of skin or sort_cell re-sizes the neighbour list; after a change of any knob, MD runs
+ * and host-pointer evaluations capture their step again.
  * Results differ only in the rounding order of the FP32 / FP64 partial sums. */
 typedef struct {
   double skin;
@@ -241,7 +242,8 @@ int pmb_md_get_box_noise(const pmb_md *md, unsigned long long *seeds, long long 
  * (written to config_path + ".tmp" and renamed, as WriteConfig does) in CheckpointConfigWriter's
  * layout (io/CheckpointConfigWriter.cpp:11-25): "!Checkpoint File!", #ID, #Step (first_step +
  * the steps taken), #Random and #Integrator.  #Random holds this library's noise state,
- * "philox4x32-10 <seed> <half kicks drawn>", in place of the reference's serial generator;
+ * "philox4x32-10 <seed> <half kicks drawn>" of the first box (every box's stream:
+ * pmb_md_get_box_noise), in place of the reference's serial generator;
  * #Integrator is empty, as the leapfrog and Langevin integrators write nothing there.  The files
  * of checkpoint id - 1 are removed, as the reference removes them. */
 int pmb_md_write_checkpoint(pmb_md *md, const char *config_path, int id, long long first_step,

@@ -331,8 +331,9 @@ struct pmb_system {
   int pair_ctas = 0;         // resident CTAs per SM of the pair kernel (0: as many as fit)
   NbListDev nb{};
   Allocs nba;
-  long long nb_gen = 0;      // list storage generation: MD graphs captured before a reallocation
-                             // hold its old buffers and are captured again
+  long long nb_gen = 0;      // list storage and pair launch generation: graphs captured before a
+                             // reallocation (or a change of the pair kernel's CTAs per SM) hold
+                             // the old buffers (or launch shape) and are captured again
   int n_bonded = 0;
   // stage profiler: events recorded between launches when non-null
   std::vector<std::pair<std::string, cudaEvent_t>> *prof = nullptr;
@@ -1147,6 +1148,7 @@ int pmb_system_set_tuning(pmb_system *s, const pmb_tuning *t) {
   if (!(t->sort_cell >= 0.5) || t->sort_cell > 50.0) return fail(PMB_ERR_ARG, "sort_cell must be in [0.5, 50] A");
   if (t->pair_ctas_per_sm < 0 || t->pair_ctas_per_sm > 32) return fail(PMB_ERR_ARG, "pair_ctas_per_sm in [0, 32]");
   CK(cudaStreamSynchronize(s->stream));
+  if (t->pair_ctas_per_sm != s->pair_ctas) s->nb_gen++;  // captured steps hold the old launch shape
   s->pair_ctas = t->pair_ctas_per_sm;
   if (t->skin != s->skin || t->sort_cell != s->sort_cell) {
     s->skin = t->skin;
@@ -1292,7 +1294,9 @@ pmb_force *pmb_force_create(pmb_system *s, const pmb_force_desc *d) {
   }
   if (d->real) {
     if (upload(f->a, f->d_lattice, lat_all)) return bad(PMB_ERR_CUDA, "upload failed");
-    if (cudaMemcpy(s->d_box, s->hbox.data(), sizeof(BoxDev) * nbox, cudaMemcpyHostToDevice) != cudaSuccess)
+    // (no kernel of the system may still read the box records)
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+        cudaMemcpy(s->d_box, s->hbox.data(), sizeof(BoxDev) * nbox, cudaMemcpyHostToDevice) != cudaSuccess)
       return bad(PMB_ERR_CUDA, "upload failed");
     s->nb_ready = false;  // list culling depends on multi_image
   }
@@ -1643,14 +1647,12 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
   const bool direct = graphed && forces && nf > 0 && host_pinned(forces, nf);
   // page-locked positions as well: every copy is a node of the evaluation's graph (one launch)
   const bool embed = direct && host_pinned(pos, nf);
-  if (direct && !s->d_fin) {
-    if (cudaMalloc(&s->d_fin, sizeof(double) * nf) != cudaSuccess) {
-      s->d_fin = nullptr;
-      return fail(PMB_ERR_CUDA, "cudaMalloc failed for the force upload");
-    }
+  if (direct && !s->copy) {  // (the copy stream last: a failure part-way is taken up again here)
+    if (!s->d_fin) s->d_fin = s->a.get<double>((size_t)nf, false);  // freed with the system
+    if (!s->d_fin) return fail(PMB_ERR_CUDA, "cudaMalloc failed for the force upload");
+    if (!s->ev_pos) CK(cudaEventCreateWithFlags(&s->ev_pos, cudaEventDisableTiming));
+    if (!s->ev_fin) CK(cudaEventCreateWithFlags(&s->ev_fin, cudaEventDisableTiming));
     CK(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&s->ev_pos, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&s->ev_fin, cudaEventDisableTiming));
   }
   for (int attempt = 0; attempt < 3; attempt++) {
     if (!embed) CK(cudaMemcpyAsync(s->d_pos, pos, sizeof(double) * nf, cudaMemcpyHostToDevice, st));
@@ -1674,7 +1676,11 @@ int pmb_evaluate(pmb_system *s, pmb_force *const *fs, int n, const double *pos, 
       rc = pmb_evaluate_device(s, fs, n, nullptr, s->d_fout, s->d_eout, virial);
       if (!rc) rc = enqueue_eval_copies(s);
     }
-    if (rc) return rc;
+    if (rc) {  // no copy from the caller's arrays is left in flight
+      cudaStreamSynchronize(st);
+      if (s->copy) cudaStreamSynchronize(s->copy);
+      return rc;
+    }
     const clk::time_point t1 = clk::now();
     CK(cudaEventSynchronize(s->ev_out[0]));
     const clk::time_point t2 = clk::now();
@@ -2109,9 +2115,10 @@ int md_force_frame(pmb_md *m, double *d_out) {
   return PMB_OK;
 }
 
-int md_noise(pmb_md *m, int *kind, unsigned long long *seed) {
+int md_noise(pmb_md *m, int *kind, unsigned long long *seed, long long *steps) {
   *kind = m->d.kind;
-  *seed = m->d.seed;
+  *seed = m->h_box_seed[0];
+  *steps = m->h_box_step0[0] + m->steps;
   return PMB_OK;
 }
 }  // namespace pmb

@@ -45,8 +45,8 @@ namespace pmb {
 int md_frame_source(pmb_md *md, const double **d_pos, int *n_atoms, cudaStream_t *stream, int *device);
 // enqueues the MD run's forces (of its last evaluation) as FP64 into d_out on its stream
 int md_force_frame(pmb_md *md, double *d_out);
-// the MD run's integrator kind and noise seed
-int md_noise(pmb_md *md, int *kind, unsigned long long *seed);
+// the MD run's integrator kind and the noise stream of its first box (seed, steps drawn)
+int md_noise(pmb_md *md, int *kind, unsigned long long *seed, long long *steps);
 }  // namespace pmb
 
 using namespace pmb;
@@ -533,7 +533,8 @@ int pmb_md_write_checkpoint(pmb_md *md, const char *config_path, int id, long lo
   rc = pmb_md_get_checkpoint(md, x.data(), v.data(), nullptr, &steps);
   if (rc) return rc;
   unsigned long long seed = 0;
-  md_noise(md, &kind, &seed);
+  long long noise_steps = 0;  // the first box's stream: its seed and step count
+  md_noise(md, &kind, &seed, &noise_steps);
   const std::string pos_file = std::string(pos_base) + std::to_string(id) + ".pos";
   const std::string vel_file = std::string(vel_base) + std::to_string(id) + ".vel";
   if (!write_file(pos_file, xyz_text(n, nm, x.data())))
@@ -549,7 +550,7 @@ int pmb_md_write_checkpoint(pmb_md *md, const char *config_path, int id, long lo
     << "#Step" << std::endl
     << first_step + steps << std::endl
     << "#Random" << std::endl
-    << "philox4x32-10 " << seed << " " << (kind == PMB_LANGEVIN ? 2 * steps : 0) << std::endl
+    << "philox4x32-10 " << seed << " " << (kind == PMB_LANGEVIN ? 2 * noise_steps : 0) << std::endl
     << "#Integrator" << std::endl
     << std::endl;
   const std::string tmp = std::string(config_path) + ".tmp";

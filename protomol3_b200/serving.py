@@ -105,6 +105,8 @@ class GpuSegment:
 
     def release(self):
         self.md.close()
+        for f in self.fl:  # (their device tables go in the same release batch)
+            f._release()
         self.topo.close()
 
 
@@ -252,6 +254,8 @@ class GpuCohort:
 
     def release(self):
         self.md.close()
+        for f in self.fl:  # (their device tables go in the same release batch)
+            f._release()
         self.topo.close()
 
     def idle(self):

@@ -104,6 +104,12 @@ def test_checkpoint_files_in_the_reference_layout(tmp_path):
     assert [got[k] for k in (1, 3, 5, 7)] == [gold[k] for k in (1, 3, 5, 7)] == ["#ID", "#Step", "#Random", "#Integrator"]
     assert got[2] == "3" and got[4] == "1015" and got[8:] == gold[8:]
     assert got[6] == "philox4x32-10 5 30"  # seed, half kicks drawn (2 per step)
+    # a run given its noise stream (a system moved from another run): the stream's seed and the
+    # half kicks drawn on it, not the run's own
+    md.set_box_noise(seeds=[9], steps=[100])
+    md.run(4)
+    md.write_checkpoint(tmp_path / "run.chk", 4, tmp_path / "w.", tmp_path / "v.", names)
+    assert (tmp_path / "run.chk").read_text().split("\n")[6] == "philox4x32-10 9 208"
     md.close()
     topo.close()
 

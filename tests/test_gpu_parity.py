@@ -338,6 +338,30 @@ def test_page_locked_force_array_gets_the_same_sum(precision, n_waters, pinned_p
     topo.close()
 
 
+def test_systems_with_page_locked_evaluations_free_their_device_memory():
+    """A system that added forces to a page-locked array on the device (which needs a device copy
+    of the array) gives every byte back when it is destroyed: eight systems of 60,000 atoms made,
+    evaluated and destroyed one after another leave the device's free memory where the first left
+    it (each one's copy of the forces alone is 1.44 MB)."""
+    import torch
+    b = W.water_box(20000, seed=12)
+    fl = [F.NonbondedCutoffSystemForce(lj=("C2", 7.0, 8.0))]
+
+    def cycle():
+        topo = F.Topology(b, "mixed")
+        frc = pinned_array((topo.n_atoms, 3), 0.0)
+        F.evaluate_all(topo, fl, b["pos"], frc, F.ScalarStructure(1))
+        assert np.abs(frc).max() > 0
+        topo.close()
+    cycle()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(8):
+        cycle()
+    torch.cuda.synchronize()
+    assert free0 - torch.cuda.mem_get_info()[0] <= 4 << 20
+
+
 @pytest.mark.parametrize("pinned", [False, True, "both"])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_non_finite_position_is_an_error_and_changes_nothing(precision, pinned):
