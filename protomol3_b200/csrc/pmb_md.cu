@@ -262,8 +262,10 @@ __global__ void k_fma_probe(float *out, int iters, float a, float b) {
 // writes positions, velocities and (SHAKE) the reference vectors for the next application.  The
 // scan stops two sweeps past the last count; when that is not enough a second scan and apply
 // continue from there up to the cap.
-// Every operation is rounded as the reference's C++ rounds it (no fused multiply-adds).  The
-// virial term of the modifiers is not accumulated.
+// Every operation is rounded as the reference's C++ rounds it (no fused multiply-adds).  With the
+// virial on, RATTLE adds its constraint virial (ModifierRattle.cpp:58); SHAKE's term
+// (ModifierShake.cpp:65-68) is left out, since the energies are cleared by the force evaluation
+// that follows every SHAKE application (integrator/STSIntegrator.cpp:44) and it is never seen.
 template <int MA, int MC>
 struct ConGroup {
   int nc;
