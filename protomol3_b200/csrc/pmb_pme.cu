@@ -316,8 +316,10 @@ __device__ __forceinline__ T pick4(const T v[4], int p) {
   return p == 0 ? v[0] : (p == 1 ? v[1] : (p == 2 ? v[2] : v[3]));
 }
 
-// Order 4 with four threads per atom slot: thread p adds the 16 points of x-plane p of the
-// stencil (the same values, in the same order of products, as the one-thread form).
+// Order 4 with four threads per atom slot: thread p adds the 16 points of z-offset p of the
+// stencil (the same values, in the same order of products, as the one-thread form), so that at
+// every step the slot's four threads add to four consecutive grid words (one or two 32-byte
+// sectors) rather than to four x-planes (four sectors).
 template <bool MIXED>
 __global__ void k_spread4(NbListDev nb, PmeDev pm) {
   using T = typename std::conditional<MIXED, float, double>::type;
@@ -338,17 +340,17 @@ __global__ void k_spread4(NbListDev nb, PmeDev pm) {
   weights4<MIXED, false>(pl, f4, p4, th, th, base, q);
   const int nx = pl.n[0], ny = pl.n[1], nz = pl.n[2];
   long long *g = pm.qgrid + pl.grid0;
-  const T a = q * pick4(th[0], p);
-  const int i1 = wrap3(p + base[0], nx);
+  const T c2 = pick4(th[2], p);
+  long long *col = g + wrap3(p + base[2], nz);
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const T ab = a * th[1][j];
-    const int j1 = wrap3(j + base[1], ny);
-    long long *row = g + ((long long)i1 * ny + j1) * nz;
+  for (int i = 0; i < 4; i++) {
+    const T a = q * th[0][i];
+    const int i1 = wrap3(i + base[0], nx);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const long long v = f2fix(ab * th[2][k], (T)GRID_SCALE);
-      if (v) red_add(row + wrap3(k + base[2], nz), v);
+    for (int j = 0; j < 4; j++) {
+      const int j1 = wrap3(j + base[1], ny);
+      const long long v = f2fix(a * th[1][j] * c2, (T)GRID_SCALE);
+      if (v) red_add(col + ((long long)i1 * ny + j1) * nz, v);
     }
   }
 }
