@@ -161,12 +161,9 @@ struct PmeDev {
   double alpha, a2pi;
   int virial;
 };
-// Block sizes of the warp-transform x kernel (one column per warp) and of the gather.
+// Block size of the warp-transform x kernel (one column per warp).
 #ifndef PME_WX_THREADS
 #define PME_WX_THREADS 256
-#endif
-#ifndef PME_GATHER_THREADS
-#define PME_GATHER_THREADS 256
 #endif
 // Optional stage marker (profiling): called on the host between kernel launches.
 typedef void (*StageMark)(void *ctx, const char *stage);

@@ -355,13 +355,8 @@ __global__ void k_spread4(NbListDev nb, PmeDev pm) {
   }
 }
 
-#if defined(GATHER_MINB) && GATHER_MINB > 0
-#define GATHER_BOUNDS __launch_bounds__(PME_GATHER_THREADS, GATHER_MINB)
-#else
-#define GATHER_BOUNDS
-#endif
 template <bool MIXED, int PC>
-__global__ void GATHER_BOUNDS k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
+__global__ void k_gather(const SystemDev s, NbListDev nb, PmeDev pm) {
   using T = typename std::conditional<MIXED, float, double>::type;
   int sl = blockIdx.x * blockDim.x + threadIdx.x;
   if (sl >= nb.nslot) return;
@@ -421,6 +416,61 @@ __global__ void GATHER_BOUNDS k_gather(const SystemDev s, NbListDev nb, PmeDev p
   red_add(f, f2fix((double)(fx * T(pl.hr[0]) * q), FORCE_SCALE));
   red_add(f + 1, f2fix((double)(fy * T(pl.hr[1]) * q), FORCE_SCALE));
   red_add(f + 2, f2fix((double)(fz * T(pl.hr[2]) * q), FORCE_SCALE));
+}
+
+// Order 4 with four threads per atom slot: thread p reads z-offset p of the stencil, so that at
+// every step the slot's four threads read four consecutive grid words; the four partial forces
+// are summed over the slot's lanes.  Every lane takes part in the shuffles (slots out of range
+// or padding add zeros).
+template <bool MIXED>
+__global__ void k_gather4(const SystemDev s, NbListDev nb, PmeDev pm) {
+  using T = typename std::conditional<MIXED, float, double>::type;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int sl = (int)(t >> 2), p = (int)(t & 3);
+  const bool in = sl < nb.nslot;
+  const int4 m = in ? nb.slot_meta[sl] : make_int4(-1, -1, 0, 0);
+  uint4 f4 = make_uint4(0, 0, 0, 0);
+  double4 pq = make_double4(0, 0, 0, 0);
+  if (in) {
+    if constexpr (MIXED) f4 = nb.slot_fx[sl];
+    else pq = nb.slot_pq[sl];
+  }
+  const bool ok = m.x >= 0;
+  T fx = 0, fy = 0, fz = 0, q = 0;
+  const PmeBoxPlan *pl = ok ? pm.plan + m.w : nullptr;
+  if (ok) {
+    T th[3][4], dth[3][4];
+    int base[3];
+    weights4<MIXED, true>(*pl, f4, pq, th, dth, base, q);
+    const int nx = pl->n[0], ny = pl->n[1], nz = pl->n[2];
+    const T *col = reinterpret_cast<const T *>(pm.rgrid) + pl->grid0 + wrap3(p + base[2], nz);
+    const T tz = pick4(th[2], p), dz = pick4(dth[2], p);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int i1 = wrap3(i + base[0], nx);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int j1 = wrap3(j + base[1], ny);
+        const T xij = dth[0][i] * th[1][j], yij = th[0][i] * dth[1][j], zij = th[0][i] * th[1][j];
+        const T term = col[((long long)i1 * ny + j1) * nz];
+        fx -= term * xij * tz;
+        fy -= term * yij * tz;
+        fz -= term * zij * dz;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (ok && p == 0) {
+    long long *f = s.facc + 3 * (long long)m.x;
+    red_add(f, f2fix((double)(fx * T(pl->hr[0]) * q), FORCE_SCALE));
+    red_add(f + 1, f2fix((double)(fy * T(pl->hr[1]) * q), FORCE_SCALE));
+    red_add(f + 2, f2fix((double)(fz * T(pl->hr[2]) * q), FORCE_SCALE));
+  }
 }
 
 constexpr int ZT = 128;         // threads of the z-line kernels
@@ -970,8 +1020,7 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
     default: k_fft_z_inv<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   }
   if (mark) mark(mctx, "pme_fft");
-  constexpr int TG = PME_GATHER_THREADS;
-  if (pm.order == 4) k_gather<MIXED, 4><<<(nb.nslot + TG - 1) / TG, TG, 0, st>>>(s, nb, pm);
+  if (pm.order == 4) k_gather4<MIXED><<<(unsigned)((4ll * nb.nslot + TB - 1) / TB), TB, 0, st>>>(s, nb, pm);
   else k_gather<MIXED, 0><<<(nb.nslot + TB - 1) / TB, TB, 0, st>>>(s, nb, pm);
   if (mark) mark(mctx, "pme_gather");
   return 0;
