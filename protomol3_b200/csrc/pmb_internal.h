@@ -25,6 +25,15 @@ enum {
   PMB_OK_ = 0,
 };
 
+// Index of the current device for per-device one-time settings (a kernel's attributes, such as
+// its dynamic shared-memory limit, belong to the device they were set on).
+constexpr int PMB_MAX_DEVICES = 64;
+inline int device_slot() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= PMB_MAX_DEVICES) d = 0;
+  return d;
+}
+
 // ------------------------------------------------------------------ neighbour list (nblist.cu)
 struct NbListDev {
   // per block

@@ -925,9 +925,11 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
   size_t ljbytes = ((size_t)2 * ntt * sizeof(T2) + 15) & ~(size_t)15;
   size_t smem = ljbytes + PAIR_WARPS * (warp_stage_bytes<MIXED>() + sizeof(WarpCtx) +
                                         (VIR ? 8 : 2) * 32 * sizeof(long long) + warp_pref_bytes<MIXED>());
-  static int n_sm = 0, occupancy = 0;
-  static size_t conf_smem = 0;
-  if (!n_sm || conf_smem != smem) {
+  // per device: the SM count, the resident blocks and the shared-memory limit they were found for
+  static int n_sm[PMB_MAX_DEVICES] = {}, occupancy[PMB_MAX_DEVICES] = {};
+  static size_t conf_smem[PMB_MAX_DEVICES] = {};
+  const int slot = device_slot();
+  if (!n_sm[slot] || conf_smem[slot] != smem) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int dev = 0, nsm = 0, occ = 0;
@@ -935,14 +937,15 @@ int launch_t(const SystemDev &s, const NbListDev &nb, const PairLaunch &pl, cuda
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, PAIR_THREADS, smem);
     if (occ < 1) occ = 1;
-    n_sm = nsm;
-    occupancy = occ;
-    conf_smem = smem;
+    n_sm[slot] = nsm;
+    occupancy[slot] = occ;
+    conf_smem[slot] = smem;
   }
   // persistent: every resident CTA walks its share of the tiles (chunks claimed from a counter,
   // so any grid size gives the same result)
-  const int per_sm = pl.ctas_per_sm > 0 && pl.ctas_per_sm < occupancy ? pl.ctas_per_sm : occupancy;
-  const int grid = n_sm * per_sm;
+  const int occ = occupancy[slot];
+  const int per_sm = pl.ctas_per_sm > 0 && pl.ctas_per_sm < occ ? pl.ctas_per_sm : occ;
+  const int grid = n_sm[slot] * per_sm;
   using T = typename std::conditional<MIXED, float, double>::type;
   kern<<<grid, PAIR_THREADS, smem, st>>>(s, nb, pl.p, params_t<T>(pl.p), pl.lj, pl.lattice, pl.blk_lo, pl.blk_hi,
                                          pl.wslot);

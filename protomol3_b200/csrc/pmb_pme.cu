@@ -975,21 +975,21 @@ int recip_t(const SystemDev &s, const NbListDev &nb, const PmeDev &pm, cudaStrea
   if (mark) mark(mctx, "pme_spread");
   // shared memory sized to the largest work item of the plan (caps ZMAXE / LMAXE)
   const size_t zsmem = sizeof(T2) * (256 + 2 * (size_t)pm.zbuf);
-  static bool zconf = false;
-  if (!zconf) {
+  static bool zconf[PMB_MAX_DEVICES] = {}, lconf[PMB_MAX_DEVICES] = {};  // per device
+  const int dev = device_slot();
+  if (!zconf[dev]) {
     const int zcap = (int)(sizeof(T2) * (256 + 2 * (size_t)ZMAXE));
     cudaFuncSetAttribute(k_fft_z_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, zcap);
     cudaFuncSetAttribute(k_fft_z_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, zcap);
-    zconf = true;
+    zconf[dev] = true;
   }
   k_fft_z_fwd<T><<<pm.nzwork, ZT, zsmem, st>>>(pm);
   const size_t lsmem = 32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)pm.lbuf);
-  static bool lconf = false;
-  if (!lconf) {
+  if (!lconf[dev]) {
     const int lcap = (int)(32 * sizeof(double) + sizeof(T2) * (256 + 2 * (size_t)LMAXE));
     cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lcap);
     cudaFuncSetAttribute(k_fft_x_infl<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lcap);
-    lconf = true;
+    lconf[dev] = true;
   }
   auto fft_y = [&](int sign) {
     switch (pm.wy) {
