@@ -7,7 +7,9 @@
  *
  * Every entry point returns 0 (PMB_OK) or a PMB_ERR_* status; pmb_last_error() gives the message
  * (thread local).  Handles are not re-entrant: one host thread drives a system at a time, as
- * ProtoMol drives SystemForce::evaluate.
+ * ProtoMol drives SystemForce::evaluate.  A system, its forces, MD runs and trajectories belong
+ * to the CUDA device that was current when the system was created; calls on them are made with
+ * that device current (as for its streams and memory).
  *
  * A system is a batch of one or more independent periodic boxes.  Per-atom host arrays are the
  * concatenation of the boxes' atoms in box order; per-box outputs are PMB_E_STRIDE doubles each:
